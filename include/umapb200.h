@@ -1,0 +1,292 @@
+/*
+ * umapb200.h - C ABI of the B200 UMAP engine (libumapb200.so).
+ *
+ * This is the drop-in boundary that replaces the PyO3 class `UmapCore` of
+ * umapers (umap_rs/src/lib.rs:540-1320) and the `rust_umap::UmapModel` entry
+ * points it forwards to (rust_umap/src/lib.rs:570-1966).  Every function
+ * takes plain pointers and sizes; no pointer passed in is retained after the
+ * call returns.  Host pointers are ordinary (pageable or pinned) host memory;
+ * functions with the `_device` suffix take device pointers on the device that
+ * was current when the model was created.
+ *
+ * All functions return an `umapb_status`.  The status codes map 1:1 onto the
+ * reference's `UmapError` variants (rust_umap/src/lib.rs:197-244); the binding
+ * raises RuntimeError for UMAPB_NOT_FITTED and UMAPB_ERR_CUDA and ValueError
+ * for the rest, as umap_rs/src/lib.rs:147-157 does.  The message of the last
+ * failure on the calling thread is returned by umapb_last_error().
+ */
+#ifndef UMAPB200_H
+#define UMAPB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Every declaration below is exported from libumapb200.so even though the
+ * library is compiled with hidden default visibility. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define UMAPB_ABI_VERSION 1
+
+typedef enum umapb_status {
+    UMAPB_OK = 0,
+    UMAPB_ERR_EMPTY_DATA = 1,            /* UmapError::EmptyData */
+    UMAPB_ERR_NEED_TWO_SAMPLES = 2,      /* UmapError::NeedAtLeastTwoSamples */
+    UMAPB_ERR_INCONSISTENT_DIMS = 3,     /* UmapError::InconsistentDimensions */
+    UMAPB_ERR_FEATURE_MISMATCH = 4,      /* UmapError::FeatureMismatch */
+    UMAPB_ERR_EMBEDDING_DIM_MISMATCH = 5,/* UmapError::EmbeddingDimensionMismatch */
+    UMAPB_ERR_NOT_FITTED = 6,            /* UmapError::NotFitted */
+    UMAPB_ERR_INVALID_PARAMETER = 7,     /* UmapError::InvalidParameter(msg) */
+    UMAPB_ERR_CUDA = 8,                  /* device failure (no reference counterpart) */
+    UMAPB_ERR_OUT_OF_MEMORY = 9          /* device allocation failure */
+} umapb_status;
+
+/* Metric enum order follows rust_umap::Metric (rust_umap/src/lib.rs:88-101). */
+typedef enum umapb_metric {
+    UMAPB_METRIC_EUCLIDEAN = 0,
+    UMAPB_METRIC_MANHATTAN = 1,
+    UMAPB_METRIC_COSINE = 2,
+    UMAPB_METRIC_CHEBYSHEV = 3,
+    UMAPB_METRIC_MINKOWSKI = 4,
+    UMAPB_METRIC_CORRELATION = 5,
+    UMAPB_METRIC_CANBERRA = 6,
+    UMAPB_METRIC_BRAYCURTIS = 7
+} umapb_metric;
+
+typedef enum umapb_init {
+    UMAPB_INIT_RANDOM = 0,
+    UMAPB_INIT_SPECTRAL = 1
+} umapb_init;
+
+/* How exact kNN distance tiles are computed on the GPU.  Both produce the
+ * same neighbour indices (ties broken by lower index) and the same FP32
+ * distances as the reference's AVX2 summation order. */
+typedef enum umapb_knn_backend {
+    UMAPB_KNN_AUTO = 0,    /* tensor-core path where supported, else plain */
+    UMAPB_KNN_TENSOR = 1,  /* tcgen05 BF16 split GEMM + FP32 re-rank */
+    UMAPB_KNN_PLAIN = 2    /* FP32 CUDA-core tiles in reference order */
+} umapb_knn_backend;
+
+/* Mirrors rust_umap::UmapParams (rust_umap/src/lib.rs:128-152) with the
+ * defaults of lib.rs:170-195; umapb_params_default() fills them in. */
+typedef struct umapb_params {
+    int64_t n_neighbors;          /* 15 */
+    int64_t n_components;         /* 2 */
+    int64_t n_epochs;             /* -1 = None (500 if n<=10000 else 200) */
+    int32_t metric;               /* umapb_metric, euclidean */
+    float metric_p;               /* minkowski p */
+    float learning_rate;          /* 1.0 */
+    float min_dist;               /* 0.1 */
+    float spread;                 /* 1.0 */
+    float local_connectivity;     /* 1.0 */
+    float set_op_mix_ratio;       /* 1.0 */
+    float repulsion_strength;     /* 1.0 */
+    int64_t negative_sample_rate; /* 5 */
+    uint64_t random_seed;         /* 42 */
+    int32_t init;                 /* umapb_init, spectral */
+    int32_t use_approximate_knn;  /* 1 */
+    int64_t approx_knn_candidates;/* 50 */
+    int64_t approx_knn_iters;     /* 14 */
+    int64_t approx_knn_threshold; /* 4096 */
+    int32_t densmap;              /* 0 */
+    float dens_lambda;            /* 2.0 */
+    float dens_frac;              /* 0.3 */
+    float dens_var_shift;         /* 0.1 */
+    int32_t output_dens;          /* 0 */
+    int32_t knn_backend;          /* umapb_knn_backend (B200 knob), auto */
+} umapb_params;
+
+/* Same fields as FitTimingBreakdown (rust_umap/src/lib.rs:51-68); stage times
+ * are measured with CUDA events on the model's stream, in seconds. */
+typedef struct umapb_timings {
+    double validation_sec;
+    double knn_sec;
+    double curve_params_sec;
+    double knn_validate_trim_sec;
+    double smooth_knn_sec;
+    double density_original_sec;
+    double membership_sec;
+    double symmetrize_sec;
+    double target_intersection_sec;
+    double prune_sec;
+    double init_sec;
+    double optimize_sec;
+    double density_embedding_sec;
+    double output_copy_sec;
+    double store_state_sec;
+    double total_sec;
+} umapb_timings;
+
+/* Fields of ProfiledFit (rust_umap/src/lib.rs:71-79) besides the embedding,
+ * plus kNN counters of the B200 path. */
+typedef struct umapb_fit_info {
+    int32_t used_approximate_knn;
+    int32_t knn_backend_used;     /* umapb_knn_backend actually run */
+    int64_t n_samples;
+    int64_t n_features;
+    int64_t n_epochs;
+    int64_t n_edges;
+    int64_t knn_fallback_rows;    /* rows re-run on the plain path */
+    int64_t n_components_graph;   /* connected components of the fuzzy graph */
+    double knn_kernel_sec;        /* dominant kNN kernel, CUDA events */
+    double sgd_edge_samples;      /* attractive edge samples over all epochs */
+} umapb_fit_info;
+
+typedef struct umapb_model umapb_model;
+
+/* ---- library ---------------------------------------------------------- */
+
+/* Replaces umapers.__version__ (umap_rs/src/lib.rs:1551-1558). */
+const char* umapb_version(void);
+int32_t umapb_abi_version(void);
+/* Message of the last failing call on this thread ("" if none). */
+const char* umapb_last_error(void);
+/* Number of kernels this library has launched in the process so far (no
+ * reference counterpart; used to attribute device work in benchmarks). */
+uint64_t umapb_kernel_launches(void);
+/* Defaults of UmapParams::default (rust_umap/src/lib.rs:170-195). */
+void umapb_params_default(umapb_params* params);
+
+/* ---- model lifecycle: UmapCore.__new__ (umap_rs/src/lib.rs:549-630) ---- */
+
+int32_t umapb_create(const umapb_params* params, umapb_model** out_model);
+void umapb_destroy(umapb_model* model);
+
+/* ---- fit / transform --------------------------------------------------- */
+
+/* UmapCore.fit (umap_rs/src/lib.rs:632-646) -> UmapModel::fit_dense (lib.rs:705). */
+int32_t umapb_fit(umapb_model* model, const float* data, int64_t n_rows, int64_t n_cols);
+
+/* UmapCore.fit_transform / fit_transform_into (umap_rs/src/lib.rs:687-710,
+ * 809-835) -> UmapModel::fit_transform_dense (rust_umap/src/lib.rs:769-794).
+ * `out` is n_rows x n_components float32, row-major. */
+int32_t umapb_fit_transform(umapb_model* model, const float* data, int64_t n_rows,
+                            int64_t n_cols, float* out);
+
+/* UmapCore.fit_transform_stateless (umap_rs/src/lib.rs:779-807) ->
+ * rust_umap::fit_transform_dense (rust_umap/src/lib.rs:1928-1942): same as
+ * fit_transform but no state is kept. */
+int32_t umapb_fit_transform_stateless(const umapb_params* params, const float* data,
+                                      int64_t n_rows, int64_t n_cols, float* out);
+
+/* UmapCore.fit_transform_with_knn[_into] (umap_rs/src/lib.rs:916-1017) ->
+ * UmapModel::fit_transform_with_knn_metric_dense_i64_flat (rust_umap/src/lib.rs:1159-1212).
+ * knn_indices int64 [idx_rows x idx_cols], knn_dists float32 [dist_rows x dist_cols]. */
+int32_t umapb_fit_transform_with_knn(umapb_model* model, const float* data, int64_t n_rows,
+                                     int64_t n_cols, const int64_t* knn_indices,
+                                     int64_t idx_rows, int64_t idx_cols,
+                                     const float* knn_dists, int64_t dist_rows,
+                                     int64_t dist_cols, int32_t knn_metric,
+                                     int32_t validate_precomputed, float* out);
+
+/* UmapCore.transform / transform_into (umap_rs/src/lib.rs:1147-1200) ->
+ * UmapModel::transform_dense (rust_umap/src/lib.rs:1593-1685). */
+int32_t umapb_transform(umapb_model* model, const float* query, int64_t n_rows,
+                        int64_t n_cols, float* out);
+
+/* UmapCore.profile_fit_transform (umap_rs/src/lib.rs:712-744) ->
+ * UmapModel::profile_fit_transform_dense (rust_umap/src/lib.rs:796-962). */
+int32_t umapb_profile_fit_transform(umapb_model* model, const float* data, int64_t n_rows,
+                                    int64_t n_cols, float* out, umapb_timings* timings,
+                                    umapb_fit_info* info);
+
+/* Device-resident variants of fit_transform / transform: `data`, `query` and
+ * `out` are device pointers (no host copies inside).  They have no reference
+ * counterpart; they exist so a caller that keeps its matrices in HBM pays no
+ * PCIe traffic.  `timings`/`info` may be NULL. */
+int32_t umapb_fit_transform_device(umapb_model* model, const float* data, int64_t n_rows,
+                                   int64_t n_cols, float* out, umapb_timings* timings,
+                                   umapb_fit_info* info);
+int32_t umapb_transform_device(umapb_model* model, const float* query, int64_t n_rows,
+                               int64_t n_cols, float* out);
+
+/* ---- fitted-state getters (umap_rs/src/lib.rs:1260-1320) --------------- */
+
+int64_t umapb_n_components(const umapb_model* model);
+int64_t umapb_n_neighbors(const umapb_model* model);
+/* -1 when the model is not fitted. */
+int64_t umapb_n_features(const umapb_model* model);
+int64_t umapb_n_samples(const umapb_model* model);
+/* Copies the fitted embedding (n_samples x n_components) into `out`. */
+int32_t umapb_get_embedding(const umapb_model* model, float* out, int64_t n_rows,
+                            int64_t n_cols);
+/* Copies the curve parameters resolved by the last fit (UmapModel::ab_params,
+ * rust_umap/src/lib.rs:604-610). */
+int32_t umapb_get_ab(const umapb_model* model, float* a, float* b);
+
+/* ---- stage entry points (host buffers) --------------------------------- *
+ * Each runs one stage of the fit on the current device and exists so that a
+ * caller (or a parity test) can drive the stages separately. */
+
+/* find_ab_params (rust_umap/src/lib.rs:5672-5746), host arithmetic. */
+int32_t umapb_find_ab_params(float spread, float min_dist, float* a, float* b);
+
+/* Exact kNN of every row against all rows, self included
+ * (exact_nearest_neighbors, rust_umap/src/lib.rs:2911-2928).  Euclidean
+ * distances are sqrt of FP32 squared distances in the reference's
+ * summation order (lib.rs:2445-2492); ties go to the lower index.
+ * `fallback_rows` (may be NULL) receives the number of rows the tensor path
+ * could not certify and recomputed on the plain path. */
+int32_t umapb_knn_exact(const float* data, int64_t n_rows, int64_t n_cols, int64_t k,
+                        int32_t metric, int32_t backend, int64_t* indices, float* dists,
+                        int64_t* fallback_rows);
+
+/* Exact kNN of query rows against reference rows
+ * (exact_nearest_neighbors_to_reference, rust_umap/src/lib.rs:3346-3399). */
+int32_t umapb_knn_query(const float* query, int64_t n_query, const float* reference,
+                        int64_t n_reference, int64_t n_cols, int64_t k, int32_t metric,
+                        int32_t backend, int64_t* indices, float* dists);
+
+/* NN-descent variant (approximate_nearest_neighbors_with_distance,
+ * rust_umap/src/lib.rs:3086-3151) on the GPU; `seed` plays the role of
+ * random_seed ^ 0xC0FE_FEED_1234_ABCD (lib.rs:2327). */
+int32_t umapb_nndescent(const float* data, int64_t n_rows, int64_t n_cols, int64_t k,
+                        int32_t metric, int64_t candidate_pool, int64_t n_iters,
+                        uint64_t seed, int64_t* indices, float* dists, int64_t* iters_run);
+
+/* smooth_knn_dist (rust_umap/src/lib.rs:3424-3523): dists is n_rows x n_cols. */
+int32_t umapb_smooth_knn_dist(const float* dists, int64_t n_rows, int64_t n_cols, float k,
+                              float local_connectivity, float bandwidth,
+                              int32_t include_self, float* sigmas, float* rhos);
+
+/* Fuzzy simplicial set of a kNN graph: self detection (lib.rs:3402-3417),
+ * smooth_knn_dist, compute_membership_strengths (3525-3560),
+ * symmetrize_fuzzy_graph (3597-3649) and, when n_epochs > 0, prune_edges
+ * (3804-3822).  Edges come back sorted by (head, tail); `capacity` must be
+ * >= 2 * n_rows * k.  `sigmas`/`rhos` (length n_rows) may be NULL. */
+int32_t umapb_fuzzy_graph(const int64_t* indices, const float* dists, int64_t n_rows,
+                          int64_t k, float set_op_mix_ratio, float local_connectivity,
+                          int64_t n_epochs, int32_t* heads, int32_t* tails, float* weights,
+                          int64_t capacity, int64_t* n_edges, float* sigmas, float* rhos);
+
+/* spectral_init (rust_umap/src/lib.rs:3871-3888, connected and
+ * multi-component); `data` (n_rows x n_cols) feeds the component centroids
+ * of the meta layout (lib.rs:4463-4485).  Writes n_rows x n_components.
+ * Returns UMAPB_OK with *used_spectral = 0 when the reference would fall
+ * back to random init (out then holds random_init's layout). */
+int32_t umapb_spectral_init(const float* data, int64_t n_rows, int64_t n_cols,
+                            const int32_t* heads, const int32_t* tails, const float* weights,
+                            int64_t n_edges, int64_t n_components, uint64_t seed, float* out,
+                            int32_t* used_spectral);
+
+/* optimize_layout_training (rust_umap/src/lib.rs:5137-5321) on the GPU:
+ * embedding (n_vertices x dim) is updated in place. */
+int32_t umapb_optimize_layout(float* embedding, int64_t n_vertices, int64_t dim,
+                              const int32_t* heads, const int32_t* tails, const float* weights,
+                              int64_t n_edges, int64_t n_epochs, float a, float b,
+                              float learning_rate, int64_t negative_sample_rate,
+                              float repulsion_strength, uint64_t seed);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UMAPB200_H */

@@ -1,0 +1,56 @@
+"""Exact kNN on the GPU against the oracle: indices bit-exact (ties to the
+lower index) and FP32 distances bit-exact, for the scalar (dim < 64) and
+AVX2 lane (dim >= 64) summation orders, euclidean and cosine, self joins
+and query-to-reference searches."""
+import numpy as np
+import pytest
+
+from umapers_b200 import workloads
+from tests import gpu_util as gu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n,d,k", [(1000, 32, 15), (2000, 64, 15), (1500, 100, 10), (700, 8, 5),
+                                   (513, 200, 30)])
+def test_plain_knn_bit_exact(orc, n, d, k):
+    x = workloads.isotropic_mixture(n, d, 6, 3.0, seed=n + d)
+    gi, gd, _ = gu.knn_exact(x, k, backend="plain")
+    oi, od = orc.exact_knn(x, k)
+    np.testing.assert_array_equal(gi, oi)
+    np.testing.assert_array_equal(gd, od)
+
+
+def test_plain_knn_cosine_bit_exact(orc):
+    x = workloads.isotropic_mixture(1200, 72, 5, 2.0, seed=9)
+    x[5] = 0.0  # zero-norm row: distance 1 to everything, 0 to itself
+    gi, gd, _ = gu.knn_exact(x, 12, metric="cosine", backend="plain")
+    oi, od = orc.exact_knn(x, 12, metric="cosine")
+    np.testing.assert_array_equal(gi, oi)
+    np.testing.assert_array_equal(gd, od)
+
+
+def test_knn_query_bit_exact(orc):
+    fit, q = workloads.transform_mixture(n_fit=3000, n_query=700, d=64, n_comp=8)
+    gi, gd = gu.knn_query(q, fit, 15)
+    oi, od = orc.knn_query(q, fit, 15)
+    np.testing.assert_array_equal(gi, oi)
+    np.testing.assert_array_equal(gd, od)
+
+
+def test_duplicate_rows_resolve_to_lower_index(orc):
+    x = workloads.gaussian(400, 16, seed=5)
+    x[100:110] = x[50]
+    gi, gd, _ = gu.knn_exact(x, 12)
+    oi, od = orc.exact_knn(x, 12)
+    np.testing.assert_array_equal(gi, oi)
+    assert list(gi[105, :11]) == [50] + list(range(100, 110))
+
+
+def test_mixture_20000x192_sampled_rows_bit_exact(orc):
+    x = workloads.isotropic_mixture(20_000, 192, 10, 4.0, seed=7)
+    gi, gd, _ = gu.knn_exact(x, 15, backend="plain")
+    rows = np.random.default_rng(7).choice(20_000, 200, replace=False)
+    oi, od = orc.exact_knn_rows(x, rows, 15)
+    np.testing.assert_array_equal(gi[rows], oi)
+    np.testing.assert_array_equal(gd[rows], od)

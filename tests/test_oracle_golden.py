@@ -1,0 +1,133 @@
+"""The CPU oracle against the reference's own known-answer tests (golden
+vectors transcribed by tests/golden/make_pins.py) and its internal
+consistency properties.  No GPU needed."""
+import numpy as np
+import pytest
+
+from umapers_b200 import workloads
+
+
+def test_find_ab_params_bits_match_reference(orc, pins):
+    # rust_umap/src/lib.rs:5781-5795
+    for case in pins["find_ab_params"]:
+        a_bits, b_bits = orc.find_ab_bits(case["spread"], case["min_dist"])
+        assert (a_bits, b_bits) == (case["a_bits"], case["b_bits"]), case
+
+
+@pytest.mark.parametrize("case_idx", [0, 1])
+def test_smooth_knn_self_and_non_self_layouts_agree(orc, pins, case_idx):
+    # rust_umap/src/lib.rs:6975-7020
+    case = pins["smooth_knn_cases"][case_idx]
+    s1, r1 = orc.smooth_knn(np.array(case["with_self"]), case["k"], include_self=True)
+    s2, r2 = orc.smooth_knn(np.array(case["without_self"]), case["k"], include_self=False)
+    assert np.all(np.abs(s1 - s2) <= case["sigma_tol"])
+    assert np.all(np.abs(r1 - r2) <= case["rho_tol"])
+
+
+def test_laplacian_from_edges_matches_dense_affinity(orc, pins):
+    # rust_umap/src/lib.rs:7457-7538
+    lap = pins["laplacian_edges"]
+    e = np.array(lap["edges"])
+    l1, l2 = orc.laplacians(lap["n"], e[:, 0], e[:, 1], e[:, 2])
+    assert np.max(np.abs(l1 - l2)) < lap["tol"]
+
+
+def test_smooth_knn_fp32_tracks_fp64(orc):
+    rng = np.random.default_rng(0)
+    d = np.sort(rng.gamma(2.0, 1.0, size=(500, 15)).astype(np.float32), axis=1)
+    d[:, 0] = 0.0
+    s32, r32 = orc.smooth_knn(d, 15.0)
+    s64, r64 = orc.smooth_knn_f64(d, 15.0)
+    np.testing.assert_array_equal(r32, r64.astype(np.float32))
+    # the bisection stops at |psum - target| < 1e-5, so sigma agrees to that scale
+    assert np.median(np.abs(s32 - s64) / s64) < 1e-5
+    assert np.max(np.abs(s32 - s64) / s64) < 1e-3
+
+
+def test_exact_knn_orders_by_distance_then_index(orc):
+    x = workloads.gaussian(300, 70, seed=3)
+    x[10] = x[20]  # an exact duplicate pair: ties resolve to the lower index
+    idx, dist = orc.exact_knn(x, 8)
+    rows = np.arange(300)
+    assert np.all(idx[rows != 20, 0] == rows[rows != 20])
+    assert idx[20, 0] == 10 and idx[20, 1] == 20 and dist[20, 0] == 0.0 and dist[20, 1] == 0.0
+    assert idx[10, 0] == 10 and idx[10, 1] == 20
+    assert np.all(np.diff(dist, axis=1) >= 0)
+    # same sets as a float64 brute force wherever no near-tie straddles the cut
+    d64 = ((x[:, None, :].astype(np.float64) - x[None, :, :]) ** 2).sum(-1)
+    order = np.argsort(d64, axis=1, kind="stable")[:, :8]
+    agree = np.mean([set(order[i]) == set(idx[i]) for i in range(300)])
+    assert agree > 0.99
+
+
+def test_squared_distance_uses_lane_order(orc):
+    # dim >= 64: eight lane sums added in order, then the scalar tail
+    rng = np.random.default_rng(1)
+    x = rng.normal(size=67).astype(np.float32) * 1000
+    y = rng.normal(size=67).astype(np.float32)
+    lanes = np.zeros(8, np.float32)
+    for i in range(0, 64, 8):
+        df = x[i:i + 8] - y[i:i + 8]
+        lanes = (lanes + df * df).astype(np.float32)
+    s = np.float32(lanes[0])
+    for v in lanes[1:]:
+        s = np.float32(s + v)
+    for i in range(64, 67):
+        df = np.float32(x[i] - y[i])
+        s = np.float32(s + np.float32(df * df))
+    assert orc.squared_distance(x, y) == s
+
+
+def test_nndescent_recall_reference_threshold(orc):
+    # rust_umap/src/lib.rs:6733-6748: recall >= 0.70 excluding self
+    x = workloads.reference_synthetic(240, 8)
+    ex, _ = orc.exact_knn(x, 12)
+    ap, _, _ = orc.nndescent(x, 12, 30, 8, 0x123456789ABCDEF0)
+    hits = sum(len(set(ex[i, 1:]) & set(ap[i, 1:])) for i in range(240))
+    assert hits / (240 * 11) >= 0.70
+
+
+def test_oracle_fit_is_deterministic(orc):
+    # rust_umap/src/lib.rs:6172-6190
+    x = workloads.reference_synthetic(60, 6)
+    kw = dict(n_neighbors=10, n_epochs=40, init="random", random_seed=1234)
+    a = orc.fit_transform(x, **kw)
+    b = orc.fit_transform(x, **kw)
+    np.testing.assert_array_equal(a, b)
+    assert np.all(np.isfinite(a))
+
+
+def test_transform_sgd_thread_count_deterministic(orc, pins):
+    # rust_umap/src/lib.rs:6193-6236
+    p = pins["transform_determinism"]
+    base = np.array([[np.sin(i * 0.07), np.cos(i * 0.11)] for i in range(p["n_tail"])], np.float32)
+    init = np.array([[np.sin(i * 0.03), np.cos(i * 0.05)] for i in range(p["n_heads"])], np.float32)
+    heads = np.repeat(np.arange(p["n_heads"]), 12)
+    tails = np.array([(h * 7 + o * 11) % p["n_tail"] for h in range(p["n_heads"]) for o in range(12)])
+    w = np.array([1.0 - o * 0.04 for _ in range(p["n_heads"]) for o in range(12)], np.float32)
+    args = (init, base, heads, tails, w, p["n_epochs"], p["a"], p["b"], p["alpha"], p["neg_rate"],
+            p["repulsion"], p["seed"])
+    orc.set_threads(1)
+    one = orc.optimize_layout_transform(*args)
+    orc.set_threads(4)
+    four = orc.optimize_layout_transform(*args)
+    orc.set_threads(orc.max_threads())
+    np.testing.assert_array_equal(one, four)
+
+
+def test_spectral_disconnected_beats_random(orc):
+    # rust_umap/src/lib.rs:7541-7570
+    x, labels = workloads.disconnected_components(4, 60)
+    idx, dist = orc.exact_knn(x, 10)
+    h, t, w, _, _ = orc.fuzzy_graph(idx, dist)
+    spec, used, ncomp = orc.spectral_init(x, h, t, w, 2, 42)
+    assert used and ncomp == 4
+    rnd = orc.random_init(x.shape[0], 2, 42)
+
+    def ratio(e):
+        cents = np.stack([e[labels == c].mean(0) for c in range(4)])
+        sep = min(np.linalg.norm(cents[i] - cents[j]) for i in range(4) for j in range(i + 1, 4))
+        std = max(np.sqrt(((e[labels == c] - cents[c]) ** 2).mean(0).sum()) for c in range(4))
+        return sep / (std + 1e-6)
+
+    assert ratio(spec) > ratio(rnd) * 1.2

@@ -1,0 +1,42 @@
+"""The Hogwild SGD layout against the oracle's sequential SGD from the
+same graph and initial embedding: trustworthiness@15 and 15-NN
+preservation within 0.005 (statistical parity: the reference's single RNG
+stream and edge order are not reproduced)."""
+import numpy as np
+import pytest
+
+from umapers_b200 import diagnostics, workloads
+from tests import gpu_util as gu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def problem(orc):
+    x = workloads.isotropic_mixture(6000, 32, 12, 2.5, seed=13)
+    idx, dist = orc.exact_knn(x, 15)
+    h, t, w, _, _ = orc.fuzzy_graph(idx, dist, n_epochs=200)
+    init, _, _ = orc.spectral_init(x, h, t, w, 2, 42)
+    a, b = orc.find_ab_params(1.0, 0.1)
+    return x, h, t, w, init, a, b
+
+
+def test_layout_quality_matches_oracle(orc, problem):
+    x, h, t, w, init, a, b = problem
+    o_emb, _ = orc.optimize_layout(init, h, t, w, 200, a, b, seed=7)
+    g_emb = gu.optimize_layout(init, h, t, w, 200, a, b, seed=7)
+    assert np.all(np.isfinite(g_emb))
+    qo = diagnostics.quality(x, o_emb)
+    qg = diagnostics.quality(x, g_emb)
+    print("oracle", qo, "gpu", qg)
+    assert abs(qo["trustworthiness"] - qg["trustworthiness"]) <= 0.005
+    assert abs(qo["knn_preservation"] - qg["knn_preservation"]) <= 0.005 or \
+        qg["knn_preservation"] > qo["knn_preservation"]
+
+
+def test_layout_three_dimensions(orc, problem):
+    x, h, t, w, _, a, b = problem
+    init = orc.random_init(x.shape[0], 3, 5)
+    g = gu.optimize_layout(init, h, t, w, 100, a, b, seed=3)
+    assert g.shape == (x.shape[0], 3) and np.all(np.isfinite(g))
+    assert diagnostics.quality(x, g)["trustworthiness"] > 0.85

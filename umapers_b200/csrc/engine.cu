@@ -1,0 +1,945 @@
+// engine.cu - the C ABI of libumapb200 and the host pipeline behind it.
+//
+// Mirrors rust_umap::UmapModel (rust_umap/src/lib.rs:570-1966): parameter
+// and data validation with the reference's messages (lib.rs:1968-2283), the
+// kNN switch (lib.rs:2285-2331), build_dense_fit_artifacts (lib.rs:1367-1464)
+// and transform_rows / transform_from_knn (lib.rs:1604-1780).  Every stage
+// after the input upload runs on the model's CUDA stream; the training matrix,
+// the embedding and the graph stay in HBM.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <unordered_set>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace umapb {
+std::atomic<unsigned long long> g_kernel_launches{0};
+}  // namespace umapb
+
+using namespace umapb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr const char* kVersion = "1.1.4+b200.1";
+constexpr float kSmoothKTolerance = 1e-5f;  // lib.rs:19
+
+std::string fmt_float(float v) {
+    // Rust's Display for f32 prints the shortest round-trip representation.
+    char buf[64];
+    for (int prec = 1; prec <= 9; ++prec) {
+        std::snprintf(buf, sizeof(buf), "%.*g", prec, static_cast<double>(v));
+        if (std::strtof(buf, nullptr) == v) break;
+    }
+    std::string s(buf);
+    if (s.find_first_of(".eE") == std::string::npos && s.find("inf") == std::string::npos &&
+        s.find("nan") == std::string::npos)
+        ;  // integers print without a decimal point in Rust's Display
+    return s;
+}
+
+const char* metric_debug_name(int32_t m) {
+    switch (m) {
+        case UMAPB_METRIC_EUCLIDEAN: return "Euclidean";
+        case UMAPB_METRIC_MANHATTAN: return "Manhattan";
+        case UMAPB_METRIC_COSINE: return "Cosine";
+        case UMAPB_METRIC_CHEBYSHEV: return "Chebyshev";
+        case UMAPB_METRIC_MINKOWSKI: return "Minkowski";
+        case UMAPB_METRIC_CORRELATION: return "Correlation";
+        case UMAPB_METRIC_CANBERRA: return "Canberra";
+        case UMAPB_METRIC_BRAYCURTIS: return "BrayCurtis";
+        default: return "Unknown";
+    }
+}
+
+std::string metric_debug(int32_t m, float p) {
+    if (m == UMAPB_METRIC_MINKOWSKI) return "Minkowski { p: " + fmt_float(p) + " }";
+    return metric_debug_name(m);
+}
+
+template <typename F>
+int32_t guarded(F&& fn) {
+    try {
+        fn();
+        g_last_error.clear();
+        return UMAPB_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return UMAPB_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return UMAPB_ERR_CUDA;
+    }
+}
+
+// ------------------------------------------------------------ validation
+// validate_data (lib.rs:2113-2138) on host memory; the finiteness scan is
+// split across threads for large inputs.
+void validate_data_host(const float* data, int64_t n, int64_t d) {
+    if (n == 0) throw Error(UMAPB_ERR_EMPTY_DATA, "input data is empty");
+    if (n < 2) throw Error(UMAPB_ERR_NEED_TWO_SAMPLES, "need at least two samples");
+    if (d == 0) invalid("input rows must have at least one feature");
+    const int64_t total = n * d;
+    int n_threads = 1;
+    if (total >= (int64_t(1) << 22))
+        n_threads = static_cast<int>(std::min<unsigned>(16, std::max(1u, std::thread::hardware_concurrency())));
+    std::vector<int64_t> first(n_threads, INT64_MAX);
+    auto scan = [&](int t) {
+        const int64_t rows_per = ceil_div(n, n_threads);
+        const int64_t r0 = t * rows_per, r1 = std::min(n, r0 + rows_per);
+        for (int64_t r = r0; r < r1; ++r) {
+            const uint32_t* row = reinterpret_cast<const uint32_t*>(data + r * d);
+            uint32_t bad = 0;
+            for (int64_t c = 0; c < d; ++c) bad |= ((row[c] & 0x7f800000u) == 0x7f800000u);
+            if (bad) {
+                first[t] = r;
+                return;
+            }
+        }
+    };
+    if (n_threads == 1) {
+        scan(0);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < n_threads; ++t) th.emplace_back(scan, t);
+        for (auto& t : th) t.join();
+    }
+    const int64_t bad = *std::min_element(first.begin(), first.end());
+    if (bad != INT64_MAX)
+        invalid("input contains non-finite value at row " + std::to_string(bad));
+}
+
+void validate_data_device(const float* data, int64_t n, int64_t d, cudaStream_t s) {
+    if (n == 0) throw Error(UMAPB_ERR_EMPTY_DATA, "input data is empty");
+    if (n < 2) throw Error(UMAPB_ERR_NEED_TWO_SAMPLES, "need at least two samples");
+    if (d == 0) invalid("input rows must have at least one feature");
+    const int64_t bad = first_nonfinite_row(data, n, static_cast<int>(d), s);
+    if (bad != INT64_MAX)
+        invalid("input contains non-finite value at row " + std::to_string(bad));
+}
+
+bool finite(float v) { return std::isfinite(v); }
+
+// validate_params (lib.rs:2140-2228) and validate_metric (lib.rs:2230-2239).
+void validate_params(const umapb_params& p, int64_t n_samples) {
+    if (p.metric == UMAPB_METRIC_MINKOWSKI && (!finite(p.metric_p) || p.metric_p <= 0.0f))
+        invalid("minkowski metric requires finite p > 0");
+    if (p.n_neighbors < 2) invalid("n_neighbors must be >= 2");
+    if (p.n_neighbors >= n_samples)
+        invalid("n_neighbors (" + std::to_string(p.n_neighbors) +
+                ") must be smaller than number of samples (" + std::to_string(n_samples) + ")");
+    if (p.n_components <= 0) invalid("n_components must be >= 1");
+    if (!finite(p.learning_rate) || p.learning_rate <= 0.0f)
+        invalid("learning_rate must be finite and > 0");
+    if (!finite(p.min_dist) || p.min_dist < 0.0f) invalid("min_dist must be finite and >= 0");
+    if (!finite(p.spread) || p.spread <= 0.0f) invalid("spread must be finite and > 0");
+    if (p.min_dist > p.spread) invalid("min_dist must be <= spread");
+    if (!finite(p.set_op_mix_ratio) || p.set_op_mix_ratio < 0.0f || p.set_op_mix_ratio > 1.0f)
+        invalid("set_op_mix_ratio must be finite and in [0, 1]");
+    if (!finite(p.repulsion_strength) || p.repulsion_strength < 0.0f)
+        invalid("repulsion_strength must be finite and >= 0");
+    if (p.negative_sample_rate <= 0) invalid("negative_sample_rate must be >= 1");
+    if (!finite(p.local_connectivity) || p.local_connectivity < 0.0f)
+        invalid("local_connectivity must be finite and >= 0");
+    if (p.approx_knn_candidates <= 0) invalid("approx_knn_candidates must be >= 1");
+    if (p.approx_knn_iters <= 0) invalid("approx_knn_iters must be >= 1");
+    if (!finite(p.dens_lambda) || p.dens_lambda < 0.0f) invalid("dens_lambda must be finite and >= 0");
+    if (!finite(p.dens_frac) || p.dens_frac < 0.0f || p.dens_frac > 1.0f)
+        invalid("dens_frac must be finite and in [0, 1]");
+    if (!finite(p.dens_var_shift) || p.dens_var_shift <= 0.0f)
+        invalid("dens_var_shift must be finite and > 0");
+}
+
+// The parts of the reference surface the GPU engine does not implement.
+void check_engine_support(const umapb_params& p) {
+    if (p.metric != UMAPB_METRIC_EUCLIDEAN && p.metric != UMAPB_METRIC_COSINE)
+        invalid(std::string("metric ") + metric_debug_name(p.metric) +
+                " is not supported by the B200 engine (supported: euclidean, cosine)");
+    if (p.densmap || p.output_dens)
+        invalid("densmap and output_dens are not supported by the B200 engine");
+    if (p.n_components > 16) invalid("n_components above 16 is not supported by the B200 engine");
+}
+
+// should_use_approximate_knn (lib.rs:2285-2311).
+bool should_use_approximate_knn(const umapb_params& p, int64_t n, int64_t d) {
+    if (!p.use_approximate_knn || n <= p.approx_knn_threshold) return false;
+    if (p.approx_knn_threshold > 0) {
+        const int64_t mult = 4;  // both branches of lib.rs:2300-2307 use 4
+        (void)d;
+        if (n <= p.approx_knn_threshold * mult) return false;
+    }
+    return true;
+}
+
+int64_t default_epochs(const umapb_params& p, int64_t n) {
+    return p.n_epochs >= 0 ? p.n_epochs : (n <= 10000 ? 500 : 200);
+}
+
+double now_sec() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct StageClock {
+    cudaStream_t s;
+    bool on;
+    double t0;
+    StageClock(cudaStream_t st, bool enabled) : s(st), on(enabled), t0(now_sec()) {}
+    double lap() {
+        if (!on) return 0.0;
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        const double t = now_sec();
+        const double dt = t - t0;
+        t0 = t;
+        return dt;
+    }
+};
+
+}  // namespace
+
+struct umapb_model {
+    umapb_params p{};
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    float a = 0.0f, b = 0.0f;
+    bool fitted = false;
+    int64_t n_fit = 0, d_fit = 0;
+    DevBuf<float> X;    // training rows, n_fit x d_fit
+    DevBuf<float> emb;  // fitted embedding, n_fit x n_components
+
+    void ensure_device() {
+        if (stream) {
+            UMAPB_CUDA(cudaSetDevice(device));
+            return;
+        }
+        UMAPB_CUDA(cudaGetDevice(&device));
+        UMAPB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        // keep freed pool memory cached across fits
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    void resolve_ab() {
+        // resolve_ab_params (lib.rs:613-622): computed once, reused by later fits
+        if (a > 0.0f && b > 0.0f) return;
+        umapb::find_ab_params(p.spread, p.min_dist, &a, &b);
+    }
+};
+
+namespace {
+
+struct FitOutputs {
+    umapb_timings t{};
+    umapb_fit_info info{};
+};
+
+// Exact kNN on the device (exact_nearest_neighbors{,_to_reference}).
+void knn_exact_device(const float* Q, int64_t nq, const float* R, int64_t nr, int d, int k,
+                      int metric, int backend, int32_t* idx, float* dist, int64_t* fallback,
+                      double* kernel_sec, int32_t* backend_used, cudaStream_t s) {
+    const bool use_tc = backend == UMAPB_KNN_TENSOR ||
+                        (backend == UMAPB_KNN_AUTO && knn_tc_supported(d, k, metric));
+    if (backend == UMAPB_KNN_TENSOR && !knn_tc_supported(d, k, metric))
+        invalid("the tensor-core kNN path does not support this metric/shape on this device");
+    if (use_tc) {
+        TcKnnStats st;
+        knn_tc(Q, nq, R, nr, d, k, metric, idx, dist, &st, s);
+        if (fallback) *fallback = st.fallback_rows;
+        if (kernel_sec) *kernel_sec = st.kernel_ms * 1e-3;
+        if (backend_used) *backend_used = UMAPB_KNN_TENSOR;
+        return;
+    }
+    DevBuf<float> qn, rn;
+    if (metric == UMAPB_METRIC_COSINE) {
+        qn.alloc(nq, s);
+        row_norms(Q, nq, d, qn.get(), nullptr, s);
+        if (R == Q) {
+            rn.ptr = nullptr;
+        } else {
+            rn.alloc(nr, s);
+            row_norms(R, nr, d, rn.get(), nullptr, s);
+        }
+    }
+    cudaEvent_t e0, e1;
+    UMAPB_CUDA(cudaEventCreate(&e0));
+    UMAPB_CUDA(cudaEventCreate(&e1));
+    UMAPB_CUDA(cudaEventRecord(e0, s));
+    knn_plain(Q, nullptr, nq, R, nr, d, k, metric, qn.get(), rn.get() ? rn.get() : qn.get(), idx,
+              dist, s);
+    UMAPB_CUDA(cudaEventRecord(e1, s));
+    UMAPB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    UMAPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (fallback) *fallback = 0;
+    if (kernel_sec) *kernel_sec = ms * 1e-3;
+    if (backend_used) *backend_used = UMAPB_KNN_PLAIN;
+}
+
+// build_dense_fit_artifacts (lib.rs:1367-1464) from a device kNN graph;
+// writes the embedding into model->emb.
+void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const int32_t* idx,
+                  const float* dist, int k, FitOutputs* out, StageClock& clk) {
+    cudaStream_t s = m->stream;
+    const umapb_params& p = m->p;
+    const int64_t n_epochs = default_epochs(p, n);
+    m->resolve_ab();
+    if (out) out->t.curve_params_sec = clk.lap();
+    const bool self = knn_includes_self(idx, dist, n, k, s);
+    if (out) out->t.knn_validate_trim_sec = clk.lap();
+    DevBuf<float> sig(n, s), rho(n, s);
+    smooth_knn(dist, n, k, static_cast<float>(p.n_neighbors), p.local_connectivity, 1.0f, self,
+               sig.get(), rho.get(), s);
+    if (out) out->t.smooth_knn_sec = clk.lap();
+    Graph g;
+    fuzzy_union(idx, dist, sig.get(), rho.get(), n, k, p.set_op_mix_ratio, n_epochs, g, s);
+    if (out) {
+        out->t.symmetrize_sec = clk.lap();
+        out->info.n_edges = g.n_edges;
+    }
+    const int dim = static_cast<int>(p.n_components);
+    DevBuf<float> emb(n * dim, s);
+    bool spectral_ok = false;
+    if (p.init == UMAPB_INIT_SPECTRAL) {
+        const SpectralResult r =
+            spectral_init(Xd, n, static_cast<int>(d), g, dim, p.random_seed, emb.get(), s);
+        spectral_ok = r.used_spectral;
+        if (out) out->info.n_components_graph = r.n_components;
+    }
+    if (!spectral_ok) random_init(n, dim, p.random_seed, -10.0f, 10.0f, emb.get(), s);
+    if (out) out->t.init_sec = clk.lap();
+    float sgd_ms = 0.0f;
+    const double samples = optimize_layout(
+        emb.get(), n, dim, g, n_epochs, m->a, m->b, p.learning_rate, p.negative_sample_rate,
+        p.repulsion_strength, p.random_seed ^ 0x9E3779B97F4A7C15ULL, out != nullptr,
+        out ? &sgd_ms : nullptr, s);
+    if (out) {
+        out->t.optimize_sec = clk.lap();
+        out->info.sgd_edge_samples = samples;
+        out->info.n_epochs = n_epochs;
+    }
+    m->emb = std::move(emb);
+}
+
+// Full dense fit on device-resident rows `Xd` (owned copy is taken).
+void fit_device(umapb_model* m, const float* Xd, int64_t n, int64_t d, bool copy_rows,
+                FitOutputs* out, StageClock& clk) {
+    cudaStream_t s = m->stream;
+    const umapb_params& p = m->p;
+    const int k = static_cast<int>(p.n_neighbors);
+    DevBuf<float> Xown;
+    const float* X = Xd;
+    if (copy_rows) {
+        Xown.alloc(n * d, s);
+        UMAPB_CUDA(cudaMemcpyAsync(Xown.get(), Xd, n * d * 4, cudaMemcpyDeviceToDevice, s));
+        X = Xown.get();
+    }
+    DevBuf<int32_t> idx(n * k, s);
+    DevBuf<float> dist(n * k, s);
+    const bool approx = should_use_approximate_knn(p, n, d);
+    if (out) out->info.used_approximate_knn = approx;
+    if (approx) {
+        nndescent(X, n, static_cast<int>(d), k, p.metric, p.approx_knn_candidates,
+                  p.approx_knn_iters, p.random_seed ^ 0xC0FEFEED1234ABCDULL, idx.get(),
+                  dist.get(), s);
+        if (out) out->info.knn_backend_used = -1;
+    } else {
+        int64_t fb = 0;
+        double ks = 0.0;
+        int32_t used = 0;
+        knn_exact_device(X, n, X, n, static_cast<int>(d), k, p.metric, p.knn_backend, idx.get(),
+                         dist.get(), &fb, &ks, &used, s);
+        if (out) {
+            out->info.knn_fallback_rows = fb;
+            out->info.knn_kernel_sec = ks;
+            out->info.knn_backend_used = used;
+        }
+    }
+    if (out) out->t.knn_sec = clk.lap();
+    fit_from_knn(m, X, n, d, idx.get(), dist.get(), k, out, clk);
+    if (copy_rows) m->X = std::move(Xown);
+    m->n_fit = n;
+    m->d_fit = d;
+    m->fitted = true;
+}
+
+void upload(DevBuf<float>& dst, const float* src, int64_t count, cudaStream_t s) {
+    dst.alloc(count, s);
+    if (count > 0)
+        UMAPB_CUDA(cudaMemcpyAsync(dst.get(), src, count * 4, cudaMemcpyHostToDevice, s));
+}
+
+void copy_embedding_out(umapb_model* m, float* out) {
+    const int64_t cnt = m->n_fit * m->p.n_components;
+    UMAPB_CUDA(cudaMemcpyAsync(out, m->emb.get(), cnt * 4, cudaMemcpyDeviceToHost, m->stream));
+    UMAPB_CUDA(cudaStreamSynchronize(m->stream));
+}
+
+void fit_host(umapb_model* m, const float* data, int64_t n, int64_t d, FitOutputs* out,
+              float* emb_out) {
+    StageClock clk(nullptr, out != nullptr);
+    const double t_start = now_sec();
+    validate_data_host(data, n, d);
+    validate_params(m->p, n);
+    check_engine_support(m->p);
+    m->ensure_device();
+    clk.s = m->stream;
+    DevBuf<float> X;
+    upload(X, data, n * d, m->stream);
+    if (out) out->t.validation_sec = clk.lap();
+    m->fitted = false;
+    fit_device(m, X.get(), n, d, false, out, clk);
+    m->X = std::move(X);
+    if (emb_out) copy_embedding_out(m, emb_out);
+    if (out) {
+        out->t.output_copy_sec = clk.lap();
+        out->t.total_sec = now_sec() - t_start;
+        out->info.n_samples = n;
+        out->info.n_features = d;
+    }
+}
+
+// validate_and_trim_precomputed_knn (lib.rs:1968-2040) on host arrays that
+// already passed the shape checks; writes the trimmed k columns.
+void trim_precomputed(const int64_t* idx, const float* dist, int64_t n, int64_t cols, int64_t k,
+                      std::vector<int32_t>& idx_out, std::vector<float>& dist_out) {
+    idx_out.resize(n * k);
+    dist_out.resize(n * k);
+    std::unordered_set<int64_t> seen;
+    seen.reserve(k * 2);
+    for (int64_t r = 0; r < n; ++r) {
+        seen.clear();
+        float prev = -INFINITY;
+        for (int64_t c = 0; c < k; ++c) {
+            const int64_t j = idx[r * cols + c];
+            const float dv = dist[r * cols + c];
+            if (j >= n)
+                invalid("precomputed knn index out of range at row " + std::to_string(r) +
+                        ", col " + std::to_string(c));
+            if (!std::isfinite(dv) || dv < 0.0f)
+                invalid("precomputed knn distance must be finite and >= 0 at row " +
+                        std::to_string(r) + ", col " + std::to_string(c));
+            if (!seen.insert(j).second)
+                invalid("precomputed knn row " + std::to_string(r) + " contains duplicate index " +
+                        std::to_string(j));
+            if (c > 0 && dv + kSmoothKTolerance < prev)
+                invalid("precomputed knn distances must be non-decreasing within each row; row " +
+                        std::to_string(r) + " has dist[" + std::to_string(c) + "]=" +
+                        fmt_float(dv) + " < dist[" + std::to_string(c - 1) + "]=" +
+                        fmt_float(prev));
+            prev = dv;
+            idx_out[r * k + c] = static_cast<int32_t>(j);
+            dist_out[r * k + c] = dv;
+        }
+    }
+}
+
+void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out_dev) {
+    cudaStream_t s = m->stream;
+    const umapb_params& p = m->p;
+    const int dim = static_cast<int>(p.n_components);
+    const int k = static_cast<int>(std::min<int64_t>(p.n_neighbors, m->n_fit));
+    const int64_t n_epochs = p.n_epochs >= 0 ? std::max<int64_t>(p.n_epochs, 1)
+                                             : (nq <= 10000 ? 100 : 30);
+    DevBuf<int32_t> idx(nq * k, s);
+    DevBuf<float> dist(nq * k, s);
+    knn_exact_device(Qd, nq, m->X.get(), m->n_fit, static_cast<int>(d), k, p.metric,
+                     p.knn_backend, idx.get(), dist.get(), nullptr, nullptr, nullptr, s);
+    DevBuf<float> sig(nq, s), rho(nq, s);
+    const float lc = std::max(p.local_connectivity - 1.0f, 0.0f);
+    smooth_knn(dist.get(), nq, k, static_cast<float>(k), lc, 1.0f, false, sig.get(), rho.get(), s);
+    Graph g;
+    bipartite_graph(idx.get(), dist.get(), sig.get(), rho.get(), nq, k, n_epochs, g, s);
+    transform_layout(out_dev, nq, dim, m->emb.get(), m->n_fit, g, n_epochs, m->a, m->b,
+                     p.learning_rate / 4.0f, p.negative_sample_rate, p.repulsion_strength,
+                     p.random_seed ^ 0xA24BAED40B53C117ULL, s);
+}
+
+// transform_rows checks (lib.rs:1608-1643)
+void check_transform(umapb_model* m, int64_t n_cols) {
+    if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+    (void)n_cols;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* umapb_version(void) { return kVersion; }
+int32_t umapb_abi_version(void) { return UMAPB_ABI_VERSION; }
+const char* umapb_last_error(void) { return g_last_error.c_str(); }
+uint64_t umapb_kernel_launches(void) { return g_kernel_launches.load(); }
+
+void umapb_params_default(umapb_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->n_neighbors = 15;
+    p->n_components = 2;
+    p->n_epochs = -1;
+    p->metric = UMAPB_METRIC_EUCLIDEAN;
+    p->metric_p = 0.0f;
+    p->learning_rate = 1.0f;
+    p->min_dist = 0.1f;
+    p->spread = 1.0f;
+    p->local_connectivity = 1.0f;
+    p->set_op_mix_ratio = 1.0f;
+    p->repulsion_strength = 1.0f;
+    p->negative_sample_rate = 5;
+    p->random_seed = 42;
+    p->init = UMAPB_INIT_SPECTRAL;
+    p->use_approximate_knn = 1;
+    p->approx_knn_candidates = 50;
+    p->approx_knn_iters = 14;
+    p->approx_knn_threshold = 4096;
+    p->densmap = 0;
+    p->dens_lambda = 2.0f;
+    p->dens_frac = 0.3f;
+    p->dens_var_shift = 0.1f;
+    p->output_dens = 0;
+    p->knn_backend = UMAPB_KNN_AUTO;
+}
+
+int32_t umapb_create(const umapb_params* params, umapb_model** out_model) {
+    return guarded([&] {
+        if (!params || !out_model) invalid("null argument");
+        if (params->init != UMAPB_INIT_RANDOM && params->init != UMAPB_INIT_SPECTRAL)
+            invalid("unsupported init, expected random|spectral");
+        if (params->metric < 0 || params->metric > UMAPB_METRIC_BRAYCURTIS)
+            invalid("unsupported metric");
+        auto* m = new umapb_model();
+        m->p = *params;
+        *out_model = m;
+    });
+}
+
+void umapb_destroy(umapb_model* m) {
+    if (!m) return;
+    {
+        std::lock_guard<std::mutex> lk(m->mu);
+        if (m->stream) {
+            cudaSetDevice(m->device);
+            m->X.release();
+            m->emb.release();
+            cudaStreamSynchronize(m->stream);
+            cudaStreamDestroy(m->stream);
+        }
+    }
+    delete m;
+}
+
+int32_t umapb_fit(umapb_model* m, const float* data, int64_t n_rows, int64_t n_cols) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        fit_host(m, data, n_rows, n_cols, nullptr, nullptr);
+    });
+}
+
+int32_t umapb_fit_transform(umapb_model* m, const float* data, int64_t n_rows, int64_t n_cols,
+                            float* out) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        fit_host(m, data, n_rows, n_cols, nullptr, out);
+    });
+}
+
+int32_t umapb_fit_transform_stateless(const umapb_params* params, const float* data,
+                                      int64_t n_rows, int64_t n_cols, float* out) {
+    umapb_model* m = nullptr;
+    int32_t st = umapb_create(params, &m);
+    if (st != UMAPB_OK) return st;
+    st = umapb_fit_transform(m, data, n_rows, n_cols, out);
+    const std::string err = g_last_error;
+    umapb_destroy(m);
+    g_last_error = err;
+    return st;
+}
+
+int32_t umapb_profile_fit_transform(umapb_model* m, const float* data, int64_t n_rows,
+                                    int64_t n_cols, float* out, umapb_timings* timings,
+                                    umapb_fit_info* info) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        FitOutputs fo;
+        fit_host(m, data, n_rows, n_cols, &fo, out);
+        if (timings) *timings = fo.t;
+        if (info) *info = fo.info;
+    });
+}
+
+int32_t umapb_fit_transform_device(umapb_model* m, const float* data, int64_t n_rows,
+                                   int64_t n_cols, float* out, umapb_timings* timings,
+                                   umapb_fit_info* info) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        m->ensure_device();
+        FitOutputs fo;
+        StageClock clk(m->stream, timings != nullptr || info != nullptr);
+        const double t_start = now_sec();
+        validate_data_device(data, n_rows, n_cols, m->stream);
+        validate_params(m->p, n_rows);
+        check_engine_support(m->p);
+        fo.t.validation_sec = clk.lap();
+        m->fitted = false;
+        fit_device(m, data, n_rows, n_cols, true, &fo, clk);
+        if (out)
+            UMAPB_CUDA(cudaMemcpyAsync(out, m->emb.get(), n_rows * m->p.n_components * 4,
+                                       cudaMemcpyDeviceToDevice, m->stream));
+        UMAPB_CUDA(cudaStreamSynchronize(m->stream));
+        fo.t.total_sec = now_sec() - t_start;
+        fo.info.n_samples = n_rows;
+        fo.info.n_features = n_cols;
+        if (timings) *timings = fo.t;
+        if (info) *info = fo.info;
+    });
+}
+
+int32_t umapb_fit_transform_with_knn(umapb_model* m, const float* data, int64_t n_rows,
+                                     int64_t n_cols, const int64_t* knn_indices,
+                                     int64_t idx_rows, int64_t idx_cols,
+                                     const float* knn_dists, int64_t dist_rows,
+                                     int64_t dist_cols, int32_t knn_metric,
+                                     int32_t validate_precomputed, float* out) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        const umapb_params& p = m->p;
+        // fit_transform_with_knn_metric_dense_i64_flat (lib.rs:1159-1212)
+        if (knn_metric != p.metric)
+            invalid("precomputed knn metric (" + metric_debug(knn_metric, p.metric_p) +
+                    ") must match model metric (" + metric_debug(p.metric, p.metric_p) + ")");
+        validate_data_host(data, n_rows, n_cols);
+        validate_params(p, n_rows);
+        // validate_precomputed_array_shapes (lib.rs:2042-2066)
+        if (idx_rows != dist_rows || idx_cols != dist_cols)
+            invalid("knn_indices and knn_dists must have identical shapes");
+        if (idx_rows != n_rows) invalid("knn row count must match data row count");
+        if (idx_cols < p.n_neighbors)
+            invalid("knn columns must be >= n_neighbors (" + std::to_string(p.n_neighbors) + ")");
+        if (validate_precomputed) {
+            // validate_precomputed_distance_values_flat (lib.rs:2068-2082)
+            const int64_t total = dist_rows * dist_cols;
+            for (int64_t i = 0; i < total; ++i) {
+                if (!std::isfinite(knn_dists[i])) invalid("knn_dists must contain only finite values");
+                if (knn_dists[i] < 0.0f) invalid("knn_dists must be non-negative");
+            }
+        }
+        // precomputed_knn_indices_from_i64_flat (lib.rs:2084-2111)
+        for (int64_t i = 0; i < idx_rows * idx_cols; ++i)
+            if (knn_indices[i] < 0) invalid("knn indices must be non-negative integers");
+        check_engine_support(p);
+        const int64_t k = p.n_neighbors;
+        std::vector<int32_t> idx_h;
+        std::vector<float> dist_h;
+        trim_precomputed(knn_indices, knn_dists, n_rows, idx_cols, k, idx_h, dist_h);
+        m->ensure_device();
+        cudaStream_t s = m->stream;
+        DevBuf<float> X;
+        upload(X, data, n_rows * n_cols, s);
+        DevBuf<int32_t> idx(n_rows * k, s);
+        DevBuf<float> dist;
+        upload(dist, dist_h.data(), n_rows * k, s);
+        UMAPB_CUDA(cudaMemcpyAsync(idx.get(), idx_h.data(), n_rows * k * 4, cudaMemcpyHostToDevice, s));
+        m->fitted = false;
+        StageClock clk(s, false);
+        fit_from_knn(m, X.get(), n_rows, n_cols, idx.get(), dist.get(), static_cast<int>(k),
+                     nullptr, clk);
+        m->X = std::move(X);
+        m->n_fit = n_rows;
+        m->d_fit = n_cols;
+        m->fitted = true;
+        if (out) copy_embedding_out(m, out);
+    });
+}
+
+int32_t umapb_transform(umapb_model* m, const float* query, int64_t n_rows, int64_t n_cols,
+                        float* out) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        if (n_rows == 0) return;
+        if (n_cols != m->d_fit)
+            throw Error(UMAPB_ERR_FEATURE_MISMATCH,
+                        "feature mismatch: expected " + std::to_string(m->d_fit) + ", got " +
+                            std::to_string(n_cols));
+        for (int64_t r = 0; r < n_rows; ++r)
+            for (int64_t c = 0; c < n_cols; ++c)
+                if (!std::isfinite(query[r * n_cols + c]))
+                    invalid("input contains non-finite value at row " + std::to_string(r));
+        m->ensure_device();
+        cudaStream_t s = m->stream;
+        DevBuf<float> Q, outd(n_rows * m->p.n_components, s);
+        upload(Q, query, n_rows * n_cols, s);
+        transform_device(m, Q.get(), n_rows, n_cols, outd.get());
+        UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * m->p.n_components * 4,
+                                   cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int32_t umapb_transform_device(umapb_model* m, const float* query, int64_t n_rows,
+                               int64_t n_cols, float* out) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        if (n_rows == 0) return;
+        if (n_cols != m->d_fit)
+            throw Error(UMAPB_ERR_FEATURE_MISMATCH,
+                        "feature mismatch: expected " + std::to_string(m->d_fit) + ", got " +
+                            std::to_string(n_cols));
+        m->ensure_device();
+        const int64_t bad = first_nonfinite_row(query, n_rows, static_cast<int>(n_cols), m->stream);
+        if (bad != INT64_MAX) invalid("input contains non-finite value at row " + std::to_string(bad));
+        transform_device(m, query, n_rows, n_cols, out);
+        UMAPB_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+int64_t umapb_n_components(const umapb_model* m) { return m ? m->p.n_components : -1; }
+int64_t umapb_n_neighbors(const umapb_model* m) { return m ? m->p.n_neighbors : -1; }
+int64_t umapb_n_features(const umapb_model* m) { return (m && m->fitted) ? m->d_fit : -1; }
+int64_t umapb_n_samples(const umapb_model* m) { return (m && m->fitted) ? m->n_fit : -1; }
+
+int32_t umapb_get_embedding(const umapb_model* cm, float* out, int64_t n_rows, int64_t n_cols) {
+    auto* m = const_cast<umapb_model*>(cm);
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        if (n_rows != m->n_fit || n_cols != m->p.n_components)
+            invalid("output buffer shape mismatch");
+        UMAPB_CUDA(cudaSetDevice(m->device));
+        copy_embedding_out(m, out);
+    });
+}
+
+int32_t umapb_get_ab(const umapb_model* m, float* a, float* b) {
+    return guarded([&] {
+        if (!(m->a > 0.0f && m->b > 0.0f)) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        *a = m->a;
+        *b = m->b;
+    });
+}
+
+// ----------------------------------------------------------- stage APIs
+
+int32_t umapb_find_ab_params(float spread, float min_dist, float* a, float* b) {
+    return guarded([&] { umapb::find_ab_params(spread, min_dist, a, b); });
+}
+
+namespace {
+struct ScopedStream {
+    cudaStream_t s = nullptr;
+    ScopedStream() { UMAPB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~ScopedStream() {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    }
+};
+
+void to_i64(const std::vector<int32_t>& v, int64_t* out) {
+    for (size_t i = 0; i < v.size(); ++i) out[i] = v[i];
+}
+}  // namespace
+
+int32_t umapb_knn_exact(const float* data, int64_t n, int64_t d, int64_t k, int32_t metric,
+                        int32_t backend, int64_t* indices, float* dists, int64_t* fallback_rows) {
+    return guarded([&] {
+        if (n <= 0 || d <= 0) invalid("empty input");
+        if (k < 1 || k > n) invalid("k must be in [1, n_rows]");
+        ScopedStream ss;
+        DevBuf<float> X;
+        upload(X, data, n * d, ss.s);
+        DevBuf<int32_t> idx(n * k, ss.s);
+        DevBuf<float> dist(n * k, ss.s);
+        int64_t fb = 0;
+        knn_exact_device(X.get(), n, X.get(), n, static_cast<int>(d), static_cast<int>(k), metric,
+                         backend, idx.get(), dist.get(), &fb, nullptr, nullptr, ss.s);
+        std::vector<int32_t> ih(n * k);
+        UMAPB_CUDA(cudaMemcpyAsync(ih.data(), idx.get(), n * k * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaMemcpyAsync(dists, dist.get(), n * k * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        to_i64(ih, indices);
+        if (fallback_rows) *fallback_rows = fb;
+    });
+}
+
+int32_t umapb_knn_query(const float* query, int64_t nq, const float* reference, int64_t nr,
+                        int64_t d, int64_t k, int32_t metric, int32_t backend, int64_t* indices,
+                        float* dists) {
+    return guarded([&] {
+        if (nr <= 0 || d <= 0) invalid("empty reference");
+        if (k < 1 || k > nr) invalid("k must be in [1, n_reference]");
+        if (nq == 0) return;
+        ScopedStream ss;
+        DevBuf<float> Q, R;
+        upload(Q, query, nq * d, ss.s);
+        upload(R, reference, nr * d, ss.s);
+        DevBuf<int32_t> idx(nq * k, ss.s);
+        DevBuf<float> dist(nq * k, ss.s);
+        knn_exact_device(Q.get(), nq, R.get(), nr, static_cast<int>(d), static_cast<int>(k),
+                         metric, backend, idx.get(), dist.get(), nullptr, nullptr, nullptr, ss.s);
+        std::vector<int32_t> ih(nq * k);
+        UMAPB_CUDA(cudaMemcpyAsync(ih.data(), idx.get(), nq * k * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaMemcpyAsync(dists, dist.get(), nq * k * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        to_i64(ih, indices);
+    });
+}
+
+int32_t umapb_nndescent(const float* data, int64_t n, int64_t d, int64_t k, int32_t metric,
+                        int64_t candidate_pool, int64_t n_iters, uint64_t seed, int64_t* indices,
+                        float* dists, int64_t* iters_run) {
+    return guarded([&] {
+        if (n <= 1 || d <= 0) invalid("need at least two rows");
+        if (k < 1 || k >= n) invalid("k must be in [1, n_rows)");
+        ScopedStream ss;
+        DevBuf<float> X;
+        upload(X, data, n * d, ss.s);
+        DevBuf<int32_t> idx(n * k, ss.s);
+        DevBuf<float> dist(n * k, ss.s);
+        const int64_t ran = umapb::nndescent(X.get(), n, static_cast<int>(d), static_cast<int>(k),
+                                             metric, candidate_pool, n_iters, seed, idx.get(),
+                                             dist.get(), ss.s);
+        std::vector<int32_t> ih(n * k);
+        UMAPB_CUDA(cudaMemcpyAsync(ih.data(), idx.get(), n * k * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaMemcpyAsync(dists, dist.get(), n * k * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        to_i64(ih, indices);
+        if (iters_run) *iters_run = ran;
+    });
+}
+
+int32_t umapb_smooth_knn_dist(const float* dists, int64_t n, int64_t cols, float k,
+                              float local_connectivity, float bandwidth, int32_t include_self,
+                              float* sigmas, float* rhos) {
+    return guarded([&] {
+        if (n == 0) return;
+        ScopedStream ss;
+        DevBuf<float> D, sg(n, ss.s), rh(n, ss.s);
+        upload(D, dists, n * cols, ss.s);
+        smooth_knn(D.get(), n, static_cast<int>(cols), k, local_connectivity, bandwidth,
+                   include_self != 0, sg.get(), rh.get(), ss.s);
+        UMAPB_CUDA(cudaMemcpyAsync(sigmas, sg.get(), n * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaMemcpyAsync(rhos, rh.get(), n * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+    });
+}
+
+int32_t umapb_fuzzy_graph(const int64_t* indices, const float* dists, int64_t n, int64_t k,
+                          float set_op_mix_ratio, float local_connectivity, int64_t n_epochs,
+                          int32_t* heads, int32_t* tails, float* weights, int64_t capacity,
+                          int64_t* n_edges, float* sigmas, float* rhos) {
+    return guarded([&] {
+        if (n <= 0 || k <= 0) invalid("empty kNN graph");
+        if (capacity < 2 * n * k) invalid("capacity must be >= 2 * n_rows * k");
+        ScopedStream ss;
+        std::vector<int32_t> ih(n * k);
+        for (int64_t i = 0; i < n * k; ++i) {
+            if (indices[i] < 0 || indices[i] >= n) invalid("kNN index out of range");
+            ih[i] = static_cast<int32_t>(indices[i]);
+        }
+        DevBuf<int32_t> idx(n * k, ss.s);
+        DevBuf<float> dist;
+        UMAPB_CUDA(cudaMemcpyAsync(idx.get(), ih.data(), n * k * 4, cudaMemcpyHostToDevice, ss.s));
+        upload(dist, dists, n * k, ss.s);
+        const bool self = knn_includes_self(idx.get(), dist.get(), n, static_cast<int>(k), ss.s);
+        DevBuf<float> sg(n, ss.s), rh(n, ss.s);
+        smooth_knn(dist.get(), n, static_cast<int>(k), static_cast<float>(k), local_connectivity,
+                   1.0f, self, sg.get(), rh.get(), ss.s);
+        Graph g;
+        fuzzy_union(idx.get(), dist.get(), sg.get(), rh.get(), n, static_cast<int>(k),
+                    set_op_mix_ratio, n_epochs, g, ss.s);
+        if (g.n_edges > 0) {
+            UMAPB_CUDA(cudaMemcpyAsync(heads, g.heads.get(), g.n_edges * 4, cudaMemcpyDeviceToHost, ss.s));
+            UMAPB_CUDA(cudaMemcpyAsync(tails, g.tails.get(), g.n_edges * 4, cudaMemcpyDeviceToHost, ss.s));
+            UMAPB_CUDA(cudaMemcpyAsync(weights, g.weights.get(), g.n_edges * 4, cudaMemcpyDeviceToHost, ss.s));
+        }
+        if (sigmas) UMAPB_CUDA(cudaMemcpyAsync(sigmas, sg.get(), n * 4, cudaMemcpyDeviceToHost, ss.s));
+        if (rhos) UMAPB_CUDA(cudaMemcpyAsync(rhos, rh.get(), n * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        *n_edges = g.n_edges;
+    });
+}
+
+namespace {
+void graph_from_host(const int32_t* heads, const int32_t* tails, const float* weights,
+                     int64_t ne, int64_t n, Graph& g, cudaStream_t s) {
+    for (int64_t e = 0; e < ne; ++e) {
+        if (heads[e] < 0 || heads[e] >= n || tails[e] < 0 || tails[e] >= n)
+            invalid("edge endpoint out of range");
+        if (e > 0 && heads[e] < heads[e - 1]) invalid("edges must be sorted by head");
+    }
+    g.n = n;
+    g.n_edges = ne;
+    g.heads.alloc(std::max<int64_t>(ne, 1), s);
+    g.tails.alloc(std::max<int64_t>(ne, 1), s);
+    g.weights.alloc(std::max<int64_t>(ne, 1), s);
+    if (ne > 0) {
+        UMAPB_CUDA(cudaMemcpyAsync(g.heads.get(), heads, ne * 4, cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(g.tails.get(), tails, ne * 4, cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(g.weights.get(), weights, ne * 4, cudaMemcpyHostToDevice, s));
+    }
+    g.row_ptr.alloc(n + 1, s);
+    build_row_ptr(g.heads.get(), ne, n, g.row_ptr.get(), s);
+}
+}  // namespace
+
+int32_t umapb_spectral_init(const float* data, int64_t n, int64_t d, const int32_t* heads,
+                            const int32_t* tails, const float* weights, int64_t n_edges,
+                            int64_t n_components, uint64_t seed, float* out,
+                            int32_t* used_spectral) {
+    return guarded([&] {
+        if (n <= 0 || d <= 0 || n_components <= 0) invalid("empty input");
+        ScopedStream ss;
+        DevBuf<float> X, emb(n * n_components, ss.s);
+        upload(X, data, n * d, ss.s);
+        Graph g;
+        graph_from_host(heads, tails, weights, n_edges, n, g, ss.s);
+        const SpectralResult r = spectral_init(X.get(), n, static_cast<int>(d), g,
+                                               static_cast<int>(n_components), seed, emb.get(), ss.s);
+        if (!r.used_spectral)
+            random_init(n, static_cast<int>(n_components), seed, -10.0f, 10.0f, emb.get(), ss.s);
+        UMAPB_CUDA(cudaMemcpyAsync(out, emb.get(), n * n_components * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        if (used_spectral) *used_spectral = r.used_spectral ? 1 : 0;
+    });
+}
+
+int32_t umapb_optimize_layout(float* embedding, int64_t n, int64_t dim, const int32_t* heads,
+                              const int32_t* tails, const float* weights, int64_t n_edges,
+                              int64_t n_epochs, float a, float b, float learning_rate,
+                              int64_t negative_sample_rate, float repulsion_strength,
+                              uint64_t seed) {
+    return guarded([&] {
+        if (n <= 0 || dim <= 0) invalid("empty embedding");
+        if (negative_sample_rate <= 0) invalid("negative_sample_rate must be >= 1");
+        ScopedStream ss;
+        DevBuf<float> emb;
+        upload(emb, embedding, n * dim, ss.s);
+        Graph g;
+        graph_from_host(heads, tails, weights, n_edges, n, g, ss.s);
+        optimize_layout(emb.get(), n, static_cast<int>(dim), g, n_epochs, a, b, learning_rate,
+                        negative_sample_rate, repulsion_strength, seed, false, nullptr, ss.s);
+        UMAPB_CUDA(cudaMemcpyAsync(embedding, emb.get(), n * dim * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,318 @@
+// nndescent.cu - the reference's NN-descent variant on the device.
+//
+// approximate_nearest_neighbors_with_distance (rust_umap/src/lib.rs:3086-3151)
+// with its candidate rule (collect_approx_candidate_indices, lib.rs:3051-3084):
+// pool = min(max(cand, k), n-1); max_candidates = 4*max(cand, k) + 1; the
+// initial lists are self + `pool` unique random rows; every iteration a row's
+// candidates are its neighbours, their neighbours, itself and
+// max(4, min(k/2, max_candidates)) random rows, de-duplicated and sorted by
+// index, cut to max_candidates by a random partial Fisher-Yates shuffle, all
+// evaluated, best k kept by (distance, index).  Iterations read the previous
+// lists and write new ones (as the reference's collect-then-replace does) and
+// stop when no row changed.  One warp owns one row; candidates live in shared
+// memory and are ordered with warp bitonic sorts.  Distances use the
+// reference's summation order (euclidean = sqrt of the squared distance,
+// lib.rs:3167).  Random streams are counter-based per (row, iteration).
+#include <climits>
+
+#include "kernels.cuh"
+
+namespace umapb {
+namespace {
+
+constexpr int kWarps = 4;
+
+__device__ inline float sqdist_ref(const float* __restrict__ x, const float* __restrict__ y, int d) {
+    if (d >= 64) {
+        float lane[8];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) lane[l] = 0.0f;
+        int i = 0;
+        for (; i + 8 <= d; i += 8)
+#pragma unroll
+            for (int l = 0; l < 8; ++l) {
+                const float df = __fsub_rn(x[i + l], y[i + l]);
+                lane[l] = __fadd_rn(lane[l], __fmul_rn(df, df));
+            }
+        float s = lane[0];
+#pragma unroll
+        for (int l = 1; l < 8; ++l) s = __fadd_rn(s, lane[l]);
+        for (; i < d; ++i) {
+            const float df = __fsub_rn(x[i], y[i]);
+            s = __fadd_rn(s, __fmul_rn(df, df));
+        }
+        return s;
+    }
+    float s = 0.0f;
+    for (int i = 0; i < d; ++i) {
+        const float df = __fsub_rn(x[i], y[i]);
+        s = __fadd_rn(s, __fmul_rn(df, df));
+    }
+    return s;
+}
+
+__device__ inline float dot_ref(const float* __restrict__ x, const float* __restrict__ y, int d) {
+    if (d >= 64) {
+        float lane[8];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) lane[l] = 0.0f;
+        int i = 0;
+        for (; i + 8 <= d; i += 8)
+#pragma unroll
+            for (int l = 0; l < 8; ++l) lane[l] = __fadd_rn(lane[l], __fmul_rn(x[i + l], y[i + l]));
+        float s = lane[0];
+#pragma unroll
+        for (int l = 1; l < 8; ++l) s = __fadd_rn(s, lane[l]);
+        for (; i < d; ++i) s = __fadd_rn(s, __fmul_rn(x[i], y[i]));
+        return s;
+    }
+    float s = 0.0f;
+    for (int i = 0; i < d; ++i) s = __fadd_rn(s, __fmul_rn(x[i], y[i]));
+    return s;
+}
+
+__device__ inline float pair_distance(const float* X, const float* norms, int64_t i, int64_t j,
+                                      int d, bool cosine) {
+    const float* x = X + i * d;
+    const float* y = X + j * d;
+    if (!cosine) return __fsqrt_rn(sqdist_ref(x, y, d));
+    const float xn = norms[i], yn = norms[j];
+    const float dot = dot_ref(x, y, d);
+    if (xn == 0.0f && yn == 0.0f) return 0.0f;
+    if (xn == 0.0f || yn == 0.0f) return 1.0f;
+    float c = __fdiv_rn(dot, __fmul_rn(xn, yn));
+    c = fminf(fmaxf(c, -1.0f), 1.0f);
+    return __fsub_rn(1.0f, c);
+}
+
+// Bitonic sort of `cnt` (<= cap, cap a power of two) 64-bit keys in shared
+// memory by one warp; slots past `cnt` must hold ~0.
+__device__ inline void warp_sort_u64(uint64_t* a, int cap) {
+    const int lane = threadIdx.x & 31;
+    for (int size = 2; size <= cap; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = lane; t < cap / 2; t += 32) {
+                const int lo = 2 * t - (t & (stride - 1));
+                const int hi = lo + stride;
+                const bool up = ((lo & size) == 0);
+                const uint64_t x = a[lo], y = a[hi];
+                if ((x > y) == up) {
+                    a[lo] = y;
+                    a[hi] = x;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+struct NdArgs {
+    const float* X;
+    const float* norms;
+    int64_t n;
+    int d;
+    int k;
+    int pool;
+    int maxc;
+    int expl;
+    int cap;  // power of two >= k + k*k + 1 + expl
+    bool cosine;
+    uint64_t seed;
+    const int32_t* old_idx;
+    const float* old_dist;
+    int32_t* new_idx;
+    float* new_dist;
+    int* changed;
+};
+
+// initial lists: self + `pool` unique random rows, best k kept (lib.rs:3100-3115)
+__global__ void __launch_bounds__(kWarps * 32) nd_init_kernel(NdArgs p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint64_t* keys = reinterpret_cast<uint64_t*>(smem) + warp * p.cap;
+    int32_t* cand = reinterpret_cast<int32_t*>(reinterpret_cast<uint64_t*>(smem) + kWarps * p.cap) +
+                    warp * p.cap;
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
+    if (i >= p.n) return;
+    int cnt = 0;
+    if (lane == 0) {
+        cand[cnt++] = static_cast<int32_t>(i);
+        uint64_t ctr = 0;
+        while (cnt < p.pool + 1) {
+            const int32_t j = static_cast<int32_t>(
+                rng_below(rng_word(p.seed, static_cast<uint64_t>(i), ctr++), static_cast<uint32_t>(p.n)));
+            bool dup = false;
+            for (int c = 0; c < cnt; ++c) dup |= cand[c] == j;
+            if (!dup) cand[cnt++] = j;
+        }
+    }
+    cnt = __shfl_sync(0xffffffffu, cnt, 0);
+    __syncwarp();
+    for (int c = lane; c < p.cap; c += 32) {
+        uint64_t key = ~0ULL;
+        if (c < cnt) {
+            const int32_t j = cand[c];
+            key = knn_key(pair_distance(p.X, p.norms, i, j, p.d, p.cosine), static_cast<uint32_t>(j));
+        }
+        keys[c] = key;
+    }
+    __syncwarp();
+    warp_sort_u64(keys, p.cap);
+    for (int c = lane; c < p.k; c += 32) {
+        p.new_idx[i * p.k + c] = static_cast<int32_t>(key_index(keys[c]));
+        p.new_dist[i * p.k + c] = key_dist(keys[c]);
+    }
+}
+
+__global__ void __launch_bounds__(kWarps * 32) nd_iter_kernel(NdArgs p, uint64_t iteration) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint64_t* keys = reinterpret_cast<uint64_t*>(smem) + warp * p.cap;
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
+    if (i >= p.n) return;
+    const int k = p.k;
+    // neighbours and neighbours of neighbours, as index keys (duplicates removed after sorting)
+    int cnt = 0;
+    for (int c = lane; c < k; c += 32) keys[c] = static_cast<uint64_t>(p.old_idx[i * k + c]);
+    for (int t = lane; t < k * k; t += 32) {
+        const int32_t nb = p.old_idx[i * k + t / k];
+        keys[k + t] = static_cast<uint64_t>(p.old_idx[static_cast<int64_t>(nb) * k + t % k]);
+    }
+    cnt = k + k * k;
+    if (lane == 0) keys[cnt] = static_cast<uint64_t>(i);
+    ++cnt;
+    const uint64_t rbase = iteration << 40;
+    for (int e = lane; e < p.expl; e += 32)
+        keys[cnt + e] = rng_below(rng_word(p.seed, static_cast<uint64_t>(i), rbase + e),
+                                  static_cast<uint32_t>(p.n));
+    cnt += p.expl;
+    for (int c = cnt + lane; c < p.cap; c += 32) keys[c] = ~0ULL;
+    __syncwarp();
+    warp_sort_u64(keys, p.cap);
+    // unique (sorted by index, as out.sort_unstable() leaves it)
+    int uniq = 0;
+    for (int base = 0; base < cnt; base += 32) {
+        const int c = base + lane;
+        const uint64_t v = c < cnt ? keys[c] : ~0ULL;
+        const uint64_t prev = (c > 0 && c < cnt) ? keys[c - 1] : ~0ULL - 1;
+        const bool keep = c < cnt && v != prev;
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        __syncwarp();
+        if (keep) keys[uniq + __popc(mask & ((1u << lane) - 1))] = v;
+        __syncwarp();
+        uniq += __popc(mask);
+    }
+    // random partial Fisher-Yates down to max_candidates (lib.rs:3076-3083)
+    if (uniq > p.maxc && lane == 0) {
+        uint64_t ctr = 1u << 20;
+        for (int s = 0; s < p.maxc; ++s) {
+            const uint32_t span = static_cast<uint32_t>(uniq - s);
+            const int r = s + static_cast<int>(rng_below(
+                                  rng_word(p.seed, static_cast<uint64_t>(i), rbase + ctr++), span));
+            const uint64_t t = keys[s];
+            keys[s] = keys[r];
+            keys[r] = t;
+        }
+    }
+    __syncwarp();
+    const int m = min(uniq, p.maxc);
+    // evaluate every candidate
+    for (int c = lane; c < p.cap; c += 32) {
+        uint64_t key = ~0ULL;
+        if (c < m) {
+            const int64_t j = static_cast<int64_t>(keys[c]);
+            key = knn_key(pair_distance(p.X, p.norms, i, j, p.d, p.cosine), static_cast<uint32_t>(j));
+        }
+        __syncwarp();
+        keys[c] = key;
+    }
+    __syncwarp();
+    warp_sort_u64(keys, p.cap);
+    bool diff = false;
+    for (int c = lane; c < k; c += 32) {
+        const int32_t ni = static_cast<int32_t>(key_index(keys[c]));
+        const float nd = key_dist(keys[c]);
+        diff |= (ni != p.old_idx[i * k + c]) || (nd != p.old_dist[i * k + c]);
+        p.new_idx[i * k + c] = ni;
+        p.new_dist[i * k + c] = nd;
+    }
+    if (__any_sync(0xffffffffu, diff) && lane == 0) *p.changed = 1;
+}
+
+}  // namespace
+
+int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t candidate_pool,
+                  int64_t n_iters, uint64_t seed, int32_t* out_idx, float* out_dist,
+                  cudaStream_t s) {
+    if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE)
+        invalid("the B200 NN-descent kernel supports metric euclidean and cosine");
+    if (n < 2 || k < 1 || k >= n) invalid("NN-descent needs 1 <= k < n_rows");
+    const int64_t ck = std::max<int64_t>(candidate_pool, k);
+    const int pool = static_cast<int>(std::min<int64_t>(ck, n - 1));
+    const int maxc = static_cast<int>(ck * 4 + 1);
+    const int expl = static_cast<int>(std::min<int64_t>(std::max<int64_t>(k / 2, 4), maxc));
+    int cap = 32;
+    const int need = std::max(k + k * k + 1 + expl, pool + 1);
+    while (cap < need) cap <<= 1;
+    const size_t smem = static_cast<size_t>(kWarps) * cap * 12;
+    if (smem > 200 * 1024) invalid("n_neighbors too large for the NN-descent kernel");
+    DevBuf<float> norms;
+    if (metric == UMAPB_METRIC_COSINE) {
+        norms.alloc(n, s);
+        row_norms(X, n, d, norms.get(), nullptr, s);
+    }
+    DevBuf<int32_t> idx_b(n * k, s);
+    DevBuf<float> dist_b(n * k, s);
+    DevBuf<int> changed(1, s);
+    NdArgs p{};
+    p.X = X;
+    p.norms = norms.get();
+    p.n = n;
+    p.d = d;
+    p.k = k;
+    p.pool = pool;
+    p.maxc = maxc;
+    p.expl = expl;
+    p.cap = cap;
+    p.cosine = metric == UMAPB_METRIC_COSINE;
+    p.seed = seed;
+    p.changed = changed.get();
+    UMAPB_CUDA(cudaFuncSetAttribute(nd_init_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+    UMAPB_CUDA(cudaFuncSetAttribute(nd_iter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+    const unsigned grid = static_cast<unsigned>(ceil_div(n, kWarps));
+    // lists alternate between the output arrays and the scratch pair
+    int32_t* cur_i = out_idx;
+    float* cur_d = out_dist;
+    int32_t* nxt_i = idx_b.get();
+    float* nxt_d = dist_b.get();
+    p.new_idx = cur_i;
+    p.new_dist = cur_d;
+    nd_init_kernel<<<grid, kWarps * 32, smem, s>>>(p);
+    UMAPB_LAUNCH_CHECK();
+    int64_t ran = 0;
+    for (int64_t it = 0; it < n_iters; ++it) {
+        UMAPB_CUDA(cudaMemsetAsync(changed.get(), 0, 4, s));
+        p.old_idx = cur_i;
+        p.old_dist = cur_d;
+        p.new_idx = nxt_i;
+        p.new_dist = nxt_d;
+        nd_iter_kernel<<<grid, kWarps * 32, smem, s>>>(p, static_cast<uint64_t>(it + 1));
+        UMAPB_LAUNCH_CHECK();
+        std::swap(cur_i, nxt_i);
+        std::swap(cur_d, nxt_d);
+        ran = it + 1;
+        int h = 0;
+        UMAPB_CUDA(cudaMemcpyAsync(&h, changed.get(), 4, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        if (!h) break;
+    }
+    if (cur_i != out_idx) {
+        UMAPB_CUDA(cudaMemcpyAsync(out_idx, cur_i, n * k * 4, cudaMemcpyDeviceToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(out_dist, cur_d, n * k * 4, cudaMemcpyDeviceToDevice, s));
+    }
+    return ran;
+}
+
+}  // namespace umapb

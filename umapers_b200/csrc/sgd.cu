@@ -1,0 +1,434 @@
+// sgd.cu - layout optimisation on the device.
+//
+// optimize_layout: the training SGD of rust_umap/src/lib.rs:5137-5321.  The
+// reference walks the edges of one epoch sequentially with a single RNG
+// stream; here one thread owns one edge per epoch (Hogwild): it keeps the
+// reference's per-edge schedule (epoch_of_next_sample, epoch_of_next_negative
+// sample, eps/neg_rate) exactly, moves its head point in registers through the
+// attractive step and all of its negative samples, and publishes the head and
+// tail moves with red.global.add, so concurrent edges never lose an update.
+// Negative samples come from a counter-based stream keyed by (edge, epoch,
+// sample) instead of the reference's shared SmallRng, so results do not depend
+// on scheduling.  The embedding (n x dim FP32, 8 MB at 1M x 2) stays in L2.
+//
+// transform_layout: init_graph_transform (lib.rs:4793-4836) followed by
+// optimize_layout_transform (lib.rs:5444-5544).  Queries never interact, so
+// one thread runs one query's whole schedule sequentially, as the reference's
+// per-query closure does.
+#include <cfloat>
+
+#include "kernels.cuh"
+
+namespace umapb {
+namespace {
+
+__device__ inline float clip4(float v) { return fminf(fmaxf(v, -4.0f), 4.0f); }  // lib.rs:4962
+
+// floor(v).max(0.0) as usize, saturating (lib.rs:5204-5206)
+__device__ inline uint32_t floor_count(float v) {
+    const float f = floorf(v);
+    if (!(f > 0.0f)) return 0u;
+    if (f >= 4294967295.0f) return 0xffffffffu;
+    return static_cast<uint32_t>(f);
+}
+
+__global__ void epochs_per_sample_kernel(const float* __restrict__ w, int64_t m, float max_w,
+                                         float n_epochs_f, float neg_rate_f,
+                                         float* __restrict__ eps, float* __restrict__ next,
+                                         float* __restrict__ next_neg) {
+    // make_epochs_per_sample (lib.rs:4937-4960)
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= m) return;
+    const float ns = __fmul_rn(n_epochs_f, __fdiv_rn(w[e], max_w));
+    const float v = ns > 0.0f ? __fdiv_rn(n_epochs_f, ns) : INFINITY;
+    eps[e] = v;
+    if (next) next[e] = v;
+    if (next_neg) next_neg[e] = __fdiv_rn(v, neg_rate_f);
+}
+
+struct SgdArgs {
+    float* emb;
+    const int32_t* heads;
+    const int32_t* tails;
+    const float* eps;
+    float* next;
+    float* next_neg;
+    int64_t n_edges;
+    uint32_t n_vertices;
+    int dim;
+    float epoch_f;
+    float alpha;
+    float a, b;
+    float att_factor;  // -2ab
+    float rep_factor;  // 2 * repulsion * b
+    float neg_rate_f;
+    uint64_t seed;
+    uint64_t epoch;
+    unsigned long long* samples;
+};
+
+// One epoch for dim == 2 (the reference's flat fast path, lib.rs:5172-5244).
+__global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool sampled = false;
+    if (e < p.n_edges) {
+        const float nxt = p.next[e];
+        if (!(nxt > p.epoch_f)) {
+            sampled = true;
+            const int32_t head = p.heads[e];
+            const int32_t tail = p.tails[e];
+            float2* emb = reinterpret_cast<float2*>(p.emb);
+            const float2 h0 = emb[head];
+            float hx = h0.x, hy = h0.y;
+            if (head != tail) {
+                const float2 t = emb[tail];
+                const float dx = __fsub_rn(hx, t.x), dy = __fsub_rn(hy, t.y);
+                const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+                if (d2 > 0.0f) {
+                    const float pb = powf(d2, p.b);
+                    const float gc = __fdiv_rn(__fmul_rn(p.att_factor, __fdiv_rn(pb, d2)),
+                                               __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
+                    const float gx = clip4(__fmul_rn(gc, dx)), gy = clip4(__fmul_rn(gc, dy));
+                    const float mx = __fmul_rn(gx, p.alpha), my = __fmul_rn(gy, p.alpha);
+                    hx = __fadd_rn(hx, mx);
+                    hy = __fadd_rn(hy, my);
+                    atomicAdd(&p.emb[2 * tail], -mx);
+                    atomicAdd(&p.emb[2 * tail + 1], -my);
+                }
+            }
+            const float eps = p.eps[e];
+            p.next[e] = __fadd_rn(nxt, eps);
+            const float en = __fdiv_rn(eps, p.neg_rate_f);
+            if (isfinite(en) && en > 0.0f) {
+                const float nn = p.next_neg[e];
+                const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(p.epoch_f, nn), en));
+                for (uint32_t s = 0; s < n_neg; ++s) {
+                    const uint64_t word = rng_word(p.seed, static_cast<uint64_t>(e),
+                                                   (p.epoch << 32) | s);
+                    const uint32_t neg = rng_below(word, p.n_vertices);
+                    if (neg == static_cast<uint32_t>(head)) continue;
+                    const float2 o = emb[neg];
+                    const float dx = __fsub_rn(hx, o.x), dy = __fsub_rn(hy, o.y);
+                    const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+                    if (d2 > 0.0f) {
+                        const float pb = powf(d2, p.b);
+                        const float gc =
+                            __fdiv_rn(p.rep_factor, __fmul_rn(__fadd_rn(0.001f, d2),
+                                                              __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
+                        if (gc > 0.0f) {
+                            hx = __fadd_rn(hx, __fmul_rn(clip4(__fmul_rn(gc, dx)), p.alpha));
+                            hy = __fadd_rn(hy, __fmul_rn(clip4(__fmul_rn(gc, dy)), p.alpha));
+                        }
+                    }
+                }
+                p.next_neg[e] = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), en));
+            }
+            if (hx != h0.x) atomicAdd(&p.emb[2 * head], __fsub_rn(hx, h0.x));
+            if (hy != h0.y) atomicAdd(&p.emb[2 * head + 1], __fsub_rn(hy, h0.y));
+        }
+    }
+    if (p.samples) {
+        const unsigned ballot = __ballot_sync(0xffffffffu, sampled);
+        if ((threadIdx.x & 31) == 0 && ballot)
+            atomicAdd(p.samples, static_cast<unsigned long long>(__popc(ballot)));
+    }
+}
+
+// One epoch for any dim (lib.rs:5248-5318).  The head moves in a per-thread
+// copy of at most kMaxDim coordinates.
+constexpr int kMaxDim = 16;
+
+__global__ void __launch_bounds__(256) sgd_epoch_nd(SgdArgs p) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool sampled = false;
+    if (e < p.n_edges) {
+        const float nxt = p.next[e];
+        if (!(nxt > p.epoch_f)) {
+            sampled = true;
+            const int dim = p.dim;
+            const int32_t head = p.heads[e];
+            const int32_t tail = p.tails[e];
+            float h0[kMaxDim], h[kMaxDim];
+            for (int c = 0; c < dim; ++c) h0[c] = h[c] = p.emb[static_cast<int64_t>(head) * dim + c];
+            if (head != tail) {
+                const float* t = p.emb + static_cast<int64_t>(tail) * dim;
+                float d2 = 0.0f;
+                for (int c = 0; c < dim; ++c) {
+                    const float df = __fsub_rn(h[c], t[c]);
+                    d2 = __fadd_rn(d2, __fmul_rn(df, df));
+                }
+                if (d2 > 0.0f) {
+                    const float pb = powf(d2, p.b);
+                    const float gc = __fdiv_rn(__fmul_rn(p.att_factor, __fdiv_rn(pb, d2)),
+                                               __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
+                    for (int c = 0; c < dim; ++c) {
+                        const float tv = t[c];
+                        const float g = clip4(__fmul_rn(gc, __fsub_rn(h[c], tv)));
+                        const float mv = __fmul_rn(g, p.alpha);
+                        h[c] = __fadd_rn(h[c], mv);
+                        atomicAdd(&p.emb[static_cast<int64_t>(tail) * dim + c], -mv);
+                    }
+                }
+            }
+            const float eps = p.eps[e];
+            p.next[e] = __fadd_rn(nxt, eps);
+            const float en = __fdiv_rn(eps, p.neg_rate_f);
+            if (isfinite(en) && en > 0.0f) {
+                const float nn = p.next_neg[e];
+                const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(p.epoch_f, nn), en));
+                for (uint32_t s = 0; s < n_neg; ++s) {
+                    const uint64_t word = rng_word(p.seed, static_cast<uint64_t>(e),
+                                                   (p.epoch << 32) | s);
+                    const uint32_t neg = rng_below(word, p.n_vertices);
+                    if (neg == static_cast<uint32_t>(head)) continue;
+                    const float* o = p.emb + static_cast<int64_t>(neg) * dim;
+                    float d2 = 0.0f;
+                    for (int c = 0; c < dim; ++c) {
+                        const float df = __fsub_rn(h[c], o[c]);
+                        d2 = __fadd_rn(d2, __fmul_rn(df, df));
+                    }
+                    if (d2 > 0.0f) {
+                        const float pb = powf(d2, p.b);
+                        const float gc =
+                            __fdiv_rn(p.rep_factor, __fmul_rn(__fadd_rn(0.001f, d2),
+                                                              __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
+                        if (gc > 0.0f)
+                            for (int c = 0; c < dim; ++c)
+                                h[c] = __fadd_rn(
+                                    h[c], __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(h[c], o[c]))),
+                                                    p.alpha));
+                    }
+                }
+                p.next_neg[e] = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), en));
+            }
+            for (int c = 0; c < dim; ++c)
+                if (h[c] != h0[c])
+                    atomicAdd(&p.emb[static_cast<int64_t>(head) * dim + c], __fsub_rn(h[c], h0[c]));
+        }
+    }
+    if (p.samples) {
+        const unsigned ballot = __ballot_sync(0xffffffffu, sampled);
+        if ((threadIdx.x & 31) == 0 && ballot)
+            atomicAdd(p.samples, static_cast<unsigned long long>(__popc(ballot)));
+    }
+}
+
+// ------------------------------------------------------------ transform --
+struct TransformArgs {
+    float* out;
+    const float* base;
+    const int32_t* row_ptr;
+    const int32_t* tails;
+    const float* weights;
+    const float* eps;
+    float* next;
+    float* next_neg;
+    int64_t nq;
+    uint32_t n_base;
+    int dim;
+    int64_t n_epochs;
+    float a, b, lr, rep, neg_rate_f;
+    uint64_t seed;
+};
+
+__device__ inline bool row_finite(const float* v, int dim) {
+    for (int c = 0; c < dim; ++c)
+        if (!isfinite(v[c])) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__(128) transform_kernel(TransformArgs p) {
+    const int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= p.nq) return;
+    const int dim = p.dim;
+    const int32_t st = p.row_ptr[q], en = p.row_ptr[q + 1];
+    float cur[kMaxDim];
+    // init_graph_transform (lib.rs:4793-4836)
+    if (st == en) {
+        for (int c = 0; c < dim; ++c) cur[c] = NAN;
+    } else {
+        int32_t copy_from = -1;
+        for (int32_t e = st; e < en; ++e)
+            if (fabsf(__fsub_rn(p.weights[e], 1.0f)) < FLT_EPSILON) {
+                copy_from = p.tails[e];
+                break;
+            }
+        if (copy_from >= 0) {
+            for (int c = 0; c < dim; ++c) cur[c] = p.base[static_cast<int64_t>(copy_from) * dim + c];
+        } else {
+            float sum = 0.0f;
+            for (int32_t e = st; e < en; ++e) sum = __fadd_rn(sum, p.weights[e]);
+            if (sum <= 0.0f) {
+                for (int c = 0; c < dim; ++c) cur[c] = NAN;
+            } else {
+                for (int c = 0; c < dim; ++c) cur[c] = 0.0f;
+                for (int32_t e = st; e < en; ++e) {
+                    const float w = __fdiv_rn(p.weights[e], sum);
+                    const float* bt = p.base + static_cast<int64_t>(p.tails[e]) * dim;
+                    for (int c = 0; c < dim; ++c) cur[c] = __fadd_rn(cur[c], __fmul_rn(w, bt[c]));
+                }
+            }
+        }
+    }
+    // optimize_layout_transform (lib.rs:5444-5544)
+    const uint64_t qseed = mix64(p.seed ^ mix64(static_cast<uint64_t>(q)));
+    for (int64_t epoch = 0; epoch < p.n_epochs && st < en; ++epoch) {
+        const float alpha = __fmul_rn(
+            p.lr, __fsub_rn(1.0f, __fdiv_rn(static_cast<float>(epoch),
+                                            static_cast<float>(p.n_epochs))));
+        const float ef = static_cast<float>(epoch);
+        for (int32_t e = st; e < en; ++e) {
+            if (p.next[e] > ef || !row_finite(cur, dim)) continue;
+            const float* other = p.base + static_cast<int64_t>(p.tails[e]) * dim;
+            float d2 = 0.0f;
+            for (int c = 0; c < dim; ++c) {
+                const float df = __fsub_rn(cur[c], other[c]);
+                d2 = __fadd_rn(d2, __fmul_rn(df, df));
+            }
+            float gc = 0.0f;
+            if (d2 > 0.0f) {
+                const float pb = powf(d2, p.b);
+                gc = __fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(-2.0f, p.a), p.b), powf(d2, p.b - 1.0f)),
+                               __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
+            }
+            for (int c = 0; c < dim; ++c)
+                cur[c] = __fadd_rn(cur[c], __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(cur[c], other[c]))),
+                                                     alpha));
+            p.next[e] = __fadd_rn(p.next[e], p.eps[e]);
+            const float eneg = __fdiv_rn(p.eps[e], p.neg_rate_f);
+            if (!isfinite(eneg) || eneg <= 0.0f) continue;
+            const float nn = p.next_neg[e];
+            const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(ef, nn), eneg));
+            for (uint32_t s = 0; s < n_neg; ++s) {
+                const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                                               (static_cast<uint64_t>(epoch) << 32) | s);
+                const uint32_t neg = rng_below(word, p.n_base);
+                const float* o = p.base + static_cast<int64_t>(neg) * dim;
+                float dd = 0.0f;
+                for (int c = 0; c < dim; ++c) {
+                    const float df = __fsub_rn(cur[c], o[c]);
+                    dd = __fadd_rn(dd, __fmul_rn(df, df));
+                }
+                float g2 = 0.0f;
+                if (dd > 0.0f) {
+                    const float pb = powf(dd, p.b);
+                    g2 = __fdiv_rn(__fmul_rn(__fmul_rn(2.0f, p.rep), p.b),
+                                   __fmul_rn(__fadd_rn(0.001f, dd), __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
+                }
+                if (g2 > 0.0f)
+                    for (int c = 0; c < dim; ++c)
+                        cur[c] = __fadd_rn(
+                            cur[c], __fmul_rn(clip4(__fmul_rn(g2, __fsub_rn(cur[c], o[c]))), alpha));
+            }
+            p.next_neg[e] = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), eneg));
+        }
+    }
+    for (int c = 0; c < dim; ++c) p.out[q * dim + c] = cur[c];
+}
+
+}  // namespace
+
+double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, int64_t n_epochs,
+                       float a, float b, float lr, int64_t neg_rate, float repulsion,
+                       uint64_t seed, bool count_samples, float* kernel_ms, cudaStream_t s) {
+    const int64_t m = g.n_edges;
+    if (m == 0 || n_vertices == 0 || n_epochs == 0) return 0.0;
+    if (dim > kMaxDim) invalid("n_components above 16 is not supported by the GPU layout kernel");
+    const float mx = std::max(max_weight(g.weights.get(), m, s), 1e-12f);
+    DevBuf<float> eps(m, s), next(m, s), next_neg(m, s);
+    const float nef = static_cast<float>(n_epochs);
+    const float nrf = static_cast<float>(neg_rate);
+    epochs_per_sample_kernel<<<static_cast<unsigned>(ceil_div(m, 256)), 256, 0, s>>>(
+        g.weights.get(), m, mx, nef, nrf, eps.get(), next.get(), next_neg.get());
+    UMAPB_LAUNCH_CHECK();
+    DevBuf<unsigned long long> samples(1, s);
+    UMAPB_CUDA(cudaMemsetAsync(samples.get(), 0, 8, s));
+    SgdArgs p{};
+    p.emb = emb;
+    p.heads = g.heads.get();
+    p.tails = g.tails.get();
+    p.eps = eps.get();
+    p.next = next.get();
+    p.next_neg = next_neg.get();
+    p.n_edges = m;
+    p.n_vertices = static_cast<uint32_t>(n_vertices);
+    p.dim = dim;
+    p.a = a;
+    p.b = b;
+    p.att_factor = -2.0f * a * b;
+    p.rep_factor = 2.0f * repulsion * b;
+    p.neg_rate_f = nrf;
+    p.seed = seed;
+    p.samples = count_samples ? samples.get() : nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (kernel_ms) {
+        UMAPB_CUDA(cudaEventCreate(&e0));
+        UMAPB_CUDA(cudaEventCreate(&e1));
+        UMAPB_CUDA(cudaEventRecord(e0, s));
+    }
+    const unsigned grid = static_cast<unsigned>(ceil_div(m, 256));
+    for (int64_t epoch = 0; epoch < n_epochs; ++epoch) {
+        // alpha = initial_alpha * (1 - epoch / n_epochs) in FP32 (lib.rs:5174)
+        p.alpha = lr * (1.0f - static_cast<float>(epoch) / nef);
+        p.epoch_f = static_cast<float>(epoch);
+        p.epoch = static_cast<uint64_t>(epoch);
+        if (dim == 2)
+            sgd_epoch_2d<<<grid, 256, 0, s>>>(p);
+        else
+            sgd_epoch_nd<<<grid, 256, 0, s>>>(p);
+        UMAPB_LAUNCH_CHECK();
+    }
+    if (kernel_ms) {
+        UMAPB_CUDA(cudaEventRecord(e1, s));
+        UMAPB_CUDA(cudaEventSynchronize(e1));
+        UMAPB_CUDA(cudaEventElapsedTime(kernel_ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (!count_samples) return 0.0;
+    unsigned long long h = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&h, samples.get(), 8, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    return static_cast<double>(h);
+}
+
+void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_t n_base,
+                      const Graph& g, int64_t n_epochs, float a, float b, float lr,
+                      int64_t neg_rate, float repulsion, uint64_t seed, cudaStream_t s) {
+    if (nq == 0) return;
+    if (dim > kMaxDim) invalid("n_components above 16 is not supported by the GPU layout kernel");
+    const int64_t m = g.n_edges;
+    DevBuf<float> eps(std::max<int64_t>(m, 1), s), next(std::max<int64_t>(m, 1), s),
+        next_neg(std::max<int64_t>(m, 1), s);
+    const float nef = static_cast<float>(n_epochs);
+    const float nrf = static_cast<float>(neg_rate);
+    if (m > 0) {
+        const float mx = std::max(max_weight(g.weights.get(), m, s), 1e-12f);
+        epochs_per_sample_kernel<<<static_cast<unsigned>(ceil_div(m, 256)), 256, 0, s>>>(
+            g.weights.get(), m, mx, nef, nrf, eps.get(), next.get(), next_neg.get());
+        UMAPB_LAUNCH_CHECK();
+    }
+    TransformArgs p{};
+    p.out = out;
+    p.base = base;
+    p.row_ptr = g.row_ptr.get();
+    p.tails = g.tails.get();
+    p.weights = g.weights.get();
+    p.eps = eps.get();
+    p.next = next.get();
+    p.next_neg = next_neg.get();
+    p.nq = nq;
+    p.n_base = static_cast<uint32_t>(n_base);
+    p.dim = dim;
+    p.n_epochs = n_epochs;
+    p.a = a;
+    p.b = b;
+    p.lr = lr;
+    p.rep = repulsion;
+    p.neg_rate_f = nrf;
+    p.seed = seed;
+    transform_kernel<<<static_cast<unsigned>(ceil_div(nq, 128)), 128, 0, s>>>(p);
+    UMAPB_LAUNCH_CHECK();
+}
+
+}  // namespace umapb

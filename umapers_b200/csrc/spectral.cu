@@ -1,0 +1,854 @@
+// spectral.cu - spectral initialisation (rust_umap/src/lib.rs:3841-4791).
+//
+// The reference runs, per connected component, block subspace iteration on
+// the shifted operator I + D^-1/2 W D^-1/2: 256 iterations, s = (dim+1)*6
+// columns, modified Gram-Schmidt applied twice in FP64, then a Rayleigh-Ritz
+// step (lib.rs:4227-4326).  Here all components of the graph that take the
+// iterative path run at once: the sparse product is one pull-style SpMM over
+// the CSR graph (components never share edges, so the operator is block
+// diagonal), the block is kept in FP32 (N x s, L2 resident at 1M rows), and
+// orthonormalisation is CholQR2 per component: the s x s Gram matrix is
+// reduced in FP64, factored in FP64 on the device, and its inverse factor is
+// applied in FP64.  CholQR and MGS produce the same orthonormal basis in exact
+// arithmetic (the unique QR factor with positive diagonal); the MGS failure
+// test (column norm^2 <= 1e-12 after projection, lib.rs:4188) is the
+// Cholesky pivot test.  The Ritz matrices are solved on the host.
+//
+// Small pieces follow the reference on the host: the dense Laplacian path
+// (lib.rs:4007-4069, 3917-3957) for components below 128 nodes or connected
+// inputs with <= 8 features and <= 2048 rows, random init for components
+// with fewer than 2*dim nodes, and the meta layout of component centroids
+// (lib.rs:4519-4554).  Random numbers (initial block, noise, random layouts)
+// come from counter-based streams, not the reference's SmallRng sequence.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace umapb {
+namespace {
+
+constexpr int kIters = 256;             // SPECTRAL_ITERATIVE_MAX_ITERS (lib.rs:31)
+constexpr int kOversampling = 6;        // lib.rs:32
+constexpr int64_t kComponentIterThreshold = 128;  // lib.rs:30
+constexpr int64_t kDenseFallbackMax = 4096;       // lib.rs:33
+constexpr double kOrthoEps = 1e-12;     // lib.rs:34
+constexpr float kInitMaxCoord = 10.0f;  // lib.rs:22
+constexpr float kInitNoise = 1e-4f;     // lib.rs:23
+constexpr int kMaxS = 32;               // s <= 32 -> n_components <= 4
+
+inline unsigned grid_for(int64_t n, int t = 256) {
+    return static_cast<unsigned>(ceil_div(std::max<int64_t>(n, 1), t));
+}
+
+// ---------------------------------------------------- components (device)
+__device__ inline int32_t find_root(const int32_t* parent, int32_t x) {
+    int32_t p = parent[x];
+    while (p != x) {
+        x = p;
+        p = parent[x];
+    }
+    return x;
+}
+
+__global__ void cc_init(int32_t* parent, int64_t n) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) parent[i] = static_cast<int32_t>(i);
+}
+
+__global__ void cc_hook(const int32_t* __restrict__ heads, const int32_t* __restrict__ tails,
+                        int64_t m, int32_t* parent, int* changed) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= m) return;
+    const int32_t u = heads[e], v = tails[e];
+    if (u >= v) return;  // each undirected pair once
+    const int32_t ru = find_root(parent, u), rv = find_root(parent, v);
+    if (ru == rv) return;
+    const int32_t hi = ru > rv ? ru : rv, lo = ru > rv ? rv : ru;
+    atomicMin(&parent[hi], lo);
+    *changed = 1;
+}
+
+__global__ void cc_compress(int32_t* parent, int64_t n) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) parent[i] = find_root(parent, static_cast<int32_t>(i));
+}
+
+__global__ void cc_is_root(const int32_t* parent, int64_t n, int32_t* flag) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = parent[i] == i ? 1 : 0;
+}
+
+__global__ void cc_label(const int32_t* parent, const int32_t* rank, int64_t n, int32_t* label) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) label[i] = rank[parent[i]];
+}
+
+__global__ void iota_kernel(int32_t* v, int64_t n) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = static_cast<int32_t>(i);
+}
+
+// --------------------------------------------------- subspace iteration --
+__global__ void degree_kernel(const int32_t* __restrict__ row_ptr, const float* __restrict__ w,
+                              int64_t n, double* __restrict__ deg, float* __restrict__ dinv) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int32_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e) s += static_cast<double>(w[e]);
+    deg[i] = s;
+    dinv[i] = s > 0.0 ? static_cast<float>(1.0 / sqrt(s)) : 0.0f;
+}
+
+__global__ void norm_weight_kernel(const int32_t* __restrict__ heads,
+                                   const int32_t* __restrict__ tails, const float* __restrict__ w,
+                                   const double* __restrict__ deg, int64_t m,
+                                   float* __restrict__ nw) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= m) return;
+    const double di = deg[heads[e]], dj = deg[tails[e]];
+    const double ii = di > 0.0 ? 1.0 / sqrt(di) : 0.0, ij = dj > 0.0 ? 1.0 / sqrt(dj) : 0.0;
+    nw[e] = static_cast<float>(static_cast<double>(w[e]) * ii * ij);
+}
+
+// Initial block: column 0 = sqrt(degree), the others U(-1, 1) (lib.rs:4254-4261).
+__global__ void init_block_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
+                                  const int32_t* __restrict__ slot_of_node,
+                                  const uint64_t* __restrict__ slot_seed,
+                                  const double* __restrict__ deg, int s, int sp,
+                                  float* __restrict__ X) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    const int32_t i = nodes[t];
+    const uint64_t seed = slot_seed[slot_of_node[t]] ^ 0x7A5B3D91CE42A117ULL;
+    float* row = X + static_cast<int64_t>(i) * sp;
+    row[0] = static_cast<float>(sqrt(deg[i]));
+    for (int c = 1; c < sp; ++c) {
+        float v = 0.0f;
+        if (c < s) v = static_cast<float>(-1.0 + 2.0 * rng_unit_f64(rng_word(seed, i, c)));
+        row[c] = v;
+    }
+}
+
+// Y = X + A_hat X over the rows of the iterative components.
+template <int SP>
+__global__ void __launch_bounds__(256)
+    spmm_kernel(const int32_t* __restrict__ nodes, int64_t cnt, const int32_t* __restrict__ row_ptr,
+                const int32_t* __restrict__ tails, const float* __restrict__ nw,
+                const float* __restrict__ X, float* __restrict__ Y) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    const int32_t i = nodes[t];
+    constexpr int V = SP / 4;
+    float4 acc[V];
+    const float4* xi = reinterpret_cast<const float4*>(X + static_cast<int64_t>(i) * SP);
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = xi[v];
+    const int32_t st = row_ptr[i], en = row_ptr[i + 1];
+    for (int32_t e = st; e < en; ++e) {
+        const float wv = nw[e];
+        const float4* xj = reinterpret_cast<const float4*>(X + static_cast<int64_t>(tails[e]) * SP);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const float4 q = __ldg(xj + v);
+            acc[v].x = fmaf(wv, q.x, acc[v].x);
+            acc[v].y = fmaf(wv, q.y, acc[v].y);
+            acc[v].z = fmaf(wv, q.z, acc[v].z);
+            acc[v].w = fmaf(wv, q.w, acc[v].w);
+        }
+    }
+    float4* yi = reinterpret_cast<float4*>(Y + static_cast<int64_t>(i) * SP);
+#pragma unroll
+    for (int v = 0; v < V; ++v) yi[v] = acc[v];
+}
+
+struct Chunk {
+    int32_t slot;
+    int32_t start;  // into the node list
+    int32_t end;
+};
+
+// Upper triangle of A^T B per component slot, FP64 accumulation.
+constexpr int kGramRows = 64;
+__global__ void __launch_bounds__(256)
+    gram_kernel(const Chunk* __restrict__ chunks, const int32_t* __restrict__ nodes,
+                const float* __restrict__ A, const float* __restrict__ B, int s, int sp,
+                double* __restrict__ G) {
+    const Chunk ch = chunks[blockIdx.x];
+    __shared__ float As[kGramRows][kMaxS];
+    __shared__ float Bs[kGramRows][kMaxS];
+    const int tid = threadIdx.x;
+    const int n_ent = s * (s + 1) / 2;  // <= 528 for s <= 32: at most 3 entries per thread
+    int ea[3], eb[3];
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < 3; ++q) {
+        int t = tid + q * static_cast<int>(blockDim.x), a = 0;
+        ea[q] = eb[q] = -1;
+        if (t >= n_ent) continue;
+        while (t >= s - a) {
+            t -= s - a;
+            ++a;
+        }
+        ea[q] = a;
+        eb[q] = a + t;
+    }
+    for (int r0 = ch.start; r0 < ch.end; r0 += kGramRows) {
+        const int rows = min(kGramRows, ch.end - r0);
+        __syncthreads();
+        for (int e = tid; e < rows * s; e += blockDim.x) {
+            const int r = e / s, c = e % s;
+            const int64_t node = nodes[r0 + r];
+            As[r][c] = A[node * sp + c];
+            Bs[r][c] = B[node * sp + c];
+        }
+        __syncthreads();
+        for (int q = 0; q < 3; ++q) {
+            if (ea[q] < 0) continue;
+            double v = 0.0;
+            for (int r = 0; r < rows; ++r)
+                v += static_cast<double>(As[r][ea[q]]) * static_cast<double>(Bs[r][eb[q]]);
+            acc[q] += v;
+        }
+    }
+    for (int q = 0; q < 3; ++q)
+        if (ea[q] >= 0)
+            atomicAdd(&G[static_cast<int64_t>(ch.slot) * s * s + ea[q] * s + eb[q]], acc[q]);
+}
+
+// Cholesky G = L L^T per slot and Rinv = L^-T (upper triangular).
+__global__ void chol_kernel(const double* __restrict__ G, int s, double* __restrict__ Rinv,
+                            int* __restrict__ fail) {
+    if (threadIdx.x != 0) return;
+    const int slot = blockIdx.x;
+    const double* g = G + static_cast<int64_t>(slot) * s * s;
+    double L[kMaxS][kMaxS];
+    for (int i = 0; i < s; ++i)
+        for (int j = 0; j < s; ++j) L[i][j] = 0.0;
+    bool ok = true;
+    for (int j = 0; j < s && ok; ++j) {
+        double d = g[j * s + j];  // upper triangle holds (a <= b)
+        for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+        if (!(d > kOrthoEps) || !isfinite(d)) {
+            ok = false;
+            break;
+        }
+        const double ljj = sqrt(d);
+        L[j][j] = ljj;
+        for (int i = j + 1; i < s; ++i) {
+            double v = g[j * s + i];
+            for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k];
+            L[i][j] = v / ljj;
+        }
+    }
+    double* R = Rinv + static_cast<int64_t>(slot) * s * s;
+    if (!ok) {
+        fail[slot] = 1;
+        for (int i = 0; i < s * s; ++i) R[i] = 0.0;
+        for (int i = 0; i < s; ++i) R[i * s + i] = 1.0;
+        return;
+    }
+    // Linv lower triangular; Rinv = Linv^T
+    double Li[kMaxS][kMaxS];
+    for (int i = 0; i < s; ++i)
+        for (int j = 0; j < s; ++j) Li[i][j] = 0.0;
+    for (int i = 0; i < s; ++i) {
+        Li[i][i] = 1.0 / L[i][i];
+        for (int j = 0; j < i; ++j) {
+            double v = 0.0;
+            for (int k = j; k < i; ++k) v += L[i][k] * Li[k][j];
+            Li[i][j] = -v / L[i][i];
+        }
+    }
+    for (int a = 0; a < s; ++a)
+        for (int c = 0; c < s; ++c) R[a * s + c] = Li[c][a];
+}
+
+// X = Y Rinv (row times upper-triangular), FP64 arithmetic.
+__global__ void apply_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
+                             const int32_t* __restrict__ slot_of_node,
+                             const double* __restrict__ Rinv, int s, int sp,
+                             const float* __restrict__ Y, float* __restrict__ X) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    const int64_t i = nodes[t];
+    const double* R = Rinv + static_cast<int64_t>(slot_of_node[t]) * s * s;
+    double y[kMaxS];
+    for (int a = 0; a < s; ++a) y[a] = static_cast<double>(Y[i * sp + a]);
+    for (int c = 0; c < s; ++c) {
+        double v = 0.0;
+        for (int a = 0; a <= c; ++a) v += y[a] * R[a * s + c];
+        X[i * sp + c] = static_cast<float>(v);
+    }
+}
+
+// coords = X V (V: s x dim per slot), FP64; and per-slot max |coord|.
+__global__ void project_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
+                               const int32_t* __restrict__ slot_of_node,
+                               const double* __restrict__ V, int s, int sp, int dim,
+                               const float* __restrict__ X, float* __restrict__ out,
+                               unsigned* __restrict__ max_abs_bits) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    const int64_t i = nodes[t];
+    const int slot = slot_of_node[t];
+    const double* v = V + static_cast<int64_t>(slot) * s * dim;
+    float mx = 0.0f;
+    for (int oc = 0; oc < dim; ++oc) {
+        double acc = 0.0;
+        for (int b = 0; b < s; ++b) acc += static_cast<double>(X[i * sp + b]) * v[b * dim + oc];
+        const float f = static_cast<float>(acc);
+        out[i * dim + oc] = f;
+        mx = fmaxf(mx, fabsf(f));
+    }
+    atomicMax(&max_abs_bits[slot], __float_as_uint(mx));
+}
+
+// coord = coord * expansion + N(0, noise) + anchor (noisy_scale_coords,
+// lib.rs:4766-4791, and the per-component placement of lib.rs:4713-4752).
+__global__ void finish_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
+                              const int32_t* __restrict__ slot_of_node,
+                              const float* __restrict__ expansion,
+                              const float* __restrict__ anchors, const uint64_t* __restrict__ nseed,
+                              int dim, float noise, float* __restrict__ out) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= cnt) return;
+    const int64_t i = nodes[t];
+    const int slot = slot_of_node[t];
+    for (int c = 0; c < dim; ++c) {
+        const uint64_t w1 = rng_word(nseed[slot], static_cast<uint64_t>(i), 2 * c);
+        const uint64_t w2 = rng_word(nseed[slot], static_cast<uint64_t>(i), 2 * c + 1);
+        double u1 = rng_unit_f64(w1);
+        if (u1 < 1e-300) u1 = 1e-300;
+        const double z = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * rng_unit_f64(w2));
+        const float v = out[i * dim + c] * expansion[slot] + static_cast<float>(noise * z);
+        out[i * dim + c] = v + anchors[slot * dim + c];
+    }
+}
+
+__global__ void random_init_kernel(int64_t n, int dim, uint64_t seed, float low, float high,
+                                   float* out) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n * dim) return;
+    const float u = rng_unit_f32(rng_word(seed, static_cast<uint64_t>(t / dim), t % dim));
+    out[t] = low + u * (high - low);
+}
+
+__global__ void scatter_rows_kernel(const int32_t* __restrict__ nodes, int64_t cnt, int dim,
+                                    const float* __restrict__ vals, float* __restrict__ out) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= cnt * dim) return;
+    out[static_cast<int64_t>(nodes[t / dim]) * dim + t % dim] = vals[t];
+}
+
+// centroid sums per component (FP64) over the component-sorted node list
+__global__ void centroid_kernel(const Chunk* __restrict__ chunks, const int32_t* __restrict__ nodes,
+                                const float* __restrict__ X, int d, double* __restrict__ cent) {
+    const Chunk ch = chunks[blockIdx.x];
+    for (int f = threadIdx.x; f < d; f += blockDim.x) {
+        double acc = 0.0;
+        for (int r = ch.start; r < ch.end; ++r)
+            acc += static_cast<double>(X[static_cast<int64_t>(nodes[r]) * d + f]);
+        atomicAdd(&cent[static_cast<int64_t>(ch.slot) * d + f], acc);
+    }
+}
+
+// ------------------------------------------------------------ host side --
+using HostCoords = std::vector<float>;  // row-major n x dim
+
+bool finite_all(const std::vector<float>& v) {
+    for (float x : v)
+        if (!std::isfinite(x)) return false;
+    return true;
+}
+
+// normalized_laplacian_from_edges + spectral_embedding_from_laplacian
+// (lib.rs:4007-4069, 3917-3957) for a small component given its local edges.
+bool dense_spectral(int64_t n, int dim, const std::vector<std::array<int64_t, 2>>& pairs,
+                    const std::vector<float>& w, HostCoords& out) {
+    if (n <= dim + 1 || pairs.empty()) return false;
+    std::vector<double> L(n * n, 0.0), deg(n, 0.0);
+    for (int64_t i = 0; i < n; ++i) L[i * n + i] = 1.0;
+    std::vector<std::pair<int64_t, int64_t>> und;
+    for (size_t e = 0; e < pairs.size(); ++e) {
+        const int64_t h = pairs[e][0], t = pairs[e][1];
+        if (h == t) continue;
+        const double wv = static_cast<double>(std::max(w[e], 0.0f));
+        if (wv <= 0.0) continue;
+        const int64_t i = std::min(h, t), j = std::max(h, t);
+        const double prev = L[i * n + j];
+        if (wv > prev) {
+            if (prev == 0.0) und.emplace_back(i, j);
+            const double delta = wv - prev;
+            L[i * n + j] = wv;
+            L[j * n + i] = wv;
+            deg[i] += delta;
+            deg[j] += delta;
+        }
+    }
+    bool any = false;
+    for (double v : deg) any |= v > 0.0;
+    if (!any) return false;
+    std::vector<double> inv(n);
+    for (int64_t i = 0; i < n; ++i) inv[i] = deg[i] > 0 ? 1.0 / std::sqrt(deg[i]) : 0.0;
+    for (auto [i, j] : und) {
+        const double v = L[i * n + j] * inv[i] * inv[j];
+        L[i * n + j] = -v;
+        L[j * n + i] = -v;
+    }
+    for (int64_t i = 0; i < n; ++i) L[i * n + i] = 1.0;
+    std::vector<double> ev, V;
+    symmetric_eigen(L, static_cast<int>(n), ev, V);
+    if (n <= dim + 1) return false;
+    out.assign(n * dim, 0.0f);
+    for (int c = 0; c < dim; ++c)
+        for (int64_t r = 0; r < n; ++r) out[r * dim + c] = static_cast<float>(V[r * n + c + 1]);
+    return finite_all(out);
+}
+
+void host_random(int64_t n, int dim, uint64_t seed, float low, float high, HostCoords& out) {
+    out.resize(n * dim);
+    for (int64_t t = 0; t < n * dim; ++t) {
+        const float u = rng_unit_f32(rng_word(seed, static_cast<uint64_t>(t / dim), t % dim));
+        out[t] = low + u * (high - low);
+    }
+}
+
+double host_normal(uint64_t seed, uint64_t a, uint64_t b) {
+    double u1 = rng_unit_f64(rng_word(seed, a, 2 * b));
+    if (u1 < 1e-300) u1 = 1e-300;
+    return std::sqrt(-2.0 * std::log(u1)) *
+           std::cos(6.283185307179586 * rng_unit_f64(rng_word(seed, a, 2 * b + 1)));
+}
+
+// meta_component_layout_from_centroids (lib.rs:4519-4554)
+bool meta_layout(const std::vector<double>& cents, int64_t m, int d, int dim, uint64_t seed,
+                 HostCoords& out) {
+    if (m == 0) return false;
+    if (m == 1) {
+        out.assign(dim, 0.0f);
+        return true;
+    }
+    if (m <= 2 * dim) {
+        const int64_t k = (m + 1) / 2;
+        out.assign(m * dim, 0.0f);
+        for (int64_t i = 0; i < m; ++i) out[i * dim + (i % k)] = i < k ? 1.0f : -1.0f;
+        return true;
+    }
+    std::vector<double> aff(m * m, 0.0), deg(m, 0.0);
+    for (int64_t i = 0; i < m; ++i) {
+        aff[i * m + i] = 1.0;
+        for (int64_t j = i + 1; j < m; ++j) {
+            double d2 = 0.0;
+            for (int f = 0; f < d; ++f) {
+                const double dd = cents[i * d + f] - cents[j * d + f];
+                d2 += dd * dd;
+            }
+            const double wv = std::exp(-d2);
+            aff[i * m + j] = wv;
+            aff[j * m + i] = wv;
+        }
+    }
+    for (int64_t i = 0; i < m; ++i)
+        for (int64_t j = 0; j < m; ++j) deg[i] += aff[i * m + j];
+    std::vector<double> inv(m), L(m * m, 0.0);
+    for (int64_t i = 0; i < m; ++i) inv[i] = deg[i] > 0 ? 1.0 / std::sqrt(deg[i]) : 0.0;
+    for (int64_t i = 0; i < m; ++i) L[i * m + i] = 1.0;
+    for (int64_t i = 0; i < m; ++i) {
+        if (deg[i] <= 0) continue;
+        for (int64_t j = 0; j < m; ++j) {
+            if (deg[j] <= 0) continue;
+            if (aff[i * m + j] > 0.0) L[i * m + j] -= aff[i * m + j] * inv[i] * inv[j];
+        }
+    }
+    std::vector<double> ev, V;
+    symmetric_eigen(L, static_cast<int>(m), ev, V);
+    if (m <= dim + 1) return false;
+    out.assign(m * dim, 0.0f);
+    for (int c = 0; c < dim; ++c)
+        for (int64_t r = 0; r < m; ++r) out[r * dim + c] = static_cast<float>(V[r * m + c + 1]);
+    // noisy_scale_coords(seed ^ 0xC85E7D6ADA318F21, 10, 1e-4)
+    float mx = 0.0f;
+    for (float v : out) mx = std::max(mx, std::fabs(v));
+    const float expansion = mx > 0.0f ? kInitMaxCoord / mx : 1.0f;
+    const uint64_t ns = seed ^ 0xC85E7D6ADA318F21ULL;
+    for (int64_t r = 0; r < m; ++r)
+        for (int c = 0; c < dim; ++c)
+            out[r * dim + c] = out[r * dim + c] * expansion +
+                               static_cast<float>(kInitNoise * host_normal(ns, r, c));
+    return finite_all(out);
+}
+
+}  // namespace
+
+void random_init(int64_t n, int dim, uint64_t seed, float low, float high, float* out,
+                 cudaStream_t s) {
+    if (n == 0) return;
+    random_init_kernel<<<grid_for(n * dim), 256, 0, s>>>(n, dim, seed, low, high, out);
+    UMAPB_LAUNCH_CHECK();
+}
+
+SpectralResult spectral_init(const float* X, int64_t n, int d, const Graph& g, int dim,
+                             uint64_t seed, float* out, cudaStream_t s) {
+    SpectralResult res;
+    const int64_t m = g.n_edges;
+    if (n <= dim + 1 || m == 0) return res;
+    const int sdim = std::max((dim + 1) * kOversampling, dim + 1);
+    if (sdim > kMaxS) invalid("spectral init supports n_components <= 4 on the GPU path");
+    const int sp = (sdim + 3) / 4 * 4;
+
+    // ---- connected components (union-find with atomicMin hooking)
+    DevBuf<int32_t> parent(n, s);
+    cc_init<<<grid_for(n), 256, 0, s>>>(parent.get(), n);
+    UMAPB_LAUNCH_CHECK();
+    DevBuf<int> changed(1, s);
+    for (int round = 0; round < 64; ++round) {
+        UMAPB_CUDA(cudaMemsetAsync(changed.get(), 0, 4, s));
+        cc_hook<<<grid_for(m), 256, 0, s>>>(g.heads.get(), g.tails.get(), m, parent.get(),
+                                            changed.get());
+        UMAPB_LAUNCH_CHECK();
+        cc_compress<<<grid_for(n), 256, 0, s>>>(parent.get(), n);
+        UMAPB_LAUNCH_CHECK();
+        int h = 0;
+        UMAPB_CUDA(cudaMemcpyAsync(&h, changed.get(), 4, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        if (!h) break;
+    }
+    DevBuf<int32_t> isroot(n, s), rank(n, s), label(n, s), order(n, s), lab_sorted(n, s),
+        iota(n, s);
+    cc_is_root<<<grid_for(n), 256, 0, s>>>(parent.get(), n, isroot.get());
+    UMAPB_LAUNCH_CHECK();
+    {
+        size_t tb = 0;
+        UMAPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, isroot.get(), rank.get(), n, s));
+        DevBuf<unsigned char> tmp(tb, s);
+        UMAPB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, isroot.get(), rank.get(), n, s));
+    }
+    int32_t last_rank = 0, last_root = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&last_rank, rank.get() + n - 1, 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(&last_root, isroot.get() + n - 1, 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    const int64_t n_comp = static_cast<int64_t>(last_rank) + last_root;
+    res.n_components = n_comp;
+    cc_label<<<grid_for(n), 256, 0, s>>>(parent.get(), rank.get(), n, label.get());
+    UMAPB_LAUNCH_CHECK();
+    iota_kernel<<<grid_for(n), 256, 0, s>>>(iota.get(), n);
+    UMAPB_LAUNCH_CHECK();
+    {
+        int bits = 1;
+        while ((int64_t(1) << bits) < n_comp + 1) ++bits;
+        size_t tb = 0;
+        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, label.get(), lab_sorted.get(),
+                                                   iota.get(), order.get(), n, 0, bits, s));
+        DevBuf<unsigned char> tmp(tb, s);
+        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, label.get(), lab_sorted.get(),
+                                                   iota.get(), order.get(), n, 0, bits, s));
+    }
+    // component sizes on the host from the sorted labels
+    std::vector<int32_t> lab_h(n), order_h;
+    UMAPB_CUDA(cudaMemcpyAsync(lab_h.data(), lab_sorted.get(), n * 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int64_t> cstart(n_comp + 1, 0);
+    for (int64_t i = 0; i < n; ++i) cstart[lab_h[i] + 1]++;
+    for (int64_t c = 0; c < n_comp; ++c) cstart[c + 1] += cstart[c];
+
+    // ---- decide the path of every component
+    enum Kind { kIter, kDense, kRandom };
+    std::vector<Kind> kind(n_comp);
+    std::vector<uint64_t> cseed(n_comp);
+    const bool multi = n_comp > 1;
+    for (int64_t c = 0; c < n_comp; ++c) {
+        const int64_t sz = cstart[c + 1] - cstart[c];
+        if (!multi) {
+            const int64_t thr = d <= 8 ? 2049 : 0;  // spectral_iterative_connected_threshold
+            kind[c] = (sz >= thr && sz > sdim) ? kIter : kDense;
+            cseed[c] = seed;
+        } else {
+            if (sz < 2 * dim || sz <= dim + 1)
+                kind[c] = kRandom;
+            else
+                kind[c] = (sz >= kComponentIterThreshold && sz > sdim) ? kIter : kDense;
+            cseed[c] = seed ^ (static_cast<uint64_t>(c + 1) * 0xBF58476D1CE4E5B9ULL);
+        }
+    }
+    if (!multi && kind[0] == kDense && n > kDenseFallbackMax && n >= (d <= 8 ? 2049 : 0))
+        return res;
+
+    // ---- meta layout (anchors) and per-component ranges
+    std::vector<float> anchors(n_comp * dim, 0.0f), data_range(n_comp, 1.0f);
+    if (multi) {
+        std::vector<double> cents;
+        if (n_comp > 2 * dim) {
+            std::vector<Chunk> chunks;
+            for (int64_t c = 0; c < n_comp; ++c)
+                for (int64_t st = cstart[c]; st < cstart[c + 1]; st += 4096)
+                    chunks.push_back({static_cast<int32_t>(c), static_cast<int32_t>(st),
+                                      static_cast<int32_t>(std::min(cstart[c + 1], st + 4096))});
+            DevBuf<Chunk> dch(chunks.size(), s);
+            DevBuf<double> dcent(n_comp * d, s);
+            UMAPB_CUDA(cudaMemcpyAsync(dch.get(), chunks.data(), chunks.size() * sizeof(Chunk),
+                                       cudaMemcpyHostToDevice, s));
+            UMAPB_CUDA(cudaMemsetAsync(dcent.get(), 0, n_comp * d * 8, s));
+            centroid_kernel<<<static_cast<unsigned>(chunks.size()), 128, 0, s>>>(
+                dch.get(), order.get(), X, d, dcent.get());
+            UMAPB_LAUNCH_CHECK();
+            cents.resize(n_comp * d);
+            UMAPB_CUDA(cudaMemcpyAsync(cents.data(), dcent.get(), n_comp * d * 8,
+                                       cudaMemcpyDeviceToHost, s));
+            UMAPB_CUDA(cudaStreamSynchronize(s));
+            for (int64_t c = 0; c < n_comp; ++c) {
+                const double sc = 1.0 / static_cast<double>(cstart[c + 1] - cstart[c]);
+                for (int f = 0; f < d; ++f) cents[c * d + f] *= sc;
+            }
+        }
+        HostCoords layout;
+        if (!meta_layout(cents, n_comp, d, dim, seed ^ 0xA13F52A92D4CB801ULL, layout)) return res;
+        anchors = layout;
+        for (int64_t c = 0; c < n_comp; ++c) {
+            float r = INFINITY;
+            for (int64_t o = 0; o < n_comp; ++o) {
+                if (o == c) continue;
+                float d2 = 0.0f;
+                for (int k = 0; k < dim; ++k) {
+                    const float df = anchors[c * dim + k] - anchors[o * dim + k];
+                    d2 += df * df;
+                }
+                const float dist = std::sqrt(d2);
+                if (dist > 0.0f) r = std::min(r, dist / 2.0f);
+            }
+            if (!std::isfinite(r) || r <= 0.0f) r = 1.0f;
+            data_range[c] = r;
+        }
+    }
+
+    // ---- host components (dense spectral / random)
+    bool need_host_graph = false;
+    for (int64_t c = 0; c < n_comp; ++c) need_host_graph |= kind[c] == kDense;
+    std::vector<int32_t> rp_h, tl_h;
+    std::vector<float> w_h;
+    if (need_host_graph) {
+        rp_h.resize(n + 1);
+        tl_h.resize(m);
+        w_h.resize(m);
+        order_h.resize(n);
+        UMAPB_CUDA(cudaMemcpyAsync(rp_h.data(), g.row_ptr.get(), (n + 1) * 4, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaMemcpyAsync(tl_h.data(), g.tails.get(), m * 4, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaMemcpyAsync(w_h.data(), g.weights.get(), m * 4, cudaMemcpyDeviceToHost, s));
+    }
+    if (order_h.empty()) order_h.resize(n);
+    UMAPB_CUDA(cudaMemcpyAsync(order_h.data(), order.get(), n * 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+
+    std::vector<int32_t> host_nodes;
+    std::vector<float> host_vals;
+    std::vector<int64_t> local_of(need_host_graph ? n : 0, -1);
+    for (int64_t c = 0; c < n_comp; ++c) {
+        if (kind[c] == kIter) continue;
+        const int64_t sz = cstart[c + 1] - cstart[c];
+        HostCoords local;
+        if (kind[c] == kRandom) {
+            host_random(sz, dim, seed ^ (static_cast<uint64_t>(c + 1) * 0x9E3779B9ULL),
+                        -data_range[c], data_range[c], local);
+        } else {
+            for (int64_t li = 0; li < sz; ++li) local_of[order_h[cstart[c] + li]] = li;
+            std::vector<std::array<int64_t, 2>> pairs;
+            std::vector<float> pw;
+            for (int64_t li = 0; li < sz; ++li) {
+                const int64_t node = order_h[cstart[c] + li];
+                for (int32_t e = rp_h[node]; e < rp_h[node + 1]; ++e) {
+                    pairs.push_back({li, local_of[tl_h[e]]});
+                    pw.push_back(w_h[e]);
+                }
+            }
+            if (!dense_spectral(sz, dim, pairs, pw, local)) return res;
+            float mx = 0.0f;
+            for (float v : local) mx = std::max(mx, std::fabs(v));
+            const float target = multi ? data_range[c] : kInitMaxCoord;
+            const float expansion = mx > 0.0f ? target / mx : 1.0f;
+            const uint64_t ns = multi ? seed ^ (static_cast<uint64_t>(c + 1) * 0x94D049BBULL)
+                                      : seed ^ 0x5DEECE66DULL;
+            for (int64_t li = 0; li < sz; ++li)
+                for (int k = 0; k < dim; ++k)
+                    local[li * dim + k] = local[li * dim + k] * expansion +
+                                          static_cast<float>(kInitNoise * host_normal(ns, li, k));
+        }
+        for (int64_t li = 0; li < sz; ++li) {
+            host_nodes.push_back(order_h[cstart[c] + li]);
+            for (int k = 0; k < dim; ++k)
+                host_vals.push_back(local[li * dim + k] + (multi ? anchors[c * dim + k] : 0.0f));
+        }
+    }
+    if (!host_nodes.empty()) {
+        const int64_t cnt = static_cast<int64_t>(host_nodes.size());
+        DevBuf<int32_t> hn(cnt, s);
+        DevBuf<float> hv(cnt * dim, s);
+        UMAPB_CUDA(cudaMemcpyAsync(hn.get(), host_nodes.data(), cnt * 4, cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(hv.get(), host_vals.data(), cnt * dim * 4, cudaMemcpyHostToDevice, s));
+        scatter_rows_kernel<<<grid_for(cnt * dim), 256, 0, s>>>(hn.get(), cnt, dim, hv.get(), out);
+        UMAPB_LAUNCH_CHECK();
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+    }
+
+    // ---- iterative components on the device
+    std::vector<int64_t> it_comps;
+    for (int64_t c = 0; c < n_comp; ++c)
+        if (kind[c] == kIter) it_comps.push_back(c);
+    if (!it_comps.empty()) {
+        const int64_t n_slots = static_cast<int64_t>(it_comps.size());
+        std::vector<int32_t> nodes_h, slot_h;
+        std::vector<Chunk> chunks;
+        std::vector<uint64_t> slot_seed(n_slots), noise_seed(n_slots);
+        std::vector<float> expand_target(n_slots), slot_anchor(n_slots * dim);
+        for (int64_t sl = 0; sl < n_slots; ++sl) {
+            const int64_t c = it_comps[sl];
+            const int32_t base = static_cast<int32_t>(nodes_h.size());
+            for (int64_t p = cstart[c]; p < cstart[c + 1]; ++p) {
+                nodes_h.push_back(order_h[p]);
+                slot_h.push_back(static_cast<int32_t>(sl));
+            }
+            const int32_t end = static_cast<int32_t>(nodes_h.size());
+            for (int32_t st = base; st < end; st += 2048)
+                chunks.push_back({static_cast<int32_t>(sl), st, std::min(end, st + 2048)});
+            slot_seed[sl] = cseed[c];
+            noise_seed[sl] = multi ? seed ^ (static_cast<uint64_t>(c + 1) * 0x94D049BBULL)
+                                   : seed ^ 0x5DEECE66DULL;
+            expand_target[sl] = multi ? data_range[c] : kInitMaxCoord;
+            for (int k = 0; k < dim; ++k)
+                slot_anchor[sl * dim + k] = multi ? anchors[c * dim + k] : 0.0f;
+        }
+        const int64_t cnt = static_cast<int64_t>(nodes_h.size());
+        DevBuf<int32_t> nodes(cnt, s), slots(cnt, s);
+        DevBuf<Chunk> dch(chunks.size(), s);
+        DevBuf<uint64_t> dseed(n_slots, s), dnseed(n_slots, s);
+        UMAPB_CUDA(cudaMemcpyAsync(nodes.get(), nodes_h.data(), cnt * 4, cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(slots.get(), slot_h.data(), cnt * 4, cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(dch.get(), chunks.data(), chunks.size() * sizeof(Chunk),
+                                   cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(dseed.get(), slot_seed.data(), n_slots * 8, cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(dnseed.get(), noise_seed.data(), n_slots * 8, cudaMemcpyHostToDevice, s));
+
+        DevBuf<double> deg(n, s);
+        DevBuf<float> dinv(n, s), nw(m, s);
+        degree_kernel<<<grid_for(n), 256, 0, s>>>(g.row_ptr.get(), g.weights.get(), n, deg.get(),
+                                                  dinv.get());
+        UMAPB_LAUNCH_CHECK();
+        norm_weight_kernel<<<grid_for(m), 256, 0, s>>>(g.heads.get(), g.tails.get(),
+                                                       g.weights.get(), deg.get(), m, nw.get());
+        UMAPB_LAUNCH_CHECK();
+        DevBuf<float> Xb(n * sp, s), Yb(n * sp, s);
+        UMAPB_CUDA(cudaMemsetAsync(Xb.get(), 0, n * sp * 4, s));
+        UMAPB_CUDA(cudaMemsetAsync(Yb.get(), 0, n * sp * 4, s));
+        DevBuf<double> G(n_slots * sdim * sdim, s), Rinv(n_slots * sdim * sdim, s);
+        DevBuf<int> fail(n_slots, s);
+        UMAPB_CUDA(cudaMemsetAsync(fail.get(), 0, n_slots * 4, s));
+        init_block_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(), dseed.get(),
+                                                        deg.get(), sdim, sp, Xb.get());
+        UMAPB_LAUNCH_CHECK();
+        const unsigned nch = static_cast<unsigned>(chunks.size());
+        auto cholqr = [&](float* src, float* dst) {
+            // two passes: src -> dst, dst -> src... ends with the result in dst
+            for (int pass = 0; pass < 2; ++pass) {
+                float* a = pass == 0 ? src : dst;
+                float* b = pass == 0 ? dst : src;
+                UMAPB_CUDA(cudaMemsetAsync(G.get(), 0, n_slots * sdim * sdim * 8, s));
+                gram_kernel<<<nch, 256, 0, s>>>(dch.get(), nodes.get(), a, a, sdim, sp, G.get());
+                UMAPB_LAUNCH_CHECK();
+                chol_kernel<<<static_cast<unsigned>(n_slots), 32, 0, s>>>(G.get(), sdim, Rinv.get(),
+                                                                          fail.get());
+                UMAPB_LAUNCH_CHECK();
+                apply_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(),
+                                                           Rinv.get(), sdim, sp, a, b);
+                UMAPB_LAUNCH_CHECK();
+            }
+            // result of pass 2 is in `src`; copy semantics handled by the caller
+        };
+        auto spmm = [&](const float* x, float* y) {
+            if (sp == 20)
+                spmm_kernel<20><<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(),
+                                                              g.tails.get(), nw.get(), x, y);
+            else if (sp == 12)
+                spmm_kernel<12><<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(),
+                                                              g.tails.get(), nw.get(), x, y);
+            else if (sp == 24)
+                spmm_kernel<24><<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(),
+                                                              g.tails.get(), nw.get(), x, y);
+            else if (sp == 32)
+                spmm_kernel<32><<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(),
+                                                              g.tails.get(), nw.get(), x, y);
+            else
+                invalid("unsupported spectral block width");
+            UMAPB_LAUNCH_CHECK();
+        };
+        // orthonormalize the initial block: X -> (Y) -> X
+        cholqr(Xb.get(), Yb.get());
+        for (int it = 0; it < kIters; ++it) {
+            spmm(Xb.get(), Yb.get());          // Y = (I + A) X
+            cholqr(Yb.get(), Xb.get());        // Y -> X -> Y; result in Y
+            std::swap(Xb, Yb);                 // X holds the orthonormal block
+        }
+        UMAPB_LAUNCH_CHECK();
+        spmm(Xb.get(), Yb.get());
+        UMAPB_CUDA(cudaMemsetAsync(G.get(), 0, n_slots * sdim * sdim * 8, s));
+        gram_kernel<<<nch, 256, 0, s>>>(dch.get(), nodes.get(), Xb.get(), Yb.get(), sdim, sp,
+                                        G.get());
+        UMAPB_LAUNCH_CHECK();
+        std::vector<double> G_h(n_slots * sdim * sdim);
+        std::vector<int> fail_h(n_slots);
+        UMAPB_CUDA(cudaMemcpyAsync(G_h.data(), G.get(), G_h.size() * 8, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaMemcpyAsync(fail_h.data(), fail.get(), n_slots * 4, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        for (int64_t sl = 0; sl < n_slots; ++sl)
+            if (fail_h[sl]) return res;  // reference: orthonormalize failure -> None
+        // Rayleigh-Ritz per slot: eigenvectors by descending eigenvalue, skip the first
+        std::vector<double> Vsel(n_slots * sdim * dim);
+        for (int64_t sl = 0; sl < n_slots; ++sl) {
+            std::vector<double> R(sdim * sdim);
+            const double* gs = G_h.data() + sl * sdim * sdim;
+            for (int i = 0; i < sdim; ++i)
+                for (int j = i; j < sdim; ++j) {
+                    R[i * sdim + j] = gs[i * sdim + j];
+                    R[j * sdim + i] = gs[i * sdim + j];
+                }
+            std::vector<double> ev, V;
+            symmetric_eigen(R, sdim, ev, V);
+            std::vector<int> ord(sdim);
+            std::iota(ord.begin(), ord.end(), 0);
+            std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return ev[a] > ev[b]; });
+            for (int oc = 0; oc < dim; ++oc)
+                for (int b = 0; b < sdim; ++b)
+                    Vsel[(sl * sdim + b) * dim + oc] = V[b * sdim + ord[oc + 1]];
+        }
+        DevBuf<double> dV(Vsel.size(), s);
+        DevBuf<unsigned> maxbits(n_slots, s);
+        UMAPB_CUDA(cudaMemcpyAsync(dV.get(), Vsel.data(), Vsel.size() * 8, cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemsetAsync(maxbits.get(), 0, n_slots * 4, s));
+        project_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(), dV.get(), sdim,
+                                                     sp, dim, Xb.get(), out, maxbits.get());
+        UMAPB_LAUNCH_CHECK();
+        std::vector<unsigned> mb(n_slots);
+        UMAPB_CUDA(cudaMemcpyAsync(mb.data(), maxbits.get(), n_slots * 4, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        std::vector<float> expansion(n_slots);
+        for (int64_t sl = 0; sl < n_slots; ++sl) {
+            float mx;
+            std::memcpy(&mx, &mb[sl], 4);
+            if (!std::isfinite(mx)) return res;
+            expansion[sl] = mx > 0.0f ? expand_target[sl] / mx : 1.0f;
+        }
+        DevBuf<float> dexp(n_slots, s), danch(n_slots * dim, s);
+        UMAPB_CUDA(cudaMemcpyAsync(dexp.get(), expansion.data(), n_slots * 4, cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(danch.get(), slot_anchor.data(), n_slots * dim * 4,
+                                   cudaMemcpyHostToDevice, s));
+        finish_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(), dexp.get(),
+                                                    danch.get(), dnseed.get(), dim, kInitNoise, out);
+        UMAPB_LAUNCH_CHECK();
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+    }
+    res.used_spectral = true;
+    return res;
+}
+
+}  // namespace umapb
