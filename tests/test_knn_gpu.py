@@ -54,3 +54,58 @@ def test_mixture_20000x192_sampled_rows_bit_exact(orc):
     oi, od = orc.exact_knn_rows(x, rows, 15)
     np.testing.assert_array_equal(gi[rows], oi)
     np.testing.assert_array_equal(gd[rows], od)
+
+
+@pytest.mark.parametrize("n,d,k", [(300, 32, 15), (2000, 64, 15), (1500, 100, 10), (3000, 16, 30),
+                                   (700, 8, 5), (2500, 130, 15)])
+def test_tensor_knn_matches_plain_and_oracle(orc, n, d, k):
+    x = workloads.isotropic_mixture(n, d, 6, 3.0, seed=n + 3 * d)
+    ti, td, fb = gu.knn_exact(x, k, backend="tensor")
+    oi, od = orc.exact_knn(x, k)
+    np.testing.assert_array_equal(ti, oi)
+    np.testing.assert_array_equal(td, od)
+    assert fb <= n // 20  # certification keeps almost every row on the tensor path
+
+
+def test_tensor_knn_duplicates_and_ties(orc):
+    x = workloads.gaussian(600, 64, seed=5)
+    x[100:140] = x[50]  # 41 identical rows: far more ties than the shortlist holds
+    ti, td, fb = gu.knn_exact(x, 15, backend="tensor")
+    oi, od = orc.exact_knn(x, 15)
+    np.testing.assert_array_equal(ti, oi)
+    np.testing.assert_array_equal(td, od)
+    assert fb >= 41  # rows whose ties exceed the shortlist go to the plain kernel
+
+
+def test_tensor_knn_query_to_reference(orc):
+    fit, q = workloads.transform_mixture(n_fit=5000, n_query=900, d=128, n_comp=10)
+    ti, td = gu.knn_query(q, fit, 15, backend="tensor")
+    oi, od = orc.knn_query(q, fit, 15)
+    np.testing.assert_array_equal(ti, oi)
+    np.testing.assert_array_equal(td, od)
+
+
+def test_tensor_knn_mixture_20000x192_sampled_rows(orc):
+    x = workloads.isotropic_mixture(20_000, 192, 10, 4.0, seed=7)
+    ti, td, fb = gu.knn_exact(x, 15, backend="tensor")
+    pi, pd, _ = gu.knn_exact(x, 15, backend="plain")
+    np.testing.assert_array_equal(ti, pi)
+    np.testing.assert_array_equal(td, pd)
+    rows = np.random.default_rng(1).choice(20_000, 200, replace=False)
+    oi, od = orc.exact_knn_rows(x, rows, 15)
+    np.testing.assert_array_equal(ti[rows], oi)
+    assert fb <= 1000
+
+
+def test_tensor_knn_1m_x_64_sampled_rows(orc):
+    x = workloads.anisotropic_mixture(1_000_000, 64, 50, seed=11)
+    ti, td, fb = gu.knn_exact(x, 15, backend="tensor")
+    rows = np.random.default_rng(11).choice(1_000_000, 64, replace=False)
+    oi, od = orc.exact_knn_rows(x, rows, 15)
+    np.testing.assert_array_equal(ti[rows], oi)
+    np.testing.assert_array_equal(td[rows], od)
+    # size-independent properties on every row: self first at 0, sorted rows
+    assert np.all(ti[:, 0] == np.arange(1_000_000)) and np.all(td[:, 0] == 0.0)
+    assert np.all(np.diff(td, axis=1) >= 0)
+    print("fallback rows", fb)
+    assert fb <= 10_000

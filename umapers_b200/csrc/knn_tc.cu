@@ -1,20 +1,723 @@
-// knn_tc.cu - tensor-core exact kNN (tcgen05).  Placeholder until the
-// tcgen05 kernel lands: reports the path as unsupported so AUTO selects the
-// plain FP32 kernel.
+// knn_tc.cu - exact kNN through tcgen05 tensor-core distance tiles.
+//
+// Replaces exact_nearest_neighbors{,_to_reference} (rust_umap/src/lib.rs:
+// 2863-2928, 3346-3399) for euclidean rows with the same result as the
+// reference, bit for bit, in three steps:
+//
+// 1. prep: every row x becomes two BF16 operand rows of K' (a multiple of 64)
+//    columns.  With h = bf16(x), l = bf16(x - h), n = |x|^2 (FP32):
+//        A = [-2h | -2h | -2l | split3((1-c2) n) | 1 1 1 | bf16(-c1 sqrt n) | 0...]
+//        B = [  h |   l |   h | 1 1 1 | split3((1-c2) n) | bf16(sqrt n)     | 0...]
+//    so one GEMM gives L_ij = n_i + n_j - 2 x_i.x_j - e_ij, a certified lower
+//    bound of the reference's FP32 squared distance d_ij, where
+//    e_ij = c1 sqrt(n_i n_j) + c2 (n_i + n_j) bounds the BF16 split error
+//    (3.02 * 2^-16 per product, doubled), the FP32 accumulation of K' terms,
+//    and the reference's own FP32 rounding (see kBoundC1/kBoundC2 below).
+// 2. tc_knn_kernel: a persistent, warp-specialised tcgen05 kernel.  A CTA
+//    keeps MT query tiles of 128 rows of A resident in shared memory, streams
+//    128-row candidate tiles of B through a TMA ring (SWIZZLE_128B, no
+//    multicast), and one thread issues tcgen05.mma (kind::f16, BF16 in, FP32
+//    accumulate) into double-buffered TMEM accumulators.  Epilogue warps read
+//    their rows with tcgen05.ld and keep, per row, the S = 32 smallest
+//    (L, index) keys in a global list; a warp inserts cooperatively (one list
+//    entry per lane), and a per-row threshold skips a 32-column chunk with a
+//    single vote in the common case.
+// 3. rerank: one warp per row recomputes the S candidates' exact FP32
+//    distances in the reference's summation order, sorts (distance, index),
+//    and certifies the row: with U_j = L_j + 2 e_j, the shortlist provably
+//    holds every true neighbour when max_j L_j > (k-th smallest U).  Rows that
+//    fail (near-ties wider than the bound) are recomputed by knn_plain.
+//
+// Every wait on an mbarrier is bounded by a %globaltimer deadline; a timeout
+// sets an error word, stops all roles, drains in-flight copies and frees TMEM.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace umapb {
+namespace {
 
-bool knn_tc_supported(int d, int k, int metric) {
-    (void)d;
-    (void)k;
-    (void)metric;
-    return false;
+constexpr int BM = 128;     // query rows per tile (UMMA M)
+constexpr int BN = 128;     // candidate rows per tile (UMMA N)
+constexpr int BK = 64;      // bf16 columns per k-block (one 128-byte swizzle row)
+constexpr int UK = 16;      // K of one tcgen05.mma kind::f16
+constexpr int S = 32;       // shortlist length per row
+constexpr int kTileBytes = BM * BK * 2;  // 16 KiB
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
+
+// Bound constants (see header comment).  c1 covers the split products
+// (2 * 3.02 * 2^-16) with 2% slack for the BF16 rounding of the bound term;
+// c2 = (K' + D + 8) * 2^-22 covers the FP32 accumulation of the GEMM and the
+// FP32 rounding of the norms and of the reference distance.
+constexpr double kBoundC1 = 1.02 * 2.0 * 3.02 / 65536.0;
+
+inline int padded_k(int d) { return ((3 * d + 7 + BK - 1) / BK) * BK; }
+inline double bound_c2(int d) { return (padded_k(d) + d + 8) * std::ldexp(1.0, -22); }
+
+// ---------------------------------------------------------------- PTX ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-void knn_tc(const float*, int64_t, const float*, int64_t, int, int, int, int32_t*, float*,
-            TcKnnStats*, cudaStream_t) {
-    invalid("the tensor-core kNN path is not available in this build");
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred P1;\n mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n"
+        " selp.b32 %0, 1, 0, P1;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after kWaitNs or when another role aborted.  The
+// deadline clock is read only every 1024 polls so the fast path is a bare
+// try_wait loop.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    uint64_t t0 = 0;
+    for (uint32_t i = 1;; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 1023u) == 0u) {
+            if (*abort_flag) return false;
+            const uint64_t now = global_ns();
+            if (t0 == 0) {
+                t0 = now;
+            } else if (now - t0 > kWaitNs) {
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// K-major SWIZZLE_128B operand descriptor: LBO = 16 B, SBO = 1024 B (8 rows of
+// 128 B), descriptor version 1, layout type 2.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+    uint64_t d = static_cast<uint64_t>((saddr & 0x3FFFF) >> 4);
+    d |= static_cast<uint64_t>(1) << 16;
+    d |= static_cast<uint64_t>(1024 >> 4) << 32;
+    d |= static_cast<uint64_t>(1) << 46;
+    d |= static_cast<uint64_t>(2) << 61;
+    return d;
+}
+
+// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
+// K-major, N = BN, M = BM.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                            (static_cast<uint32_t>(BN >> 3) << 17) |
+                            (static_cast<uint32_t>(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+#define UMAPB_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), \
+                    "=r"(r[i + 4]), "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
+
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+        "%28, %29, %30, %31}, [%32];"
+        : UMAPB_R8(0), UMAPB_R8(8), UMAPB_R8(16), UMAPB_R8(24)
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// order-preserving map of a float to uint32 (negative values included)
+__device__ __forceinline__ uint32_t f2o(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float o2f(uint32_t o) {
+    return (o & 0x80000000u) ? __uint_as_float(o & 0x7FFFFFFFu) : __uint_as_float(~o);
+}
+
+struct TcArgs {
+    int64_t n_q;
+    int64_t n_r;
+    int kb;          // k-blocks of 64 columns
+    int64_t n_units;   // groups of MT query tiles
+    int64_t n_ctiles;  // candidate tiles
+    uint64_t* lists;   // n_q x S keys (L order-mapped << 32 | index)
+    int* err;
+};
+
+template <int MT, int ST>
+__global__ void __launch_bounds__(64 + 128 * MT, 1)
+    tc_knn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                  TcArgs p) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    const int KB = p.kb;
+    const uint32_t sA = smem_u32(smem);
+    const uint32_t sB = sA + MT * KB * kTileBytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + MT * KB * kTileBytes + ST * kTileBytes);
+    const uint32_t b_full = smem_u32(bars);
+    const uint32_t b_empty = b_full + 8 * ST;
+    const uint32_t b_tfull = b_empty + 8 * ST;
+    const uint32_t b_tempty = b_tfull + 16;
+    const uint32_t b_afull = b_tempty + 16;
+    const uint32_t b_aempty = b_afull + 8;
+    const uint32_t b_final = b_aempty + 8;
+    uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(bars + 2 * ST + 7);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr uint32_t kTmemCols = MT == 2 ? 512 : 256;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < ST; ++s) {
+            mbar_init(b_full + 8 * s, 1);
+            mbar_init(b_empty + 8 * s, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(b_tfull + 8 * b, 1);
+            mbar_init(b_tempty + 8 * b, 4 * MT);
+        }
+        mbar_init(b_afull, 1);
+        mbar_init(b_aempty, 1);
+        mbar_init(b_final, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_holder)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_holder;
+
+    auto fail = [&](int code) {
+        *abort_flag = 1;
+        atomicCAS(p.err, 0, code);
+    };
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            uint64_t it = 0;
+            int64_t u_iter = 0;
+            for (int64_t unit = blockIdx.x; unit < p.n_units && !*abort_flag;
+                 unit += gridDim.x, ++u_iter) {
+                if (u_iter > 0 && !mbar_wait(b_aempty, static_cast<uint32_t>((u_iter - 1) & 1),
+                                             abort_flag)) {
+                    fail(1);
+                    break;
+                }
+                mbar_expect_tx(b_afull, MT * KB * kTileBytes);
+                for (int mt = 0; mt < MT; ++mt)
+                    for (int kb = 0; kb < KB; ++kb)
+                        tma_load_2d(sA + (mt * KB + kb) * kTileBytes, &tmA, b_afull, kb * BK,
+                                    static_cast<int>((unit * MT + mt) * BM));
+                bool ok = true;
+                for (int64_t c = 0; c < p.n_ctiles && ok; ++c) {
+                    for (int kb = 0; kb < KB; ++kb, ++it) {
+                        const int stage = static_cast<int>(it % ST);
+                        const uint32_t round = static_cast<uint32_t>(it / ST);
+                        if (!mbar_wait(b_empty + 8 * stage, (round & 1) ^ 1, abort_flag)) {
+                            fail(2);
+                            ok = false;
+                            break;
+                        }
+                        mbar_expect_tx(b_full + 8 * stage, kTileBytes);
+                        tma_load_2d(sB + stage * kTileBytes, &tmB, b_full + 8 * stage, kb * BK,
+                                    static_cast<int>(c * BN));
+                    }
+                }
+                if (!ok) break;
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            uint64_t it = 0, cg = 0;
+            int64_t u_iter = 0;
+            bool ok = true;
+            for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x, ++u_iter) {
+                if (!mbar_wait(b_afull, static_cast<uint32_t>(u_iter & 1), abort_flag)) {
+                    fail(3);
+                    break;
+                }
+                tc_fence_after();
+                for (int64_t c = 0; c < p.n_ctiles && ok; ++c, ++cg) {
+                    const uint32_t buf = static_cast<uint32_t>(cg & 1);
+                    if (!mbar_wait(b_tempty + 8 * buf, static_cast<uint32_t>(((cg >> 1) & 1) ^ 1),
+                                   abort_flag)) {
+                        fail(4);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t dcol = tmem_base + buf * (MT * BN);
+                    for (int kb = 0; kb < KB; ++kb, ++it) {
+                        const int stage = static_cast<int>(it % ST);
+                        if (!mbar_wait(b_full + 8 * stage, static_cast<uint32_t>((it / ST) & 1),
+                                       abort_flag)) {
+                            fail(5);
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint64_t db0 = desc_sw128(sB + stage * kTileBytes);
+#pragma unroll
+                        for (int ks = 0; ks < BK / UK; ++ks) {
+#pragma unroll
+                            for (int mt = 0; mt < MT; ++mt) {
+                                const uint64_t da =
+                                    desc_sw128(sA + (mt * KB + kb) * kTileBytes) + 2 * ks;
+                                umma_f16(dcol + mt * BN, da, db0 + 2 * ks,
+                                         (kb | ks) != 0 ? 1u : 0u);
+                            }
+                        }
+                        umma_commit(b_empty + 8 * stage);
+                    }
+                    if (ok) umma_commit(b_tfull + 8 * buf);
+                }
+                if (ok) umma_commit(b_aempty);
+            }
+            // every MMA issued by this thread has completed before TMEM is freed
+            umma_commit(b_final);
+            mbar_wait(b_final, 0, abort_flag);
+        }
+    } else {
+        // --------------------------------------------------- epilogue
+        const int ew = warp - 2;
+        const int mt = ew >> 2;
+        const int quarter = warp & 3;
+        // per-warp staging of one lane's qualifying candidates (value, column)
+        float* stage_v = reinterpret_cast<float*>(tmem_holder + 2) + ew * 80;
+        int32_t* stage_i = reinterpret_cast<int32_t*>(stage_v + 32);
+        uint64_t cg = 0;
+        bool ok = true;
+        for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x) {
+            const int64_t row = (unit * MT + mt) * BM + quarter * 32 + lane;
+            const bool row_ok = row < p.n_q;
+            float tau = INFINITY;
+            for (int64_t c = 0; c < p.n_ctiles; ++c, ++cg) {
+                const uint32_t buf = static_cast<uint32_t>(cg & 1);
+                if (!mbar_wait(b_tfull + 8 * buf, static_cast<uint32_t>((cg >> 1) & 1), abort_flag)) {
+                    fail(6);
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
+                                       buf * (MT * BN) + mt * BN;
+#pragma unroll 1
+                for (int ch = 0; ch < 4; ++ch) {
+                    uint32_t r[32];
+                    tmem_ld32(taddr + ch * 32, r);
+                    tmem_wait_ld();
+                    if (ch == 3) {
+                        // the accumulator buffer can be overwritten once all 4 chunks are read
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
+                    }
+                    float m = __uint_as_float(r[0]);
+#pragma unroll
+                    for (int j = 1; j < 32; ++j) m = fminf(m, __uint_as_float(r[j]));
+                    unsigned pend = __ballot_sync(0xffffffffu, row_ok && m < tau);
+                    if (pend == 0) continue;
+                    const int64_t col0 = c * BN + ch * 32;
+                    const int64_t valid_cols = p.n_r - col0;
+                    while (pend) {
+                        const int src = __ffs(pend) - 1;
+                        pend &= pend - 1;
+                        if (lane == src) {
+                            int n = 0;
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const float v = __uint_as_float(r[j]);
+                                if (v < tau && j < valid_cols) {
+                                    stage_v[n] = v;
+                                    stage_i[n] = j;
+                                    ++n;
+                                }
+                            }
+                            stage_i[32 + 0] = n;  // count slot after the index list
+                        }
+                        __syncwarp();
+                        const int n = stage_i[32];
+                        const int64_t srow = __shfl_sync(0xffffffffu, row, src);
+                        float stau = __shfl_sync(0xffffffffu, tau, src);
+                        uint64_t* lst = p.lists + srow * S;
+                        uint64_t lk = lst[lane];
+#pragma unroll 1
+                        for (int t = 0; t < n; ++t) {
+                            const float val = stage_v[t];
+                            if (!(val < stau)) continue;
+                            const uint64_t key = (static_cast<uint64_t>(f2o(val)) << 32) |
+                                                 static_cast<uint32_t>(col0 + stage_i[t]);
+                            const int pos = __popc(__ballot_sync(0xffffffffu, lk < key));
+                            const uint64_t up = __shfl_up_sync(0xffffffffu, lk, 1);
+                            if (lane > pos)
+                                lk = up;
+                            else if (lane == pos)
+                                lk = key;
+                            const uint64_t last = __shfl_sync(0xffffffffu, lk, S - 1);
+                            stau = last == ~0ull ? INFINITY : o2f(static_cast<uint32_t>(last >> 32));
+                        }
+                        lst[lane] = lk;
+                        if (lane == src) tau = stau;
+                        __syncwarp();
+                    }
+                }
+            }
+        }
+    }
+
+    __syncthreads();
+    if (*abort_flag) {
+        // let copies already in flight land before the CTA's shared memory goes away
+        const uint64_t t0 = global_ns();
+        while (global_ns() - t0 < 2000000ull) {
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+// ------------------------------------------------------------ operands --
+__global__ void prep_kernel(const float* __restrict__ X, const float* __restrict__ sq, int64_t n,
+                            int d, int kp, float c1, float c2, bool is_query,
+                            __nv_bfloat16* __restrict__ out) {
+    const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* x = X + row * d;
+    __nv_bfloat16* o = out + row * kp;
+    for (int c = lane; c < d; c += 32) {
+        const float v = x[c];
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+        if (is_query) {
+            const __nv_bfloat16 h2 = __float2bfloat16_rn(-2.0f * __bfloat162float(h));
+            o[c] = h2;
+            o[d + c] = h2;
+            o[2 * d + c] = __float2bfloat16_rn(-2.0f * __bfloat162float(l));
+        } else {
+            o[c] = h;
+            o[d + c] = l;
+            o[2 * d + c] = h;
+        }
+    }
+    for (int c = 3 * d + 7 + lane; c < kp; c += 32) o[c] = __float2bfloat16_rn(0.0f);
+    if (lane == 0) {
+        const float n2 = sq[row];
+        const float v = (1.0f - c2) * n2;
+        const __nv_bfloat16 s1 = __float2bfloat16_rn(v);
+        const float r1 = v - __bfloat162float(s1);
+        const __nv_bfloat16 s2 = __float2bfloat16_rn(r1);
+        const __nv_bfloat16 s3 = __float2bfloat16_rn(r1 - __bfloat162float(s2));
+        const __nv_bfloat16 one = __float2bfloat16_rn(1.0f);
+        const float rn = sqrtf(n2);
+        __nv_bfloat16* a = o + 3 * d;
+        if (is_query) {
+            a[0] = s1; a[1] = s2; a[2] = s3;
+            a[3] = one; a[4] = one; a[5] = one;
+            a[6] = __float2bfloat16_rn(-c1 * rn);
+        } else {
+            a[0] = one; a[1] = one; a[2] = one;
+            a[3] = s1; a[4] = s2; a[5] = s3;
+            a[6] = __float2bfloat16_rn(rn);
+        }
+    }
+}
+
+// ------------------------------------------------------------ re-rank ---
+__device__ __forceinline__ float sqdist_ref(const float* __restrict__ x, const float* __restrict__ y,
+                                            int d) {
+    if (d >= 64) {
+        float lane[8];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) lane[l] = 0.0f;
+        int i = 0;
+        for (; i + 8 <= d; i += 8)
+#pragma unroll
+            for (int l = 0; l < 8; ++l) {
+                const float df = __fsub_rn(x[i + l], y[i + l]);
+                lane[l] = __fadd_rn(lane[l], __fmul_rn(df, df));
+            }
+        float s = lane[0];
+#pragma unroll
+        for (int l = 1; l < 8; ++l) s = __fadd_rn(s, lane[l]);
+        for (; i < d; ++i) {
+            const float df = __fsub_rn(x[i], y[i]);
+            s = __fadd_rn(s, __fmul_rn(df, df));
+        }
+        return s;
+    }
+    float s = 0.0f;
+    for (int i = 0; i < d; ++i) {
+        const float df = __fsub_rn(x[i], y[i]);
+        s = __fadd_rn(s, __fmul_rn(df, df));
+    }
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sort_asc(T v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const T o = __shfl_xor_sync(0xffffffffu, v, stride);
+            const bool up = (lane & size) == 0;
+            const bool lower = (lane & stride) == 0;
+            v = (lower == up) ? (v < o ? v : o) : (v < o ? o : v);
+        }
+    }
+    return v;
+}
+
+__global__ void rerank_kernel(const float* __restrict__ Q, const float* __restrict__ R,
+                              const float* __restrict__ qsq, const float* __restrict__ rsq,
+                              const uint64_t* __restrict__ lists, int64_t n_q, int64_t n_r, int d,
+                              int k, double c1, double c2, int32_t* __restrict__ out_idx,
+                              float* __restrict__ out_dist, int* __restrict__ fb_count,
+                              int32_t* __restrict__ fb_rows) {
+    const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n_q) return;
+    const uint64_t lk = lists[row * S + lane];
+    const bool valid = lk != ~0ull;
+    const uint32_t j = static_cast<uint32_t>(lk);
+    double U = INFINITY;
+    float L = -INFINITY;
+    uint64_t key = ~0ull;
+    if (valid) {
+        L = o2f(static_cast<uint32_t>(lk >> 32));
+        const double nq = qsq[row], nc = rsq[j];
+        U = static_cast<double>(L) + 2.0 * (c1 * sqrt(nq * nc) + c2 * (nq + nc));
+        const float d2 = sqdist_ref(Q + row * d, R + static_cast<int64_t>(j) * d, d);
+        key = knn_key(d2, j);
+    }
+    const int n_valid = __popc(__ballot_sync(0xffffffffu, valid));
+    const double u_sorted = warp_sort_asc<double>(U);
+    const double u_k = __shfl_sync(0xffffffffu, u_sorted, k - 1);
+    float lmax = L;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    // all candidates were kept (n_r <= S) or the cut provably separates them
+    const bool certified = (n_valid < S && n_valid >= n_r) ||
+                           (n_valid == S && static_cast<double>(lmax) > u_k);
+    const uint64_t sorted = warp_sort_asc<uint64_t>(key);
+    if (lane < k) {
+        out_idx[row * k + lane] = static_cast<int32_t>(key_index(sorted));
+        out_dist[row * k + lane] = __fsqrt_rn(key_dist(sorted));
+    }
+    if (!certified && lane == 0) fb_rows[atomicAdd(fb_count, 1)] = static_cast<int32_t>(row);
+}
+
+// --------------------------------------------------------------- host ----
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encoder() {
+    static EncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeFn>(p);
+    });
+    if (!fn) throw Error(UMAPB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    return fn;
+}
+
+CUtensorMap make_map(const void* base, int64_t rows, int kp) {
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(kp), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(kp) * 2};
+    const cuuint32_t box[2] = {BK, BM};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base),
+                                 dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(UMAPB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+int query_tiles_for(int kb) { return kb <= 4 ? 2 : (kb <= 10 ? 1 : 0); }
+
+template <int MT, int ST>
+void launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, cudaStream_t s) {
+    // tiles + 1 KiB alignment slack + barriers/flags (256 B) + epilogue staging
+    const size_t smem = static_cast<size_t>(MT * a.kb + ST) * kTileBytes + 1024 + 256 +
+                        4 * MT * 80 * 4;
+    auto kern = tc_knn_kernel<MT, ST>;
+    UMAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+    int dev = 0, sms = 0;
+    UMAPB_CUDA(cudaGetDevice(&dev));
+    UMAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t grid = std::min<int64_t>(a.n_units, sms);
+    kern<<<static_cast<unsigned>(grid), 64 + 128 * MT, smem, s>>>(ma, mb, a);
+    UMAPB_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+bool knn_tc_supported(int d, int k, int metric) {
+    if (metric != UMAPB_METRIC_EUCLIDEAN) return false;
+    if (k < 1 || k > S - 2 || d < 1) return false;
+    if (query_tiles_for(padded_k(d) / BK) == 0) return false;
+    int dev = 0, major = 0, minor = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    return major == 10 && minor == 0;
+}
+
+void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int k, int metric,
+            int32_t* out_idx, float* out_dist, TcKnnStats* stats, cudaStream_t s) {
+    if (!knn_tc_supported(d, k, metric))
+        invalid("the tensor-core kNN path does not support this metric/shape on this device");
+    if (n_q == 0) return;
+    if (k > n_r) invalid("kNN needs k <= number of reference rows");
+    const bool self = Q == R && n_q == n_r;
+    const int kp = padded_k(d);
+    const int kb = kp / BK;
+    const double c1 = kBoundC1;
+    const double c2 = bound_c2(d);
+    DevBuf<float> qsq(n_q, s), rsq;
+    row_norms(Q, n_q, d, nullptr, qsq.get(), s);
+    if (!self) {
+        rsq.alloc(n_r, s);
+        row_norms(R, n_r, d, nullptr, rsq.get(), s);
+    }
+    const float* rsq_p = self ? qsq.get() : rsq.get();
+    DevBuf<__nv_bfloat16> A(n_q * kp, s), B(n_r * kp, s);
+    prep_kernel<<<static_cast<unsigned>(ceil_div(n_q * 32, 256)), 256, 0, s>>>(
+        Q, qsq.get(), n_q, d, kp, static_cast<float>(c1), static_cast<float>(c2), true, A.get());
+    UMAPB_LAUNCH_CHECK();
+    prep_kernel<<<static_cast<unsigned>(ceil_div(n_r * 32, 256)), 256, 0, s>>>(
+        R, rsq_p, n_r, d, kp, static_cast<float>(c1), static_cast<float>(c2), false, B.get());
+    UMAPB_LAUNCH_CHECK();
+    DevBuf<uint64_t> lists(n_q * S, s);
+    UMAPB_CUDA(cudaMemsetAsync(lists.get(), 0xFF, n_q * S * 8, s));
+    DevBuf<int> err(1, s), fb_count(1, s);
+    UMAPB_CUDA(cudaMemsetAsync(err.get(), 0, 4, s));
+    UMAPB_CUDA(cudaMemsetAsync(fb_count.get(), 0, 4, s));
+    const CUtensorMap ma = make_map(A.get(), n_q, kp);
+    const CUtensorMap mb = make_map(B.get(), n_r, kp);
+    const int mt = query_tiles_for(kb);
+    TcArgs a{};
+    a.n_q = n_q;
+    a.n_r = n_r;
+    a.kb = kb;
+    a.n_units = ceil_div(n_q, static_cast<int64_t>(BM) * mt);
+    a.n_ctiles = ceil_div(n_r, BN);
+    a.lists = lists.get();
+    a.err = err.get();
+    cudaEvent_t e0, e1;
+    UMAPB_CUDA(cudaEventCreate(&e0));
+    UMAPB_CUDA(cudaEventCreate(&e1));
+    UMAPB_CUDA(cudaEventRecord(e0, s));
+    if (mt == 2)
+        launch_tc<2, 5>(ma, mb, a, s);
+    else
+        launch_tc<1, 3>(ma, mb, a, s);
+    UMAPB_CUDA(cudaEventRecord(e1, s));
+    int err_h = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&err_h, err.get(), 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    UMAPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err_h != 0)
+        throw Error(UMAPB_ERR_CUDA,
+                    "tensor-core kNN kernel stopped on a wait timeout (code " +
+                        std::to_string(err_h) + ")");
+    DevBuf<int32_t> fb_rows(n_q, s);
+    rerank_kernel<<<static_cast<unsigned>(ceil_div(n_q * 32, 256)), 256, 0, s>>>(
+        Q, R, qsq.get(), rsq_p, lists.get(), n_q, n_r, d, k, c1, c2, out_idx, out_dist,
+        fb_count.get(), fb_rows.get());
+    UMAPB_LAUNCH_CHECK();
+    int fb = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&fb, fb_count.get(), 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    if (fb > 0) knn_plain(Q, fb_rows.get(), fb, R, n_r, d, k, metric, nullptr, nullptr, out_idx,
+                          out_dist, s);
+    if (stats) {
+        stats->fallback_rows = fb;
+        stats->kernel_ms = ms;
+        stats->shortlist = S;
+    }
 }
 
 }  // namespace umapb
