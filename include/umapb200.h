@@ -235,6 +235,24 @@ int32_t umapb_knn_exact(const float* data, int64_t n_rows, int64_t n_cols, int64
                         int32_t metric, int32_t backend, int64_t* indices, float* dists,
                         int64_t* fallback_rows);
 
+/* Allocation-free exact kNN (euclidean, self join, tensor-core path) for
+ * callers that cannot allocate device memory: for example a host that hands
+ * all HBM to its own arena before loading this library, or code that runs
+ * where the CUDA allocator may not be called.  It has no counterpart in the
+ * reference.  `data` (n_rows x n_cols f32), `indices` (n_rows x k int32) and
+ * `dists` (n_rows x k f32) are device pointers; `stream` is a cudaStream_t
+ * (NULL = legacy default stream).  Results equal umapb_knn_exact's.
+ * Scratch comes from one static device array of 64 MiB that every GPU loading
+ * the library holds until exit: about 50,000 rows at 64 columns; larger
+ * inputs are rejected with UMAPB_ERR_INVALID_PARAMETER naming the limit.  No
+ * cudaMalloc/cudaFree or allocating library routine is called.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress),
+ * so make that first call before any stream capture.  Every call reuses the
+ * same array: calls that overlap on the GPU (other streams, other threads)
+ * race and must be serialised by the caller. */
+int32_t umapb_knn_exact_noalloc(const float* data, int64_t n_rows, int64_t n_cols, int64_t k,
+                                int32_t* indices, float* dists, void* stream);
+
 /* Exact kNN of query rows against reference rows
  * (exact_nearest_neighbors_to_reference, rust_umap/src/lib.rs:3346-3399). */
 int32_t umapb_knn_query(const float* query, int64_t n_query, const float* reference,

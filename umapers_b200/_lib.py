@@ -155,6 +155,7 @@ SIGNATURES = {
     "umapb_get_ab": (_i32, [_vp, _f32p, _f32p]),
     "umapb_find_ab_params": (_i32, [_f32, _f32, _f32p, _f32p]),
     "umapb_knn_exact": (_i32, [_vp, _i64, _i64, _i64, _i32, _i32, _vp, _vp, _i64p]),
+    "umapb_knn_exact_noalloc": (_i32, [_vp, _i64, _i64, _i64, _vp, _vp, _vp]),
     "umapb_knn_query": (_i32, [_vp, _i64, _vp, _i64, _i64, _i64, _i32, _i32, _vp, _vp]),
     "umapb_nndescent": (_i32, [_vp, _i64, _i64, _i64, _i32, _i64, _i64, _u64, _vp, _vp, _i64p]),
     "umapb_smooth_knn_dist": (_i32, [_vp, _i64, _i64, _f32, _f32, _f32, _i32, _vp, _vp]),

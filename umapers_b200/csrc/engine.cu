@@ -209,6 +209,10 @@ struct StageClock {
 
 }  // namespace
 
+namespace umapb {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace umapb
+
 struct umapb_model {
     umapb_params p{};
     int device = -1;

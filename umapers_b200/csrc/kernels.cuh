@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -107,6 +108,10 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
 void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_t n_base,
                       const Graph& g, int64_t n_epochs, float a, float b, float lr,
                       int64_t neg_rate, float repulsion, uint64_t seed, cudaStream_t s);
+
+// ------------------------------------------------------------ engine.cu
+// Records the message umapb_last_error() returns on this thread.
+void set_last_error(const std::string& msg);
 
 // ------------------------------------------------------------- hostmath
 void find_ab_params(float spread, float min_dist, float* a, float* b);

@@ -721,3 +721,146 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
 }
 
 }  // namespace umapb
+
+// ===================================================== allocation-free entry
+// umapb_knn_exact_noalloc: the tensor-core exact kNN for callers that cannot
+// allocate device memory.  Its scratch (operands, shortlists, flags) lives in
+// one file-scope device array of kNoAllocScratchBytes that every GPU loading
+// this library holds until the process exits.  In host code the array's name
+// is only a host-side stand-in, so the device address is fetched once per
+// device with cudaGetSymbolAddress (on the first call made with that device
+// current) and reused afterwards.
+namespace umapb {
+namespace {
+constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(64) << 20;
+}  // namespace
+}  // namespace umapb
+
+static __device__ __align__(256) unsigned char umapb_noalloc_scratch[umapb::kNoAllocScratchBytes];
+
+namespace umapb {
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+
+unsigned char* noalloc_scratch() {
+    int dev = 0;
+    UMAPB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) invalid("device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        UMAPB_CUDA(cudaGetSymbolAddress(&p, umapb_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+inline size_t round256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
+
+// bytes of scratch one call needs for n rows of d features
+size_t noalloc_need(int64_t n, int d) {
+    const size_t rows = static_cast<size_t>(n);
+    const size_t kp = static_cast<size_t>(padded_k(d));
+    return round256(rows * 4) + 2 * round256(rows * kp * 2) + round256(rows * S * 8) +
+           round256(8) + round256(rows * 4);
+}
+
+void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, float* out_dist,
+                 cudaStream_t s) {
+    if (n < 1 || d < 1) invalid("empty input");
+    if (k < 1 || k > n) invalid("k must be in [1, n_rows]");
+    if (!knn_tc_supported(d, k, UMAPB_METRIC_EUCLIDEAN))
+        invalid("the allocation-free kNN runs the tensor-core path only (sm_100, euclidean, "
+                "k <= 30, n_cols <= 210)");
+    const size_t need = noalloc_need(n, d);
+    if (need > kNoAllocScratchBytes) {
+        int64_t max_rows = 0;
+        while (noalloc_need(max_rows + 1024, d) <= kNoAllocScratchBytes) max_rows += 1024;
+        invalid("the allocation-free kNN needs " + std::to_string(need) +
+                " bytes of scratch, above its static limit of " +
+                std::to_string(kNoAllocScratchBytes) + " bytes (about " +
+                std::to_string(max_rows) + " rows at " + std::to_string(d) + " columns)");
+    }
+    const int kp = padded_k(d);
+    const int kb = kp / BK;
+    const double c1 = kBoundC1;
+    const double c2 = bound_c2(d);
+    unsigned char* base = noalloc_scratch();
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        unsigned char* p = base + off;
+        off += round256(bytes);
+        return p;
+    };
+    float* sq = reinterpret_cast<float*>(carve(static_cast<size_t>(n) * 4));
+    __nv_bfloat16* A = reinterpret_cast<__nv_bfloat16*>(carve(static_cast<size_t>(n) * kp * 2));
+    __nv_bfloat16* B = reinterpret_cast<__nv_bfloat16*>(carve(static_cast<size_t>(n) * kp * 2));
+    uint64_t* lists = reinterpret_cast<uint64_t*>(carve(static_cast<size_t>(n) * S * 8));
+    int* flags = reinterpret_cast<int*>(carve(8));  // [0] = kernel error, [1] = fallback count
+    int32_t* fb_rows = reinterpret_cast<int32_t*>(carve(static_cast<size_t>(n) * 4));
+
+    // every call starts from cleared shortlists and flags (the array keeps
+    // the previous call's contents)
+    UMAPB_CUDA(cudaMemsetAsync(lists, 0xFF, static_cast<size_t>(n) * S * 8, s));
+    UMAPB_CUDA(cudaMemsetAsync(flags, 0, 8, s));
+    row_norms(X, n, d, nullptr, sq, s);
+    prep_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
+        X, sq, n, d, kp, static_cast<float>(c1), static_cast<float>(c2), true, A);
+    UMAPB_LAUNCH_CHECK();
+    prep_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
+        X, sq, n, d, kp, static_cast<float>(c1), static_cast<float>(c2), false, B);
+    UMAPB_LAUNCH_CHECK();
+    const CUtensorMap ma = make_map(A, n, kp);
+    const CUtensorMap mb = make_map(B, n, kp);
+    const int mt = query_tiles_for(kb);
+    TcArgs a{};
+    a.n_q = n;
+    a.n_r = n;
+    a.kb = kb;
+    a.n_units = ceil_div(n, static_cast<int64_t>(BM) * mt);
+    a.n_ctiles = ceil_div(n, BN);
+    a.lists = lists;
+    a.err = flags;
+    if (mt == 2)
+        launch_tc<2, 5>(ma, mb, a, s);
+    else
+        launch_tc<1, 3>(ma, mb, a, s);
+    int flags_h[2] = {0, 0};
+    UMAPB_CUDA(cudaMemcpyAsync(flags_h, flags, 8, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    if (flags_h[0] != 0)
+        throw Error(UMAPB_ERR_CUDA, "tensor-core kNN kernel stopped on a wait timeout (code " +
+                                        std::to_string(flags_h[0]) + ")");
+    rerank_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
+        X, X, sq, sq, lists, n, n, d, k, c1, c2, out_idx, out_dist, flags + 1, fb_rows);
+    UMAPB_LAUNCH_CHECK();
+    UMAPB_CUDA(cudaMemcpyAsync(flags_h, flags, 8, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    if (flags_h[1] > 0)
+        knn_plain(X, fb_rows, flags_h[1], X, n, d, k, UMAPB_METRIC_EUCLIDEAN, nullptr, nullptr,
+                  out_idx, out_dist, s);
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+}  // namespace umapb
+
+extern "C" int32_t umapb_knn_exact_noalloc(const float* data, int64_t n_rows, int64_t n_cols,
+                                           int64_t k, int32_t* indices, float* dists,
+                                           void* stream) {
+    try {
+        umapb::knn_noalloc(data, n_rows, static_cast<int>(n_cols), static_cast<int>(k), indices,
+                           dists, static_cast<cudaStream_t>(stream));
+        umapb::set_last_error("");
+        return UMAPB_OK;
+    } catch (const umapb::Error& e) {
+        umapb::set_last_error(e.what());
+        return e.status;
+    } catch (const std::exception& e) {
+        umapb::set_last_error(e.what());
+        return UMAPB_ERR_CUDA;
+    }
+}
