@@ -93,22 +93,29 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: false after kWaitNs or when another role aborted.  The
-// deadline clock is read only every 1024 polls so the fast path is a bare
-// try_wait loop.
+// try_wait with a suspend-time hint: the thread sleeps in hardware until the
+// phase completes or the hint elapses, instead of spinning on issue slots.
+__device__ __forceinline__ bool mbar_try_suspend(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred P1;\n mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n"
+        " selp.b32 %0, 1, 0, P1;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after kWaitNs or when another role aborted.  Each try
+// suspends for at most 1 ms, so the deadline and the abort flag are checked
+// at least that often.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-    uint64_t t0 = 0;
-    for (uint32_t i = 1;; ++i) {
-        if (mbar_try(bar, parity)) return true;
-        if ((i & 1023u) == 0u) {
-            if (*abort_flag) return false;
-            const uint64_t now = global_ns();
-            if (t0 == 0) {
-                t0 = now;
-            } else if (now - t0 > kWaitNs) {
-                return false;
-            }
-        }
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (true) {
+        if (mbar_try_suspend(bar, parity, 1000000u)) return true;
+        if (*abort_flag) return false;
+        if (global_ns() - t0 > kWaitNs) return false;
     }
 }
 
@@ -185,10 +192,23 @@ __device__ __forceinline__ float o2f(uint32_t o) {
     return (o & 0x80000000u) ? __uint_as_float(o & 0x7FFFFFFFu) : __uint_as_float(~o);
 }
 
+// Candidate tile visited at step t by CTA b: CTAs start at staggered tiles
+// inside a window of kStaggerTiles (4 MiB of B at K' = 256, L2-resident), so
+// they do not all request the same tile at once.  The shortlist certificate
+// does not depend on the visiting order.
+constexpr int64_t kStaggerGroups = 16, kStaggerStep = 4;
+
+__device__ __forceinline__ int64_t tile_at(int64_t t, int64_t n_ctiles) {
+    const int64_t off = (static_cast<int64_t>(blockIdx.x) % kStaggerGroups) * kStaggerStep;
+    int64_t c = t + (off < n_ctiles ? off : 0);
+    return c >= n_ctiles ? c - n_ctiles : c;
+}
+
 struct TcArgs {
     int64_t n_q;
     int64_t n_r;
     int kb;          // k-blocks of 64 columns
+    int ks_last;     // k-steps of 16 columns holding data in the last k-block
     int64_t n_units;   // groups of MT query tiles
     int64_t n_ctiles;  // candidate tiles
     uint64_t* lists;   // n_q x S keys (L order-mapped << 32 | index)
@@ -280,7 +300,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                         }
                         mbar_expect_tx(b_full + 8 * stage, kTileBytes);
                         tma_load_2d(sB + stage * kTileBytes, &tmB, b_full + 8 * stage, kb * BK,
-                                    static_cast<int>(c * BN));
+                                    static_cast<int>(tile_at(c, p.n_ctiles) * BN));
                     }
                 }
                 if (!ok) break;
@@ -318,8 +338,10 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                         }
                         tc_fence_after();
                         const uint64_t db0 = desc_sw128(sB + stage * kTileBytes);
-#pragma unroll
-                        for (int ks = 0; ks < BK / UK; ++ks) {
+                        // the columns past 3d + 7 are zero: their k-steps are skipped
+                        const int n_ks = kb == KB - 1 ? p.ks_last : BK / UK;
+#pragma unroll 4
+                        for (int ks = 0; ks < n_ks; ++ks) {
 #pragma unroll
                             for (int mt = 0; mt < MT; ++mt) {
                                 const uint64_t da =
@@ -362,23 +384,28 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                 tc_fence_after();
                 const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
                                        buf * (MT * BN) + mt * BN;
-#pragma unroll 1
-                for (int ch = 0; ch < 4; ++ch) {
-                    uint32_t r[32];
-                    tmem_ld32(taddr + ch * 32, r);
-                    tmem_wait_ld();
-                    if (ch == 3) {
-                        // the accumulator buffer can be overwritten once all 4 chunks are read
-                        tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
-                    }
-                    float m = __uint_as_float(r[0]);
+                uint32_t r[4][32];
 #pragma unroll
-                    for (int j = 1; j < 32; ++j) m = fminf(m, __uint_as_float(r[j]));
-                    unsigned pend = __ballot_sync(0xffffffffu, row_ok && m < tau);
+                for (int ch = 0; ch < 4; ++ch) tmem_ld32(taddr + ch * 32, r[ch]);
+                tmem_wait_ld();
+                // the accumulator buffer can be overwritten as soon as it is in registers
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
+                float m = __uint_as_float(r[0][0]);
+#pragma unroll
+                for (int ch = 0; ch < 4; ++ch)
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) m = fminf(m, __uint_as_float(r[ch][j]));
+                if (__ballot_sync(0xffffffffu, row_ok && m < tau) == 0) continue;
+#pragma unroll
+                for (int ch = 0; ch < 4; ++ch) {
+                    float mc = __uint_as_float(r[ch][0]);
+#pragma unroll
+                    for (int j = 1; j < 32; ++j) mc = fminf(mc, __uint_as_float(r[ch][j]));
+                    unsigned pend = __ballot_sync(0xffffffffu, row_ok && mc < tau);
                     if (pend == 0) continue;
-                    const int64_t col0 = c * BN + ch * 32;
+                    const int64_t col0 = tile_at(c, p.n_ctiles) * BN + ch * 32;
                     const int64_t valid_cols = p.n_r - col0;
                     while (pend) {
                         const int src = __ffs(pend) - 1;
@@ -387,7 +414,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                             int n = 0;
 #pragma unroll
                             for (int j = 0; j < 32; ++j) {
-                                const float v = __uint_as_float(r[j]);
+                                const float v = __uint_as_float(r[ch][j]);
                                 if (v < tau && j < valid_cols) {
                                     stage_v[n] = v;
                                     stage_i[n] = j;
@@ -679,6 +706,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     a.n_q = n_q;
     a.n_r = n_r;
     a.kb = kb;
+    a.ks_last = static_cast<int>(ceil_div(3 * d + 7 - (kb - 1) * BK, UK));
     a.n_units = ceil_div(n_q, static_cast<int64_t>(BM) * mt);
     a.n_ctiles = ceil_div(n_r, BN);
     a.lists = lists.get();
@@ -820,6 +848,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     a.n_q = n;
     a.n_r = n;
     a.kb = kb;
+    a.ks_last = static_cast<int>(ceil_div(3 * d + 7 - (kb - 1) * BK, UK));
     a.n_units = ceil_div(n, static_cast<int64_t>(BM) * mt);
     a.n_ctiles = ceil_div(n, BN);
     a.lists = lists;

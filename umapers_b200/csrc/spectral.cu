@@ -115,17 +115,52 @@ __global__ void norm_weight_kernel(const int32_t* __restrict__ heads,
     nw[e] = static_cast<float>(static_cast<double>(w[e]) * ii * ij);
 }
 
+// The iterative components' rows are processed in "position" order: the
+// nodes of slot 0, then slot 1, ... (slots = components on the iterative
+// path).  Blocks X and Y are stored in that order, so every pass except the
+// SpMM gathers streams contiguous memory.
+
+__global__ void pos_kernel(const int32_t* __restrict__ nodes, int64_t cnt, int32_t* __restrict__ pos) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p < cnt) pos[nodes[p]] = static_cast<int32_t>(p);
+}
+
+__global__ void prow_len_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
+                                const int32_t* __restrict__ row_ptr, int32_t* __restrict__ len) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p < cnt) {
+        const int32_t v = nodes[p];
+        len[p] = row_ptr[v + 1] - row_ptr[v];
+    }
+}
+
+// CSR of the shifted operator in position order (tails mapped to positions).
+__global__ void pcsr_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
+                            const int32_t* __restrict__ row_ptr, const int32_t* __restrict__ tails,
+                            const float* __restrict__ nw, const int32_t* __restrict__ pos,
+                            const int32_t* __restrict__ prow_ptr, int32_t* __restrict__ ptails,
+                            float* __restrict__ pnw) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= cnt) return;
+    const int32_t v = nodes[p];
+    int32_t o = prow_ptr[p];
+    for (int32_t e = row_ptr[v]; e < row_ptr[v + 1]; ++e, ++o) {
+        ptails[o] = pos[tails[e]];
+        pnw[o] = nw[e];
+    }
+}
+
 // Initial block: column 0 = sqrt(degree), the others U(-1, 1) (lib.rs:4254-4261).
 __global__ void init_block_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
-                                  const int32_t* __restrict__ slot_of_node,
+                                  const int32_t* __restrict__ slot_of_pos,
                                   const uint64_t* __restrict__ slot_seed,
                                   const double* __restrict__ deg, int s, int sp,
                                   float* __restrict__ X) {
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= cnt) return;
     const int32_t i = nodes[t];
-    const uint64_t seed = slot_seed[slot_of_node[t]] ^ 0x7A5B3D91CE42A117ULL;
-    float* row = X + static_cast<int64_t>(i) * sp;
+    const uint64_t seed = slot_seed[slot_of_pos[t]] ^ 0x7A5B3D91CE42A117ULL;
+    float* row = X + t * sp;
     row[0] = static_cast<float>(sqrt(deg[i]));
     for (int c = 1; c < sp; ++c) {
         float v = 0.0f;
@@ -134,24 +169,23 @@ __global__ void init_block_kernel(const int32_t* __restrict__ nodes, int64_t cnt
     }
 }
 
-// Y = X + A_hat X over the rows of the iterative components.
+// Y = X + A_hat X in position order.
 template <int SP>
 __global__ void __launch_bounds__(256)
-    spmm_kernel(const int32_t* __restrict__ nodes, int64_t cnt, const int32_t* __restrict__ row_ptr,
-                const int32_t* __restrict__ tails, const float* __restrict__ nw,
+    spmm_kernel(int64_t cnt, const int32_t* __restrict__ prow_ptr,
+                const int32_t* __restrict__ ptails, const float* __restrict__ pnw,
                 const float* __restrict__ X, float* __restrict__ Y) {
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= cnt) return;
-    const int32_t i = nodes[t];
     constexpr int V = SP / 4;
     float4 acc[V];
-    const float4* xi = reinterpret_cast<const float4*>(X + static_cast<int64_t>(i) * SP);
+    const float4* xi = reinterpret_cast<const float4*>(X + t * SP);
 #pragma unroll
     for (int v = 0; v < V; ++v) acc[v] = xi[v];
-    const int32_t st = row_ptr[i], en = row_ptr[i + 1];
+    const int32_t st = prow_ptr[t], en = prow_ptr[t + 1];
     for (int32_t e = st; e < en; ++e) {
-        const float wv = nw[e];
-        const float4* xj = reinterpret_cast<const float4*>(X + static_cast<int64_t>(tails[e]) * SP);
+        const float wv = pnw[e];
+        const float4* xj = reinterpret_cast<const float4*>(X + static_cast<int64_t>(ptails[e]) * SP);
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             const float4 q = __ldg(xj + v);
@@ -161,36 +195,37 @@ __global__ void __launch_bounds__(256)
             acc[v].w = fmaf(wv, q.w, acc[v].w);
         }
     }
-    float4* yi = reinterpret_cast<float4*>(Y + static_cast<int64_t>(i) * SP);
+    float4* yi = reinterpret_cast<float4*>(Y + t * SP);
 #pragma unroll
     for (int v = 0; v < V; ++v) yi[v] = acc[v];
 }
 
 struct Chunk {
     int32_t slot;
-    int32_t start;  // into the node list
+    int32_t start;  // position range [start, end)
     int32_t end;
 };
 
-// Upper triangle of A^T B per component slot, FP64 accumulation.
+// Upper triangle of A^T B per slot over contiguous position ranges, FP64.
 constexpr int kGramRows = 64;
+template <int S, int SP>
 __global__ void __launch_bounds__(256)
-    gram_kernel(const Chunk* __restrict__ chunks, const int32_t* __restrict__ nodes,
-                const float* __restrict__ A, const float* __restrict__ B, int s, int sp,
-                double* __restrict__ G) {
+    gram_kernel(const Chunk* __restrict__ chunks, const float* __restrict__ A,
+                const float* __restrict__ B, double* __restrict__ G) {
     const Chunk ch = chunks[blockIdx.x];
-    __shared__ float As[kGramRows][kMaxS];
-    __shared__ float Bs[kGramRows][kMaxS];
+    __shared__ __align__(16) float As[kGramRows * SP];
+    __shared__ __align__(16) float Bs[kGramRows * SP];
     const int tid = threadIdx.x;
-    const int n_ent = s * (s + 1) / 2;  // <= 528 for s <= 32: at most 3 entries per thread
-    int ea[3], eb[3];
-    double acc[3] = {0.0, 0.0, 0.0};
-    for (int q = 0; q < 3; ++q) {
-        int t = tid + q * static_cast<int>(blockDim.x), a = 0;
+    constexpr int NE = S * (S + 1) / 2;  // <= 465 for S <= 30: at most 2 entries per thread
+    int ea[2], eb[2];
+    double acc[2] = {0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        int t = tid + q * 256, a = 0;
         ea[q] = eb[q] = -1;
-        if (t >= n_ent) continue;
-        while (t >= s - a) {
-            t -= s - a;
+        if (t >= NE) continue;
+        while (t >= S - a) {
+            t -= S - a;
             ++a;
         }
         ea[q] = a;
@@ -199,107 +234,129 @@ __global__ void __launch_bounds__(256)
     for (int r0 = ch.start; r0 < ch.end; r0 += kGramRows) {
         const int rows = min(kGramRows, ch.end - r0);
         __syncthreads();
-        for (int e = tid; e < rows * s; e += blockDim.x) {
-            const int r = e / s, c = e % s;
-            const int64_t node = nodes[r0 + r];
-            As[r][c] = A[node * sp + c];
-            Bs[r][c] = B[node * sp + c];
+        const float4* a4 = reinterpret_cast<const float4*>(A + static_cast<int64_t>(r0) * SP);
+        const float4* b4 = reinterpret_cast<const float4*>(B + static_cast<int64_t>(r0) * SP);
+        for (int e = tid; e < rows * SP / 4; e += 256) {
+            reinterpret_cast<float4*>(As)[e] = a4[e];
+            reinterpret_cast<float4*>(Bs)[e] = b4[e];
         }
         __syncthreads();
-        for (int q = 0; q < 3; ++q) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
             if (ea[q] < 0) continue;
             double v = 0.0;
             for (int r = 0; r < rows; ++r)
-                v += static_cast<double>(As[r][ea[q]]) * static_cast<double>(Bs[r][eb[q]]);
+                v += static_cast<double>(As[r * SP + ea[q]]) * static_cast<double>(Bs[r * SP + eb[q]]);
             acc[q] += v;
         }
     }
-    for (int q = 0; q < 3; ++q)
-        if (ea[q] >= 0)
-            atomicAdd(&G[static_cast<int64_t>(ch.slot) * s * s + ea[q] * s + eb[q]], acc[q]);
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+        if (ea[q] >= 0) atomicAdd(&G[static_cast<int64_t>(ch.slot) * S * S + ea[q] * S + eb[q]], acc[q]);
 }
 
-// Cholesky G = L L^T per slot and Rinv = L^-T (upper triangular).
-__global__ void chol_kernel(const double* __restrict__ G, int s, double* __restrict__ Rinv,
-                            int* __restrict__ fail) {
-    if (threadIdx.x != 0) return;
+// G = L L^T per slot, one warp: lane i keeps row i; right-looking updates
+// with the pivot column shared by shuffles.  A pivot <= 1e-12 is the MGS
+// failure of the reference (column norm^2 after projection).
+template <int S>
+__global__ void chol_kernel(const double* __restrict__ G, double* __restrict__ Lout,
+                            double* __restrict__ dinv, int* __restrict__ fail) {
     const int slot = blockIdx.x;
-    const double* g = G + static_cast<int64_t>(slot) * s * s;
-    double L[kMaxS][kMaxS];
-    for (int i = 0; i < s; ++i)
-        for (int j = 0; j < s; ++j) L[i][j] = 0.0;
+    const int lane = threadIdx.x;
+    const double* g = G + static_cast<int64_t>(slot) * S * S;
+    double row[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+        double v = 0.0;
+        if (lane < S) v = lane <= k ? g[lane * S + k] : g[k * S + lane];
+        row[k] = v;
+    }
     bool ok = true;
-    for (int j = 0; j < s && ok; ++j) {
-        double d = g[j * s + j];  // upper triangle holds (a <= b)
-        for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
-        if (!(d > kOrthoEps) || !isfinite(d)) {
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        const double pivot = __shfl_sync(0xffffffffu, row[j], j);
+        if (!(pivot > kOrthoEps) || !isfinite(pivot)) {
             ok = false;
             break;
         }
-        const double ljj = sqrt(d);
-        L[j][j] = ljj;
-        for (int i = j + 1; i < s; ++i) {
-            double v = g[j * s + i];
-            for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k];
-            L[i][j] = v / ljj;
+        const double ljj = sqrt(pivot);
+        const double lij = lane == j ? ljj : row[j] / ljj;
+        if (lane >= j) row[j] = lij;
+#pragma unroll
+        for (int k = j + 1; k < S; ++k) {
+            const double lkj = __shfl_sync(0xffffffffu, lij, k);
+            if (lane > j) row[k] -= lij * lkj;
         }
     }
-    double* R = Rinv + static_cast<int64_t>(slot) * s * s;
     if (!ok) {
-        fail[slot] = 1;
-        for (int i = 0; i < s * s; ++i) R[i] = 0.0;
-        for (int i = 0; i < s; ++i) R[i * s + i] = 1.0;
+        if (lane == 0) fail[slot] = 1;
+        if (lane < S) {
+#pragma unroll
+            for (int k = 0; k < S; ++k) Lout[static_cast<int64_t>(slot) * S * S + lane * S + k] = lane == k;
+            dinv[slot * S + lane] = 1.0;
+        }
         return;
     }
-    // Linv lower triangular; Rinv = Linv^T
-    double Li[kMaxS][kMaxS];
-    for (int i = 0; i < s; ++i)
-        for (int j = 0; j < s; ++j) Li[i][j] = 0.0;
-    for (int i = 0; i < s; ++i) {
-        Li[i][i] = 1.0 / L[i][i];
-        for (int j = 0; j < i; ++j) {
-            double v = 0.0;
-            for (int k = j; k < i; ++k) v += L[i][k] * Li[k][j];
-            Li[i][j] = -v / L[i][i];
-        }
+    if (lane < S) {
+#pragma unroll
+        for (int k = 0; k < S; ++k)
+            Lout[static_cast<int64_t>(slot) * S * S + lane * S + k] = k <= lane ? row[k] : 0.0;
+        dinv[slot * S + lane] = 1.0 / row[lane];
     }
-    for (int a = 0; a < s; ++a)
-        for (int c = 0; c < s; ++c) R[a * s + c] = Li[c][a];
 }
 
-// X = Y Rinv (row times upper-triangular), FP64 arithmetic.
-__global__ void apply_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
-                             const int32_t* __restrict__ slot_of_node,
-                             const double* __restrict__ Rinv, int s, int sp,
-                             const float* __restrict__ Y, float* __restrict__ X) {
+// X = Y L^-T by forward substitution per row, FP64.
+template <int S, int SP>
+__global__ void __launch_bounds__(256)
+    apply_kernel(int64_t cnt, const int32_t* __restrict__ slot_of_pos,
+                 const double* __restrict__ L, const double* __restrict__ dinv,
+                 const float* __restrict__ Y, float* __restrict__ X) {
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= cnt) return;
-    const int64_t i = nodes[t];
-    const double* R = Rinv + static_cast<int64_t>(slot_of_node[t]) * s * s;
-    double y[kMaxS];
-    for (int a = 0; a < s; ++a) y[a] = static_cast<double>(Y[i * sp + a]);
-    for (int c = 0; c < s; ++c) {
-        double v = 0.0;
-        for (int a = 0; a <= c; ++a) v += y[a] * R[a * s + c];
-        X[i * sp + c] = static_cast<float>(v);
+    const int slot = slot_of_pos[t];
+    const double* Ls = L + static_cast<int64_t>(slot) * S * S;
+    const double* di = dinv + slot * S;
+    float y[SP];
+    const float4* y4 = reinterpret_cast<const float4*>(Y + t * SP);
+#pragma unroll
+    for (int v = 0; v < SP / 4; ++v) {
+        const float4 q = y4[v];
+        y[4 * v] = q.x;
+        y[4 * v + 1] = q.y;
+        y[4 * v + 2] = q.z;
+        y[4 * v + 3] = q.w;
     }
+    double x[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+        double v = static_cast<double>(y[c]);
+#pragma unroll
+        for (int a = 0; a < c; ++a) v -= x[a] * __ldg(Ls + c * S + a);
+        x[c] = v * __ldg(di + c);
+    }
+    float o[SP];
+#pragma unroll
+    for (int c = 0; c < SP; ++c) o[c] = c < S ? static_cast<float>(x[c]) : 0.0f;
+    float4* x4 = reinterpret_cast<float4*>(X + t * SP);
+#pragma unroll
+    for (int v = 0; v < SP / 4; ++v) x4[v] = make_float4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
 }
 
 // coords = X V (V: s x dim per slot), FP64; and per-slot max |coord|.
 __global__ void project_kernel(const int32_t* __restrict__ nodes, int64_t cnt,
-                               const int32_t* __restrict__ slot_of_node,
+                               const int32_t* __restrict__ slot_of_pos,
                                const double* __restrict__ V, int s, int sp, int dim,
                                const float* __restrict__ X, float* __restrict__ out,
                                unsigned* __restrict__ max_abs_bits) {
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= cnt) return;
     const int64_t i = nodes[t];
-    const int slot = slot_of_node[t];
+    const int slot = slot_of_pos[t];
     const double* v = V + static_cast<int64_t>(slot) * s * dim;
     float mx = 0.0f;
     for (int oc = 0; oc < dim; ++oc) {
         double acc = 0.0;
-        for (int b = 0; b < s; ++b) acc += static_cast<double>(X[i * sp + b]) * v[b * dim + oc];
+        for (int b = 0; b < s; ++b) acc += static_cast<double>(X[t * sp + b]) * v[b * dim + oc];
         const float f = static_cast<float>(acc);
         out[i * dim + oc] = f;
         mx = fmaxf(mx, fabsf(f));
@@ -482,6 +539,170 @@ bool meta_layout(const std::vector<double>& cents, int64_t m, int d, int dim, ui
     return finite_all(out);
 }
 
+// Block subspace iteration for every iterative component at once; writes
+// the scaled, noised and anchored coordinates of their nodes into `out`.
+// Returns false where the reference would return None (an orthonormalisation
+// failure or a non-finite result).
+template <int S, int SP>
+bool run_iterative(const std::vector<int64_t>& it_comps, const std::vector<int64_t>& cstart,
+                   const std::vector<int32_t>& order_h, const std::vector<uint64_t>& cseed,
+                   const std::vector<float>& data_range, const std::vector<float>& anchors,
+                   bool multi, uint64_t seed, int dim, int64_t n, const Graph& g, float* out,
+                   cudaStream_t s) {
+    const int64_t m = g.n_edges;
+    const int64_t n_slots = static_cast<int64_t>(it_comps.size());
+    std::vector<int32_t> nodes_h, slot_h;
+    std::vector<Chunk> chunks;
+    std::vector<uint64_t> slot_seed(n_slots), noise_seed(n_slots);
+    std::vector<float> expand_target(n_slots), slot_anchor(n_slots * dim);
+    for (int64_t sl = 0; sl < n_slots; ++sl) {
+        const int64_t c = it_comps[sl];
+        const int32_t base = static_cast<int32_t>(nodes_h.size());
+        for (int64_t q = cstart[c]; q < cstart[c + 1]; ++q) {
+            nodes_h.push_back(order_h[q]);
+            slot_h.push_back(static_cast<int32_t>(sl));
+        }
+        const int32_t end = static_cast<int32_t>(nodes_h.size());
+        for (int32_t st = base; st < end; st += 1024)
+            chunks.push_back({static_cast<int32_t>(sl), st, std::min(end, st + 1024)});
+        slot_seed[sl] = cseed[c];
+        noise_seed[sl] = multi ? seed ^ (static_cast<uint64_t>(c + 1) * 0x94D049BBULL)
+                               : seed ^ 0x5DEECE66DULL;
+        expand_target[sl] = multi ? data_range[c] : kInitMaxCoord;
+        for (int k = 0; k < dim; ++k) slot_anchor[sl * dim + k] = multi ? anchors[c * dim + k] : 0.0f;
+    }
+    const int64_t cnt = static_cast<int64_t>(nodes_h.size());
+    DevBuf<int32_t> nodes(cnt, s), slots(cnt, s), pos(n, s), plen(cnt + 1, s), prow(cnt + 1, s);
+    DevBuf<Chunk> dch(chunks.size(), s);
+    DevBuf<uint64_t> dseed(n_slots, s), dnseed(n_slots, s);
+    UMAPB_CUDA(cudaMemcpyAsync(nodes.get(), nodes_h.data(), cnt * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(slots.get(), slot_h.data(), cnt * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(dch.get(), chunks.data(), chunks.size() * sizeof(Chunk),
+                               cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(dseed.get(), slot_seed.data(), n_slots * 8, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(dnseed.get(), noise_seed.data(), n_slots * 8, cudaMemcpyHostToDevice, s));
+
+    // degrees and normalised weights in node space
+    DevBuf<double> deg(n, s);
+    DevBuf<float> dinvn(n, s), nw(std::max<int64_t>(m, 1), s);
+    degree_kernel<<<grid_for(n), 256, 0, s>>>(g.row_ptr.get(), g.weights.get(), n, deg.get(),
+                                              dinvn.get());
+    UMAPB_LAUNCH_CHECK();
+    norm_weight_kernel<<<grid_for(m), 256, 0, s>>>(g.heads.get(), g.tails.get(), g.weights.get(),
+                                                   deg.get(), m, nw.get());
+    UMAPB_LAUNCH_CHECK();
+    // position-ordered CSR
+    pos_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, pos.get());
+    UMAPB_LAUNCH_CHECK();
+    prow_len_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(), plen.get());
+    UMAPB_LAUNCH_CHECK();
+    UMAPB_CUDA(cudaMemsetAsync(plen.get() + cnt, 0, 4, s));
+    {
+        size_t tb = 0;
+        UMAPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, plen.get(), prow.get(), cnt + 1, s));
+        DevBuf<unsigned char> tmp(tb, s);
+        UMAPB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, plen.get(), prow.get(), cnt + 1, s));
+    }
+    int32_t m_it = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&m_it, prow.get() + cnt, 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    DevBuf<int32_t> ptails(std::max<int32_t>(m_it, 1), s);
+    DevBuf<float> pnw(std::max<int32_t>(m_it, 1), s);
+    pcsr_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(), g.tails.get(),
+                                              nw.get(), pos.get(), prow.get(), ptails.get(), pnw.get());
+    UMAPB_LAUNCH_CHECK();
+
+    DevBuf<float> Xb(cnt * SP, s), Yb(cnt * SP, s);
+    DevBuf<double> G(n_slots * S * S, s), L(n_slots * S * S, s), dg(n_slots * S, s);
+    DevBuf<int> fail(n_slots, s);
+    UMAPB_CUDA(cudaMemsetAsync(fail.get(), 0, n_slots * 4, s));
+    init_block_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(), dseed.get(),
+                                                    deg.get(), S, SP, Xb.get());
+    UMAPB_LAUNCH_CHECK();
+    const unsigned nch = static_cast<unsigned>(chunks.size());
+    const unsigned gr = grid_for(cnt);
+    // CholQR2: src -> dst -> src; the orthonormal block ends in src
+    auto cholqr = [&](float* src, float* dst) {
+        for (int pass = 0; pass < 2; ++pass) {
+            float* a = pass == 0 ? src : dst;
+            float* b = pass == 0 ? dst : src;
+            UMAPB_CUDA(cudaMemsetAsync(G.get(), 0, n_slots * S * S * 8, s));
+            gram_kernel<S, SP><<<nch, 256, 0, s>>>(dch.get(), a, a, G.get());
+            UMAPB_LAUNCH_CHECK();
+            chol_kernel<S><<<static_cast<unsigned>(n_slots), 32, 0, s>>>(G.get(), L.get(), dg.get(),
+                                                                        fail.get());
+            UMAPB_LAUNCH_CHECK();
+            apply_kernel<S, SP><<<gr, 256, 0, s>>>(cnt, slots.get(), L.get(), dg.get(), a, b);
+            UMAPB_LAUNCH_CHECK();
+        }
+    };
+    auto spmm = [&](const float* x, float* y) {
+        spmm_kernel<SP><<<gr, 256, 0, s>>>(cnt, prow.get(), ptails.get(), pnw.get(), x, y);
+        UMAPB_LAUNCH_CHECK();
+    };
+    cholqr(Xb.get(), Yb.get());
+    for (int it = 0; it < kIters; ++it) {
+        spmm(Xb.get(), Yb.get());    // Y = (I + A) X
+        cholqr(Yb.get(), Xb.get());  // orthonormal block back in Y
+        std::swap(Xb, Yb);
+    }
+    spmm(Xb.get(), Yb.get());
+    UMAPB_CUDA(cudaMemsetAsync(G.get(), 0, n_slots * S * S * 8, s));
+    gram_kernel<S, SP><<<nch, 256, 0, s>>>(dch.get(), Xb.get(), Yb.get(), G.get());
+    UMAPB_LAUNCH_CHECK();
+    std::vector<double> G_h(n_slots * S * S);
+    std::vector<int> fail_h(n_slots);
+    UMAPB_CUDA(cudaMemcpyAsync(G_h.data(), G.get(), G_h.size() * 8, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(fail_h.data(), fail.get(), n_slots * 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    for (int64_t sl = 0; sl < n_slots; ++sl)
+        if (fail_h[sl]) return false;  // orthonormalize_columns failed (lib.rs:4262-4273)
+    // Rayleigh-Ritz: eigenvectors by descending eigenvalue, skipping the first
+    std::vector<double> Vsel(n_slots * S * dim);
+    for (int64_t sl = 0; sl < n_slots; ++sl) {
+        std::vector<double> R(S * S);
+        const double* gs = G_h.data() + sl * S * S;
+        for (int i = 0; i < S; ++i)
+            for (int j = i; j < S; ++j) {
+                R[i * S + j] = gs[i * S + j];
+                R[j * S + i] = gs[i * S + j];
+            }
+        std::vector<double> ev, V;
+        symmetric_eigen(R, S, ev, V);
+        std::vector<int> ord(S);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return ev[a] > ev[b]; });
+        for (int oc = 0; oc < dim; ++oc)
+            for (int b = 0; b < S; ++b) Vsel[(sl * S + b) * dim + oc] = V[b * S + ord[oc + 1]];
+    }
+    DevBuf<double> dV(Vsel.size(), s);
+    DevBuf<unsigned> maxbits(n_slots, s);
+    UMAPB_CUDA(cudaMemcpyAsync(dV.get(), Vsel.data(), Vsel.size() * 8, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemsetAsync(maxbits.get(), 0, n_slots * 4, s));
+    project_kernel<<<gr, 256, 0, s>>>(nodes.get(), cnt, slots.get(), dV.get(), S, SP, dim, Xb.get(),
+                                      out, maxbits.get());
+    UMAPB_LAUNCH_CHECK();
+    std::vector<unsigned> mb(n_slots);
+    UMAPB_CUDA(cudaMemcpyAsync(mb.data(), maxbits.get(), n_slots * 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    std::vector<float> expansion(n_slots);
+    for (int64_t sl = 0; sl < n_slots; ++sl) {
+        float mx;
+        std::memcpy(&mx, &mb[sl], 4);
+        if (!std::isfinite(mx)) return false;
+        expansion[sl] = mx > 0.0f ? expand_target[sl] / mx : 1.0f;
+    }
+    DevBuf<float> dexp(n_slots, s), danch(n_slots * dim, s);
+    UMAPB_CUDA(cudaMemcpyAsync(dexp.get(), expansion.data(), n_slots * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(danch.get(), slot_anchor.data(), n_slots * dim * 4,
+                               cudaMemcpyHostToDevice, s));
+    finish_kernel<<<gr, 256, 0, s>>>(nodes.get(), cnt, slots.get(), dexp.get(), danch.get(),
+                                     dnseed.get(), dim, kInitNoise, out);
+    UMAPB_LAUNCH_CHECK();
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    return true;
+}
+
 }  // namespace
 
 void random_init(int64_t n, int dim, uint64_t seed, float low, float high, float* out,
@@ -498,7 +719,6 @@ SpectralResult spectral_init(const float* X, int64_t n, int d, const Graph& g, i
     if (n <= dim + 1 || m == 0) return res;
     const int sdim = std::max((dim + 1) * kOversampling, dim + 1);
     if (sdim > kMaxS) invalid("spectral init supports n_components <= 4 on the GPU path");
-    const int sp = (sdim + 3) / 4 * 4;
 
     // ---- connected components (union-find with atomicMin hooking)
     DevBuf<int32_t> parent(n, s);
@@ -697,155 +917,19 @@ SpectralResult spectral_init(const float* X, int64_t n, int d, const Graph& g, i
     for (int64_t c = 0; c < n_comp; ++c)
         if (kind[c] == kIter) it_comps.push_back(c);
     if (!it_comps.empty()) {
-        const int64_t n_slots = static_cast<int64_t>(it_comps.size());
-        std::vector<int32_t> nodes_h, slot_h;
-        std::vector<Chunk> chunks;
-        std::vector<uint64_t> slot_seed(n_slots), noise_seed(n_slots);
-        std::vector<float> expand_target(n_slots), slot_anchor(n_slots * dim);
-        for (int64_t sl = 0; sl < n_slots; ++sl) {
-            const int64_t c = it_comps[sl];
-            const int32_t base = static_cast<int32_t>(nodes_h.size());
-            for (int64_t p = cstart[c]; p < cstart[c + 1]; ++p) {
-                nodes_h.push_back(order_h[p]);
-                slot_h.push_back(static_cast<int32_t>(sl));
-            }
-            const int32_t end = static_cast<int32_t>(nodes_h.size());
-            for (int32_t st = base; st < end; st += 2048)
-                chunks.push_back({static_cast<int32_t>(sl), st, std::min(end, st + 2048)});
-            slot_seed[sl] = cseed[c];
-            noise_seed[sl] = multi ? seed ^ (static_cast<uint64_t>(c + 1) * 0x94D049BBULL)
-                                   : seed ^ 0x5DEECE66DULL;
-            expand_target[sl] = multi ? data_range[c] : kInitMaxCoord;
-            for (int k = 0; k < dim; ++k)
-                slot_anchor[sl * dim + k] = multi ? anchors[c * dim + k] : 0.0f;
+        bool ok = false;
+        switch (sdim) {
+            case 12: ok = run_iterative<12, 12>(it_comps, cstart, order_h, cseed, data_range, anchors,
+                                               multi, seed, dim, n, g, out, s); break;
+            case 18: ok = run_iterative<18, 20>(it_comps, cstart, order_h, cseed, data_range, anchors,
+                                               multi, seed, dim, n, g, out, s); break;
+            case 24: ok = run_iterative<24, 24>(it_comps, cstart, order_h, cseed, data_range, anchors,
+                                               multi, seed, dim, n, g, out, s); break;
+            case 30: ok = run_iterative<30, 32>(it_comps, cstart, order_h, cseed, data_range, anchors,
+                                               multi, seed, dim, n, g, out, s); break;
+            default: invalid("unsupported spectral block width");
         }
-        const int64_t cnt = static_cast<int64_t>(nodes_h.size());
-        DevBuf<int32_t> nodes(cnt, s), slots(cnt, s);
-        DevBuf<Chunk> dch(chunks.size(), s);
-        DevBuf<uint64_t> dseed(n_slots, s), dnseed(n_slots, s);
-        UMAPB_CUDA(cudaMemcpyAsync(nodes.get(), nodes_h.data(), cnt * 4, cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemcpyAsync(slots.get(), slot_h.data(), cnt * 4, cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemcpyAsync(dch.get(), chunks.data(), chunks.size() * sizeof(Chunk),
-                                   cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemcpyAsync(dseed.get(), slot_seed.data(), n_slots * 8, cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemcpyAsync(dnseed.get(), noise_seed.data(), n_slots * 8, cudaMemcpyHostToDevice, s));
-
-        DevBuf<double> deg(n, s);
-        DevBuf<float> dinv(n, s), nw(m, s);
-        degree_kernel<<<grid_for(n), 256, 0, s>>>(g.row_ptr.get(), g.weights.get(), n, deg.get(),
-                                                  dinv.get());
-        UMAPB_LAUNCH_CHECK();
-        norm_weight_kernel<<<grid_for(m), 256, 0, s>>>(g.heads.get(), g.tails.get(),
-                                                       g.weights.get(), deg.get(), m, nw.get());
-        UMAPB_LAUNCH_CHECK();
-        DevBuf<float> Xb(n * sp, s), Yb(n * sp, s);
-        UMAPB_CUDA(cudaMemsetAsync(Xb.get(), 0, n * sp * 4, s));
-        UMAPB_CUDA(cudaMemsetAsync(Yb.get(), 0, n * sp * 4, s));
-        DevBuf<double> G(n_slots * sdim * sdim, s), Rinv(n_slots * sdim * sdim, s);
-        DevBuf<int> fail(n_slots, s);
-        UMAPB_CUDA(cudaMemsetAsync(fail.get(), 0, n_slots * 4, s));
-        init_block_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(), dseed.get(),
-                                                        deg.get(), sdim, sp, Xb.get());
-        UMAPB_LAUNCH_CHECK();
-        const unsigned nch = static_cast<unsigned>(chunks.size());
-        auto cholqr = [&](float* src, float* dst) {
-            // two passes: src -> dst, dst -> src... ends with the result in dst
-            for (int pass = 0; pass < 2; ++pass) {
-                float* a = pass == 0 ? src : dst;
-                float* b = pass == 0 ? dst : src;
-                UMAPB_CUDA(cudaMemsetAsync(G.get(), 0, n_slots * sdim * sdim * 8, s));
-                gram_kernel<<<nch, 256, 0, s>>>(dch.get(), nodes.get(), a, a, sdim, sp, G.get());
-                UMAPB_LAUNCH_CHECK();
-                chol_kernel<<<static_cast<unsigned>(n_slots), 32, 0, s>>>(G.get(), sdim, Rinv.get(),
-                                                                          fail.get());
-                UMAPB_LAUNCH_CHECK();
-                apply_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(),
-                                                           Rinv.get(), sdim, sp, a, b);
-                UMAPB_LAUNCH_CHECK();
-            }
-            // result of pass 2 is in `src`; copy semantics handled by the caller
-        };
-        auto spmm = [&](const float* x, float* y) {
-            if (sp == 20)
-                spmm_kernel<20><<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(),
-                                                              g.tails.get(), nw.get(), x, y);
-            else if (sp == 12)
-                spmm_kernel<12><<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(),
-                                                              g.tails.get(), nw.get(), x, y);
-            else if (sp == 24)
-                spmm_kernel<24><<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(),
-                                                              g.tails.get(), nw.get(), x, y);
-            else if (sp == 32)
-                spmm_kernel<32><<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, g.row_ptr.get(),
-                                                              g.tails.get(), nw.get(), x, y);
-            else
-                invalid("unsupported spectral block width");
-            UMAPB_LAUNCH_CHECK();
-        };
-        // orthonormalize the initial block: X -> (Y) -> X
-        cholqr(Xb.get(), Yb.get());
-        for (int it = 0; it < kIters; ++it) {
-            spmm(Xb.get(), Yb.get());          // Y = (I + A) X
-            cholqr(Yb.get(), Xb.get());        // Y -> X -> Y; result in Y
-            std::swap(Xb, Yb);                 // X holds the orthonormal block
-        }
-        UMAPB_LAUNCH_CHECK();
-        spmm(Xb.get(), Yb.get());
-        UMAPB_CUDA(cudaMemsetAsync(G.get(), 0, n_slots * sdim * sdim * 8, s));
-        gram_kernel<<<nch, 256, 0, s>>>(dch.get(), nodes.get(), Xb.get(), Yb.get(), sdim, sp,
-                                        G.get());
-        UMAPB_LAUNCH_CHECK();
-        std::vector<double> G_h(n_slots * sdim * sdim);
-        std::vector<int> fail_h(n_slots);
-        UMAPB_CUDA(cudaMemcpyAsync(G_h.data(), G.get(), G_h.size() * 8, cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaMemcpyAsync(fail_h.data(), fail.get(), n_slots * 4, cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaStreamSynchronize(s));
-        for (int64_t sl = 0; sl < n_slots; ++sl)
-            if (fail_h[sl]) return res;  // reference: orthonormalize failure -> None
-        // Rayleigh-Ritz per slot: eigenvectors by descending eigenvalue, skip the first
-        std::vector<double> Vsel(n_slots * sdim * dim);
-        for (int64_t sl = 0; sl < n_slots; ++sl) {
-            std::vector<double> R(sdim * sdim);
-            const double* gs = G_h.data() + sl * sdim * sdim;
-            for (int i = 0; i < sdim; ++i)
-                for (int j = i; j < sdim; ++j) {
-                    R[i * sdim + j] = gs[i * sdim + j];
-                    R[j * sdim + i] = gs[i * sdim + j];
-                }
-            std::vector<double> ev, V;
-            symmetric_eigen(R, sdim, ev, V);
-            std::vector<int> ord(sdim);
-            std::iota(ord.begin(), ord.end(), 0);
-            std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return ev[a] > ev[b]; });
-            for (int oc = 0; oc < dim; ++oc)
-                for (int b = 0; b < sdim; ++b)
-                    Vsel[(sl * sdim + b) * dim + oc] = V[b * sdim + ord[oc + 1]];
-        }
-        DevBuf<double> dV(Vsel.size(), s);
-        DevBuf<unsigned> maxbits(n_slots, s);
-        UMAPB_CUDA(cudaMemcpyAsync(dV.get(), Vsel.data(), Vsel.size() * 8, cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemsetAsync(maxbits.get(), 0, n_slots * 4, s));
-        project_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(), dV.get(), sdim,
-                                                     sp, dim, Xb.get(), out, maxbits.get());
-        UMAPB_LAUNCH_CHECK();
-        std::vector<unsigned> mb(n_slots);
-        UMAPB_CUDA(cudaMemcpyAsync(mb.data(), maxbits.get(), n_slots * 4, cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaStreamSynchronize(s));
-        std::vector<float> expansion(n_slots);
-        for (int64_t sl = 0; sl < n_slots; ++sl) {
-            float mx;
-            std::memcpy(&mx, &mb[sl], 4);
-            if (!std::isfinite(mx)) return res;
-            expansion[sl] = mx > 0.0f ? expand_target[sl] / mx : 1.0f;
-        }
-        DevBuf<float> dexp(n_slots, s), danch(n_slots * dim, s);
-        UMAPB_CUDA(cudaMemcpyAsync(dexp.get(), expansion.data(), n_slots * 4, cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemcpyAsync(danch.get(), slot_anchor.data(), n_slots * dim * 4,
-                                   cudaMemcpyHostToDevice, s));
-        finish_kernel<<<grid_for(cnt), 256, 0, s>>>(nodes.get(), cnt, slots.get(), dexp.get(),
-                                                    danch.get(), dnseed.get(), dim, kInitNoise, out);
-        UMAPB_LAUNCH_CHECK();
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        if (!ok) return res;
     }
     res.used_spectral = true;
     return res;
