@@ -1,14 +1,23 @@
-"""Benchmark: UMAP fit of 1,000,000 x 64 rows on B200 (one JSON line).
+"""Benchmark: UMAP fit of 1,000,000 x 64 rows on B200, and the learned
+transform surrogate against the plain transform (one JSON line).
 
-Workload: the 50-component anisotropic Gaussian mixture (seed 11, means
+Fit workload: the 50-component anisotropic Gaussian mixture (seed 11, means
 ~N(0, 5^2), per-dim std ~U(0.5, 2)), n_neighbors=15, exact kNN, spectral
 init, 200 SGD epochs, 2-D output.  One step = one complete fit.
 
   value   seconds per fit with the rows already resident in HBM
           (umapb_fit_transform_device), device-timed with CUDA events;
-  e2e     seconds per fit through the public API (Umap.fit_transform on a
-          host array): host->device copy of the rows and device->host copy
-          of the embedding inside the timed region.
+  e2e     seconds per fit through the public API (Umap.fit_transform) from
+          pinned host memory: host->device copy of the rows and
+          device->host copy of the embedding inside the timed region.
+
+Transform workload ("transform" object): fit 200,000 x 128 rows of a
+20-component mixture (means ~N(0, 4^2), unit variance, seed 5), train the
+surrogate (BF16 MLP 128-512-512-2, GELU, Adam 1e-3, batch 4096, 20 epochs),
+then embed 1,000,000 query rows of the same mixture (seed 6) through the
+surrogate with its gate and plain fallback, and through the plain transform
+(kNN to the training rows + SGD refine); rows/s device-resident and end to
+end from pinned host memory, trustworthiness@15 of both on 10,000 queries.
 
 --impl reference times the CPU restatement of the reference's path (the
 oracle) on the host cores: each step fits a 20,000-row sample of the same
@@ -37,6 +46,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "fit s @1M×64 TC vs FP32 kNN; transform rows/s MLP vs plain at equal trust@15"
 N_ROWS, N_DIM, K, EPOCHS = 1_000_000, 64, 15, 200
 SAMPLE_ROWS = 20_000
+T_FIT, T_QUERY, T_DIM = 200_000, 1_000_000, 128
+T_SAMPLE = 2_000  # queries of the CPU transform baseline
 
 
 def peaks() -> dict:
@@ -203,13 +214,15 @@ def run_gpu(args) -> None:
         torch.cuda.synchronize()
         return start.elapsed_time(stop) / 1000.0
 
+    x_pinned = torch.from_numpy(x).pin_memory().numpy()
+    out_pinned = torch.empty((N_ROWS, 2), dtype=torch.float32).pin_memory().numpy()
+
     def e2e_step() -> float:
-        host_out = np.empty((N_ROWS, 2), np.float32)
         start = torch.cuda.Event(enable_timing=True)
         stop = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         start.record()
-        model.fit_transform(x, out=host_out)
+        model.fit_transform(x_pinned, out=out_pinned)
         stop.record()
         torch.cuda.synchronize()
         return start.elapsed_time(stop) / 1000.0
@@ -246,6 +259,7 @@ def run_gpu(args) -> None:
     value = max_over_ranks(float(np.mean(dev_times)))
     e2e = max_over_ranks(float(np.mean(e2e_times)))
     emb = out_dev.cpu().numpy()
+    transform = None if args.skip_transform else transform_leg(args, lib, local)
 
     if rank == 0:
         pk = peaks()
@@ -316,6 +330,8 @@ def run_gpu(args) -> None:
             "quality": {k: round(v, 4) for k, v in q.items()},
             "clocks": sampler.summary(),
         }
+        if transform is not None:
+            line["transform"] = transform
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             v, st = cpu_reference_step(x[:SAMPLE_ROWS].copy(), threads)
@@ -330,6 +346,122 @@ def run_gpu(args) -> None:
         torch.distributed.destroy_process_group()
 
 
+def transform_leg(args, lib, device: int) -> dict:
+    """Surrogate transform against the plain transform on 1M queries."""
+    import torch
+
+    from umapers import Umap
+    from umapers_b200 import _lib, diagnostics, workloads
+
+    fit, query = workloads.transform_mixture(T_FIT, T_QUERY, T_DIM)
+    model = Umap(n_neighbors=K, random_seed=5, ann_mode="exact")
+    model.fit(fit)
+    t0 = time.perf_counter()
+    info = model.fit_surrogate()
+    train_wall = time.perf_counter() - t0
+    handle = model._core._handle
+    q_dev = torch.from_numpy(query).cuda()
+    out_sur = torch.empty((T_QUERY, 2), dtype=torch.float32, device="cuda")
+    out_plain = torch.empty_like(out_sur)
+    q_pinned = torch.from_numpy(query).pin_memory().numpy()
+    h_out = torch.empty((T_QUERY, 2), dtype=torch.float32).pin_memory().numpy()
+    n_fb = ctypes.c_int64(0)
+
+    def dev(surrogate: bool) -> float:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        if surrogate:
+            _lib.check(lib.umapb_surrogate_transform_device(
+                handle, q_dev.data_ptr(), T_QUERY, T_DIM, 1, out_sur.data_ptr(), None,
+                ctypes.byref(n_fb)))
+        else:
+            _lib.check(lib.umapb_transform_device(handle, q_dev.data_ptr(), T_QUERY, T_DIM,
+                                                  out_plain.data_ptr()))
+        stop.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop) / 1000.0
+
+    def e2e(surrogate: bool) -> float:
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        model.transform(q_pinned, out=h_out, method="surrogate" if surrogate else "plain")
+        stop.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(stop) / 1000.0
+
+    for _ in range(args.warmup):
+        dev(True)
+        dev(False)
+    launches0 = lib.umapb_kernel_launches()
+    sampler = ClockSampler(device)
+    with sampler:
+        t_sur = [dev(True) for _ in range(args.steps)]
+        sur_launches = (lib.umapb_kernel_launches() - launches0) // max(args.steps, 1)
+        t_plain = [dev(False) for _ in range(args.steps)]
+        e_sur = [e2e(True) for _ in range(args.steps)]
+        e_plain = [e2e(False) for _ in range(args.steps)]
+    ts, tp = float(np.mean(t_sur)), float(np.mean(t_plain))
+    es, ep = float(np.mean(e_sur)), float(np.mean(e_plain))
+    sur, plain = out_sur.cpu().numpy(), out_plain.cpu().numpy()
+    q_s = diagnostics.quality(query, sur, sample=10_000, seed=6)
+    q_p = diagnostics.quality(query, plain, sample=10_000, seed=6)
+    # per query row: standardise (read 128 f32), two hidden GEMMs, the head
+    # and the nearest-anchor GEMM of the gate
+    H, C = 512, int(info["n_anchors"])
+    flop_row = 2.0 * (T_DIM * H + H * H + H * 2 + T_DIM * C)
+    pk = peaks()
+    achieved = flop_row * T_QUERY / ts / 1e12
+    out = {
+        "metric": "transform rows/s, 1,000,000 queries (surrogate with gate + plain fallback)",
+        "value": round(T_QUERY / ts, 1),
+        "unit": "rows/s",
+        "higher_is_better": True,
+        "e2e": {"value": round(T_QUERY / es, 1), "unit": "rows/s",
+                "h2d_bytes_per_step": int(query.nbytes), "d2h_bytes_per_step": int(sur.nbytes)},
+        "plain": {"value": round(T_QUERY / tp, 1), "e2e": round(T_QUERY / ep, 1),
+                  "unit": "rows/s"},
+        "speedup_device": round(tp / ts, 2),
+        "speedup_e2e": round(ep / es, 2),
+        "fallback_rows": int(n_fb.value),
+        "quality": {"surrogate_trust15": round(q_s["trustworthiness"], 4),
+                    "plain_trust15": round(q_p["trustworthiness"], 4),
+                    "surrogate_knn_pres": round(q_s["knn_preservation"], 4),
+                    "plain_knn_pres": round(q_p["knn_preservation"], 4)},
+        "training": {"wall_s": round(train_wall, 3),
+                     **{k: (round(v, 4) if isinstance(v, float) else v) for k, v in info.items()}},
+        "gpu_launches": int(sur_launches),
+        "roofline": {
+            "kernel": "surrogate inference (standardise, 3 tcgen05 GEMMs, head, gate)",
+            "bound": "tensor", "achieved": round(achieved, 2), "peak": pk["bf16_tflops"],
+            "unit": "TFLOP/s", "frac": round(achieved / pk["bf16_tflops"], 4), "traffic": None,
+            "note": f"{flop_row:.0f} flop per row; peak = burst bf16 ({pk['source']})"},
+        "config": {"workload": f"fit {T_FIT} x {T_DIM} (20-component mixture, seed 5), "
+                               f"{T_QUERY} queries (seed 6), k={K}, 2-D",
+                   "surrogate": "MLP 128-512-512-2 GELU, BF16 GEMMs / FP32 master, Adam 1e-3, "
+                                "batch 4096, 20 epochs"},
+        "clocks": sampler.summary(),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle
+
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        a, b = model._core.ab_params
+        t0 = time.perf_counter()
+        oracle.transform(fit, model.embedding_, query[:T_SAMPLE], a, b, n_neighbors=K,
+                         n_epochs=30, random_seed=5)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {
+            "value": round(T_SAMPLE / dt, 1), "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": f"oracle plain transform of {T_SAMPLE} of the queries (30 epochs, the "
+                      f"count a 1M-row request uses) against the {T_FIT}-row fit"}
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -338,6 +470,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--knn-backend", default="auto", choices=["auto", "tensor", "plain"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-transform", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

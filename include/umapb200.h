@@ -299,6 +299,116 @@ int32_t umapb_optimize_layout(float* embedding, int64_t n_vertices, int64_t dim,
                               float learning_rate, int64_t negative_sample_rate,
                               float repulsion_strength, uint64_t seed);
 
+/* ---- learned transform surrogate ---------------------------------------- *
+ * No reference function: the reference's transform is UmapModel::transform_dense
+ * (rust_umap/src/lib.rs:1593-1685) and its learned model, ParametricUmapModel
+ * (rust_umap/src/parametric.rs:89-534), is a separate estimator that
+ * Umap.transform never uses.  Here a BF16 MLP n_cols -> hidden -> hidden ->
+ * n_components (GELU, FP32 master weights, Adam) is trained on the GPU on the
+ * fitted model's rows and embedding, with a loss of
+ *     mse_weight * |f(x_i) - e_i|^2
+ *   + edge_loss_weight * (UMAP cross-entropy of f(x_i) against the fitted
+ *                    positions of the row's fuzzy-graph neighbours, with
+ *                    negative samples),
+ * averaged over a batch.  Inputs are standardised per feature as in
+ * parametric.rs:634-707.  A held-out share of the rows calibrates a per-row
+ * gate: a query whose nearest anchor row (a seeded sample of the training
+ * rows) is farther than any training row assigned to it, or whose anchor cell
+ * showed held-out disagreement above `fallback_radius` too often, is
+ * recomputed by the plain transform (umapb_transform's path). */
+typedef struct umapb_surrogate_params {
+    int64_t hidden;           /* hidden width, multiple of 128 (512) */
+    int64_t epochs;           /* passes over the training rows (20) */
+    int64_t batch_size;       /* rows per Adam step, multiple of 128 (4096) */
+    float learning_rate;      /* Adam step size (1e-3; betas 0.9/0.999, eps 1e-8) */
+    float mse_weight;         /* weight of the squared error to the fitted embedding (1) */
+    float edge_loss_weight;   /* weight of the fuzzy-edge cross-entropy (0.1) */
+    int64_t negatives;        /* negative samples per row and step (5) */
+    float holdout_fraction;   /* share of rows held out for the gate (0.05) */
+    int64_t n_anchors;        /* anchor rows of the gate (256) */
+    float fallback_radius;    /* disagreement radius in embedding units; <= 0 picks 5% of
+                                 the embedding's 1%-99% extent */
+    float max_cell_failure;   /* a cell is trusted when at most this share of its held-out
+                                 rows fall outside the radius (0.1) */
+    uint64_t seed;            /* 0: the model's random_seed */
+} umapb_surrogate_params;
+
+typedef struct umapb_surrogate_info {
+    int64_t n_train;
+    int64_t n_holdout;
+    int64_t steps;
+    int64_t n_anchors;
+    int64_t cells_trusted;
+    double radius;                 /* the fallback radius used */
+    double train_sec;              /* GPU training, wall clock */
+    double calibrate_sec;          /* held-out check and gate tables */
+    double first_epoch_loss;
+    double final_epoch_loss;
+    double holdout_rmse;           /* root mean square of |f(x) - e| over the held-out rows */
+    double holdout_median_error;   /* median of |f(x) - e| over the held-out rows */
+    double holdout_within_radius;  /* share of held-out rows within the radius */
+    double holdout_gated;          /* share of held-out rows the gate sends to the plain path */
+} umapb_surrogate_info;
+
+void umapb_surrogate_params_default(umapb_surrogate_params* params);
+
+/* Trains the surrogate of a fitted model (after umapb_fit*).  `params` may be
+ * NULL (defaults), `info` may be NULL. */
+int32_t umapb_surrogate_fit(umapb_model* model, const umapb_surrogate_params* params,
+                            umapb_surrogate_info* info);
+
+/* 1 when the model holds a trained surrogate. */
+int32_t umapb_surrogate_ready(const umapb_model* model);
+
+/* Transform through the surrogate.  With `use_fallback` = 1, rows the gate
+ * rejects are recomputed by the plain transform; with 0 every row keeps the
+ * network's output.  `fallback` (may be NULL, n_rows bytes) receives 1 for
+ * each gated row; `n_fallback` (may be NULL) their count.  Host buffers. */
+int32_t umapb_surrogate_transform(umapb_model* model, const float* query, int64_t n_rows,
+                                  int64_t n_cols, int32_t use_fallback, float* out,
+                                  uint8_t* fallback, int64_t* n_fallback);
+/* The same on device pointers (`query`, `out`, `fallback`). */
+int32_t umapb_surrogate_transform_device(umapb_model* model, const float* query,
+                                         int64_t n_rows, int64_t n_cols, int32_t use_fallback,
+                                         float* out, uint8_t* fallback, int64_t* n_fallback);
+
+/* Mean training loss of each epoch of the last umapb_surrogate_fit;
+ * writes min(n, epochs) values and returns that count in *n_written. */
+int32_t umapb_surrogate_loss_history(const umapb_model* model, double* out, int64_t n,
+                                     int64_t* n_written);
+
+/* One forward and backward pass of the surrogate's network and loss on host
+ * buffers, with the GPU kernels training uses; it exists so the gradients
+ * can be checked against a CPU oracle.  `params` is the flat FP32 vector
+ * W1 (hidden x n_features), b1 (hidden), W2 (hidden x hidden), b2 (hidden),
+ * W3 (n_out x hidden), b3 (n_out); `grads` has the same layout.  Row p's
+ * edges are edge_tail/edge_weight[edge_ptr[p] .. edge_ptr[p + 1]), indices
+ * into `teacher` (n_teacher x n_out); its negatives are
+ * neg_tail[p * n_neg .. (p + 1) * n_neg). */
+typedef struct umapb_mlp_batch {
+    int64_t batch;            /* rows, multiple of 128 */
+    int64_t n_features;
+    int64_t hidden;           /* multiple of 128 */
+    int64_t n_out;            /* 1..4 */
+    const float* x;           /* batch x n_features, already standardised */
+    const float* targets;     /* batch x n_out */
+    const float* params;
+    const float* teacher;     /* n_teacher x n_out */
+    int64_t n_teacher;
+    const int64_t* edge_ptr;  /* batch + 1 */
+    const int32_t* edge_tail;
+    const float* edge_weight;
+    const int32_t* neg_tail;  /* batch x n_neg */
+    int64_t n_neg;
+    float a, b;               /* curve parameters of q = 1 / (1 + a d^(2b)) */
+    float mse_weight, edge_loss_weight;
+    float neg_scale;          /* repulsive weight per negative = neg_scale * sum of the row's
+                                 edge weights / n_neg */
+    const float* out_shift;   /* n_out: y = out_shift + out_scale * (W3 a2 + b3); NULL = 0 */
+    const float* out_scale;   /* n_out; NULL = 1 */
+} umapb_mlp_batch;
+int32_t umapb_mlp_grad(const umapb_mlp_batch* batch, float* grads, double* loss, float* y);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

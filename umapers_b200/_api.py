@@ -46,7 +46,11 @@ _PARAM_NAMES = (
     "target_weight",
     "target_n_neighbors",
     "knn_backend",
+    "transform_mode",
+    "surrogate_kwds",
 )
+
+_TRANSFORM_MODES = ("plain", "surrogate")
 
 _FITTED_ATTRS = (
     "embedding_",
@@ -57,6 +61,8 @@ _FITTED_ATTRS = (
     "rad_orig_",
     "rad_emb_",
     "knn_diagnostics_",
+    "surrogate_info_",
+    "transform_fallback_",
 )
 
 _METRIC_ALIASES = {
@@ -253,6 +259,8 @@ class Umap:
         target_weight: float = 0.5,
         target_n_neighbors: int | None = None,
         knn_backend: str = "auto",
+        transform_mode: str = "plain",
+        surrogate_kwds: dict[str, Any] | None = None,
     ) -> None:
         """Create a UMAP model.
 
@@ -285,6 +293,13 @@ class Umap:
         knn_backend:
             ``auto`` | ``tensor`` | ``plain``: how exact-kNN tiles are
             computed; every backend returns the same neighbours.
+        transform_mode:
+            ``plain`` (the reference's kNN + SGD transform) or ``surrogate``:
+            every fit also trains a BF16 MLP that maps rows straight to the
+            embedding, and ``transform`` uses it, sending the rows its gate
+            rejects to the plain transform.
+        surrogate_kwds:
+            Options of the surrogate (see ``UmapCore.fit_surrogate``).
         """
         for attr in _FITTED_ATTRS:
             if hasattr(self, attr):
@@ -322,6 +337,10 @@ class Umap:
         )
         self.output_dens = bool(output_dens)
         self.knn_backend = str(knn_backend)
+        if transform_mode not in _TRANSFORM_MODES:
+            raise ValueError(f"transform_mode must be one of {_TRANSFORM_MODES}")
+        self.transform_mode = str(transform_mode)
+        self.surrogate_kwds = None if surrogate_kwds is None else dict(surrogate_kwds)
         self._core = UmapCore(
             n_neighbors=self.n_neighbors,
             n_components=self.n_components,
@@ -370,6 +389,15 @@ class Umap:
         self.embedding_ = embedding
         self.n_features_in_ = int(n_features)
         self.n_samples_fit_ = int(n_samples)
+        if self.transform_mode == "surrogate":
+            self.fit_surrogate(**(self.surrogate_kwds or {}))
+
+    def fit_surrogate(self, **options: Any) -> dict[str, Any]:
+        """Train the learned transform surrogate of the fitted model and
+        return its training / held-out summary (also kept as
+        ``surrogate_info_``)."""
+        self.surrogate_info_ = self._core.fit_surrogate(**options)
+        return self.surrogate_info_
 
     def _reject_unsupported(self, data: Any, y: Any) -> None:
         if _is_sparse(data):
@@ -505,7 +533,8 @@ class Umap:
         return diag
 
     # ---------------------------------------------------------- transform
-    def transform(self, query: Any, *, out: np.ndarray | None = None) -> np.ndarray:
+    def transform(self, query: Any, *, out: np.ndarray | None = None,
+                  method: str | None = None) -> np.ndarray:
         """Place new samples in the fitted embedding.
 
         Parameters
@@ -514,6 +543,10 @@ class Umap:
             Dense input ``(n_samples, n_features)``.
         out:
             Optional writable ``float32`` buffer ``(n_samples, n_components)``.
+        method:
+            ``plain`` | ``surrogate``; default ``transform_mode``.  With the
+            surrogate, ``transform_fallback_`` records which rows the gate
+            sent to the plain transform.
 
         Returns
         -------
@@ -523,6 +556,17 @@ class Umap:
         if _is_sparse(query):
             raise ValueError("sparse CSR input is not supported by the B200 engine (dense float32 only)")
         arr = _f32_matrix(query, "query")
+        method = self.transform_mode if method is None else method
+        if method not in _TRANSFORM_MODES:
+            raise ValueError(f"method must be one of {_TRANSFORM_MODES}")
+        if method == "surrogate":
+            emb, flags = self._core.transform_surrogate(arr, use_fallback=True)
+            self.transform_fallback_ = flags
+            if out is None:
+                return emb
+            buf = _out_buffer(out, (arr.shape[0], self.n_components))
+            buf[...] = emb
+            return buf
         if out is None:
             return self._core.transform(arr)
         buf = _out_buffer(out, (arr.shape[0], self.n_components))

@@ -112,6 +112,77 @@ class FitInfo(ctypes.Structure):
     ]
 
 
+class SurrogateParams(ctypes.Structure):
+    """umapb_surrogate_params."""
+
+    _fields_ = [
+        ("hidden", ctypes.c_int64),
+        ("epochs", ctypes.c_int64),
+        ("batch_size", ctypes.c_int64),
+        ("learning_rate", ctypes.c_float),
+        ("mse_weight", ctypes.c_float),
+        ("edge_loss_weight", ctypes.c_float),
+        ("negatives", ctypes.c_int64),
+        ("holdout_fraction", ctypes.c_float),
+        ("n_anchors", ctypes.c_int64),
+        ("fallback_radius", ctypes.c_float),
+        ("max_cell_failure", ctypes.c_float),
+        ("seed", ctypes.c_uint64),
+    ]
+
+
+SURROGATE_INFO_FIELDS = (
+    ("n_train", ctypes.c_int64),
+    ("n_holdout", ctypes.c_int64),
+    ("steps", ctypes.c_int64),
+    ("n_anchors", ctypes.c_int64),
+    ("cells_trusted", ctypes.c_int64),
+    ("radius", ctypes.c_double),
+    ("train_sec", ctypes.c_double),
+    ("calibrate_sec", ctypes.c_double),
+    ("first_epoch_loss", ctypes.c_double),
+    ("final_epoch_loss", ctypes.c_double),
+    ("holdout_rmse", ctypes.c_double),
+    ("holdout_median_error", ctypes.c_double),
+    ("holdout_within_radius", ctypes.c_double),
+    ("holdout_gated", ctypes.c_double),
+)
+
+
+class SurrogateInfo(ctypes.Structure):
+    """umapb_surrogate_info."""
+
+    _fields_ = list(SURROGATE_INFO_FIELDS)
+
+
+class MlpBatch(ctypes.Structure):
+    """umapb_mlp_batch."""
+
+    _fields_ = [
+        ("batch", ctypes.c_int64),
+        ("n_features", ctypes.c_int64),
+        ("hidden", ctypes.c_int64),
+        ("n_out", ctypes.c_int64),
+        ("x", ctypes.c_void_p),
+        ("targets", ctypes.c_void_p),
+        ("params", ctypes.c_void_p),
+        ("teacher", ctypes.c_void_p),
+        ("n_teacher", ctypes.c_int64),
+        ("edge_ptr", ctypes.c_void_p),
+        ("edge_tail", ctypes.c_void_p),
+        ("edge_weight", ctypes.c_void_p),
+        ("neg_tail", ctypes.c_void_p),
+        ("n_neg", ctypes.c_int64),
+        ("a", ctypes.c_float),
+        ("b", ctypes.c_float),
+        ("mse_weight", ctypes.c_float),
+        ("edge_loss_weight", ctypes.c_float),
+        ("neg_scale", ctypes.c_float),
+        ("out_shift", ctypes.c_void_p),
+        ("out_scale", ctypes.c_void_p),
+    ]
+
+
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _i32p = ctypes.POINTER(ctypes.c_int32)
@@ -171,6 +242,16 @@ SIGNATURES = {
         _i32,
         [_vp, _i64, _i64, _vp, _vp, _vp, _i64, _i64, _f32, _f32, _f32, _i64, _f32, _u64],
     ),
+    "umapb_surrogate_params_default": (None, [ctypes.POINTER(SurrogateParams)]),
+    "umapb_surrogate_fit": (
+        _i32,
+        [_vp, ctypes.POINTER(SurrogateParams), ctypes.POINTER(SurrogateInfo)],
+    ),
+    "umapb_surrogate_ready": (_i32, [_vp]),
+    "umapb_surrogate_transform": (_i32, [_vp, _vp, _i64, _i64, _i32, _vp, _vp, _i64p]),
+    "umapb_surrogate_transform_device": (_i32, [_vp, _vp, _i64, _i64, _i32, _vp, _vp, _i64p]),
+    "umapb_surrogate_loss_history": (_i32, [_vp, _vp, _i64, _i64p]),
+    "umapb_mlp_grad": (_i32, [ctypes.POINTER(MlpBatch), _vp, _vp, _vp]),
 }
 
 _LIB: ctypes.CDLL | None = None

@@ -300,6 +300,54 @@ class UmapCore:
             )
         )
 
+    # ------------------------------------------------- learned surrogate
+    # No reference counterpart (the reference's ParametricUmapCore is a
+    # separate estimator): a BF16 MLP trained on this model's fit maps rows
+    # straight to the embedding; rows its gate rejects take the plain path.
+    def fit_surrogate(self, **options: Any) -> dict[str, Any]:
+        """Train the transform surrogate of the fitted model.  Keyword options
+        are the fields of ``umapb_surrogate_params`` (hidden, epochs,
+        batch_size, learning_rate, mse_weight, edge_loss_weight, negatives,
+        holdout_fraction, n_anchors, fallback_radius, max_cell_failure, seed).
+        Returns the training and calibration summary."""
+        prm = _lib.SurrogateParams()
+        self._lib.umapb_surrogate_params_default(ctypes.byref(prm))
+        names = {f[0] for f in _lib.SurrogateParams._fields_}
+        for key, value in options.items():
+            if key not in names:
+                raise ValueError(f"unknown surrogate option: {key}")
+            setattr(prm, key, value)
+        info = _lib.SurrogateInfo()
+        _lib.check(self._lib.umapb_surrogate_fit(self._handle, ctypes.byref(prm),
+                                                 ctypes.byref(info)))
+        return {name: getattr(info, name) for name, _ in _lib.SURROGATE_INFO_FIELDS}
+
+    @property
+    def surrogate_ready(self) -> bool:
+        return bool(self._lib.umapb_surrogate_ready(self._handle))
+
+    def transform_surrogate(self, query: Any, use_fallback: bool = True
+                            ) -> tuple[np.ndarray, np.ndarray]:
+        """Embedding of new rows through the surrogate and, per row, whether
+        the gate sent it to the plain transform (recomputed there when
+        ``use_fallback``)."""
+        arr = _matrix(query, "query")
+        out = np.empty((arr.shape[0], self.n_components), dtype=np.float32)
+        flags = np.empty(arr.shape[0], dtype=np.uint8)
+        n_fb = ctypes.c_int64(0)
+        _lib.check(self._lib.umapb_surrogate_transform(
+            self._handle, _lib.ptr(arr), arr.shape[0], arr.shape[1], 1 if use_fallback else 0,
+            _lib.ptr(out), _lib.ptr(flags), ctypes.byref(n_fb)))
+        return out, flags.astype(bool)
+
+    def surrogate_loss_history(self) -> np.ndarray:
+        """Mean training loss of each epoch of the last fit_surrogate."""
+        buf = np.empty(4096, dtype=np.float64)
+        n = ctypes.c_int64(0)
+        _lib.check(self._lib.umapb_surrogate_loss_history(self._handle, _lib.ptr(buf), buf.size,
+                                                          ctypes.byref(n)))
+        return buf[: n.value].copy()
+
     def transform_sparse_csr(self, *args: Any, **kwargs: Any) -> np.ndarray:
         raise ValueError(_SPARSE_MSG)
 

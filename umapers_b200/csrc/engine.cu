@@ -223,6 +223,9 @@ struct umapb_model {
     int64_t n_fit = 0, d_fit = 0;
     DevBuf<float> X;    // training rows, n_fit x d_fit
     DevBuf<float> emb;  // fitted embedding, n_fit x n_components
+    Graph graph;        // the fit's fuzzy graph (CSR by head), the surrogate's edge loss
+    SurrogatePtr surrogate;
+    std::vector<double> surrogate_loss;
 
     void ensure_device() {
         if (stream) {
@@ -339,6 +342,10 @@ void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const i
         out->info.n_epochs = n_epochs;
     }
     m->emb = std::move(emb);
+    g.heads.release();
+    m->graph = std::move(g);
+    m->surrogate.reset();
+    m->surrogate_loss.clear();
 }
 
 // Full dense fit on device-resident rows `Xd` (owned copy is taken).
@@ -454,13 +461,17 @@ void trim_precomputed(const int64_t* idx, const float* dist, int64_t n, int64_t 
     }
 }
 
-void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out_dev) {
+// transform_dense (lib.rs:1593-1685) on device rows.  The default epoch
+// count follows the size of the whole request, `epoch_rows` (lib.rs:1650-1657).
+void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out_dev,
+                      int64_t epoch_rows = -1) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int dim = static_cast<int>(p.n_components);
     const int k = static_cast<int>(std::min<int64_t>(p.n_neighbors, m->n_fit));
+    if (epoch_rows < 0) epoch_rows = nq;
     const int64_t n_epochs = p.n_epochs >= 0 ? std::max<int64_t>(p.n_epochs, 1)
-                                             : (nq <= 10000 ? 100 : 30);
+                                             : (epoch_rows <= 10000 ? 100 : 30);
     DevBuf<int32_t> idx(nq * k, s);
     DevBuf<float> dist(nq * k, s);
     knn_exact_device(Qd, nq, m->X.get(), m->n_fit, static_cast<int>(d), k, p.metric,
@@ -473,6 +484,39 @@ void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, fl
     transform_layout(out_dev, nq, dim, m->emb.get(), m->n_fit, g, n_epochs, m->a, m->b,
                      p.learning_rate / 4.0f, p.negative_sample_rate, p.repulsion_strength,
                      p.random_seed ^ 0xA24BAED40B53C117ULL, s);
+}
+
+// Surrogate transform of device rows: network outputs for every row, then
+// (use_fallback) the plain transform for the rows the gate rejects.
+void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d,
+                                bool use_fallback, float* out, uint8_t* flags_out,
+                                int64_t* n_fallback) {
+    cudaStream_t s = m->stream;
+    const int dim = static_cast<int>(m->p.n_components);
+    DevBuf<uint8_t> own;
+    uint8_t* flags = flags_out;
+    if (!flags) {
+        own.alloc(nq, s);
+        flags = own.get();
+    }
+    const int64_t nf = surrogate_infer(*m->surrogate, Qd, nq, static_cast<int>(d), out, flags, s);
+    if (n_fallback) *n_fallback = nf;
+    if (!use_fallback || nf == 0) return;
+    DevBuf<int32_t> ids(nf, s);
+    select_flagged(flags, nq, ids.get(), s);
+    DevBuf<float> sub(nf * d, s), sub_out(nf * dim, s);
+    gather_rows(Qd, ids.get(), nf, static_cast<int>(d), sub.get(), s);
+    transform_device(m, sub.get(), nf, d, sub_out.get(), nq);
+    scatter_rows(sub_out.get(), ids.get(), nf, dim, out, s);
+}
+
+void check_surrogate_query(umapb_model* m, int64_t n_cols) {
+    if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+    if (!m->surrogate) throw Error(UMAPB_ERR_NOT_FITTED, "the transform surrogate is not trained");
+    if (n_cols != m->d_fit)
+        throw Error(UMAPB_ERR_FEATURE_MISMATCH, "feature mismatch: expected " +
+                                                    std::to_string(m->d_fit) + ", got " +
+                                                    std::to_string(n_cols));
 }
 
 // transform_rows checks (lib.rs:1608-1643)
@@ -539,6 +583,8 @@ void umapb_destroy(umapb_model* m) {
         std::lock_guard<std::mutex> lk(m->mu);
         if (m->stream) {
             cudaSetDevice(m->device);
+            m->surrogate.reset();
+            m->graph = Graph();
             m->X.release();
             m->emb.release();
             cudaStreamSynchronize(m->stream);
@@ -681,14 +727,13 @@ int32_t umapb_transform(umapb_model* m, const float* query, int64_t n_rows, int6
             throw Error(UMAPB_ERR_FEATURE_MISMATCH,
                         "feature mismatch: expected " + std::to_string(m->d_fit) + ", got " +
                             std::to_string(n_cols));
-        for (int64_t r = 0; r < n_rows; ++r)
-            for (int64_t c = 0; c < n_cols; ++c)
-                if (!std::isfinite(query[r * n_cols + c]))
-                    invalid("input contains non-finite value at row " + std::to_string(r));
         m->ensure_device();
         cudaStream_t s = m->stream;
         DevBuf<float> Q, outd(n_rows * m->p.n_components, s);
         upload(Q, query, n_rows * n_cols, s);
+        // the finiteness scan of transform_rows (lib.rs:1630-1640) runs on the uploaded rows
+        const int64_t bad = first_nonfinite_row(Q.get(), n_rows, static_cast<int>(n_cols), s);
+        if (bad != INT64_MAX) invalid("input contains non-finite value at row " + std::to_string(bad));
         transform_device(m, Q.get(), n_rows, n_cols, outd.get());
         UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * m->p.n_components * 4,
                                    cudaMemcpyDeviceToHost, s));
@@ -943,6 +988,113 @@ int32_t umapb_optimize_layout(float* embedding, int64_t n, int64_t dim, const in
                         negative_sample_rate, repulsion_strength, seed, false, nullptr, ss.s);
         UMAPB_CUDA(cudaMemcpyAsync(embedding, emb.get(), n * dim * 4, cudaMemcpyDeviceToHost, ss.s));
         UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+    });
+}
+
+// ------------------------------------------------------------ surrogate
+void umapb_surrogate_params_default(umapb_surrogate_params* p) {
+    if (!p) return;
+    p->hidden = 512;
+    p->epochs = 20;
+    p->batch_size = 4096;
+    p->learning_rate = 1e-3f;
+    p->mse_weight = 1.0f;
+    p->edge_loss_weight = 0.1f;
+    p->negatives = 5;
+    p->holdout_fraction = 0.05f;
+    p->n_anchors = 256;
+    p->fallback_radius = 0.0f;
+    p->max_cell_failure = 0.1f;
+    p->seed = 0;
+}
+
+int32_t umapb_surrogate_fit(umapb_model* m, const umapb_surrogate_params* params,
+                            umapb_surrogate_info* info) {
+    return guarded([&] {
+        if (!m) invalid("null model");
+        std::lock_guard<std::mutex> lk(m->mu);
+        if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        if (!m->X.get() || !m->graph.row_ptr.get())
+            invalid("the surrogate needs a model fitted on rows (not a stateless fit)");
+        umapb_surrogate_params p;
+        umapb_surrogate_params_default(&p);
+        if (params) p = *params;
+        m->ensure_device();
+        const uint64_t seed = p.seed != 0 ? p.seed : (m->p.random_seed ^ 0x51A7E5EEDull);
+        umapb_surrogate_info local{};
+        m->surrogate.reset();
+        m->surrogate = surrogate_train(m->X.get(), m->n_fit, static_cast<int>(m->d_fit),
+                                       m->emb.get(), static_cast<int>(m->p.n_components),
+                                       m->graph, m->a, m->b, m->p.negative_sample_rate, p, seed,
+                                       &local, &m->surrogate_loss, m->stream);
+        if (info) *info = local;
+    });
+}
+
+int32_t umapb_surrogate_ready(const umapb_model* m) { return (m && m->surrogate) ? 1 : 0; }
+
+int32_t umapb_surrogate_transform(umapb_model* m, const float* query, int64_t n_rows,
+                                  int64_t n_cols, int32_t use_fallback, float* out,
+                                  uint8_t* fallback, int64_t* n_fallback) {
+    return guarded([&] {
+        if (!m) invalid("null model");
+        std::lock_guard<std::mutex> lk(m->mu);
+        check_surrogate_query(m, n_cols);
+        if (n_fallback) *n_fallback = 0;
+        if (n_rows == 0) return;
+        m->ensure_device();
+        cudaStream_t s = m->stream;
+        const int64_t dim = m->p.n_components;
+        DevBuf<float> Q, outd(n_rows * dim, s);
+        DevBuf<uint8_t> fl(n_rows, s);
+        upload(Q, query, n_rows * n_cols, s);
+        const int64_t bad = first_nonfinite_row(Q.get(), n_rows, static_cast<int>(n_cols), s);
+        if (bad != INT64_MAX) invalid("input contains non-finite value at row " + std::to_string(bad));
+        surrogate_transform_device(m, Q.get(), n_rows, n_cols, use_fallback != 0, outd.get(),
+                                   fl.get(), n_fallback);
+        UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * dim * 4, cudaMemcpyDeviceToHost, s));
+        if (fallback)
+            UMAPB_CUDA(cudaMemcpyAsync(fallback, fl.get(), n_rows, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int32_t umapb_surrogate_transform_device(umapb_model* m, const float* query, int64_t n_rows,
+                                         int64_t n_cols, int32_t use_fallback, float* out,
+                                         uint8_t* fallback, int64_t* n_fallback) {
+    return guarded([&] {
+        if (!m) invalid("null model");
+        std::lock_guard<std::mutex> lk(m->mu);
+        check_surrogate_query(m, n_cols);
+        if (n_fallback) *n_fallback = 0;
+        if (n_rows == 0) return;
+        m->ensure_device();
+        const int64_t bad =
+            first_nonfinite_row(query, n_rows, static_cast<int>(n_cols), m->stream);
+        if (bad != INT64_MAX)
+            invalid("input contains non-finite value at row " + std::to_string(bad));
+        surrogate_transform_device(m, query, n_rows, n_cols, use_fallback != 0, out, fallback,
+                                   n_fallback);
+        UMAPB_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+int32_t umapb_surrogate_loss_history(const umapb_model* m, double* out, int64_t n,
+                                     int64_t* n_written) {
+    return guarded([&] {
+        if (!m) invalid("null model");
+        if (!m->surrogate) throw Error(UMAPB_ERR_NOT_FITTED, "the transform surrogate is not trained");
+        const int64_t cnt = std::min<int64_t>(n, static_cast<int64_t>(m->surrogate_loss.size()));
+        for (int64_t i = 0; i < cnt; ++i) out[i] = m->surrogate_loss[i];
+        if (n_written) *n_written = cnt;
+    });
+}
+
+int32_t umapb_mlp_grad(const umapb_mlp_batch* batch, float* grads, double* loss, float* y) {
+    return guarded([&] {
+        if (!batch || !grads) invalid("null argument");
+        ScopedStream ss;
+        mlp_grad(*batch, grads, loss, y, ss.s);
     });
 }
 

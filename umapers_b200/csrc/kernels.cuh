@@ -1,9 +1,11 @@
 // kernels.cuh - internal launcher API shared by the engine and the kernels.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -43,6 +45,45 @@ bool knn_tc_supported(int d, int k, int metric);
 // certified are recomputed by knn_plain.  Q may equal R (self join).
 void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int k, int metric,
             int32_t* out_idx, float* out_dist, TcKnnStats* stats, cudaStream_t s);
+
+// ------------------------------------------------------------ gemm_tc.cu
+// C[M x N] = A[M x K] B[N x K]^T on tcgen05 tensor cores: BF16 operands
+// (row-major, K contiguous, K % 64 == 0, 16-byte aligned), FP32 accumulation
+// in TMEM, one 128 x 128 output tile per CTA, and a fused epilogue.
+enum GemmEpilogue : int {
+    kEpiF32 = 0,           // c = A B^T                                 (fp32, ld N)
+    kEpiBiasGelu = 1,      // z = A B^T + bias (fp32, optional); act = bf16(gelu(z)); act_t
+    kEpiGeluBwd = 2,       // act = bf16((A B^T) * gelu'(z_in)); act_t
+    kEpiBiasGeluHead = 3,  // kEpiBiasGelu, plus head_part[tile][row][o] = sum over the tile's
+                           // columns n of act[row][n] * head_w[o][n]
+    kEpiRowMin = 4,        // per row and column tile: min over columns n < n_valid of
+                           // col_sq[n] - 2 (A B^T)[row][n], and its n
+};
+constexpr int kGemmMaxHead = 4;
+
+struct GemmOut {
+    const float* bias = nullptr;           // [N]
+    const float* z_in = nullptr;           // kEpiGeluBwd: [M x N] pre-activation
+    float* c = nullptr;                    // kEpiF32: [M x N]
+    float* z = nullptr;                    // optional pre-activation output [M x N]
+    __nv_bfloat16* act = nullptr;          // optional [M x N]
+    __nv_bfloat16* act_t = nullptr;        // optional transposed output [N x ld_t]
+    int64_t ld_t = 0;
+    const float* head_w = nullptr;         // kEpiBiasGeluHead: [head_dim x N]
+    int head_dim = 0;
+    float* head_part = nullptr;            // [N / 128][M][head_dim]
+    const float* col_sq = nullptr;         // kEpiRowMin: [n_valid]
+    int64_t n_valid = 0;
+    float* min_val = nullptr;              // kEpiRowMin: [ceil(N / 128)][M]
+    int32_t* min_idx = nullptr;
+};
+
+void gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int64_t M, int64_t N, int64_t K,
+                  int epilogue, const GemmOut& out, cudaStream_t s);
+
+// Reads and clears the device error word the GEMM kernels set when a
+// bounded wait runs out (0 = no error since the last call).
+int gemm_take_error(cudaStream_t s);
 
 // ---------------------------------------------------------- nndescent.cu
 int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t candidate_pool,
@@ -108,6 +149,39 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
 void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_t n_base,
                       const Graph& g, int64_t n_epochs, float a, float b, float lr,
                       int64_t neg_rate, float repulsion, uint64_t seed, cudaStream_t s);
+
+// --------------------------------------------------------- surrogate.cu
+struct Surrogate;
+struct SurrogateDeleter {
+    void operator()(Surrogate* s) const;
+};
+using SurrogatePtr = std::unique_ptr<Surrogate, SurrogateDeleter>;
+
+// Trains the transform surrogate on fitted rows X (n x d, device), their
+// embedding `emb` (n x dim, device) and the fit's fuzzy graph `g` (CSR by
+// head); calibrates its gate on the held-out rows.
+SurrogatePtr surrogate_train(const float* X, int64_t n, int d, const float* emb, int dim,
+                             const Graph& g, float a, float b, int64_t neg_rate,
+                             const umapb_surrogate_params& p, uint64_t seed,
+                             umapb_surrogate_info* info, std::vector<double>* history,
+                             cudaStream_t s);
+
+// Network outputs of nq query rows (device) into out (nq x dim); `flags`
+// (nullable) receives 1 for each row the gate rejects.  Returns the number of
+// rejected rows (0 when flags is null).
+int64_t surrogate_infer(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
+                        uint8_t* flags, cudaStream_t s);
+
+// dst[r] = src[ids[r]] and dst[ids[r]] = src[r] for rows of d floats.
+void gather_rows(const float* src, const int32_t* ids, int64_t n, int d, float* dst,
+                 cudaStream_t s);
+void scatter_rows(const float* src, const int32_t* ids, int64_t n, int d, float* dst,
+                  cudaStream_t s);
+// Ascending indices of the non-zero flags; returns their count.
+int64_t select_flagged(const uint8_t* flags, int64_t n, int32_t* ids, cudaStream_t s);
+
+// umapb_mlp_grad on host buffers.
+void mlp_grad(const umapb_mlp_batch& mb, float* grads, double* loss, float* y, cudaStream_t s);
 
 // ------------------------------------------------------------ engine.cu
 // Records the message umapb_last_error() returns on this thread.

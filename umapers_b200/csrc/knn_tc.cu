@@ -37,17 +37,20 @@
 #include <mutex>
 
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 
 namespace umapb {
 namespace {
 
+using namespace tc;
+
 constexpr int BM = 128;     // query rows per tile (UMMA M)
 constexpr int BN = 128;     // candidate rows per tile (UMMA N)
-constexpr int BK = 64;      // bf16 columns per k-block (one 128-byte swizzle row)
-constexpr int UK = 16;      // K of one tcgen05.mma kind::f16
+constexpr int BK = kBK;     // bf16 columns per k-block (one 128-byte swizzle row)
+constexpr int UK = kUK;     // K of one tcgen05.mma kind::f16
 constexpr int S = 32;       // shortlist length per row
 constexpr int kTileBytes = BM * BK * 2;  // 16 KiB
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
+constexpr uint32_t kIdesc = idesc_bf16(BM, BN);
 
 // Bound constants (see header comment).  c1 covers the split products
 // (2 * 3.02 * 2^-16) with 2% slack for the BF16 rounding of the bound term;
@@ -57,131 +60,6 @@ constexpr double kBoundC1 = 1.02 * 2.0 * 3.02 / 65536.0;
 
 inline int padded_k(int d) { return ((3 * d + 7 + BK - 1) / BK) * BK; }
 inline double bound_c2(int d) { return (padded_k(d) + d + 8) * std::ldexp(1.0, -22); }
-
-// ---------------------------------------------------------------- PTX ----
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred P1;\n mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n"
-        " selp.b32 %0, 1, 0, P1;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// try_wait with a suspend-time hint: the thread sleeps in hardware until the
-// phase completes or the hint elapses, instead of spinning on issue slots.
-__device__ __forceinline__ bool mbar_try_suspend(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred P1;\n mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n"
-        " selp.b32 %0, 1, 0, P1;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity), "r"(hint_ns)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: false after kWaitNs or when another role aborted.  Each try
-// suspends for at most 1 ms, so the deadline and the abort flag are checked
-// at least that often.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-    if (mbar_try(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    while (true) {
-        if (mbar_try_suspend(bar, parity, 1000000u)) return true;
-        if (*abort_flag) return false;
-        if (global_ns() - t0 > kWaitNs) return false;
-    }
-}
-
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
-                                            int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
-
-// K-major SWIZZLE_128B operand descriptor: LBO = 16 B, SBO = 1024 B (8 rows of
-// 128 B), descriptor version 1, layout type 2.
-__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
-    uint64_t d = static_cast<uint64_t>((saddr & 0x3FFFF) >> 4);
-    d |= static_cast<uint64_t>(1) << 16;
-    d |= static_cast<uint64_t>(1024 >> 4) << 32;
-    d |= static_cast<uint64_t>(1) << 46;
-    d |= static_cast<uint64_t>(2) << 61;
-    return d;
-}
-
-// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
-// K-major, N = BN, M = BM.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
-                            (static_cast<uint32_t>(BN >> 3) << 17) |
-                            (static_cast<uint32_t>(BM >> 4) << 24);
-
-__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
-        : "memory");
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-    asm volatile(
-        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-        : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-#define UMAPB_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), \
-                    "=r"(r[i + 4]), "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
-
-// 32 consecutive FP32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-        "%28, %29, %30, %31}, [%32];"
-        : UMAPB_R8(0), UMAPB_R8(8), UMAPB_R8(16), UMAPB_R8(24)
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait_ld() {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
 
 // order-preserving map of a float to uint32 (negative values included)
 __device__ __forceinline__ uint32_t f2o(float f) {
@@ -255,15 +133,11 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(tmem_holder)),
-                     "r"(kTmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tmem_alloc(smem_u32(tmem_holder), kTmemCols);
     }
-    tc_fence_before();
+    fence_before();
     __syncthreads();
-    tc_fence_after();
+    fence_after();
     const uint32_t tmem_base = *tmem_holder;
 
     auto fail = [&](int code) {
@@ -317,7 +191,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                     fail(3);
                     break;
                 }
-                tc_fence_after();
+                fence_after();
                 for (int64_t c = 0; c < p.n_ctiles && ok; ++c, ++cg) {
                     const uint32_t buf = static_cast<uint32_t>(cg & 1);
                     if (!mbar_wait(b_tempty + 8 * buf, static_cast<uint32_t>(((cg >> 1) & 1) ^ 1),
@@ -326,7 +200,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                         ok = false;
                         break;
                     }
-                    tc_fence_after();
+                    fence_after();
                     const uint32_t dcol = tmem_base + buf * (MT * BN);
                     for (int kb = 0; kb < KB; ++kb, ++it) {
                         const int stage = static_cast<int>(it % ST);
@@ -336,7 +210,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                             ok = false;
                             break;
                         }
-                        tc_fence_after();
+                        fence_after();
                         const uint64_t db0 = desc_sw128(sB + stage * kTileBytes);
                         // the columns past 3d + 7 are zero: their k-steps are skipped
                         const int n_ks = kb == KB - 1 ? p.ks_last : BK / UK;
@@ -346,7 +220,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                             for (int mt = 0; mt < MT; ++mt) {
                                 const uint64_t da =
                                     desc_sw128(sA + (mt * KB + kb) * kTileBytes) + 2 * ks;
-                                umma_f16(dcol + mt * BN, da, db0 + 2 * ks,
+                                umma_bf16(dcol + mt * BN, da, db0 + 2 * ks, kIdesc,
                                          (kb | ks) != 0 ? 1u : 0u);
                             }
                         }
@@ -381,7 +255,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                     ok = false;
                     break;
                 }
-                tc_fence_after();
+                fence_after();
                 const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
                                        buf * (MT * BN) + mt * BN;
                 uint32_t r[4][32];
@@ -389,7 +263,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                 for (int ch = 0; ch < 4; ++ch) tmem_ld32(taddr + ch * 32, r[ch]);
                 tmem_wait_ld();
                 // the accumulator buffer can be overwritten as soon as it is in registers
-                tc_fence_before();
+                fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
                 float m = __uint_as_float(r[0][0]);
@@ -460,13 +334,11 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
         while (global_ns() - t0 < 2000000ull) {
         }
     }
-    tc_fence_before();
+    fence_before();
     __syncthreads();
     if (warp == 1) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                     "r"(kTmemCols)
-                     : "memory");
+        fence_after();
+        tmem_dealloc(tmem_base, kTmemCols);
     }
 }
 
@@ -604,38 +476,8 @@ __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restri
 }
 
 // --------------------------------------------------------------- host ----
-using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeFn encoder() {
-    static EncodeFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeFn>(p);
-    });
-    if (!fn) throw Error(UMAPB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
-    return fn;
-}
-
 CUtensorMap make_map(const void* base, int64_t rows, int kp) {
-    CUtensorMap m;
-    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(kp), static_cast<cuuint64_t>(rows)};
-    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(kp) * 2};
-    const cuuint32_t box[2] = {BK, BM};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base),
-                                 dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) throw Error(UMAPB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    return m;
+    return make_bf16_map(base, rows, kp, BM);
 }
 
 int query_tiles_for(int kb) { return kb <= 4 ? 2 : (kb <= 10 ? 1 : 0); }
@@ -662,11 +504,7 @@ bool knn_tc_supported(int d, int k, int metric) {
     if (metric != UMAPB_METRIC_EUCLIDEAN) return false;
     if (k < 1 || k > S - 2 || d < 1) return false;
     if (query_tiles_for(padded_k(d) / BK) == 0) return false;
-    int dev = 0, major = 0, minor = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return false;
-    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
-    return major == 10 && minor == 0;
+    return device_is_sm100();
 }
 
 void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int k, int metric,

@@ -17,6 +17,8 @@
 // per-query closure does.
 #include <cfloat>
 
+#include <vector>
+
 #include "kernels.cuh"
 
 namespace umapb {
@@ -64,8 +66,20 @@ struct SgdArgs {
     float neg_rate_f;
     uint64_t seed;
     uint64_t epoch;
-    unsigned long long* samples;
+    uint32_t* block_samples;  // (nullable) per-block count of attractive samples, all epochs
 };
+
+// Adds this block's sampled-edge count to its own slot: shared-memory
+// atomics inside the block, one plain store per block, no global atomics.
+__device__ __forceinline__ void count_block_samples(uint32_t* slots, bool sampled) {
+    __shared__ uint32_t cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    const unsigned ballot = __ballot_sync(0xffffffffu, sampled);
+    if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&cnt, static_cast<uint32_t>(__popc(ballot)));
+    __syncthreads();
+    if (threadIdx.x == 0) slots[blockIdx.x] += cnt;
+}
 
 // One epoch for dim == 2 (the reference's flat fast path, lib.rs:5172-5244).
 __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
@@ -127,11 +141,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
             if (hy != h0.y) atomicAdd(&p.emb[2 * head + 1], __fsub_rn(hy, h0.y));
         }
     }
-    if (p.samples) {
-        const unsigned ballot = __ballot_sync(0xffffffffu, sampled);
-        if ((threadIdx.x & 31) == 0 && ballot)
-            atomicAdd(p.samples, static_cast<unsigned long long>(__popc(ballot)));
-    }
+    if (p.block_samples) count_block_samples(p.block_samples, sampled);
 }
 
 // One epoch for any dim (lib.rs:5248-5318).  The head moves in a per-thread
@@ -206,11 +216,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_nd(SgdArgs p) {
                     atomicAdd(&p.emb[static_cast<int64_t>(head) * dim + c], __fsub_rn(h[c], h0[c]));
         }
     }
-    if (p.samples) {
-        const unsigned ballot = __ballot_sync(0xffffffffu, sampled);
-        if ((threadIdx.x & 31) == 0 && ballot)
-            atomicAdd(p.samples, static_cast<unsigned long long>(__popc(ballot)));
-    }
+    if (p.block_samples) count_block_samples(p.block_samples, sampled);
 }
 
 // ------------------------------------------------------------ transform --
@@ -341,8 +347,12 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
     epochs_per_sample_kernel<<<static_cast<unsigned>(ceil_div(m, 256)), 256, 0, s>>>(
         g.weights.get(), m, mx, nef, nrf, eps.get(), next.get(), next_neg.get());
     UMAPB_LAUNCH_CHECK();
-    DevBuf<unsigned long long> samples(1, s);
-    UMAPB_CUDA(cudaMemsetAsync(samples.get(), 0, 8, s));
+    const unsigned grid = static_cast<unsigned>(ceil_div(m, 256));
+    DevBuf<uint32_t> samples;
+    if (count_samples) {
+        samples.alloc(grid, s);
+        UMAPB_CUDA(cudaMemsetAsync(samples.get(), 0, grid * 4, s));
+    }
     SgdArgs p{};
     p.emb = emb;
     p.heads = g.heads.get();
@@ -359,14 +369,13 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
     p.rep_factor = 2.0f * repulsion * b;
     p.neg_rate_f = nrf;
     p.seed = seed;
-    p.samples = count_samples ? samples.get() : nullptr;
+    p.block_samples = samples.get();
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (kernel_ms) {
         UMAPB_CUDA(cudaEventCreate(&e0));
         UMAPB_CUDA(cudaEventCreate(&e1));
         UMAPB_CUDA(cudaEventRecord(e0, s));
     }
-    const unsigned grid = static_cast<unsigned>(ceil_div(m, 256));
     for (int64_t epoch = 0; epoch < n_epochs; ++epoch) {
         // alpha = initial_alpha * (1 - epoch / n_epochs) in FP32 (lib.rs:5174)
         p.alpha = lr * (1.0f - static_cast<float>(epoch) / nef);
@@ -386,10 +395,12 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
         cudaEventDestroy(e1);
     }
     if (!count_samples) return 0.0;
-    unsigned long long h = 0;
-    UMAPB_CUDA(cudaMemcpyAsync(&h, samples.get(), 8, cudaMemcpyDeviceToHost, s));
+    std::vector<uint32_t> h(grid);
+    UMAPB_CUDA(cudaMemcpyAsync(h.data(), samples.get(), grid * 4, cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
-    return static_cast<double>(h);
+    double total = 0.0;
+    for (uint32_t v : h) total += v;
+    return total;
 }
 
 void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_t n_base,
