@@ -254,12 +254,15 @@ def run_gpu(args) -> None:
             stage.append({f: getattr(timings, f) for f in _lib.TIMING_FIELDS})
         barrier()
         launches = (lib.umapb_kernel_launches() - launches0) // max(args.steps, 1)
+        for _ in range(args.warmup):  # the host path's own warm-up (pinned staging, pool)
+            e2e_step()
         e2e_times = [e2e_step() for _ in range(args.steps)]
         barrier()
     value = max_over_ranks(float(np.mean(dev_times)))
     e2e = max_over_ranks(float(np.mean(e2e_times)))
     emb = out_dev.cpu().numpy()
     transform = None if args.skip_transform else transform_leg(args, lib, local)
+    extra = None if args.skip_transform else knn_legs(args, lib, x)
 
     if rank == 0:
         pk = peaks()
@@ -325,13 +328,16 @@ def run_gpu(args) -> None:
             "roofline": dominant,
             "rooflines": {"knn": roof_knn, "sgd": roof_sgd},
             "stages_sec": {k: round(float(np.mean([s[k] for s in stage])), 4)
-                           for k in ("knn_sec", "smooth_knn_sec", "symmetrize_sec", "init_sec",
+                           for k in ("knn_sec", "smooth_knn_sec", "membership_sec", "symmetrize_sec",
+                                     "prune_sec", "init_sec",
                                      "optimize_sec", "total_sec")},
             "quality": {k: round(v, 4) for k, v in q.items()},
             "clocks": sampler.summary(),
         }
         if transform is not None:
             line["transform"] = transform
+        if extra is not None:
+            line["knn_configs"] = extra
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             v, st = cpu_reference_step(x[:SAMPLE_ROWS].copy(), threads)
@@ -344,6 +350,67 @@ def run_gpu(args) -> None:
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def knn_legs(args, lib, x: np.ndarray) -> dict:
+    """The exact-kNN precision path at 20,000 x 192 (tensor vs plain, same
+    result) and NN-descent (10 iterations, 30 candidates) at the fit's size."""
+    from umapers import Umap
+    from umapers_b200 import _lib, diagnostics, workloads
+
+    out = {}
+    xp = workloads.isotropic_mixture(20_000, 192, 10, 4.0, seed=7)
+    res, times = {}, {}
+    for backend, code in (("tensor", 1), ("plain", 2)):
+        idx = np.empty((xp.shape[0], K), np.int64)
+        dist = np.empty((xp.shape[0], K), np.float32)
+        fb = ctypes.c_int64(0)
+        best = float("inf")
+        for _ in range(max(args.warmup, 1) + 2):
+            t0 = time.perf_counter()
+            _lib.check(lib.umapb_knn_exact(xp.ctypes.data, xp.shape[0], 192, K, 0, code,
+                                           idx.ctypes.data, dist.ctypes.data, ctypes.byref(fb)))
+            best = min(best, time.perf_counter() - t0)
+        res[backend], times[backend] = (idx, dist, fb.value), best
+    fits = {}
+    for backend in ("tensor", "plain"):
+        m = Umap(n_neighbors=K, n_epochs=EPOCHS, ann_mode="exact", knn_backend=backend)
+        m.fit_transform(xp)
+        t0 = time.perf_counter()
+        emb = m.fit_transform(xp)
+        fits[backend] = (time.perf_counter() - t0, diagnostics.quality(xp, emb, sample=None))
+    out["precision_20000x192"] = {
+        "knn_s_tensor": round(times["tensor"], 4), "knn_s_plain": round(times["plain"], 4),
+        "identical_indices": bool(np.array_equal(res["tensor"][0], res["plain"][0])),
+        "identical_distances": bool(np.array_equal(res["tensor"][1], res["plain"][1])),
+        "fallback_rows": int(res["tensor"][2]),
+        "fit_s_tensor": round(fits["tensor"][0], 4), "fit_s_plain": round(fits["plain"][0], 4),
+        "trust15_tensor": round(fits["tensor"][1]["trustworthiness"], 4),
+        "trust15_plain": round(fits["plain"][1]["trustworthiness"], 4),
+        "note": "host API, 10-component mixture (means ~N(0, 4^2)), seed 7, k=15",
+    }
+    n = x.shape[0]
+    ni = np.empty((n, K), np.int64)
+    nd = np.empty((n, K), np.float32)
+    ran = ctypes.c_int64(0)
+    seed = 42 ^ 0xC0FEFEED1234ABCD
+    t_nd = float("inf")
+    for _ in range(2):
+        t0 = time.perf_counter()
+        _lib.check(lib.umapb_nndescent(x.ctypes.data, n, x.shape[1], K, 0, 30, 10, seed,
+                                       ni.ctypes.data, nd.ctypes.data, ctypes.byref(ran)))
+        t_nd = min(t_nd, time.perf_counter() - t0)
+    ei = np.empty((n, K), np.int64)
+    ed = np.empty((n, K), np.float32)
+    _lib.check(lib.umapb_knn_exact(x.ctypes.data, n, x.shape[1], K, 0, 1, ei.ctypes.data,
+                                   ed.ctypes.data, None))
+    rows = np.random.default_rng(3).choice(n, 2000, replace=False)
+    recall = float(np.mean([len(set(ni[r]) & set(ei[r])) / K for r in rows]))
+    out["nndescent_1m_x64"] = {
+        "knn_s": round(t_nd, 4), "iters": int(ran.value), "recall_at_15": round(recall, 4),
+        "note": "host API (includes the 256 MB upload), max_candidates=30, n_iters=10; recall "
+                "against the exact neighbours on 2,000 rows"}
+    return out
 
 
 def transform_leg(args, lib, device: int) -> dict:
@@ -396,6 +463,8 @@ def transform_leg(args, lib, device: int) -> dict:
     for _ in range(args.warmup):
         dev(True)
         dev(False)
+        e2e(True)
+        e2e(False)
     launches0 = lib.umapb_kernel_launches()
     sampler = ClockSampler(device)
     with sampler:

@@ -214,6 +214,15 @@ int64_t umapb_n_samples(const umapb_model* model);
 /* Copies the fitted embedding (n_samples x n_components) into `out`. */
 int32_t umapb_get_embedding(const umapb_model* model, float* out, int64_t n_rows,
                             int64_t n_cols);
+/* UmapCore.radii_original / radii_embedding (umap_rs/src/lib.rs:1306-1320) ->
+ * UmapModel::radii_original / radii_embedding: the mean log neighbour radius
+ * of every fitted row in the input space (local_radii_from_knn,
+ * rust_umap/src/lib.rs:5057-5082) and in the embedding
+ * (embedding_radii_from_knn, 5084-5108).  They exist after a fit with densmap
+ * or output_dens set; umapb_has_radii tells.  Either pointer may be NULL. */
+int32_t umapb_has_radii(const umapb_model* model);
+int32_t umapb_get_radii(const umapb_model* model, float* radii_original, float* radii_embedding,
+                        int64_t n_rows);
 /* Copies the curve parameters resolved by the last fit (UmapModel::ab_params,
  * rust_umap/src/lib.rs:604-610). */
 int32_t umapb_get_ab(const umapb_model* model, float* a, float* b);
@@ -243,7 +252,7 @@ int32_t umapb_knn_exact(const float* data, int64_t n_rows, int64_t n_cols, int64
  * `dists` (n_rows x k f32) are device pointers; `stream` is a cudaStream_t
  * (NULL = legacy default stream).  Results equal umapb_knn_exact's.
  * Scratch comes from one static device array of 64 MiB that every GPU loading
- * the library holds until exit: about 50,000 rows at 64 columns; larger
+ * the library holds until exit: about 43,000 rows at 64 columns; larger
  * inputs are rejected with UMAPB_ERR_INVALID_PARAMETER naming the limit.  No
  * cudaMalloc/cudaFree or allocating library routine is called.  The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress),

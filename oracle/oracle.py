@@ -46,6 +46,8 @@ _SIGS = {
         [_vp, _i64, _i64, _vp, _vp, _vp, _i64, _i64, _f32, _f32, _f32, _i64, _f32, _u64],
     ),
     "orc_fit_transform": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "orc_fit_transform_dens": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
+    "orc_local_radii": (None, [_vp, _vp, _i64, _i64, _f32, _vp]),
     "orc_transform": (_i32, [_vp, _i64, _vp, _vp, _i64, _i64, _vp, _f32, _f32, _vp]),
     "orc_optimize_layout_transform": (
         None,
@@ -259,6 +261,29 @@ def fit_transform(x, return_stats: bool = False, **kw):
         return out, {"knn_sec": stages[0], "graph_sec": stages[1], "init_sec": stages[2],
                      "sgd_sec": stages[3], "edge_samples": float(samples[0]),
                      "n_edges": int(ne[0])}
+    return out
+
+
+def fit_transform_dens(x, **kw):
+    """Oracle fit with densMAP / output_dens: (embedding, radii of the input
+    neighbourhoods, radii of the embedding neighbourhoods)."""
+    x = _f32m(x)
+    n, d = x.shape
+    p = _params(**kw)
+    out = np.empty((n, p.n_components), np.float32)
+    r0 = np.empty(n, np.float32)
+    r1 = np.empty(n, np.float32)
+    if load().orc_fit_transform_dens(_p(x), n, d, ctypes.byref(p), _p(out), _p(r0), _p(r1)):
+        raise ValueError("oracle does not cover these parameters")
+    return out, r0, r1
+
+
+def local_radii(idx, dist, var_shift: float = 0.1):
+    """local_radii_from_knn (lib.rs:5057-5082) of a kNN table."""
+    idx = np.ascontiguousarray(idx, np.int64)
+    dist = _f32m(dist)
+    out = np.empty(idx.shape[0], np.float32)
+    load().orc_local_radii(_p(idx), _p(dist), idx.shape[0], idx.shape[1], var_shift, _p(out))
     return out
 
 

@@ -1358,6 +1358,143 @@ double optimize_layout_training(std::vector<float>& flat, size_t n_vertices, siz
     return samples;
 }
 
+// ---------------------------------------------------------------- densMAP
+// density_start_epoch (lib.rs:5052-5055).
+size_t density_start_epoch(size_t n_epochs, float frac) {
+    const size_t active =
+        std::max<size_t>(static_cast<size_t>(std::ceil(static_cast<float>(n_epochs) * frac)), 1);
+    return n_epochs > active ? n_epochs - active : 0;
+}
+
+// local_radii_from_knn (lib.rs:5057-5082): mean over non-self neighbours of
+// ln(max(d, 0) + var_shift), FP32 sequential sum.
+std::vector<float> local_radii(const Knn& knn, float var_shift) {
+    const size_t n = knn.idx.size();
+    std::vector<float> out(n);
+    for (size_t r = 0; r < n; ++r) {
+        float sum = 0.0f;
+        size_t cnt = 0;
+        for (size_t c = 0; c < knn.idx[r].size(); ++c) {
+            const float dist = knn.dist[r][c];
+            if (knn.idx[r][c] == r && std::fabs(dist) <= SMOOTH_K_TOLERANCE) continue;
+            sum += logf(std::max(dist, 0.0f) + var_shift);
+            ++cnt;
+        }
+        out[r] = cnt == 0 ? logf(var_shift) : sum / static_cast<float>(cnt);
+    }
+    return out;
+}
+
+inline float euclid(const float* x, const float* y, size_t dim) {
+    return sqrtf(squared_distance(x, y, dim));
+}
+
+// embedding_radii_from_knn (lib.rs:5084-5108) on the flat embedding.
+std::vector<float> embedding_radii(const std::vector<float>& flat, size_t dim, const Knn& knn,
+                                   float var_shift) {
+    const size_t n = knn.idx.size();
+    std::vector<float> out(n);
+    for (size_t r = 0; r < n; ++r) {
+        float sum = 0.0f;
+        size_t cnt = 0;
+        for (size_t j : knn.idx[r]) {
+            if (j == r) continue;
+            sum += logf(std::max(euclid(&flat[r * dim], &flat[j * dim], dim), 0.0f) + var_shift);
+            ++cnt;
+        }
+        out[r] = cnt == 0 ? logf(var_shift) : sum / static_cast<float>(cnt);
+    }
+    return out;
+}
+
+struct Density {
+    std::vector<float> radii;
+    size_t start_epoch;
+    float lambda, var_shift;
+};
+
+// apply_density_gradient (lib.rs:5110-5134).
+void density_step(std::vector<float>& flat, size_t dim, size_t head, size_t tail, float alpha,
+                  const Density& dn) {
+    if (head == tail) return;
+    float* cur = &flat[head * dim];
+    float* oth = &flat[tail * dim];
+    const float dist = euclid(cur, oth, dim);
+    const float target = std::max(expf((dn.radii[head] + dn.radii[tail]) * 0.5f), 1e-6f);
+    const float coeff = 0.1f * dn.lambda * (dist - target) / (dist + dn.var_shift);
+    for (size_t c = 0; c < dim; ++c) {
+        const float dir = (cur[c] - oth[c]) / (dist + 1e-6f);
+        const float g = clip4(coeff * dir);
+        cur[c] -= g * alpha;
+        oth[c] += g * alpha;
+    }
+}
+
+// optimize_layout_training with a density term (lib.rs:5355-5440): the
+// general-dimension loop, the attractive coefficient in its powf(d2, b - 1)
+// form, then the density step for epochs >= start_epoch.
+double optimize_layout_densmap(std::vector<float>& flat, size_t n_vertices, size_t dim,
+                               const std::vector<Edge>& edges, size_t n_epochs, float a, float b,
+                               float initial_alpha, size_t neg_rate, float repulsion,
+                               uint64_t seed, const Density& dn) {
+    if (edges.empty() || n_vertices == 0 || n_epochs == 0) return 0.0;
+    std::vector<float> w(edges.size());
+    for (size_t i = 0; i < edges.size(); ++i) w[i] = edges[i].weight;
+    const auto eps = epochs_per_sample(w, n_epochs);
+    auto next = eps;
+    std::vector<float> eps_neg(eps.size());
+    for (size_t i = 0; i < eps.size(); ++i) eps_neg[i] = eps[i] / static_cast<float>(neg_rate);
+    auto next_neg = eps_neg;
+    SmallRng rng(seed);
+    double samples = 0.0;
+    for (size_t epoch = 0; epoch < n_epochs; ++epoch) {
+        const float alpha =
+            initial_alpha * (1.0f - static_cast<float>(epoch) / static_cast<float>(n_epochs));
+        const float ef = static_cast<float>(epoch);
+        for (size_t e = 0; e < edges.size(); ++e) {
+            if (next[e] > ef) continue;
+            samples += 1.0;
+            const size_t head = edges[e].head, tail = edges[e].tail;
+            if (head != tail) {
+                const float d2 = squared_distance(&flat[head * dim], &flat[tail * dim], dim);
+                float gc = 0.0f;
+                if (d2 > 0.0f) {
+                    const float pb = powf(d2, b);
+                    gc = -2.0f * a * b * powf(d2, b - 1.0f) / (a * pb + 1.0f);
+                }
+                for (size_t c = 0; c < dim; ++c) {
+                    const float hv = flat[head * dim + c], tv = flat[tail * dim + c];
+                    const float g = clip4(gc * (hv - tv));
+                    flat[head * dim + c] = hv + g * alpha;
+                    flat[tail * dim + c] = tv - g * alpha;
+                }
+            }
+            if (epoch >= dn.start_epoch) density_step(flat, dim, head, tail, alpha, dn);
+            next[e] += eps[e];
+            const float en = eps_neg[e];
+            if (!std::isfinite(en) || en <= 0.0f) continue;
+            const size_t nneg = floor_to_usize((ef - next_neg[e]) / en);
+            for (size_t s = 0; s < nneg; ++s) {
+                const size_t neg = rng.gen_range(0, n_vertices);
+                if (neg == head) continue;
+                const float d2 = squared_distance(&flat[head * dim], &flat[neg * dim], dim);
+                float gc = 0.0f;
+                if (d2 > 0.0f) {
+                    const float pb = powf(d2, b);
+                    gc = 2.0f * repulsion * b / ((0.001f + d2) * (a * pb + 1.0f));
+                }
+                if (gc > 0.0f)
+                    for (size_t c = 0; c < dim; ++c) {
+                        const float hv = flat[head * dim + c], nv = flat[neg * dim + c];
+                        flat[head * dim + c] = hv + clip4(gc * (hv - nv)) * alpha;
+                    }
+            }
+            next_neg[e] += static_cast<float>(nneg) * en;
+        }
+    }
+    return samples;
+}
+
 // init_graph_transform (lib.rs:4793-4836).
 Coords init_graph_transform(size_t nq, size_t dim, const std::vector<Edge>& edges,
                             const std::vector<float>& base) {
@@ -1647,6 +1784,9 @@ double orc_optimize_layout(float* emb, int64_t n, int64_t dim, const int32_t* he
 // Full dense fit_transform (UmapModel::fit_transform_dense, lib.rs:769-794,
 // artifacts lib.rs:1367-1464).  Returns 0 on success, -1 for parameters the
 // restatement does not cover.
+int32_t orc_fit_transform_dens(const float* x, int64_t n, int64_t d, const umapb_params* p,
+                               float* out, float* radii_orig, float* radii_emb);
+
 int32_t orc_fit_transform(const float* x, int64_t n, int64_t d, const umapb_params* p,
                           float* out, double* edge_samples, int64_t* n_edges_out,
                           double* stage_sec) {
@@ -1697,6 +1837,75 @@ int32_t orc_fit_transform(const float* x, int64_t n, int64_t d, const umapb_para
     if (stage_sec) stage_sec[3] = clock() - t0;
     std::memcpy(out, flat.data(), sizeof(float) * n * dim);
     return 0;
+}
+
+// build_dense_fit_artifacts with densMAP / output_dens (lib.rs:1367-1464):
+// the fit of orc_fit_transform plus the original radii (before the layout)
+// and the embedding radii (after it); the density term joins the SGD when
+// densmap is set and dens_lambda > 0.  radii_orig / radii_emb are n floats.
+int32_t orc_fit_transform_dens(const float* x, int64_t n, int64_t d, const umapb_params* p,
+                               float* out, float* radii_orig, float* radii_emb) {
+    const size_t k = static_cast<size_t>(p->n_neighbors);
+    bool approx = false;
+    if (p->use_approximate_knn && n > p->approx_knn_threshold) {
+        approx = true;
+        if (p->approx_knn_threshold > 0 && n <= p->approx_knn_threshold * 4) approx = false;
+    }
+    Knn knn = approx ? nndescent(x, n, d, k, p->metric, p->approx_knn_candidates,
+                                 p->approx_knn_iters, p->random_seed ^ 0xC0FEFEED1234ABCDULL,
+                                 nullptr)
+                     : exact_knn_query(x, n, x, n, d, k, p->metric);
+    const size_t n_epochs =
+        p->n_epochs >= 0 ? static_cast<size_t>(p->n_epochs) : (n <= 10000 ? 500 : 200);
+    float a, b;
+    find_ab_params(p->spread, p->min_dist, &a, &b);
+    std::vector<float> sig, rho;
+    smooth_knn_dist_t<float>(knn.dist, static_cast<float>(k), p->local_connectivity,
+                             DEFAULT_BANDWIDTH, knn_rows_include_self(knn), sig, rho);
+    const bool outputs = p->densmap || p->output_dens;
+    std::vector<float> r_orig;
+    if (outputs) r_orig = local_radii(knn, p->dens_var_shift);
+    auto edges = symmetrize(membership(knn, sig, rho), p->set_op_mix_ratio);
+    prune_edges(edges, n_epochs);
+    const size_t dim = static_cast<size_t>(p->n_components);
+    const Coords init =
+        initialize_embedding(x, n, d, dim, edges, p->init, p->random_seed, nullptr, nullptr);
+    std::vector<float> flat(n * dim);
+    for (int64_t i = 0; i < n; ++i)
+        for (size_t j = 0; j < dim; ++j) flat[i * dim + j] = init[i][j];
+    const uint64_t sgd_seed = p->random_seed ^ 0x9E3779B97F4A7C15ULL;
+    if (p->densmap && p->dens_lambda > 0.0f) {
+        Density dn{r_orig, density_start_epoch(n_epochs, p->dens_frac), p->dens_lambda,
+                   p->dens_var_shift};
+        optimize_layout_densmap(flat, n, dim, edges, n_epochs, a, b, p->learning_rate,
+                                static_cast<size_t>(p->negative_sample_rate),
+                                p->repulsion_strength, sgd_seed, dn);
+    } else {
+        optimize_layout_training(flat, n, dim, edges, n_epochs, a, b, p->learning_rate,
+                                 static_cast<size_t>(p->negative_sample_rate),
+                                 p->repulsion_strength, sgd_seed);
+    }
+    std::memcpy(out, flat.data(), sizeof(float) * n * dim);
+    if (outputs) {
+        const auto r_emb = embedding_radii(flat, dim, knn, p->dens_var_shift);
+        if (radii_orig) std::memcpy(radii_orig, r_orig.data(), sizeof(float) * n);
+        if (radii_emb) std::memcpy(radii_emb, r_emb.data(), sizeof(float) * n);
+    }
+    return 0;
+}
+
+// local_radii_from_knn on a given kNN table (idx n x k int64, dist n x k).
+void orc_local_radii(const int64_t* idx, const float* dist, int64_t n, int64_t k,
+                     float var_shift, float* out) {
+    Knn knn;
+    knn.idx.resize(n);
+    knn.dist.resize(n);
+    for (int64_t r = 0; r < n; ++r) {
+        knn.idx[r].assign(idx + r * k, idx + (r + 1) * k);
+        knn.dist[r].assign(dist + r * k, dist + (r + 1) * k);
+    }
+    const auto v = local_radii(knn, var_shift);
+    std::memcpy(out, v.data(), sizeof(float) * n);
 }
 
 // UmapModel::transform_rows + transform_from_knn (lib.rs:1604-1780) given

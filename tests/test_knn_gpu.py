@@ -69,12 +69,24 @@ def test_tensor_knn_matches_plain_and_oracle(orc, n, d, k):
 
 def test_tensor_knn_duplicates_and_ties(orc):
     x = workloads.gaussian(600, 64, seed=5)
-    x[100:140] = x[50]  # 41 identical rows: far more ties than the shortlist holds
+    # 101 identical rows: each of the two 32-entry lists a row keeps per
+    # column half sees more than 32 of them, so no list can hold all the ties
+    x[100:200] = x[50]
     ti, td, fb = gu.knn_exact(x, 15, backend="tensor")
     oi, od = orc.exact_knn(x, 15)
     np.testing.assert_array_equal(ti, oi)
     np.testing.assert_array_equal(td, od)
-    assert fb >= 41  # rows whose ties exceed the shortlist go to the plain kernel
+    assert fb >= 101  # rows whose ties exceed the shortlists go to the plain kernel
+
+
+def test_tensor_knn_ties_that_fit_the_lists_are_certified(orc):
+    x = workloads.gaussian(600, 64, seed=5)
+    x[100:140] = x[50]  # 41 ties, split 13 / 28 over the two column halves
+    ti, td, fb = gu.knn_exact(x, 15, backend="tensor")
+    oi, od = orc.exact_knn(x, 15)
+    np.testing.assert_array_equal(ti, oi)
+    np.testing.assert_array_equal(td, od)
+    assert fb < 41
 
 
 def test_tensor_knn_query_to_reference(orc):

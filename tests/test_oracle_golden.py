@@ -131,3 +131,37 @@ def test_spectral_disconnected_beats_random(orc):
         return sep / (std + 1e-6)
 
     assert ratio(spec) > ratio(rnd) * 1.2
+
+
+def test_densmap_lambda_zero_matches_standard(orc):
+    # densmap_lambda_zero_matches_standard_umap (rust_umap/src/lib.rs:6077-6104):
+    # synthetic_data(72, 7), k=8, 30 epochs, random init, seed 141, exact kNN
+    from umapers_b200 import workloads
+
+    x = workloads.reference_synthetic(72, 7)
+    kw = dict(n_neighbors=8, n_epochs=30, init=0, random_seed=141, use_approximate_knn=0)
+    std = orc.fit_transform(x, **kw)
+    dens, _, _ = orc.fit_transform_dens(x, densmap=1, dens_lambda=0.0, **kw)
+    assert np.array_equal(std, dens)
+
+
+def test_output_dens_radii_are_finite(orc):
+    # output_dens_returns_finite_radii (rust_umap/src/lib.rs:6106-6136)
+    from umapers_b200 import workloads
+
+    x = workloads.reference_synthetic(64, 6)
+    emb, r0, r1 = orc.fit_transform_dens(x, n_neighbors=8, n_epochs=30, init=0, random_seed=143,
+                                         use_approximate_knn=0, output_dens=1)
+    assert emb.shape == (64, 2) and r0.shape == (64,) and r1.shape == (64,)
+    assert np.all(np.isfinite(r0)) and np.all(np.isfinite(r1))
+
+
+def test_local_radii_follow_the_reference_rule(orc):
+    # mean over non-self neighbours of ln(max(d, 0) + var_shift) (lib.rs:5057-5082)
+    idx = np.array([[0, 1, 2], [1, 0, 2], [2, 5, 6]], np.int64)
+    dist = np.array([[0.0, 1.0, 2.0], [0.0, 1.0, 3.0], [0.0, 0.5, 0.25]], np.float32)
+    r = orc.local_radii(idx, dist, 0.1)
+    f = np.float32
+    expect = [(np.log(f(1.1)) + np.log(f(2.1))) / 2, (np.log(f(1.1)) + np.log(f(3.1))) / 2,
+              (np.log(f(0.6)) + np.log(f(0.35))) / 2]
+    np.testing.assert_allclose(r, np.array(expect, np.float32), rtol=1e-6)

@@ -95,7 +95,7 @@ def test_mlp_gradients_pure_mse_are_tight():
 
 @pytest.fixture(scope="module")
 def trained():
-    fit, query = workloads.transform_mixture(n_fit=40_000, n_query=60_000, d=64)
+    fit, query = workloads.transform_mixture(n_fit=40_000, n_query=200_000, d=64)
     m = Umap(n_neighbors=15, random_seed=5, ann_mode="exact")
     emb = m.fit_transform(fit)
     info = m.fit_surrogate(epochs=20, batch_size=1024)
@@ -144,7 +144,7 @@ def _device_transform(m, q_dev, out_dev, surrogate):
 
 
 def test_surrogate_transform_gain_over_plain(trained):
-    """What the trained network gains: the same 60 000 queries through the
+    """What the trained network gains: the same 200 000 queries through the
     plain transform (kNN to the training rows + SGD refine) and through the
     surrogate with its gate and fallback, device-resident, at equal quality."""
     import torch

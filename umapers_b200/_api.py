@@ -5,9 +5,10 @@ _api.py:324-873, 1054-1094): keyword arguments and defaults, sklearn-style
 ``get_params``/``set_params``, array normalisation (C-contiguous float32,
 int64 kNN indices), ``out=`` buffers, the ``ann_mode`` shortcut, and the
 fitted attributes ``embedding_``, ``n_features_in_``, ``n_samples_fit_``.
-Compute runs on one B200 through ``UmapCore`` (libumapb200.so).  Inputs the
-engine does not cover (sparse CSR, supervised targets, densMAP,
-inverse_transform, metrics other than euclidean/cosine) raise ValueError.
+Compute runs on one B200 through ``UmapCore`` (libumapb200.so), densMAP and
+``output_dens`` included.  Inputs the engine does not cover (sparse CSR,
+supervised targets, inverse_transform, metrics other than euclidean/cosine)
+raise ValueError.
 """
 from __future__ import annotations
 
@@ -285,8 +286,8 @@ class Umap:
         approx_knn_threshold:
             NN-descent switch and tuning.
         densmap, dens_lambda, dens_frac, dens_var_shift, output_dens:
-            densMAP controls (validated; densMAP itself is not run on the
-            GPU engine).
+            densMAP controls.  With ``output_dens``, ``fit_transform`` returns
+            ``(embedding, radii_original, radii_embedding)``.
         target_metric, target_weight, target_n_neighbors:
             Supervised-target controls (validated; the GPU engine fits
             unsupervised).
@@ -389,8 +390,24 @@ class Umap:
         self.embedding_ = embedding
         self.n_features_in_ = int(n_features)
         self.n_samples_fit_ = int(n_samples)
+        self._sync_density_attributes()
         if self.transform_mode == "surrogate":
             self.fit_surrogate(**(self.surrogate_kwds or {}))
+
+    def _sync_density_attributes(self) -> None:
+        """radii_original_ / radii_embedding_ (and their rad_* aliases) after an
+        output_dens fit, as the reference's facade keeps them (_api.py:530-541)."""
+        radii_original = self._core.radii_original
+        radii_embedding = self._core.radii_embedding
+        if not self.output_dens or radii_original is None or radii_embedding is None:
+            for attr in ("radii_original_", "radii_embedding_", "rad_orig_", "rad_emb_"):
+                if hasattr(self, attr):
+                    delattr(self, attr)
+            return
+        self.radii_original_ = radii_original
+        self.radii_embedding_ = radii_embedding
+        self.rad_orig_ = radii_original
+        self.rad_emb_ = radii_embedding
 
     def fit_surrogate(self, **options: Any) -> dict[str, Any]:
         """Train the learned transform surrogate of the fitted model and
@@ -462,6 +479,8 @@ class Umap:
         if out is None:
             emb = self._core.fit_transform(arr)
             self._set_fitted(emb, arr.shape[1], arr.shape[0])
+            if self.output_dens:
+                return emb, self.radii_original_, self.radii_embedding_
             return emb
         buf = _out_buffer(out, (arr.shape[0], self.n_components))
         self._core.fit_transform_into(arr, buf)

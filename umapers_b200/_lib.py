@@ -224,6 +224,8 @@ SIGNATURES = {
     "umapb_n_samples": (_i64, [_vp]),
     "umapb_get_embedding": (_i32, [_vp, _vp, _i64, _i64]),
     "umapb_get_ab": (_i32, [_vp, _f32p, _f32p]),
+    "umapb_has_radii": (_i32, [_vp]),
+    "umapb_get_radii": (_i32, [_vp, _vp, _vp, _i64]),
     "umapb_find_ab_params": (_i32, [_f32, _f32, _f32p, _f32p]),
     "umapb_knn_exact": (_i32, [_vp, _i64, _i64, _i64, _i32, _i32, _vp, _vp, _i64p]),
     "umapb_knn_exact_noalloc": (_i32, [_vp, _i64, _i64, _i64, _vp, _vp, _vp]),

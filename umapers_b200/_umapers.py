@@ -443,13 +443,26 @@ class UmapCore:
         _lib.check(self._lib.umapb_get_embedding(self._handle, _lib.ptr(out), n, self.n_components))
         return out
 
+    def _radii(self, which: int) -> np.ndarray | None:
+        if not self._lib.umapb_has_radii(self._handle):
+            return None
+        n = self._lib.umapb_n_samples(self._handle)
+        out = np.empty(n, dtype=np.float32)
+        ptrs = [None, None]
+        ptrs[which] = _lib.ptr(out)
+        _lib.check(self._lib.umapb_get_radii(self._handle, ptrs[0], ptrs[1], n))
+        return out
+
     @property
     def radii_original(self) -> np.ndarray | None:
-        return None
+        """Mean log neighbour radius of each fitted row in the input space
+        (densmap / output_dens fits only)."""
+        return self._radii(0)
 
     @property
     def radii_embedding(self) -> np.ndarray | None:
-        return None
+        """The same radius measured in the embedding."""
+        return self._radii(1)
 
     @property
     def ab_params(self) -> tuple[float, float] | None:

@@ -167,8 +167,6 @@ void check_engine_support(const umapb_params& p) {
     if (p.metric != UMAPB_METRIC_EUCLIDEAN && p.metric != UMAPB_METRIC_COSINE)
         invalid(std::string("metric ") + metric_debug_name(p.metric) +
                 " is not supported by the B200 engine (supported: euclidean, cosine)");
-    if (p.densmap || p.output_dens)
-        invalid("densmap and output_dens are not supported by the B200 engine");
     if (p.n_components > 16) invalid("n_components above 16 is not supported by the B200 engine");
 }
 
@@ -224,6 +222,7 @@ struct umapb_model {
     DevBuf<float> X;    // training rows, n_fit x d_fit
     DevBuf<float> emb;  // fitted embedding, n_fit x n_components
     Graph graph;        // the fit's fuzzy graph (CSR by head), the surrogate's edge loss
+    DevBuf<float> radii_orig, radii_emb;  // densMAP / output_dens radii (n_fit each)
     SurrogatePtr surrogate;
     std::vector<double> surrogate_loss;
 
@@ -240,6 +239,18 @@ struct umapb_model {
             uint64_t thr = UINT64_MAX;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
         }
+    }
+    // A new fit replaces every fitted array: release the old ones first so the
+    // fit's peak memory holds one generation only.
+    void begin_fit() {
+        fitted = false;
+        surrogate.reset();
+        surrogate_loss.clear();
+        graph = Graph();
+        radii_orig.release();
+        radii_emb.release();
+        emb.release();
+        X.release();
     }
     void resolve_ab() {
         // resolve_ab_params (lib.rs:613-622): computed once, reused by later fits
@@ -314,10 +325,22 @@ void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const i
     smooth_knn(dist, n, k, static_cast<float>(p.n_neighbors), p.local_connectivity, 1.0f, self,
                sig.get(), rho.get(), s);
     if (out) out->t.smooth_knn_sec = clk.lap();
+    // densMAP / output_dens (lib.rs:1401-1422): radii of the input neighbourhoods
+    const bool dens_outputs = p.densmap || p.output_dens;
+    DevBuf<float> r_orig;
+    if (dens_outputs) {
+        r_orig.alloc(n, s);
+        local_radii(idx, dist, n, k, p.dens_var_shift, r_orig.get(), s);
+    }
     Graph g;
-    fuzzy_union(idx, dist, sig.get(), rho.get(), n, k, p.set_op_mix_ratio, n_epochs, g, s);
+    double phases[3] = {0.0, 0.0, 0.0};
+    fuzzy_union(idx, dist, sig.get(), rho.get(), n, k, p.set_op_mix_ratio, n_epochs, g, s,
+                out ? phases : nullptr);
     if (out) {
-        out->t.symmetrize_sec = clk.lap();
+        clk.lap();
+        out->t.membership_sec = phases[0];
+        out->t.symmetrize_sec = phases[1];
+        out->t.prune_sec = phases[2];
         out->info.n_edges = g.n_edges;
     }
     const int dim = static_cast<int>(p.n_components);
@@ -332,10 +355,20 @@ void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const i
     if (!spectral_ok) random_init(n, dim, p.random_seed, -10.0f, 10.0f, emb.get(), s);
     if (out) out->t.init_sec = clk.lap();
     float sgd_ms = 0.0f;
+    DensityParams dens{r_orig.get(), density_start_epoch(n_epochs, p.dens_frac), p.dens_lambda,
+                       p.dens_var_shift};
+    const bool with_density = p.densmap && p.dens_lambda > 0.0f;
     const double samples = optimize_layout(
         emb.get(), n, dim, g, n_epochs, m->a, m->b, p.learning_rate, p.negative_sample_rate,
         p.repulsion_strength, p.random_seed ^ 0x9E3779B97F4A7C15ULL, out != nullptr,
-        out ? &sgd_ms : nullptr, s);
+        out ? &sgd_ms : nullptr, s, with_density ? &dens : nullptr);
+    if (dens_outputs) {
+        // radii of the same neighbourhoods in the embedding (lib.rs:1454-1462)
+        DevBuf<float> r_emb(n, s);
+        embedding_radii(emb.get(), dim, idx, n, k, p.dens_var_shift, r_emb.get(), s);
+        m->radii_orig = std::move(r_orig);
+        m->radii_emb = std::move(r_emb);
+    }
     if (out) {
         out->t.optimize_sec = clk.lap();
         out->info.sgd_edge_samples = samples;
@@ -411,10 +444,10 @@ void fit_host(umapb_model* m, const float* data, int64_t n, int64_t d, FitOutput
     check_engine_support(m->p);
     m->ensure_device();
     clk.s = m->stream;
+    m->begin_fit();
     DevBuf<float> X;
     upload(X, data, n * d, m->stream);
     if (out) out->t.validation_sec = clk.lap();
-    m->fitted = false;
     fit_device(m, X.get(), n, d, false, out, clk);
     m->X = std::move(X);
     if (emb_out) copy_embedding_out(m, emb_out);
@@ -583,12 +616,11 @@ void umapb_destroy(umapb_model* m) {
         std::lock_guard<std::mutex> lk(m->mu);
         if (m->stream) {
             cudaSetDevice(m->device);
-            m->surrogate.reset();
-            m->graph = Graph();
-            m->X.release();
-            m->emb.release();
+            // every device array is freed on the model's stream, before it goes
+            m->begin_fit();
             cudaStreamSynchronize(m->stream);
             cudaStreamDestroy(m->stream);
+            m->stream = nullptr;
         }
     }
     delete m;
@@ -646,7 +678,7 @@ int32_t umapb_fit_transform_device(umapb_model* m, const float* data, int64_t n_
         validate_params(m->p, n_rows);
         check_engine_support(m->p);
         fo.t.validation_sec = clk.lap();
-        m->fitted = false;
+        m->begin_fit();
         fit_device(m, data, n_rows, n_cols, true, &fo, clk);
         if (out)
             UMAPB_CUDA(cudaMemcpyAsync(out, m->emb.get(), n_rows * m->p.n_components * 4,
@@ -705,7 +737,7 @@ int32_t umapb_fit_transform_with_knn(umapb_model* m, const float* data, int64_t 
         DevBuf<float> dist;
         upload(dist, dist_h.data(), n_rows * k, s);
         UMAPB_CUDA(cudaMemcpyAsync(idx.get(), idx_h.data(), n_rows * k * 4, cudaMemcpyHostToDevice, s));
-        m->fitted = false;
+        m->begin_fit();
         StageClock clk(s, false);
         fit_from_knn(m, X.get(), n_rows, n_cols, idx.get(), dist.get(), static_cast<int>(k),
                      nullptr, clk);
@@ -773,6 +805,29 @@ int32_t umapb_get_embedding(const umapb_model* cm, float* out, int64_t n_rows, i
             invalid("output buffer shape mismatch");
         UMAPB_CUDA(cudaSetDevice(m->device));
         copy_embedding_out(m, out);
+    });
+}
+
+int32_t umapb_has_radii(const umapb_model* m) {
+    return (m && m->fitted && m->radii_orig.get() && m->radii_emb.get()) ? 1 : 0;
+}
+
+int32_t umapb_get_radii(const umapb_model* cm, float* radii_original, float* radii_embedding,
+                        int64_t n_rows) {
+    auto* m = const_cast<umapb_model*>(cm);
+    return guarded([&] {
+        if (!m || !m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        if (!m->radii_orig.get())
+            invalid("radii are computed only when densmap or output_dens is set");
+        if (n_rows != m->n_fit) invalid("radii buffers must hold n_samples values");
+        std::lock_guard<std::mutex> lk(m->mu);
+        if (radii_original)
+            UMAPB_CUDA(cudaMemcpyAsync(radii_original, m->radii_orig.get(), n_rows * 4,
+                                       cudaMemcpyDeviceToHost, m->stream));
+        if (radii_embedding)
+            UMAPB_CUDA(cudaMemcpyAsync(radii_embedding, m->radii_emb.get(), n_rows * 4,
+                                       cudaMemcpyDeviceToHost, m->stream));
+        UMAPB_CUDA(cudaStreamSynchronize(m->stream));
     });
 }
 

@@ -14,6 +14,8 @@
 #include <cfloat>
 #include <climits>
 
+#include <chrono>
+
 #include "kernels.cuh"
 
 namespace umapb {
@@ -327,7 +329,18 @@ void build_row_ptr(const int32_t* heads, int64_t m, int64_t n, int32_t* row_ptr,
 }
 
 void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, const float* rhos,
-                 int64_t n, int k, float mix, int64_t n_epochs, Graph& g, cudaStream_t s) {
+                 int64_t n, int k, float mix, int64_t n_epochs, Graph& g, cudaStream_t s,
+                 double* phase_sec) {
+    // phase clock of FitTimingBreakdown's membership / symmetrize / prune
+    // fields (lib.rs:51-68); it synchronises only when asked for
+    auto t_last = std::chrono::steady_clock::now();
+    auto phase = [&](int i) {
+        if (!phase_sec) return;
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        const auto t = std::chrono::steady_clock::now();
+        phase_sec[i] = std::chrono::duration<double>(t - t_last).count();
+        t_last = t;
+    };
     const int64_t m = n * k;
     const int b = bits_for(n);
     const int key_bits = 2 * b + 1;
@@ -348,6 +361,7 @@ void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, con
         UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmp_bytes, keys.get(), keys2.get(),
                                                    vals.get(), vals2.get(), m, 0, key_bits, s));
     }
+    phase(0);
     DevBuf<int> cnt(1, s);
     UMAPB_CUDA(cudaMemsetAsync(cnt.get(), 0, 4, s));
     DevBuf<uint64_t> sym_keys(2 * m + 2, s), sym_keys2(2 * m + 2, s);
@@ -383,6 +397,7 @@ void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, con
         UMAPB_LAUNCH_CHECK();
     }
     g.n = n;
+    phase(1);
     if (n_epochs > 0 && n_sym > 0) {
         // prune_edges (lib.rs:3804-3822)
         const float mx = max_weight(sym_w2.get(), n_sym, s);
@@ -409,6 +424,7 @@ void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, con
     }
     g.row_ptr.alloc(n + 1, s);
     build_row_ptr(g.heads.get(), g.n_edges, n, g.row_ptr.get(), s);
+    phase(2);
 }
 
 void bipartite_graph(const int32_t* idx, const float* dist, const float* sigmas,

@@ -107,8 +107,11 @@ void smooth_knn(const float* dist, int64_t n, int k, float k_f, float local_conn
 
 // compute_membership_strengths + symmetrize_fuzzy_graph (+ prune_edges when
 // n_epochs > 0): the symmetric graph sorted by (head, tail).
+// `phase_sec` (nullable, 3 values): seconds of membership, symmetrisation
+// and prune + CSR offsets, with a stream synchronisation after each.
 void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, const float* rhos,
-                 int64_t n, int k, float mix, int64_t n_epochs, Graph& g, cudaStream_t s);
+                 int64_t n, int k, float mix, int64_t n_epochs, Graph& g, cudaStream_t s,
+                 double* phase_sec = nullptr);
 
 // Bipartite membership + prune for transform (rust_umap/src/lib.rs:1738-1761):
 // edges grouped by query in kNN order; returns the edge count.
@@ -140,9 +143,24 @@ void random_init(int64_t n, int dim, uint64_t seed, float low, float high, float
 // optimize_layout_training (rust_umap/src/lib.rs:5137-5321), Hogwild over
 // edges, one launch per epoch; returns the attractive edge-sample count when
 // `count_samples` is set.
+struct DensityParams {
+    const float* radii;   // local radii of the input rows (device, n)
+    int64_t start_epoch;  // density_start_epoch (lib.rs:5052-5055)
+    float lambda, var_shift;
+};
+// With `dens`, every epoch runs the densMAP kernel (lib.rs:5355-5440).
 double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, int64_t n_epochs,
                        float a, float b, float lr, int64_t neg_rate, float repulsion,
-                       uint64_t seed, bool count_samples, float* kernel_ms, cudaStream_t s);
+                       uint64_t seed, bool count_samples, float* kernel_ms, cudaStream_t s,
+                       const DensityParams* dens = nullptr);
+
+// local_radii_from_knn / embedding_radii_from_knn (lib.rs:5057-5108) and
+// density_start_epoch (lib.rs:5052-5055).
+void local_radii(const int32_t* idx, const float* dist, int64_t n, int k, float var_shift,
+                 float* out, cudaStream_t s);
+void embedding_radii(const float* emb, int dim, const int32_t* idx, int64_t n, int k,
+                     float var_shift, float* out, cudaStream_t s);
+int64_t density_start_epoch(int64_t n_epochs, float frac);
 
 // init_graph_transform + optimize_layout_transform
 // (rust_umap/src/lib.rs:4793-4836, 5444-5544): one thread per query.

@@ -17,16 +17,22 @@
 //    keeps MT query tiles of 128 rows of A resident in shared memory, streams
 //    128-row candidate tiles of B through a TMA ring (SWIZZLE_128B, no
 //    multicast), and one thread issues tcgen05.mma (kind::f16, BF16 in, FP32
-//    accumulate) into double-buffered TMEM accumulators.  Epilogue warps read
-//    their rows with tcgen05.ld and keep, per row, the S = 32 smallest
-//    (L, index) keys in a global list; a warp inserts cooperatively (one list
-//    entry per lane), and a per-row threshold skips a 32-column chunk with a
-//    single vote in the common case.
-// 3. rerank: one warp per row recomputes the S candidates' exact FP32
-//    distances in the reference's summation order, sorts (distance, index),
-//    and certifies the row: with U_j = L_j + 2 e_j, the shortlist provably
-//    holds every true neighbour when max_j L_j > (k-th smallest U).  Rows that
-//    fail (near-ties wider than the bound) are recomputed by knn_plain.
+//    accumulate) into double-buffered TMEM accumulators.  Eight epilogue
+//    warps per query tile each own 32 rows x 64 columns of the accumulator:
+//    they read it with tcgen05.ld and keep, per (row, column half), the
+//    S = 32 smallest (L, index) keys in a global list.  A per-list threshold
+//    skips a 32-column chunk with one vote in the common case; otherwise the
+//    chunk is transposed across the warp with shuffles and its qualifying
+//    keys are inserted cooperatively (one list entry per lane).  When the
+//    query tiles are fewer than the SMs, the candidate tiles are split too,
+//    with lists per split.
+// 3. rerank: one warp per row recomputes the exact FP32 distances of every
+//    list's candidates in the reference's summation order and keeps the k
+//    smallest (distance, index) keys.  With U_j = L_j + 2 e_j and B the
+//    smallest largest-L of the full lists, every candidate missing from the
+//    lists has d >= B, so the row is certified when at least k candidates have
+//    U < B.  Rows that fail (near-ties wider than the bound) are recomputed by
+//    knn_plain.
 //
 // Every wait on an mbarrier is bounded by a %globaltimer deadline; a timeout
 // sets an error word, stops all roles, drains in-flight copies and frees TMEM.
@@ -70,31 +76,68 @@ __device__ __forceinline__ float o2f(uint32_t o) {
     return (o & 0x80000000u) ? __uint_as_float(o & 0x7FFFFFFFu) : __uint_as_float(~o);
 }
 
-// Candidate tile visited at step t by CTA b: CTAs start at staggered tiles
-// inside a window of kStaggerTiles (4 MiB of B at K' = 256, L2-resident), so
-// they do not all request the same tile at once.  The shortlist certificate
-// does not depend on the visiting order.
-constexpr int64_t kStaggerGroups = 16, kStaggerStep = 4;
-
-__device__ __forceinline__ int64_t tile_at(int64_t t, int64_t n_ctiles) {
-    const int64_t off = (static_cast<int64_t>(blockIdx.x) % kStaggerGroups) * kStaggerStep;
-    int64_t c = t + (off < n_ctiles ? off : 0);
-    return c >= n_ctiles ? c - n_ctiles : c;
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
 }
+
+// Minimum of 32 FP32 values held as bit patterns (16 three-input mins).
+__device__ __forceinline__ float min32(const uint32_t* r) {
+    float m = min3f(__uint_as_float(r[0]), __uint_as_float(r[1]), __uint_as_float(r[2]));
+#pragma unroll
+    for (int j = 3; j < 31; j += 2) m = min3f(m, __uint_as_float(r[j]), __uint_as_float(r[j + 1]));
+    return fminf(m, __uint_as_float(r[31]));
+}
+
+// CTAs begin their candidate range at staggered tiles (16 groups, 4 tiles
+// apart: a window of 4 MiB of B at K' = 256, L2-resident) so they do not all
+// request the same tile at once.  The shortlist certificate does not depend
+// on the visiting order.
+constexpr int32_t kStaggerGroups = 16, kStaggerStep = 4;
 
 struct TcArgs {
     int64_t n_q;
     int64_t n_r;
     int kb;          // k-blocks of 64 columns
     int ks_last;     // k-steps of 16 columns holding data in the last k-block
-    int64_t n_units;   // groups of MT query tiles
-    int64_t n_ctiles;  // candidate tiles
-    uint64_t* lists;   // n_q x S keys (L order-mapped << 32 | index)
+    int64_t n_units;      // work units: (group of MT query tiles, candidate split)
+    int n_split;          // candidate splits per group (1 unless query tiles are few)
+    int64_t split_tiles;  // candidate tiles per split (the last split may hold fewer)
+    int64_t n_ctiles;     // candidate tiles
+    uint64_t* lists;      // n_q x n_split x 2 x S keys (L order-mapped << 32 | index), one
+                          // list per (row, candidate split, half of each tile's columns)
     int* err;
 };
 
+// Work unit u covers query group u / n_split and the candidate tiles of
+// split u % n_split, visited from tile begin + rot onwards (cyclically).
+struct Unit {
+    int32_t group, split, begin, len, rot;  // tile counts stay far below 2^31
+};
+__device__ __forceinline__ Unit unit_of(const TcArgs& p, int64_t u) {
+    Unit r;
+    r.group = static_cast<int32_t>(u / p.n_split);
+    r.split = static_cast<int32_t>(u - static_cast<int64_t>(r.group) * p.n_split);
+    r.begin = r.split * static_cast<int32_t>(p.split_tiles);
+    r.len = static_cast<int32_t>(min(p.split_tiles, p.n_ctiles - r.begin));
+    r.rot = static_cast<int32_t>(blockIdx.x % kStaggerGroups) * kStaggerStep;
+    if (r.rot >= r.len) r.rot = 0;
+    return r;
+}
+
+// Candidate tile visited at step t of unit w.
+__device__ __forceinline__ int32_t tile_at(int32_t t, const Unit& w) {
+    const int32_t c = t + w.rot;
+    return w.begin + (c >= w.len ? c - w.len : c);
+}
+
+// Threads: warp 0 TMA, warp 1 MMA, then 8 epilogue warps per query tile.
+template <int MT>
+constexpr int tc_threads() { return 64 + 256 * MT; }
+
 template <int MT, int ST>
-__global__ void __launch_bounds__(64 + 128 * MT, 1)
+__global__ void __launch_bounds__(tc_threads<MT>(), 1)
     tc_knn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                   TcArgs p) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -124,7 +167,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(b_tfull + 8 * b, 1);
-            mbar_init(b_tempty + 8 * b, 4 * MT);
+            mbar_init(b_tempty + 8 * b, 8 * MT);
         }
         mbar_init(b_afull, 1);
         mbar_init(b_aempty, 1);
@@ -157,13 +200,14 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                     fail(1);
                     break;
                 }
+                const Unit w = unit_of(p, unit);
                 mbar_expect_tx(b_afull, MT * KB * kTileBytes);
                 for (int mt = 0; mt < MT; ++mt)
                     for (int kb = 0; kb < KB; ++kb)
                         tma_load_2d(sA + (mt * KB + kb) * kTileBytes, &tmA, b_afull, kb * BK,
-                                    static_cast<int>((unit * MT + mt) * BM));
+                                    static_cast<int>((w.group * MT + mt) * BM));
                 bool ok = true;
-                for (int64_t c = 0; c < p.n_ctiles && ok; ++c) {
+                for (int32_t c = 0; c < w.len && ok; ++c) {
                     for (int kb = 0; kb < KB; ++kb, ++it) {
                         const int stage = static_cast<int>(it % ST);
                         const uint32_t round = static_cast<uint32_t>(it / ST);
@@ -174,7 +218,7 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                         }
                         mbar_expect_tx(b_full + 8 * stage, kTileBytes);
                         tma_load_2d(sB + stage * kTileBytes, &tmB, b_full + 8 * stage, kb * BK,
-                                    static_cast<int>(tile_at(c, p.n_ctiles) * BN));
+                                    static_cast<int>(tile_at(c, w) * BN));
                     }
                 }
                 if (!ok) break;
@@ -192,7 +236,8 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                     break;
                 }
                 fence_after();
-                for (int64_t c = 0; c < p.n_ctiles && ok; ++c, ++cg) {
+                const int32_t len = unit_of(p, unit).len;
+                for (int32_t c = 0; c < len && ok; ++c, ++cg) {
                     const uint32_t buf = static_cast<uint32_t>(cg & 1);
                     if (!mbar_wait(b_tempty + 8 * buf, static_cast<uint32_t>(((cg >> 1) & 1) ^ 1),
                                    abort_flag)) {
@@ -236,19 +281,21 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
         }
     } else {
         // --------------------------------------------------- epilogue
-        const int ew = warp - 2;
-        const int mt = ew >> 2;
+        // Warp w reads TMEM lanes 32 * (w % 4) (hardware rule); the four warps
+        // of each quarter split (query tile, column half).
         const int quarter = warp & 3;
-        // per-warp staging of one lane's qualifying candidates (value, column)
-        float* stage_v = reinterpret_cast<float*>(tmem_holder + 2) + ew * 80;
-        int32_t* stage_i = reinterpret_cast<int32_t*>(stage_v + 32);
+        const int slot = (warp - 2) >> 2;
+        const int mt = slot >> 1;
+        const int half = slot & 1;
         uint64_t cg = 0;
         bool ok = true;
         for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x) {
-            const int64_t row = (unit * MT + mt) * BM + quarter * 32 + lane;
+            const Unit w = unit_of(p, unit);
+            const int32_t row = (w.group * MT + mt) * BM + quarter * 32 + lane;
             const bool row_ok = row < p.n_q;
-            float tau = INFINITY;
-            for (int64_t c = 0; c < p.n_ctiles; ++c, ++cg) {
+            const int32_t list_base = w.split * 2 + half;  // list of (row, split, half)
+            float tau = INFINITY;  // this list's current S-th smallest bound
+            for (int32_t c = 0; c < w.len; ++c, ++cg) {
                 const uint32_t buf = static_cast<uint32_t>(cg & 1);
                 if (!mbar_wait(b_tfull + 8 * buf, static_cast<uint32_t>((cg >> 1) & 1), abort_flag)) {
                     fail(6);
@@ -257,58 +304,48 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                 }
                 fence_after();
                 const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
-                                       buf * (MT * BN) + mt * BN;
-                uint32_t r[4][32];
-#pragma unroll
-                for (int ch = 0; ch < 4; ++ch) tmem_ld32(taddr + ch * 32, r[ch]);
+                                       buf * (MT * BN) + mt * BN + half * (BN / 2);
+                uint32_t r[2][32];
+                tmem_ld32(taddr, r[0]);
+                tmem_ld32(taddr + 32, r[1]);
                 tmem_wait_ld();
                 // the accumulator buffer can be overwritten as soon as it is in registers
                 fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
-                float m = __uint_as_float(r[0][0]);
+                const float m0 = min32(r[0]), m1 = min32(r[1]);
+                const unsigned pend0 = __ballot_sync(0xffffffffu, row_ok && m0 < tau);
+                const unsigned pend1 = __ballot_sync(0xffffffffu, row_ok && m1 < tau);
+                if ((pend0 | pend1) == 0) continue;
+                const int32_t colh = tile_at(c, w) * BN + half * (BN / 2);
 #pragma unroll
-                for (int ch = 0; ch < 4; ++ch)
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) m = fminf(m, __uint_as_float(r[ch][j]));
-                if (__ballot_sync(0xffffffffu, row_ok && m < tau) == 0) continue;
-#pragma unroll
-                for (int ch = 0; ch < 4; ++ch) {
-                    float mc = __uint_as_float(r[ch][0]);
-#pragma unroll
-                    for (int j = 1; j < 32; ++j) mc = fminf(mc, __uint_as_float(r[ch][j]));
-                    unsigned pend = __ballot_sync(0xffffffffu, row_ok && mc < tau);
-                    if (pend == 0) continue;
-                    const int64_t col0 = tile_at(c, p.n_ctiles) * BN + ch * 32;
-                    const int64_t valid_cols = p.n_r - col0;
+                for (int ch = 0; ch < 2; ++ch) {
+                    unsigned pend = ch == 0 ? pend0 : pend1;
+                    const int32_t col0 = colh + ch * 32;
+                    const int32_t valid_cols = static_cast<int32_t>(p.n_r - col0);
                     while (pend) {
                         const int src = __ffs(pend) - 1;
                         pend &= pend - 1;
-                        if (lane == src) {
-                            int n = 0;
-#pragma unroll
-                            for (int j = 0; j < 32; ++j) {
-                                const float v = __uint_as_float(r[ch][j]);
-                                if (v < tau && j < valid_cols) {
-                                    stage_v[n] = v;
-                                    stage_i[n] = j;
-                                    ++n;
-                                }
-                            }
-                            stage_i[32 + 0] = n;  // count slot after the index list
-                        }
-                        __syncwarp();
-                        const int n = stage_i[32];
-                        const int64_t srow = __shfl_sync(0xffffffffu, row, src);
+                        const int32_t srow = __shfl_sync(0xffffffffu, row, src);
                         float stau = __shfl_sync(0xffffffffu, tau, src);
-                        uint64_t* lst = p.lists + srow * S;
-                        uint64_t lk = lst[lane];
-#pragma unroll 1
-                        for (int t = 0; t < n; ++t) {
-                            const float val = stage_v[t];
+                        uint64_t* lst =
+                            p.lists + (static_cast<int64_t>(srow) * 2 * p.n_split + list_base) * S;
+                        uint64_t lk = lst[lane];  // in flight while the row is transposed
+                        // lane j takes column j of the source row
+                        float mine = 0.0f;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const float t = __shfl_sync(0xffffffffu, __uint_as_float(r[ch][j]), src);
+                            if (lane == j) mine = t;
+                        }
+                        unsigned q = __ballot_sync(0xffffffffu, mine < stau && lane < valid_cols);
+                        while (q) {
+                            const int b = __ffs(q) - 1;
+                            q &= q - 1;
+                            const float val = __shfl_sync(0xffffffffu, mine, b);
                             if (!(val < stau)) continue;
                             const uint64_t key = (static_cast<uint64_t>(f2o(val)) << 32) |
-                                                 static_cast<uint32_t>(col0 + stage_i[t]);
+                                                 static_cast<uint32_t>(col0 + b);
                             const int pos = __popc(__ballot_sync(0xffffffffu, lk < key));
                             const uint64_t up = __shfl_up_sync(0xffffffffu, lk, 1);
                             if (lane > pos)
@@ -320,7 +357,6 @@ __global__ void __launch_bounds__(64 + 128 * MT, 1)
                         }
                         lst[lane] = lk;
                         if (lane == src) tau = stau;
-                        __syncwarp();
                     }
                 }
             }
@@ -438,41 +474,60 @@ __device__ __forceinline__ T warp_sort_asc(T v) {
 
 __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restrict__ R,
                               const float* __restrict__ qsq, const float* __restrict__ rsq,
-                              const uint64_t* __restrict__ lists, int64_t n_q, int64_t n_r, int d,
-                              int k, double c1, double c2, int32_t* __restrict__ out_idx,
+                              const uint64_t* __restrict__ lists, int n_lists, int64_t n_q,
+                              int d, int k, double c1, double c2, int32_t* __restrict__ out_idx,
                               float* __restrict__ out_dist, int* __restrict__ fb_count,
                               int32_t* __restrict__ fb_rows) {
     const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n_q) return;
-    const uint64_t lk = lists[row * S + lane];
-    const bool valid = lk != ~0ull;
-    const uint32_t j = static_cast<uint32_t>(lk);
-    double U = INFINITY;
-    float L = -INFINITY;
-    uint64_t key = ~0ull;
-    if (valid) {
-        L = o2f(static_cast<uint32_t>(lk >> 32));
-        const double nq = qsq[row], nc = rsq[j];
-        U = static_cast<double>(L) + 2.0 * (c1 * sqrt(nq * nc) + c2 * (nq + nc));
-        const float d2 = sqdist_ref(Q + row * d, R + static_cast<int64_t>(j) * d, d);
-        key = knn_key(d2, j);
-    }
-    const int n_valid = __popc(__ballot_sync(0xffffffffu, valid));
-    const double u_sorted = warp_sort_asc<double>(U);
-    const double u_k = __shfl_sync(0xffffffffu, u_sorted, k - 1);
-    float lmax = L;
+    const uint64_t* rl = lists + row * n_lists * S;
+    // The smallest bound a candidate missing from every list can have: a full
+    // list left out only candidates with L >= its largest entry, a list that
+    // is not full kept every candidate of its range.
+    double bound = INFINITY;
+    for (int h = 0; h < n_lists; ++h) {
+        const uint64_t lk = rl[h * S + lane];
+        const bool valid = lk != ~0ull;
+        float lmax = valid ? o2f(static_cast<uint32_t>(lk >> 32)) : -INFINITY;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    // all candidates were kept (n_r <= S) or the cut provably separates them
-    const bool certified = (n_valid < S && n_valid >= n_r) ||
-                           (n_valid == S && static_cast<double>(lmax) > u_k);
-    const uint64_t sorted = warp_sort_asc<uint64_t>(key);
-    if (lane < k) {
-        out_idx[row * k + lane] = static_cast<int32_t>(key_index(sorted));
-        out_dist[row * k + lane] = __fsqrt_rn(key_dist(sorted));
+        for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+        if (__popc(__ballot_sync(0xffffffffu, valid)) == S)
+            bound = fmin(bound, static_cast<double>(lmax));
     }
-    if (!certified && lane == 0) fb_rows[atomicAdd(fb_count, 1)] = static_cast<int32_t>(row);
+    // Exact keys in the reference's order; the 32 smallest of all lists are
+    // kept sorted across the warp (bitonic merge of each sorted list into
+    // them), and k candidates with d <= U < bound certify the row.
+    const double nq = qsq[row];
+    int below = 0;
+    uint64_t top = ~0ull;
+    for (int h = 0; h < n_lists; ++h) {
+        const uint64_t lk = rl[h * S + lane];
+        double U = INFINITY;
+        uint64_t key = ~0ull;
+        if (lk != ~0ull) {
+            const uint32_t j = static_cast<uint32_t>(lk);
+            const double nc = rsq[j];
+            U = static_cast<double>(o2f(static_cast<uint32_t>(lk >> 32))) +
+                2.0 * (c1 * sqrt(nq * nc) + c2 * (nq + nc));
+            key = knn_key(sqdist_ref(Q + row * d, R + static_cast<int64_t>(j) * d, d), j);
+        }
+        below += __popc(__ballot_sync(0xffffffffu, U < bound));
+        const uint64_t b = warp_sort_asc<uint64_t>(key);
+        const uint64_t br = __shfl_sync(0xffffffffu, b, 31 - lane);
+        uint64_t m = top < br ? top : br;
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+            const uint64_t o = __shfl_xor_sync(0xffffffffu, m, st);
+            m = (lane & st) ? (m > o ? m : o) : (m < o ? m : o);
+        }
+        top = m;
+    }
+    if (lane < k) {
+        out_idx[row * k + lane] = static_cast<int32_t>(key_index(top));
+        out_dist[row * k + lane] = __fsqrt_rn(key_dist(top));
+    }
+    if (below < k && lane == 0) fb_rows[atomicAdd(fb_count, 1)] = static_cast<int32_t>(row);
 }
 
 // --------------------------------------------------------------- host ----
@@ -484,9 +539,8 @@ int query_tiles_for(int kb) { return kb <= 4 ? 2 : (kb <= 10 ? 1 : 0); }
 
 template <int MT, int ST>
 void launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, cudaStream_t s) {
-    // tiles + 1 KiB alignment slack + barriers/flags (256 B) + epilogue staging
-    const size_t smem = static_cast<size_t>(MT * a.kb + ST) * kTileBytes + 1024 + 256 +
-                        4 * MT * 80 * 4;
+    // tiles + 1 KiB alignment slack + barriers/flags (256 B)
+    const size_t smem = static_cast<size_t>(MT * a.kb + ST) * kTileBytes + 1024 + 256;
     auto kern = tc_knn_kernel<MT, ST>;
     UMAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
@@ -494,8 +548,35 @@ void launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, cu
     UMAPB_CUDA(cudaGetDevice(&dev));
     UMAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int64_t grid = std::min<int64_t>(a.n_units, sms);
-    kern<<<static_cast<unsigned>(grid), 64 + 128 * MT, smem, s>>>(ma, mb, a);
+    kern<<<static_cast<unsigned>(grid), tc_threads<MT>(), smem, s>>>(ma, mb, a);
     UMAPB_LAUNCH_CHECK();
+}
+
+// Work decomposition: groups of MT query tiles; when the groups are fewer
+// than the SMs the candidate tiles are split too (at least 8 per split), so
+// small query sets still occupy the GPU.
+TcArgs plan(int64_t n_q, int64_t n_r, int d, bool allow_split) {
+    const int kp = padded_k(d);
+    TcArgs a{};
+    a.n_q = n_q;
+    a.n_r = n_r;
+    a.kb = kp / BK;
+    a.ks_last = static_cast<int>(ceil_div(3 * d + 7 - (a.kb - 1) * BK, UK));
+    a.n_ctiles = ceil_div(n_r, BN);
+    const int mt = query_tiles_for(a.kb);
+    const int64_t groups = ceil_div(n_q, static_cast<int64_t>(BM) * mt);
+    int64_t split = 1;
+    if (allow_split) {
+        int dev = 0, sms = 0;
+        UMAPB_CUDA(cudaGetDevice(&dev));
+        UMAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (groups < sms)
+            split = std::min<int64_t>(ceil_div(sms, groups), std::max<int64_t>(1, a.n_ctiles / 8));
+    }
+    a.split_tiles = ceil_div(a.n_ctiles, split);
+    a.n_split = static_cast<int>(ceil_div(a.n_ctiles, a.split_tiles));
+    a.n_units = groups * a.n_split;
+    return a;
 }
 
 }  // namespace
@@ -532,21 +613,16 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     prep_kernel<<<static_cast<unsigned>(ceil_div(n_r * 32, 256)), 256, 0, s>>>(
         R, rsq_p, n_r, d, kp, static_cast<float>(c1), static_cast<float>(c2), false, B.get());
     UMAPB_LAUNCH_CHECK();
-    DevBuf<uint64_t> lists(n_q * S, s);
-    UMAPB_CUDA(cudaMemsetAsync(lists.get(), 0xFF, n_q * S * 8, s));
+    TcArgs a = plan(n_q, n_r, d, true);
+    const int mt = query_tiles_for(kb);
+    const int n_lists = 2 * a.n_split;
+    DevBuf<uint64_t> lists(n_q * n_lists * S, s);
+    UMAPB_CUDA(cudaMemsetAsync(lists.get(), 0xFF, n_q * n_lists * S * 8, s));
     DevBuf<int> err(1, s), fb_count(1, s);
     UMAPB_CUDA(cudaMemsetAsync(err.get(), 0, 4, s));
     UMAPB_CUDA(cudaMemsetAsync(fb_count.get(), 0, 4, s));
     const CUtensorMap ma = make_map(A.get(), n_q, kp);
     const CUtensorMap mb = make_map(B.get(), n_r, kp);
-    const int mt = query_tiles_for(kb);
-    TcArgs a{};
-    a.n_q = n_q;
-    a.n_r = n_r;
-    a.kb = kb;
-    a.ks_last = static_cast<int>(ceil_div(3 * d + 7 - (kb - 1) * BK, UK));
-    a.n_units = ceil_div(n_q, static_cast<int64_t>(BM) * mt);
-    a.n_ctiles = ceil_div(n_r, BN);
     a.lists = lists.get();
     a.err = err.get();
     cudaEvent_t e0, e1;
@@ -571,7 +647,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
                         std::to_string(err_h) + ")");
     DevBuf<int32_t> fb_rows(n_q, s);
     rerank_kernel<<<static_cast<unsigned>(ceil_div(n_q * 32, 256)), 256, 0, s>>>(
-        Q, R, qsq.get(), rsq_p, lists.get(), n_q, n_r, d, k, c1, c2, out_idx, out_dist,
+        Q, R, qsq.get(), rsq_p, lists.get(), n_lists, n_q, d, k, c1, c2, out_idx, out_dist,
         fb_count.get(), fb_rows.get());
     UMAPB_LAUNCH_CHECK();
     int fb = 0;
@@ -630,7 +706,7 @@ inline size_t round256(size_t b) { return (b + 255) & ~static_cast<size_t>(255);
 size_t noalloc_need(int64_t n, int d) {
     const size_t rows = static_cast<size_t>(n);
     const size_t kp = static_cast<size_t>(padded_k(d));
-    return round256(rows * 4) + 2 * round256(rows * kp * 2) + round256(rows * S * 8) +
+    return round256(rows * 4) + 2 * round256(rows * kp * 2) + round256(rows * 2 * S * 8) +
            round256(8) + round256(rows * 4);
 }
 
@@ -664,13 +740,13 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     float* sq = reinterpret_cast<float*>(carve(static_cast<size_t>(n) * 4));
     __nv_bfloat16* A = reinterpret_cast<__nv_bfloat16*>(carve(static_cast<size_t>(n) * kp * 2));
     __nv_bfloat16* B = reinterpret_cast<__nv_bfloat16*>(carve(static_cast<size_t>(n) * kp * 2));
-    uint64_t* lists = reinterpret_cast<uint64_t*>(carve(static_cast<size_t>(n) * S * 8));
+    uint64_t* lists = reinterpret_cast<uint64_t*>(carve(static_cast<size_t>(n) * 2 * S * 8));
     int* flags = reinterpret_cast<int*>(carve(8));  // [0] = kernel error, [1] = fallback count
     int32_t* fb_rows = reinterpret_cast<int32_t*>(carve(static_cast<size_t>(n) * 4));
 
     // every call starts from cleared shortlists and flags (the array keeps
     // the previous call's contents)
-    UMAPB_CUDA(cudaMemsetAsync(lists, 0xFF, static_cast<size_t>(n) * S * 8, s));
+    UMAPB_CUDA(cudaMemsetAsync(lists, 0xFF, static_cast<size_t>(n) * 2 * S * 8, s));
     UMAPB_CUDA(cudaMemsetAsync(flags, 0, 8, s));
     row_norms(X, n, d, nullptr, sq, s);
     prep_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
@@ -682,13 +758,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     const CUtensorMap ma = make_map(A, n, kp);
     const CUtensorMap mb = make_map(B, n, kp);
     const int mt = query_tiles_for(kb);
-    TcArgs a{};
-    a.n_q = n;
-    a.n_r = n;
-    a.kb = kb;
-    a.ks_last = static_cast<int>(ceil_div(3 * d + 7 - (kb - 1) * BK, UK));
-    a.n_units = ceil_div(n, static_cast<int64_t>(BM) * mt);
-    a.n_ctiles = ceil_div(n, BN);
+    TcArgs a = plan(n, n, d, false);  // one split: the scratch holds 2 lists per row
     a.lists = lists;
     a.err = flags;
     if (mt == 2)
@@ -702,7 +772,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
         throw Error(UMAPB_ERR_CUDA, "tensor-core kNN kernel stopped on a wait timeout (code " +
                                         std::to_string(flags_h[0]) + ")");
     rerank_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
-        X, X, sq, sq, lists, n, n, d, k, c1, c2, out_idx, out_dist, flags + 1, fb_rows);
+        X, X, sq, sq, lists, 2, n, d, k, c1, c2, out_idx, out_dist, flags + 1, fb_rows);
     UMAPB_LAUNCH_CHECK();
     UMAPB_CUDA(cudaMemcpyAsync(flags_h, flags, 8, cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));

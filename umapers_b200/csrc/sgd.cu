@@ -15,7 +15,10 @@
 // optimize_layout_transform (lib.rs:5444-5544).  Queries never interact, so
 // one thread runs one query's whole schedule sequentially, as the reference's
 // per-query closure does.
+#include <cub/cub.cuh>
+
 #include <cfloat>
+#include <cmath>
 
 #include <vector>
 
@@ -48,6 +51,39 @@ __global__ void epochs_per_sample_kernel(const float* __restrict__ w, int64_t m,
     if (next_neg) next_neg[e] = __fdiv_rn(v, neg_rate_f);
 }
 
+// Sort keys of the edge order: the window of 2^kSortWindowShift consecutive edges
+// (graph order, i.e. by head) in the high word, the sampling period in the
+// low word.  Periods are positive floats or +inf, whose bit patterns order
+// as unsigned integers.
+constexpr int kSortWindowShift = 16;  // windows of 65536 edges
+
+__global__ void period_keys_kernel(const float* __restrict__ eps, int64_t m,
+                                   uint64_t* __restrict__ keys, int32_t* __restrict__ ids) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= m) return;
+    keys[e] = (static_cast<uint64_t>(e >> kSortWindowShift) << 32) | __float_as_uint(eps[e]);
+    ids[e] = static_cast<int32_t>(e);
+}
+
+// Position e of the sorted order takes edge order[e].
+__global__ void gather_edges_kernel(const int32_t* __restrict__ order,
+                                    const int32_t* __restrict__ heads,
+                                    const int32_t* __restrict__ tails,
+                                    const float* __restrict__ eps_in, float neg_rate_f, int64_t m,
+                                    int32_t* __restrict__ heads_out,
+                                    int32_t* __restrict__ tails_out, float* __restrict__ eps,
+                                    float* __restrict__ next, float* __restrict__ next_neg) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= m) return;
+    const int32_t o = order[e];
+    heads_out[e] = heads[o];
+    tails_out[e] = tails[o];
+    const float v = eps_in[o];
+    eps[e] = v;
+    next[e] = v;
+    next_neg[e] = __fdiv_rn(v, neg_rate_f);
+}
+
 struct SgdArgs {
     float* emb;
     const int32_t* heads;
@@ -67,6 +103,10 @@ struct SgdArgs {
     uint64_t seed;
     uint64_t epoch;
     uint32_t* block_samples;  // (nullable) per-block count of attractive samples, all epochs
+    // densMAP (sgd_epoch_dens only)
+    const float* radii;       // local_radii_from_knn of the input rows
+    float dens_lambda, dens_var_shift;
+    int dens_on;              // epoch >= density_start_epoch
 };
 
 // Adds this block's sampled-edge count to its own slot: shared-memory
@@ -147,6 +187,141 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
 // One epoch for any dim (lib.rs:5248-5318).  The head moves in a per-thread
 // copy of at most kMaxDim coordinates.
 constexpr int kMaxDim = 16;
+
+// One epoch of the densMAP layout (optimize_layout_training with a density
+// state, lib.rs:5355-5440): the attractive coefficient in its
+// -2ab d2^(b-1) / (a d2^b + 1) form, then, from density_start_epoch on,
+// apply_density_gradient (lib.rs:5110-5134) on the same edge, then the
+// negative samples.  Head in registers, tail moves published with atomics.
+__global__ void __launch_bounds__(256) sgd_epoch_dens(SgdArgs p) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool sampled = false;
+    if (e < p.n_edges) {
+        const float nxt = p.next[e];
+        if (!(nxt > p.epoch_f)) {
+            sampled = true;
+            const int dim = p.dim;
+            const int32_t head = p.heads[e];
+            const int32_t tail = p.tails[e];
+            float h0[kMaxDim], h[kMaxDim];
+            for (int c = 0; c < dim; ++c) h0[c] = h[c] = p.emb[static_cast<int64_t>(head) * dim + c];
+            if (head != tail) {
+                float* t = p.emb + static_cast<int64_t>(tail) * dim;
+                float d2 = 0.0f;
+                for (int c = 0; c < dim; ++c) {
+                    const float df = __fsub_rn(h[c], t[c]);
+                    d2 = __fadd_rn(d2, __fmul_rn(df, df));
+                }
+                float gc = 0.0f;
+                if (d2 > 0.0f) {
+                    const float pb = powf(d2, p.b);
+                    gc = __fdiv_rn(__fmul_rn(__fmul_rn(-2.0f * p.a, p.b), powf(d2, p.b - 1.0f)),
+                                   __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
+                }
+                for (int c = 0; c < dim; ++c) {
+                    const float g = clip4(__fmul_rn(gc, __fsub_rn(h[c], t[c])));
+                    const float mv = __fmul_rn(g, p.alpha);
+                    h[c] = __fadd_rn(h[c], mv);
+                    if (mv != 0.0f) atomicAdd(&t[c], -mv);
+                }
+                if (p.dens_on) {
+                    float sq = 0.0f;
+                    for (int c = 0; c < dim; ++c) {
+                        const float df = __fsub_rn(h[c], t[c]);
+                        sq = __fadd_rn(sq, __fmul_rn(df, df));
+                    }
+                    const float dist = __fsqrt_rn(sq);
+                    const float target =
+                        fmaxf(expf(__fmul_rn(__fadd_rn(p.radii[head], p.radii[tail]), 0.5f)), 1e-6f);
+                    const float coeff =
+                        __fdiv_rn(__fmul_rn(__fmul_rn(0.1f, p.dens_lambda), __fsub_rn(dist, target)),
+                                  __fadd_rn(dist, p.dens_var_shift));
+                    for (int c = 0; c < dim; ++c) {
+                        const float dir =
+                            __fdiv_rn(__fsub_rn(h[c], t[c]), __fadd_rn(dist, 1e-6f));
+                        const float mv = __fmul_rn(clip4(__fmul_rn(coeff, dir)), p.alpha);
+                        h[c] = __fsub_rn(h[c], mv);
+                        if (mv != 0.0f) atomicAdd(&t[c], mv);
+                    }
+                }
+            }
+            const float eps = p.eps[e];
+            p.next[e] = __fadd_rn(nxt, eps);
+            const float en = __fdiv_rn(eps, p.neg_rate_f);
+            if (isfinite(en) && en > 0.0f) {
+                const float nn = p.next_neg[e];
+                const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(p.epoch_f, nn), en));
+                for (uint32_t s = 0; s < n_neg; ++s) {
+                    const uint64_t word = rng_word(p.seed, static_cast<uint64_t>(e),
+                                                   (p.epoch << 32) | s);
+                    const uint32_t neg = rng_below(word, p.n_vertices);
+                    if (neg == static_cast<uint32_t>(head)) continue;
+                    const float* o = p.emb + static_cast<int64_t>(neg) * dim;
+                    float d2 = 0.0f;
+                    for (int c = 0; c < dim; ++c) {
+                        const float df = __fsub_rn(h[c], o[c]);
+                        d2 = __fadd_rn(d2, __fmul_rn(df, df));
+                    }
+                    if (d2 > 0.0f) {
+                        const float pb = powf(d2, p.b);
+                        const float gc =
+                            __fdiv_rn(p.rep_factor, __fmul_rn(__fadd_rn(0.001f, d2),
+                                                              __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
+                        if (gc > 0.0f)
+                            for (int c = 0; c < dim; ++c)
+                                h[c] = __fadd_rn(
+                                    h[c], __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(h[c], o[c]))),
+                                                    p.alpha));
+                    }
+                }
+                p.next_neg[e] = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), en));
+            }
+            for (int c = 0; c < dim; ++c)
+                if (h[c] != h0[c])
+                    atomicAdd(&p.emb[static_cast<int64_t>(head) * dim + c], __fsub_rn(h[c], h0[c]));
+        }
+    }
+    if (p.block_samples) count_block_samples(p.block_samples, sampled);
+}
+
+// local_radii_from_knn (lib.rs:5057-5082): one thread per row, FP32
+// sequential sum of ln(max(d, 0) + var_shift) over non-self neighbours.
+__global__ void local_radii_kernel(const int32_t* __restrict__ idx, const float* __restrict__ dist,
+                                   int64_t n, int k, float var_shift, float* __restrict__ out) {
+    const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    float sum = 0.0f;
+    int cnt = 0;
+    for (int c = 0; c < k; ++c) {
+        const float d = dist[r * k + c];
+        if (idx[r * k + c] == r && fabsf(d) <= 1e-5f) continue;  // SMOOTH_K_TOLERANCE
+        sum = __fadd_rn(sum, logf(__fadd_rn(fmaxf(d, 0.0f), var_shift)));
+        ++cnt;
+    }
+    out[r] = cnt == 0 ? logf(var_shift) : __fdiv_rn(sum, static_cast<float>(cnt));
+}
+
+// embedding_radii_from_knn (lib.rs:5084-5108) on the fitted embedding.
+__global__ void embedding_radii_kernel(const float* __restrict__ emb, int dim,
+                                       const int32_t* __restrict__ idx, int64_t n, int k,
+                                       float var_shift, float* __restrict__ out) {
+    const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    float sum = 0.0f;
+    int cnt = 0;
+    for (int c = 0; c < k; ++c) {
+        const int64_t j = idx[r * k + c];
+        if (j == r) continue;
+        float sq = 0.0f;
+        for (int t = 0; t < dim; ++t) {
+            const float df = __fsub_rn(emb[r * dim + t], emb[j * dim + t]);
+            sq = __fadd_rn(sq, __fmul_rn(df, df));
+        }
+        sum = __fadd_rn(sum, logf(__fadd_rn(fmaxf(__fsqrt_rn(sq), 0.0f), var_shift)));
+        ++cnt;
+    }
+    out[r] = cnt == 0 ? logf(var_shift) : __fdiv_rn(sum, static_cast<float>(cnt));
+}
 
 __global__ void __launch_bounds__(256) sgd_epoch_nd(SgdArgs p) {
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -243,6 +418,90 @@ __device__ inline bool row_finite(const float* v, int dim) {
     return true;
 }
 
+// The 2-D schedule of one query, the same arithmetic in the same order as
+// the general loop below.  Every position it reads is a fixed training
+// point (the edge's tail and the negatives drawn for it), so an edge's
+// positions are loaded together before the dependent updates: one memory
+// latency per edge instead of one per sample.
+constexpr int kNegPrefetch = 8;
+
+__device__ __forceinline__ void transform_schedule_2d(const TransformArgs& p, int64_t q,
+                                                      int32_t st, int32_t en, uint64_t qseed,
+                                                      float* cur) {
+    const float2* base = reinterpret_cast<const float2*>(p.base);
+    const float att = __fmul_rn(__fmul_rn(-2.0f, p.a), p.b);
+    const float rep = __fmul_rn(__fmul_rn(2.0f, p.rep), p.b);
+    float cx = cur[0], cy = cur[1];
+    for (int64_t epoch = 0; epoch < p.n_epochs && st < en; ++epoch) {
+        const float alpha = __fmul_rn(
+            p.lr, __fsub_rn(1.0f, __fdiv_rn(static_cast<float>(epoch),
+                                            static_cast<float>(p.n_epochs))));
+        const float ef = static_cast<float>(epoch);
+        for (int32_t e = st; e < en; ++e) {
+            const float nx = p.next[e];
+            if (nx > ef || !(isfinite(cx) && isfinite(cy))) continue;
+            const float eps = p.eps[e];
+            const float eneg = __fdiv_rn(eps, p.neg_rate_f);
+            const bool neg_ok = isfinite(eneg) && eneg > 0.0f;
+            const float nn = p.next_neg[e];
+            const uint32_t n_neg = neg_ok ? floor_count(__fdiv_rn(__fsub_rn(ef, nn), eneg)) : 0u;
+            // loads first: the tail and the first kNegPrefetch negatives
+            const float2 ot = base[p.tails[e]];
+            float2 ng[kNegPrefetch];
+#pragma unroll
+            for (int s = 0; s < kNegPrefetch; ++s) {
+                if (static_cast<uint32_t>(s) < n_neg) {
+                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                                                   (static_cast<uint64_t>(epoch) << 32) | s);
+                    ng[s] = base[rng_below(word, p.n_base)];
+                }
+            }
+            {
+                const float dx = __fsub_rn(cx, ot.x), dy = __fsub_rn(cy, ot.y);
+                const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+                float gc = 0.0f;
+                if (d2 > 0.0f) {
+                    const float pb = powf(d2, p.b);
+                    gc = __fdiv_rn(__fmul_rn(att, powf(d2, p.b - 1.0f)),
+                                   __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
+                }
+                cx = __fadd_rn(cx, __fmul_rn(clip4(__fmul_rn(gc, dx)), alpha));
+                cy = __fadd_rn(cy, __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(cy, ot.y))), alpha));
+            }
+            p.next[e] = __fadd_rn(nx, eps);
+            if (!neg_ok) continue;
+            for (uint32_t s = 0; s < n_neg; ++s) {
+                float2 o;
+                if (s < static_cast<uint32_t>(kNegPrefetch)) {
+                    o = ng[0];
+#pragma unroll
+                    for (int t = 1; t < kNegPrefetch; ++t)
+                        if (s == static_cast<uint32_t>(t)) o = ng[t];
+                } else {
+                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                                                   (static_cast<uint64_t>(epoch) << 32) | s);
+                    o = base[rng_below(word, p.n_base)];
+                }
+                const float dx = __fsub_rn(cx, o.x), dy = __fsub_rn(cy, o.y);
+                const float dd = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+                float g2 = 0.0f;
+                if (dd > 0.0f) {
+                    const float pb = powf(dd, p.b);
+                    g2 = __fdiv_rn(rep, __fmul_rn(__fadd_rn(0.001f, dd),
+                                                  __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
+                }
+                if (g2 > 0.0f) {
+                    cx = __fadd_rn(cx, __fmul_rn(clip4(__fmul_rn(g2, dx)), alpha));
+                    cy = __fadd_rn(cy, __fmul_rn(clip4(__fmul_rn(g2, __fsub_rn(cy, o.y))), alpha));
+                }
+            }
+            p.next_neg[e] = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), eneg));
+        }
+    }
+    cur[0] = cx;
+    cur[1] = cy;
+}
+
 __global__ void __launch_bounds__(128) transform_kernel(TransformArgs p) {
     const int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (q >= p.nq) return;
@@ -278,6 +537,12 @@ __global__ void __launch_bounds__(128) transform_kernel(TransformArgs p) {
     }
     // optimize_layout_transform (lib.rs:5444-5544)
     const uint64_t qseed = mix64(p.seed ^ mix64(static_cast<uint64_t>(q)));
+    if (dim == 2) {
+        transform_schedule_2d(p, q, st, en, qseed, cur);
+        p.out[q * 2] = cur[0];
+        p.out[q * 2 + 1] = cur[1];
+        return;
+    }
     for (int64_t epoch = 0; epoch < p.n_epochs && st < en; ++epoch) {
         const float alpha = __fmul_rn(
             p.lr, __fsub_rn(1.0f, __fdiv_rn(static_cast<float>(epoch),
@@ -334,20 +599,77 @@ __global__ void __launch_bounds__(128) transform_kernel(TransformArgs p) {
 
 }  // namespace
 
+void local_radii(const int32_t* idx, const float* dist, int64_t n, int k, float var_shift,
+                 float* out, cudaStream_t s) {
+    if (n == 0) return;
+    local_radii_kernel<<<static_cast<unsigned>(ceil_div(n, 256)), 256, 0, s>>>(idx, dist, n, k,
+                                                                             var_shift, out);
+    UMAPB_LAUNCH_CHECK();
+}
+
+void embedding_radii(const float* emb, int dim, const int32_t* idx, int64_t n, int k,
+                     float var_shift, float* out, cudaStream_t s) {
+    if (n == 0) return;
+    embedding_radii_kernel<<<static_cast<unsigned>(ceil_div(n, 256)), 256, 0, s>>>(
+        emb, dim, idx, n, k, var_shift, out);
+    UMAPB_LAUNCH_CHECK();
+}
+
+int64_t density_start_epoch(int64_t n_epochs, float frac) {
+    // lib.rs:5052-5055, the product taken in f32
+    const int64_t active = std::max<int64_t>(
+        static_cast<int64_t>(std::ceil(static_cast<float>(n_epochs) * frac)), 1);
+    return n_epochs > active ? n_epochs - active : 0;
+}
+
 double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, int64_t n_epochs,
                        float a, float b, float lr, int64_t neg_rate, float repulsion,
-                       uint64_t seed, bool count_samples, float* kernel_ms, cudaStream_t s) {
+                       uint64_t seed, bool count_samples, float* kernel_ms, cudaStream_t s,
+                       const DensityParams* dens) {
     const int64_t m = g.n_edges;
     if (m == 0 || n_vertices == 0 || n_epochs == 0) return 0.0;
     if (dim > kMaxDim) invalid("n_components above 16 is not supported by the GPU layout kernel");
     const float mx = std::max(max_weight(g.weights.get(), m, s), 1e-12f);
+    DevBuf<int32_t> sorted_heads, sorted_tails;
+    if (m > 0x7FFFFFFFll) invalid("optimize_layout: too many edges");
     DevBuf<float> eps(m, s), next(m, s), next_neg(m, s);
     const float nef = static_cast<float>(n_epochs);
     const float nrf = static_cast<float>(neg_rate);
-    epochs_per_sample_kernel<<<static_cast<unsigned>(ceil_div(m, 256)), 256, 0, s>>>(
-        g.weights.get(), m, mx, nef, nrf, eps.get(), next.get(), next_neg.get());
-    UMAPB_LAUNCH_CHECK();
     const unsigned grid = static_cast<unsigned>(ceil_div(m, 256));
+    {
+        // Edge periods (make_epochs_per_sample, lib.rs:4937-4960).  Within
+        // each window of 65536 consecutive edges (graph order, by head) the
+        // edges are ordered by period: edges with close periods fire in the
+        // same epochs, so the lanes of a warp mostly fire together, while the
+        // sweep over heads keeps the graph order across the epoch.  Each
+        // edge's schedule and arithmetic are the reference's; only the order
+        // of concurrent edges changes, as in any Hogwild order.
+        DevBuf<float> eps_raw(m, s);
+        epochs_per_sample_kernel<<<grid, 256, 0, s>>>(g.weights.get(), m, mx, nef, nrf,
+                                                      eps_raw.get(), nullptr, nullptr);
+        UMAPB_LAUNCH_CHECK();
+        DevBuf<uint64_t> keys(m, s), keys_sorted(m, s);
+        DevBuf<int32_t> ids(m, s), order(m, s);
+        period_keys_kernel<<<grid, 256, 0, s>>>(eps_raw.get(), m, keys.get(), ids.get());
+        UMAPB_LAUNCH_CHECK();
+        int window_bits = 1;
+        while ((static_cast<int64_t>(1) << window_bits) <= (m >> kSortWindowShift)) ++window_bits;
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.get(), keys_sorted.get(), ids.get(),
+                                        order.get(), static_cast<int>(m), 0, 32 + window_bits, s);
+        DevBuf<uint8_t> tmp(bytes, s);
+        cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, keys.get(), keys_sorted.get(),
+                                        ids.get(), order.get(), static_cast<int>(m), 0,
+                                        32 + window_bits, s);
+        UMAPB_CUDA(cudaGetLastError());
+        sorted_heads.alloc(m, s);
+        sorted_tails.alloc(m, s);
+        gather_edges_kernel<<<grid, 256, 0, s>>>(order.get(), g.heads.get(), g.tails.get(),
+                                                 eps_raw.get(), nrf, m, sorted_heads.get(),
+                                                 sorted_tails.get(), eps.get(), next.get(),
+                                                 next_neg.get());
+        UMAPB_LAUNCH_CHECK();
+    }
     DevBuf<uint32_t> samples;
     if (count_samples) {
         samples.alloc(grid, s);
@@ -355,8 +677,8 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
     }
     SgdArgs p{};
     p.emb = emb;
-    p.heads = g.heads.get();
-    p.tails = g.tails.get();
+    p.heads = sorted_heads.get();
+    p.tails = sorted_tails.get();
     p.eps = eps.get();
     p.next = next.get();
     p.next_neg = next_neg.get();
@@ -370,6 +692,11 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
     p.neg_rate_f = nrf;
     p.seed = seed;
     p.block_samples = samples.get();
+    if (dens) {
+        p.radii = dens->radii;
+        p.dens_lambda = dens->lambda;
+        p.dens_var_shift = dens->var_shift;
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (kernel_ms) {
         UMAPB_CUDA(cudaEventCreate(&e0));
@@ -381,10 +708,14 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
         p.alpha = lr * (1.0f - static_cast<float>(epoch) / nef);
         p.epoch_f = static_cast<float>(epoch);
         p.epoch = static_cast<uint64_t>(epoch);
-        if (dim == 2)
+        if (dens) {
+            p.dens_on = epoch >= dens->start_epoch ? 1 : 0;
+            sgd_epoch_dens<<<grid, 256, 0, s>>>(p);
+        } else if (dim == 2) {
             sgd_epoch_2d<<<grid, 256, 0, s>>>(p);
-        else
+        } else {
             sgd_epoch_nd<<<grid, 256, 0, s>>>(p);
+        }
         UMAPB_LAUNCH_CHECK();
     }
     if (kernel_ms) {
