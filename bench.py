@@ -50,6 +50,15 @@ T_FIT, T_QUERY, T_DIM = 200_000, 1_000_000, 128
 T_SAMPLE = 2_000  # queries of the CPU transform baseline
 
 
+def pool_reserved_gb(lib) -> float:
+    """GB the device's stream-ordered memory pool holds mapped right now."""
+    from umapers_b200 import _lib
+
+    reserved, used = ctypes.c_int64(0), ctypes.c_int64(0)
+    _lib.check(lib.umapb_pool_bytes(ctypes.byref(reserved), ctypes.byref(used)))
+    return round(reserved.value / 1e9, 3)
+
+
 def peaks() -> dict:
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -241,14 +250,16 @@ def run_gpu(args) -> None:
 
     for _ in range(args.warmup):
         device_step()
+    pool0 = pool_reserved_gb(lib)
     launches0 = lib.umapb_kernel_launches()
     barrier()
     sampler = ClockSampler(local)
     with sampler:
         dev_times = []
-        knn_sec, sgd_sec, stage = [], [], []
+        knn_sec, sgd_sec, stage, pool = [], [], [], []
         for _ in range(args.steps):
             dev_times.append(device_step())
+            pool.append(pool_reserved_gb(lib))
             knn_sec.append(info.knn_kernel_sec)
             sgd_sec.append(timings.optimize_sec)
             stage.append({f: getattr(timings, f) for f in _lib.TIMING_FIELDS})
@@ -333,6 +344,9 @@ def run_gpu(args) -> None:
                                      "optimize_sec", "total_sec")},
             "quality": {k: round(v, 4) for k, v in q.items()},
             "clocks": sampler.summary(),
+            # per timed step: its time, and the memory pool's mapped size after it
+            "step_sec": [round(t, 4) for t in dev_times],
+            "pool_reserved_gb": [pool0] + pool,
         }
         if transform is not None:
             line["transform"] = transform

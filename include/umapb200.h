@@ -148,6 +148,10 @@ const char* umapb_last_error(void);
 /* Number of kernels this library has launched in the process so far (no
  * reference counterpart; used to attribute device work in benchmarks). */
 uint64_t umapb_kernel_launches(void);
+/* Bytes the current device's default stream-ordered memory pool holds mapped
+ * (reserved) and hands out (used) right now; the fit's working buffers come
+ * from that pool (no reference counterpart; memory diagnostics). */
+int32_t umapb_pool_bytes(int64_t* reserved, int64_t* used);
 /* Defaults of UmapParams::default (rust_umap/src/lib.rs:170-195). */
 void umapb_params_default(umapb_params* params);
 

@@ -108,3 +108,40 @@ def test_full_fit_quality_matches_oracle_mixture(orc):
     assert abs(qg["trustworthiness"] - qo["trustworthiness"]) <= 0.005
     assert abs(qg["knn_preservation"] - qo["knn_preservation"]) <= 0.005 or \
         qg["knn_preservation"] > qo["knn_preservation"]
+
+
+def test_device_rows_are_validated_before_the_fit():
+    """transform_rows / validate_data's finiteness check (lib.rs:2113-2138)
+    on rows already on the device: the first non-finite row is named, for an
+    aligned array whose last elements do not fill a 16-byte vector and for an
+    array that starts off a 16-byte boundary."""
+    import torch
+
+    from umapers_b200 import _lib
+
+    lib = _lib.load()
+    n, d = 1001, 3
+    x = np.random.default_rng(0).normal(size=(n, d)).astype(np.float32)
+    out = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    m = Umap(n_neighbors=10, n_epochs=10, ann_mode="exact")
+
+    def fit_device(ptr):
+        _lib.check(lib.umapb_fit_transform_device(m._core._handle, ptr, n, d, out.data_ptr(),
+                                                  None, None))
+
+    bad = x.copy()
+    bad[1000, 2] = np.nan  # element 3002: past the last whole float4
+    xd = torch.from_numpy(bad).cuda()
+    assert xd.data_ptr() % 16 == 0
+    with pytest.raises(ValueError, match="non-finite value at row 1000"):
+        fit_device(xd.data_ptr())
+    bad = x.copy()
+    bad[517, 1] = np.inf
+    bad[900, 0] = np.nan
+    flat = torch.zeros(n * d + 1, dtype=torch.float32, device="cuda")
+    flat[1:] = torch.from_numpy(bad.ravel()).cuda()
+    assert (flat.data_ptr() + 4) % 16 != 0
+    with pytest.raises(ValueError, match="non-finite value at row 517"):
+        fit_device(flat.data_ptr() + 4)
+    fit_device(torch.from_numpy(x).cuda().data_ptr())  # finite rows fit
+    assert torch.isfinite(out).all()

@@ -198,6 +198,7 @@ SIGNATURES = {
     "umapb_abi_version": (_i32, []),
     "umapb_last_error": (ctypes.c_char_p, []),
     "umapb_kernel_launches": (_u64, []),
+    "umapb_pool_bytes": (_i32, [_vp, _vp]),
     "umapb_params_default": (None, [ctypes.POINTER(Params)]),
     "umapb_create": (_i32, [ctypes.POINTER(Params), ctypes.POINTER(_vp)]),
     "umapb_destroy": (None, [_vp]),

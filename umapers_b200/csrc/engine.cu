@@ -568,6 +568,21 @@ int32_t umapb_abi_version(void) { return UMAPB_ABI_VERSION; }
 const char* umapb_last_error(void) { return g_last_error.c_str(); }
 uint64_t umapb_kernel_launches(void) { return g_kernel_launches.load(); }
 
+int32_t umapb_pool_bytes(int64_t* reserved, int64_t* used) {
+    return guarded([&] {
+        if (!reserved || !used) invalid("null output pointer");
+        int dev = 0;
+        UMAPB_CUDA(cudaGetDevice(&dev));
+        cudaMemPool_t pool;
+        UMAPB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+        unsigned long long r = 0, u = 0;
+        UMAPB_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));
+        UMAPB_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+        *reserved = static_cast<int64_t>(r);
+        *used = static_cast<int64_t>(u);
+    });
+}
+
 void umapb_params_default(umapb_params* p) {
     if (!p) return;
     std::memset(p, 0, sizeof(*p));

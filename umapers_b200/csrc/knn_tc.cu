@@ -21,18 +21,20 @@
 //    warps per query tile each own 32 rows x 64 columns of the accumulator:
 //    they read it with tcgen05.ld and keep, per (row, column half), the
 //    S = 32 smallest (L, index) keys in a global list.  A per-list threshold
-//    skips a 32-column chunk with one vote in the common case; otherwise the
-//    chunk is transposed across the warp with shuffles and its qualifying
-//    keys are inserted cooperatively (one list entry per lane).  When the
-//    query tiles are fewer than the SMs, the candidate tiles are split too,
-//    with lists per split.
-// 3. rerank: one warp per row recomputes the exact FP32 distances of every
-//    list's candidates in the reference's summation order and keeps the k
-//    smallest (distance, index) keys.  With U_j = L_j + 2 e_j and B the
-//    smallest largest-L of the full lists, every candidate missing from the
-//    lists has d >= B, so the row is certified when at least k candidates have
-//    U < B.  Rows that fail (near-ties wider than the bound) are recomputed by
-//    knn_plain.
+//    skips a row's 64 columns with one vote in the common case; otherwise the
+//    row's values are transposed across the warp through a shared-memory
+//    scratch and its qualifying keys are inserted cooperatively (one list
+//    entry per lane), while the next pending row's list is already being
+//    loaded.  When the query tiles are fewer than the SMs, the candidate
+//    tiles are split too (one wave of units), with lists per split.
+// 3. rerank: one warp per row recomputes exact FP32 distances in the
+//    reference's summation order and keeps the k smallest (distance, index)
+//    keys.  With U_j = L_j + 2 e_j and B the smallest largest-L of the full
+//    lists, every candidate missing from the lists has d >= B, so the row is
+//    certified when at least k candidates have U < B.  Only listed candidates
+//    with L <= T, T the k-th smallest U, can rank in the top k, so only they
+//    are recomputed.  Rows that fail (near-ties wider than the bound) are
+//    recomputed by knn_plain.
 //
 // Every wait on an mbarrier is bounded by a %globaltimer deadline; a timeout
 // sets an error word, stops all roles, drains in-flight copies and frees TMEM.
@@ -56,6 +58,8 @@ constexpr int BK = kBK;     // bf16 columns per k-block (one 128-byte swizzle ro
 constexpr int UK = kUK;     // K of one tcgen05.mma kind::f16
 constexpr int S = 32;       // shortlist length per row
 constexpr int kTileBytes = BM * BK * 2;  // 16 KiB
+constexpr int kBarBytes = 256;           // mbarriers, TMEM address, abort flag
+constexpr int kScratchBytes = 256;       // per epilogue warp: one row's 64 values
 constexpr uint32_t kIdesc = idesc_bf16(BM, BN);
 
 // Bound constants (see header comment).  c1 covers the split products
@@ -287,6 +291,7 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
         const int slot = (warp - 2) >> 2;
         const int mt = slot >> 1;
         const int half = slot & 1;
+        const uint32_t scratch = b_full + kBarBytes + (warp - 2) * kScratchBytes;
         uint64_t cg = 0;
         bool ok = true;
         for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x) {
@@ -294,6 +299,9 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
             const int32_t row = (w.group * MT + mt) * BM + quarter * 32 + lane;
             const bool row_ok = row < p.n_q;
             const int32_t list_base = w.split * 2 + half;  // list of (row, split, half)
+            auto list_of = [&](int32_t srow) {
+                return p.lists + (static_cast<int64_t>(srow) * 2 * p.n_split + list_base) * S;
+            };
             float tau = INFINITY;  // this list's current S-th smallest bound
             for (int32_t c = 0; c < w.len; ++c, ++cg) {
                 const uint32_t buf = static_cast<uint32_t>(cg & 1);
@@ -314,38 +322,51 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
                 __syncwarp();
                 if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
                 const float m0 = min32(r[0]), m1 = min32(r[1]);
-                const unsigned pend0 = __ballot_sync(0xffffffffu, row_ok && m0 < tau);
-                const unsigned pend1 = __ballot_sync(0xffffffffu, row_ok && m1 < tau);
-                if ((pend0 | pend1) == 0) continue;
+                unsigned pend = __ballot_sync(0xffffffffu, row_ok && fminf(m0, m1) < tau);
+                if (pend == 0) continue;
                 const int32_t colh = tile_at(c, w) * BN + half * (BN / 2);
+                const int32_t valid_cols = static_cast<int32_t>(p.n_r - colh);
+                // Rows are served one at a time; the next pending row's list is
+                // loaded while the current one is merged, hiding its L2 latency.
+                int src = __ffs(pend) - 1;
+                uint64_t* lst = list_of(__shfl_sync(0xffffffffu, row, src));
+                uint64_t lk_next = lst[lane];
+                while (pend) {
+                    pend &= pend - 1;
+                    const int cur = src;
+                    uint64_t* cur_lst = lst;
+                    uint64_t lk = lk_next;
+                    if (pend) {
+                        src = __ffs(pend) - 1;
+                        lst = list_of(__shfl_sync(0xffffffffu, row, src));
+                        lk_next = lst[lane];
+                    }
+                    // transpose through the warp's scratch: lane j takes
+                    // columns j and 32 + j of the source row
+                    if (lane == cur) {
 #pragma unroll
-                for (int ch = 0; ch < 2; ++ch) {
-                    unsigned pend = ch == 0 ? pend0 : pend1;
-                    const int32_t col0 = colh + ch * 32;
-                    const int32_t valid_cols = static_cast<int32_t>(p.n_r - col0);
-                    while (pend) {
-                        const int src = __ffs(pend) - 1;
-                        pend &= pend - 1;
-                        const int32_t srow = __shfl_sync(0xffffffffu, row, src);
-                        float stau = __shfl_sync(0xffffffffu, tau, src);
-                        uint64_t* lst =
-                            p.lists + (static_cast<int64_t>(srow) * 2 * p.n_split + list_base) * S;
-                        uint64_t lk = lst[lane];  // in flight while the row is transposed
-                        // lane j takes column j of the source row
-                        float mine = 0.0f;
+                        for (int j = 0; j < 16; ++j)
+                            st_shared_v4(scratch + 16 * j, r[j >> 3][(j & 7) * 4],
+                                         r[j >> 3][(j & 7) * 4 + 1], r[j >> 3][(j & 7) * 4 + 2],
+                                         r[j >> 3][(j & 7) * 4 + 3]);
+                    }
+                    __syncwarp();
+                    const float v0 = ld_shared_f32(scratch + 4 * lane);
+                    const float v1 = ld_shared_f32(scratch + 4 * (32 + lane));
+                    __syncwarp();
+                    float stau = __shfl_sync(0xffffffffu, tau, cur);
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const float t = __shfl_sync(0xffffffffu, __uint_as_float(r[ch][j]), src);
-                            if (lane == j) mine = t;
-                        }
-                        unsigned q = __ballot_sync(0xffffffffu, mine < stau && lane < valid_cols);
+                    for (int ch = 0; ch < 2; ++ch) {
+                        const float mine = ch == 0 ? v0 : v1;
+                        unsigned q = __ballot_sync(0xffffffffu,
+                                                   mine < stau && lane + ch * 32 < valid_cols);
                         while (q) {
                             const int b = __ffs(q) - 1;
                             q &= q - 1;
                             const float val = __shfl_sync(0xffffffffu, mine, b);
                             if (!(val < stau)) continue;
                             const uint64_t key = (static_cast<uint64_t>(f2o(val)) << 32) |
-                                                 static_cast<uint32_t>(col0 + b);
+                                                 static_cast<uint32_t>(colh + ch * 32 + b);
                             const int pos = __popc(__ballot_sync(0xffffffffu, lk < key));
                             const uint64_t up = __shfl_up_sync(0xffffffffu, lk, 1);
                             if (lane > pos)
@@ -355,9 +376,9 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
                             const uint64_t last = __shfl_sync(0xffffffffu, lk, S - 1);
                             stau = last == ~0ull ? INFINITY : o2f(static_cast<uint32_t>(last >> 32));
                         }
-                        lst[lane] = lk;
-                        if (lane == src) tau = stau;
                     }
+                    cur_lst[lane] = lk;
+                    if (lane == cur) tau = stau;
                 }
             }
         }
@@ -433,6 +454,22 @@ __device__ __forceinline__ float sqdist_ref(const float* __restrict__ x, const f
 #pragma unroll
         for (int l = 0; l < 8; ++l) lane[l] = 0.0f;
         int i = 0;
+        if (((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0) {
+            // the same operations in the same order, from 16-byte loads
+            for (; i + 8 <= d; i += 8) {
+                const float4 xa = *reinterpret_cast<const float4*>(x + i);
+                const float4 xb = *reinterpret_cast<const float4*>(x + i + 4);
+                const float4 ya = __ldg(reinterpret_cast<const float4*>(y + i));
+                const float4 yb = __ldg(reinterpret_cast<const float4*>(y + i + 4));
+                const float xs[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+                const float ys[8] = {ya.x, ya.y, ya.z, ya.w, yb.x, yb.y, yb.z, yb.w};
+#pragma unroll
+                for (int l = 0; l < 8; ++l) {
+                    const float df = __fsub_rn(xs[l], ys[l]);
+                    lane[l] = __fadd_rn(lane[l], __fmul_rn(df, df));
+                }
+            }
+        }
         for (; i + 8 <= d; i += 8)
 #pragma unroll
             for (int l = 0; l < 8; ++l) {
@@ -495,24 +532,51 @@ __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restri
         if (__popc(__ballot_sync(0xffffffffu, valid)) == S)
             bound = fmin(bound, static_cast<double>(lmax));
     }
-    // Exact keys in the reference's order; the 32 smallest of all lists are
-    // kept sorted across the warp (bitonic merge of each sorted list into
-    // them), and k candidates with d <= U < bound certify the row.
+    // Upper bounds U = L + 2e (rounded up to FP32): `below` counts the
+    // candidates with U < bound (k of them certify the row), and T is the k-th
+    // smallest U.  A candidate with L > T has k others with d <= U <= T < L <= d
+    // ahead of it, so only candidates with L <= T can rank in the top k: each
+    // list (sorted by L) contributes a prefix, usually empty.
     const double nq = qsq[row];
     int below = 0;
+    float topu = INFINITY;  // the 32 smallest U, sorted across the warp
+    for (int h = 0; h < n_lists; ++h) {
+        const uint64_t lk = rl[h * S + lane];
+        const float l0 = o2f(static_cast<uint32_t>(__shfl_sync(0xffffffffu, lk, 0) >> 32));
+        double U = INFINITY;
+        if (lk != ~0ull) {
+            const double nc = rsq[static_cast<uint32_t>(lk)];
+            U = static_cast<double>(o2f(static_cast<uint32_t>(lk >> 32))) +
+                2.0 * (c1 * sqrt(nq * nc) + c2 * (nq + nc));
+        }
+        below += __popc(__ballot_sync(0xffffffffu, U < bound));
+        // a list whose smallest L already exceeds the k-th smallest U so far
+        // cannot lower it
+        if (!(l0 <= __shfl_sync(0xffffffffu, topu, k - 1))) continue;
+        const float u = warp_sort_asc<float>(__double2float_ru(U));
+        const float ur = __shfl_sync(0xffffffffu, u, 31 - lane);
+        float m = fminf(topu, ur);
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+            const float o = __shfl_xor_sync(0xffffffffu, m, st);
+            m = (lane & st) ? fmaxf(m, o) : fminf(m, o);
+        }
+        topu = m;
+    }
+    const float T = __shfl_sync(0xffffffffu, topu, k - 1);
+    // Exact keys in the reference's order for the candidates with L <= T; the
+    // 32 smallest are kept sorted across the warp (bitonic merge of each
+    // list's keys into them).
     uint64_t top = ~0ull;
     for (int h = 0; h < n_lists; ++h) {
         const uint64_t lk = rl[h * S + lane];
-        double U = INFINITY;
+        const bool take = lk != ~0ull && o2f(static_cast<uint32_t>(lk >> 32)) <= T;
+        if (__ballot_sync(0xffffffffu, take) == 0) continue;
         uint64_t key = ~0ull;
-        if (lk != ~0ull) {
+        if (take) {
             const uint32_t j = static_cast<uint32_t>(lk);
-            const double nc = rsq[j];
-            U = static_cast<double>(o2f(static_cast<uint32_t>(lk >> 32))) +
-                2.0 * (c1 * sqrt(nq * nc) + c2 * (nq + nc));
             key = knn_key(sqdist_ref(Q + row * d, R + static_cast<int64_t>(j) * d, d), j);
         }
-        below += __popc(__ballot_sync(0xffffffffu, U < bound));
         const uint64_t b = warp_sort_asc<uint64_t>(key);
         const uint64_t br = __shfl_sync(0xffffffffu, b, 31 - lane);
         uint64_t m = top < br ? top : br;
@@ -539,8 +603,9 @@ int query_tiles_for(int kb) { return kb <= 4 ? 2 : (kb <= 10 ? 1 : 0); }
 
 template <int MT, int ST>
 void launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, cudaStream_t s) {
-    // tiles + 1 KiB alignment slack + barriers/flags (256 B)
-    const size_t smem = static_cast<size_t>(MT * a.kb + ST) * kTileBytes + 1024 + 256;
+    // tiles + 1 KiB alignment slack + barriers/flags + epilogue scratch
+    const size_t smem = static_cast<size_t>(MT * a.kb + ST) * kTileBytes + 1024 + kBarBytes +
+                        static_cast<size_t>(8 * MT) * kScratchBytes;
     auto kern = tc_knn_kernel<MT, ST>;
     UMAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
@@ -553,8 +618,9 @@ void launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, cu
 }
 
 // Work decomposition: groups of MT query tiles; when the groups are fewer
-// than the SMs the candidate tiles are split too (at least 8 per split), so
-// small query sets still occupy the GPU.
+// than the SMs the candidate tiles are split too (at least 8 per split, and
+// no more units than SMs, so every unit starts at once), so small query sets
+// still occupy the GPU.
 TcArgs plan(int64_t n_q, int64_t n_r, int d, bool allow_split) {
     const int kp = padded_k(d);
     TcArgs a{};
@@ -571,7 +637,8 @@ TcArgs plan(int64_t n_q, int64_t n_r, int d, bool allow_split) {
         UMAPB_CUDA(cudaGetDevice(&dev));
         UMAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         if (groups < sms)
-            split = std::min<int64_t>(ceil_div(sms, groups), std::max<int64_t>(1, a.n_ctiles / 8));
+            split = std::min<int64_t>(std::max<int64_t>(sms / groups, 1),
+                                      std::max<int64_t>(1, a.n_ctiles / 8));
     }
     a.split_tiles = ceil_div(a.n_ctiles, split);
     a.n_split = static_cast<int>(ceil_div(a.n_ctiles, a.split_tiles));

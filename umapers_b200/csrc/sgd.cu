@@ -51,17 +51,28 @@ __global__ void epochs_per_sample_kernel(const float* __restrict__ w, int64_t m,
     if (next_neg) next_neg[e] = __fdiv_rn(v, neg_rate_f);
 }
 
-// Sort keys of the edge order: the window of 2^kSortWindowShift consecutive edges
+// Sort keys of the edge order: the window of 2^shift consecutive edges
 // (graph order, i.e. by head) in the high word, the sampling period in the
 // low word.  Periods are positive floats or +inf, whose bit patterns order
-// as unsigned integers.
-constexpr int kSortWindowShift = 16;  // windows of 65536 edges
+// as unsigned integers.  Windows hold 65536 edges at most and are cut
+// smaller on small graphs, so that a graph always spans at least 256 of them
+// (down to 512 edges): the coarse head order survives the sort.
+constexpr int kSortWindowMaxShift = 16;
+constexpr int kSortWindowMinShift = 9;
+constexpr int64_t kSortMinWindows = 256;
 
-__global__ void period_keys_kernel(const float* __restrict__ eps, int64_t m,
+int sort_window_shift(int64_t m) {
+    int shift = kSortWindowMinShift;
+    while (shift < kSortWindowMaxShift && (static_cast<int64_t>(1) << (shift + 1)) * kSortMinWindows <= m)
+        ++shift;
+    return shift;
+}
+
+__global__ void period_keys_kernel(const float* __restrict__ eps, int64_t m, int shift,
                                    uint64_t* __restrict__ keys, int32_t* __restrict__ ids) {
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= m) return;
-    keys[e] = (static_cast<uint64_t>(e >> kSortWindowShift) << 32) | __float_as_uint(eps[e]);
+    keys[e] = (static_cast<uint64_t>(e >> shift) << 32) | __float_as_uint(eps[e]);
     ids[e] = static_cast<int32_t>(e);
 }
 
@@ -502,11 +513,183 @@ __device__ __forceinline__ void transform_schedule_2d(const TransformArgs& p, in
     cur[1] = cy;
 }
 
-__global__ void __launch_bounds__(128) transform_kernel(TransformArgs p) {
-    const int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+// A 2-D query with at most kStageEdges edges keeps its whole edge state in
+// shared memory: the tail positions (fixed training points) and the
+// per-edge schedule (eps, epoch of next sample, epoch of next negative
+// sample), loaded once before the first epoch.  The schedule loop then
+// touches global memory only for the negative samples.  Slot [j][tid]
+// belongs to thread tid alone, so no barrier is needed.
+constexpr int kTransformThreads = 128;
+constexpr int kStageEdges = 16;
+
+struct TransformStage {
+    float next[kStageEdges][kTransformThreads];
+    float next_neg[kStageEdges][kTransformThreads];
+    float eps[kStageEdges][kTransformThreads];
+    float2 tail[kStageEdges][kTransformThreads];
+};
+
+// init_graph_transform (lib.rs:4793-4836) for a staged 2-D query, the same
+// arithmetic in the same order as the general path in transform_kernel.
+__device__ __forceinline__ void stage_query_2d(const TransformArgs& p, int32_t st, int cnt,
+                                               TransformStage& sm, int tid, float* cur) {
+    const float2* base = reinterpret_cast<const float2*>(p.base);
+    int32_t tl[kStageEdges];
+    float w[kStageEdges];
+#pragma unroll
+    for (int j = 0; j < kStageEdges; ++j) {
+        if (j < cnt) {
+            tl[j] = p.tails[st + j];
+            w[j] = p.weights[st + j];
+            sm.eps[j][tid] = p.eps[st + j];
+            sm.next[j][tid] = p.next[st + j];
+            sm.next_neg[j][tid] = p.next_neg[st + j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kStageEdges; ++j)
+        if (j < cnt) sm.tail[j][tid] = base[tl[j]];
+    if (cnt == 0) {
+        cur[0] = cur[1] = NAN;
+        return;
+    }
+    int copy_j = -1;
+#pragma unroll
+    for (int j = 0; j < kStageEdges; ++j)
+        if (j < cnt && copy_j < 0 && fabsf(__fsub_rn(w[j], 1.0f)) < FLT_EPSILON) copy_j = j;
+    if (copy_j >= 0) {
+        const float2 t = sm.tail[copy_j][tid];
+        cur[0] = t.x;
+        cur[1] = t.y;
+        return;
+    }
+    float sum = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kStageEdges; ++j)
+        if (j < cnt) sum = __fadd_rn(sum, w[j]);
+    if (sum <= 0.0f) {
+        cur[0] = cur[1] = NAN;
+        return;
+    }
+    cur[0] = cur[1] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kStageEdges; ++j) {
+        if (j < cnt) {
+            const float wj = __fdiv_rn(w[j], sum);
+            const float2 t = sm.tail[j][tid];
+            cur[0] = __fadd_rn(cur[0], __fmul_rn(wj, t.x));
+            cur[1] = __fadd_rn(cur[1], __fmul_rn(wj, t.y));
+        }
+    }
+}
+
+// transform_schedule_2d over the staged edge state; edge j of the query is
+// graph edge st + j, which keys its negative-sample stream.  Each epoch
+// first collects the query's due edges in a bit mask, then serves them in
+// edge order: the lanes of a warp step through their own due edges together,
+// so a warp runs as many edge updates as its busiest query has due, not as
+// many as all 32 queries have together.
+__device__ __forceinline__ void transform_schedule_2d_staged(const TransformArgs& p, int32_t st,
+                                                             int cnt, uint64_t qseed,
+                                                             TransformStage& sm, int tid,
+                                                             float* cur) {
+    const float2* base = reinterpret_cast<const float2*>(p.base);
+    const float att = __fmul_rn(__fmul_rn(-2.0f, p.a), p.b);
+    const float rep = __fmul_rn(__fmul_rn(2.0f, p.rep), p.b);
+    float cx = cur[0], cy = cur[1];
+    if (!(isfinite(cx) && isfinite(cy))) return;  // every sample would be skipped
+    for (int64_t epoch = 0; epoch < p.n_epochs; ++epoch) {
+        const float alpha = __fmul_rn(
+            p.lr, __fsub_rn(1.0f, __fdiv_rn(static_cast<float>(epoch),
+                                            static_cast<float>(p.n_epochs))));
+        const float ef = static_cast<float>(epoch);
+        uint32_t due = 0;
+#pragma unroll
+        for (int j = 0; j < kStageEdges; ++j)
+            if (j < cnt && !(sm.next[j][tid] > ef)) due |= 1u << j;
+        while (due) {
+            const int j = __ffs(due) - 1;
+            due &= due - 1;
+            if (!(isfinite(cx) && isfinite(cy))) continue;
+            const float nx = sm.next[j][tid];
+            const int64_t e = st + j;
+            const float eps = sm.eps[j][tid];
+            const float eneg = __fdiv_rn(eps, p.neg_rate_f);
+            const bool neg_ok = isfinite(eneg) && eneg > 0.0f;
+            const float nn = sm.next_neg[j][tid];
+            const uint32_t n_neg = neg_ok ? floor_count(__fdiv_rn(__fsub_rn(ef, nn), eneg)) : 0u;
+            float2 ng[kNegPrefetch];
+#pragma unroll
+            for (int s = 0; s < kNegPrefetch; ++s) {
+                if (static_cast<uint32_t>(s) < n_neg) {
+                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                                                   (static_cast<uint64_t>(epoch) << 32) | s);
+                    ng[s] = base[rng_below(word, p.n_base)];
+                }
+            }
+            const float2 ot = sm.tail[j][tid];
+            {
+                const float dx = __fsub_rn(cx, ot.x), dy = __fsub_rn(cy, ot.y);
+                const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+                float gc = 0.0f;
+                if (d2 > 0.0f) {
+                    const float pb = powf(d2, p.b);
+                    gc = __fdiv_rn(__fmul_rn(att, powf(d2, p.b - 1.0f)),
+                                   __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
+                }
+                cx = __fadd_rn(cx, __fmul_rn(clip4(__fmul_rn(gc, dx)), alpha));
+                cy = __fadd_rn(cy, __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(cy, ot.y))), alpha));
+            }
+            sm.next[j][tid] = __fadd_rn(nx, eps);
+            if (!neg_ok) continue;
+            for (uint32_t s = 0; s < n_neg; ++s) {
+                float2 o;
+                if (s < static_cast<uint32_t>(kNegPrefetch)) {
+                    o = ng[0];
+#pragma unroll
+                    for (int t = 1; t < kNegPrefetch; ++t)
+                        if (s == static_cast<uint32_t>(t)) o = ng[t];
+                } else {
+                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                                                   (static_cast<uint64_t>(epoch) << 32) | s);
+                    o = base[rng_below(word, p.n_base)];
+                }
+                const float dx = __fsub_rn(cx, o.x), dy = __fsub_rn(cy, o.y);
+                const float dd = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+                float g2 = 0.0f;
+                if (dd > 0.0f) {
+                    const float pb = powf(dd, p.b);
+                    g2 = __fdiv_rn(rep, __fmul_rn(__fadd_rn(0.001f, dd),
+                                                  __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
+                }
+                if (g2 > 0.0f) {
+                    cx = __fadd_rn(cx, __fmul_rn(clip4(__fmul_rn(g2, dx)), alpha));
+                    cy = __fadd_rn(cy, __fmul_rn(clip4(__fmul_rn(g2, __fsub_rn(cy, o.y))), alpha));
+                }
+            }
+            sm.next_neg[j][tid] = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), eneg));
+        }
+    }
+    cur[0] = cx;
+    cur[1] = cy;
+}
+
+__global__ void __launch_bounds__(kTransformThreads) transform_kernel(TransformArgs p) {
+    __shared__ TransformStage sm;
+    const int tid = threadIdx.x;
+    const int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + tid;
     if (q >= p.nq) return;
     const int dim = p.dim;
     const int32_t st = p.row_ptr[q], en = p.row_ptr[q + 1];
+    if (dim == 2 && en - st <= kStageEdges) {
+        float c2[2];
+        stage_query_2d(p, st, en - st, sm, tid, c2);
+        const uint64_t qseed = mix64(p.seed ^ mix64(static_cast<uint64_t>(q)));
+        transform_schedule_2d_staged(p, st, en - st, qseed, sm, tid, c2);
+        p.out[q * 2] = c2[0];
+        p.out[q * 2 + 1] = c2[1];
+        return;
+    }
     float cur[kMaxDim];
     // init_graph_transform (lib.rs:4793-4836)
     if (st == en) {
@@ -638,7 +821,7 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
     const unsigned grid = static_cast<unsigned>(ceil_div(m, 256));
     {
         // Edge periods (make_epochs_per_sample, lib.rs:4937-4960).  Within
-        // each window of 65536 consecutive edges (graph order, by head) the
+        // each window of consecutive edges (graph order, by head) the
         // edges are ordered by period: edges with close periods fire in the
         // same epochs, so the lanes of a warp mostly fire together, while the
         // sweep over heads keeps the graph order across the epoch.  Each
@@ -650,10 +833,11 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
         UMAPB_LAUNCH_CHECK();
         DevBuf<uint64_t> keys(m, s), keys_sorted(m, s);
         DevBuf<int32_t> ids(m, s), order(m, s);
-        period_keys_kernel<<<grid, 256, 0, s>>>(eps_raw.get(), m, keys.get(), ids.get());
+        const int shift = sort_window_shift(m);
+        period_keys_kernel<<<grid, 256, 0, s>>>(eps_raw.get(), m, shift, keys.get(), ids.get());
         UMAPB_LAUNCH_CHECK();
         int window_bits = 1;
-        while ((static_cast<int64_t>(1) << window_bits) <= (m >> kSortWindowShift)) ++window_bits;
+        while ((static_cast<int64_t>(1) << window_bits) <= (m >> shift)) ++window_bits;
         size_t bytes = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.get(), keys_sorted.get(), ids.get(),
                                         order.get(), static_cast<int>(m), 0, 32 + window_bits, s);
@@ -769,7 +953,8 @@ void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_
     p.rep = repulsion;
     p.neg_rate_f = nrf;
     p.seed = seed;
-    transform_kernel<<<static_cast<unsigned>(ceil_div(nq, 128)), 128, 0, s>>>(p);
+    transform_kernel<<<static_cast<unsigned>(ceil_div(nq, static_cast<int64_t>(kTransformThreads))),
+                       kTransformThreads, 0, s>>>(p);
     UMAPB_LAUNCH_CHECK();
 }
 

@@ -177,35 +177,37 @@ __global__ void init_block_kernel(const int32_t* __restrict__ nodes, int64_t cnt
     }
 }
 
-// Y = X + A_hat X in position order.
+// Y = X + A_hat X in position order.  SP / 4 lanes share a row, one float4
+// of it each, so every neighbour's row is gathered by one coalesced access;
+// each lane sums its components over the row's edges in edge order.
+template <int SP>
+__host__ __device__ constexpr int spmm_rows_per_warp() { return 32 / (SP / 4); }
+
 template <int SP>
 __global__ void __launch_bounds__(256)
     spmm_kernel(int64_t cnt, const int32_t* __restrict__ prow_ptr,
                 const int32_t* __restrict__ ptails, const float* __restrict__ pnw,
                 const float* __restrict__ X, float* __restrict__ Y) {
-    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= cnt) return;
     constexpr int V = SP / 4;
-    float4 acc[V];
-    const float4* xi = reinterpret_cast<const float4*>(X + t * SP);
-#pragma unroll
-    for (int v = 0; v < V; ++v) acc[v] = xi[v];
+    constexpr int RW = spmm_rows_per_warp<SP>();
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / V, v = lane - sub * V;
+    const int64_t t =
+        ((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * RW + sub;
+    if (sub >= RW || t >= cnt) return;
+    float4 acc = reinterpret_cast<const float4*>(X + t * SP)[v];
     const int32_t st = prow_ptr[t], en = prow_ptr[t + 1];
+#pragma unroll 4
     for (int32_t e = st; e < en; ++e) {
-        const float wv = pnw[e];
-        const float4* xj = reinterpret_cast<const float4*>(X + static_cast<int64_t>(ptails[e]) * SP);
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const float4 q = __ldg(xj + v);
-            acc[v].x = fmaf(wv, q.x, acc[v].x);
-            acc[v].y = fmaf(wv, q.y, acc[v].y);
-            acc[v].z = fmaf(wv, q.z, acc[v].z);
-            acc[v].w = fmaf(wv, q.w, acc[v].w);
-        }
+        const float wv = __ldg(pnw + e);
+        const float4 q =
+            __ldg(reinterpret_cast<const float4*>(X + static_cast<int64_t>(__ldg(ptails + e)) * SP) + v);
+        acc.x = fmaf(wv, q.x, acc.x);
+        acc.y = fmaf(wv, q.y, acc.y);
+        acc.z = fmaf(wv, q.z, acc.z);
+        acc.w = fmaf(wv, q.w, acc.w);
     }
-    float4* yi = reinterpret_cast<float4*>(Y + t * SP);
-#pragma unroll
-    for (int v = 0; v < V; ++v) yi[v] = acc[v];
+    reinterpret_cast<float4*>(Y + t * SP)[v] = acc;
 }
 
 struct Chunk {
@@ -644,8 +646,10 @@ bool run_iterative(const std::vector<int64_t>& it_comps, const std::vector<int64
             UMAPB_LAUNCH_CHECK();
         }
     };
+    const unsigned gr_spmm = static_cast<unsigned>(
+        ceil_div(ceil_div(cnt, static_cast<int64_t>(spmm_rows_per_warp<SP>())) * 32, 256));
     auto spmm = [&](const float* x, float* y) {
-        spmm_kernel<SP><<<gr, 256, 0, s>>>(cnt, prow.get(), ptails.get(), pnw.get(), x, y);
+        spmm_kernel<SP><<<gr_spmm, 256, 0, s>>>(cnt, prow.get(), ptails.get(), pnw.get(), x, y);
         UMAPB_LAUNCH_CHECK();
     };
     static_assert(kIters % kOrthoEvery == 0, "the last product must be orthonormalised");
