@@ -81,8 +81,21 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines: list[str] = []
+        self.others: set[str] = set()
+
+    def _other_processes(self) -> None:
+        """Compute processes other than this one on the device (they share its SMs)."""
+        try:
+            out = subprocess.run(["nvidia-smi", f"--id={self.device}",
+                                  "--query-compute-apps=pid", "--format=csv,noheader"],
+                                 capture_output=True, text=True, timeout=10).stdout
+        except (OSError, subprocess.TimeoutExpired):
+            return
+        me = str(os.getpid())
+        self.others |= {ln.strip() for ln in out.splitlines() if ln.strip() and ln.strip() != me}
 
     def __enter__(self):
+        self._other_processes()
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
@@ -99,6 +112,7 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        self._other_processes()
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -122,7 +136,8 @@ class ClockSampler:
                 if val.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "other_processes": len(self.others)}
 
 
 def dist_setup():
@@ -346,6 +361,10 @@ def run_gpu(args) -> None:
             "clocks": sampler.summary(),
             # per timed step: its time, and the memory pool's mapped size after it
             "step_sec": [round(t, 4) for t in dev_times],
+            "step_stages_sec": [[round(st[k], 4) for k in ("knn_sec", "membership_sec",
+                                                             "symmetrize_sec", "prune_sec",
+                                                             "init_sec", "optimize_sec")]
+                                for st in stage],
             "pool_reserved_gb": [pool0] + pool,
         }
         if transform is not None:

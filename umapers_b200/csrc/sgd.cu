@@ -37,6 +37,16 @@ __device__ inline uint32_t floor_count(float v) {
     return static_cast<uint32_t>(f);
 }
 
+// x^y for finite x > 0 through the base-2 logarithm, at a fraction of
+// powf's instruction count.  The relative error is about |y log2 x| * 2^-23
+// (log2f and exp2f are within 2 ulp): for the exponents used here (b and
+// b - 1, |y| <= 2) under 5e-6 at squared distances in [1e-6, 1e6] and under
+// 4e-5 anywhere in float range, far below the spread between Hogwild update
+// orders.
+__device__ __forceinline__ float pow_pos(float x, float y) {
+    return exp2f(__fmul_rn(y, log2f(x)));
+}
+
 __global__ void epochs_per_sample_kernel(const float* __restrict__ w, int64_t m, float max_w,
                                          float n_epochs_f, float neg_rate_f,
                                          float* __restrict__ eps, float* __restrict__ next,
@@ -150,7 +160,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
                 const float dx = __fsub_rn(hx, t.x), dy = __fsub_rn(hy, t.y);
                 const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
                 if (d2 > 0.0f) {
-                    const float pb = powf(d2, p.b);
+                    const float pb = pow_pos(d2, p.b);
                     const float gc = __fdiv_rn(__fmul_rn(p.att_factor, __fdiv_rn(pb, d2)),
                                                __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
                     const float gx = clip4(__fmul_rn(gc, dx)), gy = clip4(__fmul_rn(gc, dy));
@@ -176,7 +186,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
                     const float dx = __fsub_rn(hx, o.x), dy = __fsub_rn(hy, o.y);
                     const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
                     if (d2 > 0.0f) {
-                        const float pb = powf(d2, p.b);
+                        const float pb = pow_pos(d2, p.b);
                         const float gc =
                             __fdiv_rn(p.rep_factor, __fmul_rn(__fadd_rn(0.001f, d2),
                                                               __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
@@ -633,8 +643,9 @@ __device__ __forceinline__ void transform_schedule_2d_staged(const TransformArgs
                 const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
                 float gc = 0.0f;
                 if (d2 > 0.0f) {
-                    const float pb = powf(d2, p.b);
-                    gc = __fdiv_rn(__fmul_rn(att, powf(d2, p.b - 1.0f)),
+                    const float l2 = log2f(d2);
+                    const float pb = exp2f(__fmul_rn(p.b, l2));
+                    gc = __fdiv_rn(__fmul_rn(att, exp2f(__fmul_rn(p.b - 1.0f, l2))),
                                    __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
                 }
                 cx = __fadd_rn(cx, __fmul_rn(clip4(__fmul_rn(gc, dx)), alpha));
@@ -658,7 +669,7 @@ __device__ __forceinline__ void transform_schedule_2d_staged(const TransformArgs
                 const float dd = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
                 float g2 = 0.0f;
                 if (dd > 0.0f) {
-                    const float pb = powf(dd, p.b);
+                    const float pb = pow_pos(dd, p.b);
                     g2 = __fdiv_rn(rep, __fmul_rn(__fadd_rn(0.001f, dd),
                                                   __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
                 }
