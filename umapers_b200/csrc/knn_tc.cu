@@ -94,6 +94,44 @@ __device__ __forceinline__ float min32(const uint32_t* r) {
     return fminf(m, __uint_as_float(r[31]));
 }
 
+// Bitonic sort of one value per lane, ascending with the lane index.
+template <typename T>
+__device__ __forceinline__ T warp_sort_asc(T v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const T o = __shfl_xor_sync(0xffffffffu, v, stride);
+            const bool up = (lane & size) == 0;
+            const bool lower = (lane & stride) == 0;
+            v = (lower == up) ? (v < o ? v : o) : (v < o ? o : v);
+        }
+    }
+    return v;
+}
+
+// Merges 32 keys (one per lane, any order) into a list sorted ascending
+// across the lanes and keeps the 32 smallest: sort the keys, reverse them,
+// take the lane-wise minimum (a bitonic sequence holding the 32 smallest of
+// both) and sort that with five compare-exchange stages.
+__device__ __forceinline__ uint64_t warp_merge_keys(uint64_t list, uint64_t keys) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t srt = warp_sort_asc<uint64_t>(keys);
+    const uint64_t rev = __shfl_sync(0xffffffffu, srt, 31 - lane);
+    uint64_t m = list < rev ? list : rev;
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1) {
+        const uint64_t o = __shfl_xor_sync(0xffffffffu, m, st);
+        m = (lane & st) ? (m > o ? m : o) : (m < o ? m : o);
+    }
+    return m;
+}
+
+// A chunk with at least this many qualifying keys is merged in one bitonic
+// pass instead of key by key (about 6 sequential insertions cost as much).
+constexpr int kBulkMergeMin = 6;
+
 // CTAs begin their candidate range at staggered tiles (16 groups, 4 tiles
 // apart: a window of 4 MiB of B at K' = 256, L2-resident) so they do not all
 // request the same tile at once.  The shortlist certificate does not depend
@@ -358,8 +396,18 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
 #pragma unroll
                     for (int ch = 0; ch < 2; ++ch) {
                         const float mine = ch == 0 ? v0 : v1;
-                        unsigned q = __ballot_sync(0xffffffffu,
-                                                   mine < stau && lane + ch * 32 < valid_cols);
+                        const bool qual = mine < stau && lane + ch * 32 < valid_cols;
+                        unsigned q = __ballot_sync(0xffffffffu, qual);
+                        if (__popc(q) >= kBulkMergeMin) {
+                            const uint64_t key =
+                                qual ? (static_cast<uint64_t>(f2o(mine)) << 32) |
+                                           static_cast<uint32_t>(colh + ch * 32 + lane)
+                                     : ~0ull;
+                            lk = warp_merge_keys(lk, key);
+                            const uint64_t last = __shfl_sync(0xffffffffu, lk, S - 1);
+                            stau = last == ~0ull ? INFINITY : o2f(static_cast<uint32_t>(last >> 32));
+                            q = 0;
+                        }
                         while (q) {
                             const int b = __ffs(q) - 1;
                             q &= q - 1;
@@ -493,22 +541,6 @@ __device__ __forceinline__ float sqdist_ref(const float* __restrict__ x, const f
     return s;
 }
 
-template <typename T>
-__device__ __forceinline__ T warp_sort_asc(T v) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            const T o = __shfl_xor_sync(0xffffffffu, v, stride);
-            const bool up = (lane & size) == 0;
-            const bool lower = (lane & stride) == 0;
-            v = (lower == up) ? (v < o ? v : o) : (v < o ? o : v);
-        }
-    }
-    return v;
-}
-
 __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restrict__ R,
                               const float* __restrict__ qsq, const float* __restrict__ rsq,
                               const uint64_t* __restrict__ lists, int n_lists, int64_t n_q,
@@ -577,15 +609,7 @@ __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restri
             const uint32_t j = static_cast<uint32_t>(lk);
             key = knn_key(sqdist_ref(Q + row * d, R + static_cast<int64_t>(j) * d, d), j);
         }
-        const uint64_t b = warp_sort_asc<uint64_t>(key);
-        const uint64_t br = __shfl_sync(0xffffffffu, b, 31 - lane);
-        uint64_t m = top < br ? top : br;
-#pragma unroll
-        for (int st = 16; st > 0; st >>= 1) {
-            const uint64_t o = __shfl_xor_sync(0xffffffffu, m, st);
-            m = (lane & st) ? (m > o ? m : o) : (m < o ? m : o);
-        }
-        top = m;
+        top = warp_merge_keys(top, key);
     }
     if (lane < k) {
         out_idx[row * k + lane] = static_cast<int32_t>(key_index(top));
