@@ -82,9 +82,16 @@ class ClockSampler:
         self.proc = None
         self.lines: list[str] = []
         self.others: set[str] = set()
+        self.load: list[float] = []
 
     def _other_processes(self) -> None:
-        """Compute processes other than this one on the device (they share its SMs)."""
+        """Compute processes other than this one on the device (they share its
+        SMs), and the host's 1-minute load average (a loaded host delays the
+        launches and synchronisations between stages)."""
+        try:
+            self.load.append(round(os.getloadavg()[0], 2))
+        except OSError:
+            pass
         try:
             out = subprocess.run(["nvidia-smi", f"--id={self.device}",
                                   "--query-compute-apps=pid", "--format=csv,noheader"],
@@ -137,7 +144,8 @@ class ClockSampler:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
                 "reasons": sorted(reasons), "samples": len(sm),
-                "other_processes": len(self.others)}
+                "other_processes": len(self.others), "host_load_1min": self.load,
+                "host_cpus": os.cpu_count()}
 
 
 def dist_setup():
@@ -361,6 +369,7 @@ def run_gpu(args) -> None:
             "clocks": sampler.summary(),
             # per timed step: its time, and the memory pool's mapped size after it
             "step_sec": [round(t, 4) for t in dev_times],
+            "step_sec_median": round(float(np.median(dev_times)), 4),
             "step_stages_sec": [[round(st[k], 4) for k in ("knn_sec", "membership_sec",
                                                              "symmetrize_sec", "prune_sec",
                                                              "init_sec", "optimize_sec")]
@@ -383,6 +392,50 @@ def run_gpu(args) -> None:
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def sparse_leg(args, lib) -> dict:
+    """CSR input: 200,000 x 2,000 rows at about 20 stored values per row,
+    LogNormal(0, 1) values, cosine, k = 30.  The exact sparse kNN through the
+    host API (upload, index build, kernel, download), a complete fit from the
+    CSR rows, bit-exact agreement with the oracle on 200 sampled rows, and the
+    oracle's time for those rows on all host cores."""
+    from oracle import oracle
+    from umapers import Umap
+    from umapers_b200 import _lib, workloads
+
+    xs = workloads.sparse_lognormal_csr(200_000, 2000, 20, seed=3)
+    n, d, k = xs.shape[0], xs.shape[1], 30
+    ip = np.ascontiguousarray(xs.indptr, np.int64)
+    ix = np.ascontiguousarray(xs.indices, np.int64)
+    dv = np.ascontiguousarray(xs.data, np.float32)
+    idx = np.empty((n, k), np.int64)
+    dist = np.empty((n, k), np.float32)
+    t_knn = float("inf")
+    for _ in range(2):
+        t0 = time.perf_counter()
+        _lib.check(lib.umapb_knn_csr(ip.ctypes.data, ix.ctypes.data, dv.ctypes.data, n, d, k, 2,
+                                     idx.ctypes.data, dist.ctypes.data))
+        t_knn = min(t_knn, time.perf_counter() - t0)
+    m = Umap(n_neighbors=k, metric="cosine", n_epochs=EPOCHS, random_seed=3)
+    m.fit_transform(xs)
+    t0 = time.perf_counter()
+    m.fit_transform(xs)
+    t_fit = time.perf_counter() - t0
+    rows = np.random.default_rng(3).choice(n, 200, replace=False)
+    oracle.set_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    oi, od = oracle.csr_knn_rows(xs, rows, k, "cosine")
+    t_cpu = time.perf_counter() - t0
+    exact = bool(np.array_equal(oi, idx[rows]) and
+                 np.array_equal(od.view(np.uint32), dist[rows].view(np.uint32)))
+    return {"knn_s": round(t_knn, 4), "fit_s": round(t_fit, 4), "nnz": int(xs.nnz),
+            "bit_exact_on_sample": exact,
+            "cpu_knn_s_extrapolated": round(t_cpu * n / rows.shape[0], 1),
+            "cpu_cores": os.cpu_count(),
+            "note": "exact sparse kNN (the reference has no sparse NN-descent and rejects "
+                    "densMAP for sparse input); host API, 200 epochs; the CPU figure is the "
+                    "oracle on 200 rows scaled to all rows"}
 
 
 def knn_legs(args, lib, x: np.ndarray) -> dict:
@@ -439,6 +492,7 @@ def knn_legs(args, lib, x: np.ndarray) -> dict:
                                    ed.ctypes.data, None))
     rows = np.random.default_rng(3).choice(n, 2000, replace=False)
     recall = float(np.mean([len(set(ni[r]) & set(ei[r])) / K for r in rows]))
+    out["sparse_cosine_200000x2000"] = sparse_leg(args, lib)
     out["nndescent_1m_x64"] = {
         "knn_s": round(t_nd, 4), "iters": int(ran.value), "recall_at_15": round(recall, 4),
         "note": "host API (includes the 256 MB upload), max_candidates=30, n_iters=10; recall "
@@ -567,7 +621,7 @@ def transform_leg(args, lib, device: int) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--knn-backend", default="auto", choices=["auto", "tensor", "plain"])

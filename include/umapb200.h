@@ -177,6 +177,37 @@ int32_t umapb_fit_transform(umapb_model* model, const float* data, int64_t n_row
 int32_t umapb_fit_transform_stateless(const umapb_params* params, const float* data,
                                       int64_t n_rows, int64_t n_cols, float* out);
 
+/* ---- CSR input -----------------------------------------------------------
+ * indptr holds n_rows + 1 int64 offsets starting at 0; indices (int64) and
+ * data (float32) hold indptr[n_rows] entries, column indices strictly
+ * increasing within a row.  The checks of SparseCsrMatrix::new
+ * (rust_umap/src/sparse.rs:20-105) run first, with its messages.  The B200
+ * path supports the euclidean and cosine metrics and n_neighbors <= 32. */
+
+/* UmapCore.fit_sparse_csr (umap_rs/src/lib.rs:674-686) ->
+ * UmapModel::fit_sparse_csr (rust_umap/src/lib.rs:998-1014). */
+int32_t umapb_fit_csr(umapb_model* model, const int64_t* indptr, const int64_t* indices,
+                      const float* data, int64_t n_rows, int64_t n_cols);
+
+/* UmapCore.fit_transform_sparse_csr[_into] (umap_rs/src/lib.rs:869-883,
+ * 900-915) -> UmapModel::fit_transform_sparse_csr (rust_umap/src/lib.rs:1016-1036).
+ * `out` is n_rows x n_components float32. */
+int32_t umapb_fit_transform_csr(umapb_model* model, const int64_t* indptr,
+                                const int64_t* indices, const float* data, int64_t n_rows,
+                                int64_t n_cols, float* out);
+
+/* UmapCore.fit_transform_sparse_csr_stateless (umap_rs/src/lib.rs:884-899) ->
+ * rust_umap::fit_transform_sparse_csr (rust_umap/src/lib.rs:1944-1966). */
+int32_t umapb_fit_transform_csr_stateless(const umapb_params* params, const int64_t* indptr,
+                                          const int64_t* indices, const float* data,
+                                          int64_t n_rows, int64_t n_cols, float* out);
+
+/* UmapCore.transform_sparse_csr[_into] (umap_rs/src/lib.rs:1198-1227) ->
+ * UmapModel::transform_sparse_csr (rust_umap/src/lib.rs:1687-1736): sparse
+ * queries of a model fitted on CSR rows. */
+int32_t umapb_transform_csr(umapb_model* model, const int64_t* indptr, const int64_t* indices,
+                            const float* data, int64_t n_rows, int64_t n_cols, float* out);
+
 /* UmapCore.fit_transform_with_knn[_into] (umap_rs/src/lib.rs:916-1017) ->
  * UmapModel::fit_transform_with_knn_metric_dense_i64_flat (rust_umap/src/lib.rs:1159-1212).
  * knn_indices int64 [idx_rows x idx_cols], knn_dists float32 [dist_rows x dist_cols]. */
@@ -271,6 +302,21 @@ int32_t umapb_knn_exact_noalloc(const float* data, int64_t n_rows, int64_t n_col
 int32_t umapb_knn_query(const float* query, int64_t n_query, const float* reference,
                         int64_t n_reference, int64_t n_cols, int64_t k, int32_t metric,
                         int32_t backend, int64_t* indices, float* dists);
+
+/* sparse::exact_nearest_neighbors (rust_umap/src/sparse.rs:605-626): exact
+ * kNN of CSR rows against themselves (a row's distance to itself is 0),
+ * euclidean or cosine, k <= 32; indices int64 and distances float32, n_rows x k. */
+int32_t umapb_knn_csr(const int64_t* indptr, const int64_t* indices, const float* data,
+                      int64_t n_rows, int64_t n_cols, int64_t k, int32_t metric,
+                      int64_t* out_indices, float* out_dists);
+
+/* sparse::exact_nearest_neighbors_sparse_query (rust_umap/src/sparse.rs:628-657):
+ * CSR query rows against CSR reference rows. */
+int32_t umapb_knn_csr_query(const int64_t* q_indptr, const int64_t* q_indices,
+                            const float* q_data, int64_t n_query, const int64_t* r_indptr,
+                            const int64_t* r_indices, const float* r_data, int64_t n_reference,
+                            int64_t n_cols, int64_t k, int32_t metric, int64_t* out_indices,
+                            float* out_dists);
 
 /* NN-descent variant (approximate_nearest_neighbors_with_distance,
  * rust_umap/src/lib.rs:3086-3151) on the GPU; `seed` plays the role of

@@ -32,6 +32,10 @@ _SIGS = {
     "orc_exact_knn": (None, [_vp, _i64, _i64, _i64, _i32, _vp, _vp]),
     "orc_exact_knn_rows": (None, [_vp, _i64, _i64, _i64, _i32, _vp, _i64, _vp, _vp]),
     "orc_knn_query": (None, [_vp, _i64, _vp, _i64, _i64, _i64, _i32, _vp, _vp]),
+    "orc_csr_knn": (None, [_vp, _vp, _vp, _i64, _i64, _i64, _i32, _vp, _vp]),
+    "orc_csr_knn_rows": (None, [_vp, _vp, _vp, _i64, _i64, _vp, _i64, _i64, _i32, _vp, _vp]),
+    "orc_csr_knn_query": (
+        None, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _i32, _vp, _vp]),
     "orc_nndescent": (_i64, [_vp, _i64, _i64, _i64, _i32, _i64, _i64, _u64, _vp, _vp]),
     "orc_smooth_knn": (None, [_vp, _i64, _i64, _f32, _f32, _f32, _i32, _vp, _vp]),
     "orc_smooth_knn_f64": (None, [_vp, _i64, _i64, _f64, _f64, _f64, _i32, _vp, _vp]),
@@ -137,6 +141,47 @@ def knn_query(q, r, k: int, metric: str = "euclidean"):
     dist = np.empty((q.shape[0], k), np.float32)
     load().orc_knn_query(_p(q), q.shape[0], _p(r), r.shape[0], q.shape[1], k, METRIC[metric],
                          _p(idx), _p(dist))
+    return idx, dist
+
+
+def _csr_parts(m):
+    """(indptr int64, indices int64, data float32, n_rows, n_cols) of a
+    scipy.sparse matrix in canonical CSR form."""
+    m = m.tocsr()
+    m.sum_duplicates()
+    m.sort_indices()
+    return (np.ascontiguousarray(m.indptr, np.int64), np.ascontiguousarray(m.indices, np.int64),
+            np.ascontiguousarray(m.data, np.float32), m.shape[0], m.shape[1])
+
+
+def csr_knn(m, k: int, metric: str = "euclidean"):
+    """exact_nearest_neighbors of a sparse matrix (sparse.rs:605-626)."""
+    ip, ix, dv, n, d = _csr_parts(m)
+    idx = np.empty((n, k), np.int64)
+    dist = np.empty((n, k), np.float32)
+    load().orc_csr_knn(_p(ip), _p(ix), _p(dv), n, d, k, METRIC[metric], _p(idx), _p(dist))
+    return idx, dist
+
+
+def csr_knn_rows(m, rows, k: int, metric: str = "euclidean"):
+    """Rows `rows` of exact_nearest_neighbors of a sparse matrix."""
+    ip, ix, dv, n, d = _csr_parts(m)
+    rows = np.ascontiguousarray(rows, np.int64)
+    idx = np.empty((rows.shape[0], k), np.int64)
+    dist = np.empty((rows.shape[0], k), np.float32)
+    load().orc_csr_knn_rows(_p(ip), _p(ix), _p(dv), n, d, _p(rows), rows.shape[0], k,
+                            METRIC[metric], _p(idx), _p(dist))
+    return idx, dist
+
+
+def csr_knn_query(q, r, k: int, metric: str = "euclidean"):
+    """exact_nearest_neighbors_sparse_query (sparse.rs:628-657)."""
+    qp, qi, qd, nq, d = _csr_parts(q)
+    rp, ri, rd, nr, _ = _csr_parts(r)
+    idx = np.empty((nq, k), np.int64)
+    dist = np.empty((nq, k), np.float32)
+    load().orc_csr_knn_query(_p(qp), _p(qi), _p(qd), nq, _p(rp), _p(ri), _p(rd), nr, d, k,
+                             METRIC[metric], _p(idx), _p(dist))
     return idx, dist
 
 

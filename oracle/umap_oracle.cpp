@@ -1632,6 +1632,96 @@ Knn knn_from_arrays(const int64_t* idx, const float* dist, size_t n, size_t k) {
     return knn;
 }
 
+// ------------------------------------------------------------- sparse ---
+// SparseCsrMatrix (rust_umap/src/sparse.rs:8-118): a CSR view with the
+// squared norms (sum of v * v over the stored values, in stored order) and
+// the L2 norms (their square roots) of every row.
+struct CsrRows {
+    int64_t n_rows = 0, n_cols = 0;
+    const int64_t* indptr = nullptr;
+    const int64_t* indices = nullptr;
+    const float* data = nullptr;
+    std::vector<float> sq, l2;
+};
+
+CsrRows csr_rows(const int64_t* indptr, const int64_t* indices, const float* data, int64_t n_rows,
+                 int64_t n_cols) {
+    CsrRows m;
+    m.n_rows = n_rows;
+    m.n_cols = n_cols;
+    m.indptr = indptr;
+    m.indices = indices;
+    m.data = data;
+    m.sq.assign(n_rows, 0.0f);
+    m.l2.assign(n_rows, 0.0f);
+    for (int64_t r = 0; r < n_rows; ++r) {
+        float s = 0.0f;
+        for (int64_t e = indptr[r]; e < indptr[r + 1]; ++e) s += data[e] * data[e];
+        m.sq[r] = s;
+        m.l2[r] = std::sqrt(s);
+    }
+    return m;
+}
+
+// sparse_dot (sparse.rs:220-239): products of the shared columns, summed in
+// ascending column order.
+float csr_dot(const CsrRows& a, int64_t ra, const CsrRows& b, int64_t rb) {
+    int64_t i = a.indptr[ra], ie = a.indptr[ra + 1];
+    int64_t j = b.indptr[rb], je = b.indptr[rb + 1];
+    float dot = 0.0f;
+    while (i < ie && j < je) {
+        if (a.indices[i] < b.indices[j]) {
+            ++i;
+        } else if (a.indices[i] > b.indices[j]) {
+            ++j;
+        } else {
+            dot += a.data[i] * b.data[j];
+            ++i;
+            ++j;
+        }
+    }
+    return dot;
+}
+
+// euclidean_distance_from_dot (sparse.rs:241-244) and the cosine distance of
+// sparse_slices_cosine_distance (sparse.rs:540-558).  A negative or zero
+// radicand becomes +0.0.
+float csr_distance(const CsrRows& a, int64_t ra, const CsrRows& b, int64_t rb, int metric) {
+    if (metric == UMAPB_METRIC_COSINE) {
+        const float la = a.l2[ra], lb = b.l2[rb];
+        if (la == 0.0f && lb == 0.0f) return 0.0f;
+        if (la == 0.0f || lb == 0.0f) return 1.0f;
+        float c = csr_dot(a, ra, b, rb) / (la * lb);
+        if (c < -1.0f) c = -1.0f;
+        else if (c > 1.0f) c = 1.0f;
+        return 1.0f - c;
+    }
+    float t = (a.sq[ra] + b.sq[rb]) - 2.0f * csr_dot(a, ra, b, rb);
+    if (!(t > 0.0f)) t = 0.0f;
+    return std::sqrt(t);
+}
+
+// exact_nearest_neighbors / exact_nearest_neighbors_sparse_query
+// (sparse.rs:605-657): every query row against every reference row; in the
+// self-join a row's distance to itself is 0.
+Knn csr_knn(const CsrRows& q, const CsrRows& r, size_t k, int metric, bool self) {
+    Knn out;
+    out.idx.resize(q.n_rows);
+    out.dist.resize(q.n_rows);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < q.n_rows; ++i) {
+        auto& ri = out.idx[i];
+        auto& rd = out.dist[i];
+        ri.reserve(k + 1);
+        rd.reserve(k + 1);
+        for (int64_t j = 0; j < r.n_rows; ++j) {
+            const float dist = (self && i == j) ? 0.0f : csr_distance(q, i, r, j, metric);
+            push_top_k(ri, rd, static_cast<size_t>(j), dist, k);
+        }
+    }
+    return out;
+}
+
 void knn_to_arrays(const Knn& knn, size_t k, int64_t* idx, float* dist) {
     for (size_t i = 0; i < knn.idx.size(); ++i)
         for (size_t c = 0; c < k; ++c) {
@@ -1696,6 +1786,45 @@ void orc_knn_query(const float* q, int64_t nq, const float* r, int64_t nr, int64
                    int32_t metric, int64_t* idx, float* dist) {
     const Knn knn = exact_knn_query(q, nq, r, nr, d, k, metric);
     knn_to_arrays(knn, k, idx, dist);
+}
+
+// exact_nearest_neighbors (sparse.rs:605-626) of a CSR matrix
+// (indptr n_rows + 1, strictly increasing column indices per row).
+void orc_csr_knn(const int64_t* indptr, const int64_t* indices, const float* data, int64_t n_rows,
+                 int64_t n_cols, int64_t k, int32_t metric, int64_t* idx, float* dist) {
+    const CsrRows m = csr_rows(indptr, indices, data, n_rows, n_cols);
+    knn_to_arrays(csr_knn(m, m, static_cast<size_t>(k), metric, true), k, idx, dist);
+}
+
+// The rows `rows` of exact_nearest_neighbors (sparse.rs:605-626) of a CSR
+// matrix: each listed row against every row, its own distance 0.
+void orc_csr_knn_rows(const int64_t* indptr, const int64_t* indices, const float* data,
+                      int64_t n_rows, int64_t n_cols, const int64_t* rows, int64_t n_sel,
+                      int64_t k, int32_t metric, int64_t* idx, float* dist) {
+    const CsrRows m = csr_rows(indptr, indices, data, n_rows, n_cols);
+    Knn out;
+    out.idx.resize(n_sel);
+    out.dist.resize(n_sel);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t s = 0; s < n_sel; ++s) {
+        const int64_t i = rows[s];
+        for (int64_t j = 0; j < n_rows; ++j) {
+            const float d = i == j ? 0.0f : csr_distance(m, i, m, j, metric);
+            push_top_k(out.idx[s], out.dist[s], static_cast<size_t>(j), d, static_cast<size_t>(k));
+        }
+    }
+    knn_to_arrays(out, static_cast<size_t>(k), idx, dist);
+}
+
+// exact_nearest_neighbors_sparse_query (sparse.rs:628-657): CSR queries
+// against a CSR reference.
+void orc_csr_knn_query(const int64_t* q_indptr, const int64_t* q_indices, const float* q_data,
+                       int64_t nq, const int64_t* r_indptr, const int64_t* r_indices,
+                       const float* r_data, int64_t nr, int64_t n_cols, int64_t k,
+                       int32_t metric, int64_t* idx, float* dist) {
+    const CsrRows q = csr_rows(q_indptr, q_indices, q_data, nq, n_cols);
+    const CsrRows r = csr_rows(r_indptr, r_indices, r_data, nr, n_cols);
+    knn_to_arrays(csr_knn(q, r, static_cast<size_t>(k), metric, false), k, idx, dist);
 }
 
 int64_t orc_nndescent(const float* x, int64_t n, int64_t d, int64_t k, int32_t metric,

@@ -161,13 +161,45 @@ def test_transform_requires_fit():
         Umap().transform(np.zeros((3, 4), np.float32))
 
 
-def test_sparse_and_supervised_inputs_are_rejected():
+def test_sparse_input_checks_run_before_the_device():
+    """The facade's sparse routing (umapers/_api.py:562-632) and the checks of
+    sparse_csr_from_py / SparseCsrMatrix::new / the sparse fit
+    (umap_rs/src/lib.rs:242-351, rust_umap/src/sparse.rs:20-105,
+    rust_umap/src/lib.rs:2241-2258) raise before any device work."""
     sp = pytest.importorskip("scipy.sparse")
-    x = sp.random(50, 20, density=0.1, format="csr", dtype=np.float32)
-    with pytest.raises(ValueError, match="sparse"):
-        Umap().fit(x)
+    x = sp.random(50, 20, density=0.1, format="csr", dtype=np.float32, random_state=3)
+    with pytest.raises(ValueError, match="densmap and output_dens currently support dense"):
+        Umap(densmap=True).fit(x)
+    with pytest.raises(ValueError, match="categorical supervised UMAP currently supports dense"):
+        Umap(target_metric="categorical").fit(x, y=np.zeros(50))
     with pytest.raises(ValueError, match="supervised"):
         Umap(target_metric="categorical").fit(np.zeros((50, 3), np.float32), y=np.zeros(50))
+    core = UmapCore(n_neighbors=5)
+    ip = np.array([0, 2, 3], np.int64)
+    with pytest.raises(ValueError, match="indices must contain non-negative integers"):
+        core.fit_sparse_csr(ip, np.array([0, -1, 2]), np.ones(3, np.float32), 4)
+    with pytest.raises(ValueError, match="indptr cannot be empty"):
+        core.fit_sparse_csr(np.array([], np.int64), np.array([], np.int64),
+                            np.array([], np.float32), 4)
+    with pytest.raises(ValueError, match=r"csr indptr last value \(3\) must equal nnz \(2\)"):
+        core.fit_sparse_csr(ip, np.array([0, 1]), np.ones(2, np.float32), 4)
+    with pytest.raises(ValueError, match="csr indices/data lengths must match"):
+        core.fit_sparse_csr(ip, np.array([0, 1, 2]), np.ones(2, np.float32), 4)
+    with pytest.raises(ValueError, match="csr row 0 indices must be strictly increasing"):
+        core.fit_sparse_csr(ip, np.array([1, 1, 2]), np.ones(3, np.float32), 4)
+    with pytest.raises(ValueError, match="csr row 1 has column index 4 out of bounds for n_cols=4"):
+        core.fit_sparse_csr(ip, np.array([0, 1, 4]), np.ones(3, np.float32), 4)
+    with pytest.raises(ValueError, match="csr data must be finite"):
+        core.fit_sparse_csr(ip, np.array([0, 1, 2]), np.array([1, np.nan, 1], np.float32), 4)
+    with pytest.raises(ValueError, match="csr indptr must be non-decreasing"):
+        core.fit_sparse_csr(np.array([0, 3, 2, 3]), np.array([0, 1, 2]), np.ones(3, np.float32), 4)
+    with pytest.raises(ValueError, match="input data is empty"):
+        core.fit_sparse_csr(np.array([0], np.int64), np.array([], np.int64),
+                            np.array([], np.float32), 4)
+    with pytest.raises(ValueError, match="Canberra metric is currently supported for dense input"):
+        Umap(metric="canberra", n_neighbors=5).fit(x)
+    with pytest.raises(ValueError, match="n_neighbors above 32"):
+        Umap(n_neighbors=40).fit(x)
 
 
 def test_metrics_outside_the_engine_are_rejected_at_fit():

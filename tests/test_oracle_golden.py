@@ -165,3 +165,48 @@ def test_local_radii_follow_the_reference_rule(orc):
     expect = [(np.log(f(1.1)) + np.log(f(2.1))) / 2, (np.log(f(1.1)) + np.log(f(3.1))) / 2,
               (np.log(f(0.6)) + np.log(f(0.35))) / 2]
     np.testing.assert_allclose(r, np.array(expect, np.float32), rtol=1e-6)
+
+
+def _sparse_like_data(n, dim):
+    """sparse_like_data (rust_umap/src/lib.rs:5767-5778) in float32."""
+    data = np.zeros((n, dim), np.float32)
+    f = np.float32
+    for i in range(n):
+        for t in range(5):
+            col = (i * 17 + t * 13 + (i % 3) * 7) % dim
+            data[i, col] = f(f(f(i + 1) * f(t + 2)) * f(0.017)) + f(f(col) * f(1e-4))
+    return data
+
+
+def test_sparse_knn_matches_the_dense_knn(orc):
+    # sparse_csr_knn_matches_dense_euclidean (rust_umap/src/lib.rs:6376-6394)
+    sp = pytest.importorskip("scipy.sparse")
+    x = _sparse_like_data(42, 61)
+    csr = sp.csr_matrix(x)
+    si, sd = orc.csr_knn(csr, 12, "euclidean")
+    di, dd = orc.exact_knn(x, 12, "euclidean")
+    np.testing.assert_array_equal(si, di)
+    assert np.abs(sd - dd).max() <= 1e-5
+
+
+def test_sparse_knn_follows_the_reference_formulas(orc):
+    # sparse.rs:220-244, 368-384, 605-626 on a hand-made matrix: an empty row,
+    # a duplicate row, a row with no shared column
+    sp = pytest.importorskip("scipy.sparse")
+    dense = np.array([[1.0, 0.0, 2.0, 0.0],
+                      [0.0, 0.0, 0.0, 0.0],
+                      [1.0, 0.0, 2.0, 0.0],
+                      [0.0, 3.0, 0.0, -1.0]], np.float32)
+    csr = sp.csr_matrix(dense)
+    idx, dist = orc.csr_knn(csr, 4, "euclidean")
+    f = np.float32
+    # row 0: itself 0, its duplicate 0 (by the formula: 5 + 5 - 2 * 5), the
+    # empty row sqrt(5), row 3 sqrt(5 + 10)
+    np.testing.assert_array_equal(idx[0], [0, 2, 1, 3])
+    np.testing.assert_array_equal(dist[0], [0.0, 0.0, np.sqrt(f(5.0)), np.sqrt(f(15.0))])
+    idx, dist = orc.csr_knn(csr, 4, "cosine")
+    # the empty row: 0 to itself, 1 to every non-empty row (index order)
+    np.testing.assert_array_equal(idx[1], [1, 0, 2, 3])
+    np.testing.assert_array_equal(dist[1], [0.0, 1.0, 1.0, 1.0])
+    # row 3 shares no column with rows 0 / 2: cosine 1
+    assert dist[3][1] == f(1.0)

@@ -6,9 +6,10 @@ _api.py:324-873, 1054-1094): keyword arguments and defaults, sklearn-style
 int64 kNN indices), ``out=`` buffers, the ``ann_mode`` shortcut, and the
 fitted attributes ``embedding_``, ``n_features_in_``, ``n_samples_fit_``.
 Compute runs on one B200 through ``UmapCore`` (libumapb200.so), densMAP and
-``output_dens`` included.  Inputs the engine does not cover (sparse CSR,
-supervised targets, inverse_transform, metrics other than euclidean/cosine)
-raise ValueError.
+``output_dens`` (dense input) and CSR sparse input (scipy csr/csc/coo)
+included.  Inputs the engine does not cover (supervised targets,
+inverse_transform, metrics other than euclidean/cosine, sparse input with
+n_neighbors above 32) raise ValueError.
 """
 from __future__ import annotations
 
@@ -132,6 +133,45 @@ def _i64_matrix(x: Any, name: str) -> np.ndarray:
 
 def _is_sparse(x: Any) -> bool:
     return getattr(x, "format", None) in {"csr", "csc", "coo"}
+
+
+def _maybe_as_csr_parts(x: Any, name: str):
+    """(indptr, indices, data, n_rows, n_cols) of a scipy-style sparse matrix
+    in canonical CSR form, or None for dense input (the reference facade's
+    _maybe_as_csr_parts, umapers/_api.py:143-190)."""
+    fmt = getattr(x, "format", None)
+    if fmt == "csr":
+        matrix = x
+    elif fmt in {"csc", "coo"}:
+        tocsr = getattr(x, "tocsr", None)
+        if not callable(tocsr):
+            raise ValueError(f"{name} sparse input with format={fmt!r} cannot be converted to CSR")
+        matrix = tocsr()
+        if getattr(matrix, "format", None) != "csr":
+            raise ValueError(f"{name}.tocsr() must return a CSR matrix")
+    else:
+        return None
+    if getattr(matrix, "has_canonical_format", True) is False:
+        matrix = matrix.copy()
+        matrix.sum_duplicates()
+        matrix.sort_indices()
+    elif getattr(matrix, "has_sorted_indices", True) is False:
+        matrix = matrix.copy()
+        matrix.sort_indices()
+    shape = getattr(matrix, "shape", None)
+    if shape is None or len(shape) != 2:
+        raise ValueError(f"{name} must be a 2D CSR matrix")
+    n_rows, n_cols = int(shape[0]), int(shape[1])
+    if n_cols <= 0:
+        raise ValueError(f"{name} must have at least one column")
+    indptr = np.asarray(matrix.indptr, dtype=np.int64, order="C")
+    indices = np.asarray(matrix.indices, dtype=np.int64, order="C")
+    data = np.asarray(matrix.data, dtype=np.float32, order="C")
+    if indptr.ndim != 1 or indices.ndim != 1 or data.ndim != 1:
+        raise ValueError(f"{name} CSR arrays must be 1D")
+    if indices.shape[0] != data.shape[0]:
+        raise ValueError(f"{name} CSR indices/data length mismatch")
+    return indptr, indices, data, n_rows, n_cols
 
 
 def _out_buffer(out: Any, shape: tuple[int, int]) -> np.ndarray:
@@ -416,23 +456,26 @@ class Umap:
         self.surrogate_info_ = self._core.fit_surrogate(**options)
         return self.surrogate_info_
 
+    def _check_sparse_options(self, y: Any) -> None:
+        if self.densmap or self.output_dens:
+            raise ValueError("densmap and output_dens currently support dense input only")
+        if self.target_metric == "categorical" and y is not None:
+            raise ValueError("categorical supervised UMAP currently supports dense input only")
+
     def _reject_unsupported(self, data: Any, y: Any) -> None:
-        if _is_sparse(data):
-            if self.densmap or self.output_dens:
-                raise ValueError("densmap and output_dens currently support dense input only")
-            raise ValueError("sparse CSR input is not supported by the B200 engine (dense float32 only)")
         if self.target_metric == "categorical" and y is not None:
             raise ValueError("categorical supervised UMAP is not supported by the B200 engine")
 
     # ---------------------------------------------------------------- fit
     def fit(self, data: Any, y: Any | None = None) -> "Umap":
-        """Fit the model on dense input and return ``self``.
+        """Fit the model and return ``self``.
 
         Parameters
         ----------
         data:
             Converted to a C-contiguous ``float32`` matrix of shape
-            ``(n_samples, n_features)``.
+            ``(n_samples, n_features)``; a sparse matrix (csr, csc or coo) is
+            fitted through its CSR form.
         y:
             Ignored unless ``target_metric="categorical"``.
 
@@ -441,6 +484,13 @@ class Umap:
         Umap
             The fitted model.
         """
+        csr = _maybe_as_csr_parts(data, "data")
+        if csr is not None:
+            self._check_sparse_options(y)
+            indptr, indices, values, n_rows, n_cols = csr
+            self._core.fit_sparse_csr(indptr, indices, values, n_cols)
+            self._set_fitted(self._core.embedding, n_cols, n_rows)
+            return self
         self._reject_unsupported(data, y)
         arr = _f32_matrix(data, "data")
         self._core.fit(arr)
@@ -460,7 +510,7 @@ class Umap:
         ----------
         data:
             Dense input, converted to ``float32`` of shape
-            ``(n_samples, n_features)``.
+            ``(n_samples, n_features)``, or a sparse matrix (csr, csc, coo).
         y:
             Ignored unless ``target_metric="categorical"``.
         out:
@@ -472,6 +522,20 @@ class Umap:
         numpy.ndarray
             The embedding, shape ``(n_samples, n_components)``.
         """
+        csr = _maybe_as_csr_parts(data, "data")
+        if csr is not None:
+            if out is not None and self.output_dens:
+                raise ValueError("out cannot be used when output_dens=True")
+            self._check_sparse_options(y)
+            indptr, indices, values, n_rows, n_cols = csr
+            if out is None:
+                emb = self._core.fit_transform_sparse_csr(indptr, indices, values, n_cols)
+                self._set_fitted(emb, n_cols, n_rows)
+                return emb
+            buf = _out_buffer(out, (n_rows, self.n_components))
+            self._core.fit_transform_sparse_csr_into(indptr, indices, values, n_cols, buf)
+            self._set_fitted(buf, n_cols, n_rows)
+            return buf
         self._reject_unsupported(data, y)
         arr = _f32_matrix(data, "data")
         if out is not None and self.output_dens:
@@ -559,7 +623,8 @@ class Umap:
         Parameters
         ----------
         query:
-            Dense input ``(n_samples, n_features)``.
+            Dense input ``(n_samples, n_features)``, or a sparse matrix for a
+            model fitted on sparse input.
         out:
             Optional writable ``float32`` buffer ``(n_samples, n_components)``.
         method:
@@ -572,8 +637,14 @@ class Umap:
         numpy.ndarray
             The projected embedding.
         """
-        if _is_sparse(query):
-            raise ValueError("sparse CSR input is not supported by the B200 engine (dense float32 only)")
+        csr = _maybe_as_csr_parts(query, "query")
+        if csr is not None:
+            indptr, indices, values, n_rows, n_cols = csr
+            if out is None:
+                return self._core.transform_sparse_csr(indptr, indices, values, n_cols)
+            buf = _out_buffer(out, (n_rows, self.n_components))
+            self._core.transform_sparse_csr_into(indptr, indices, values, n_cols, buf)
+            return buf
         arr = _f32_matrix(query, "query")
         method = self.transform_mode if method is None else method
         if method not in _TRANSFORM_MODES:
@@ -635,7 +706,9 @@ def fit_transform(data: Any, y: Any | None = None, **kwargs: Any) -> np.ndarray:
     """
     model = Umap(**kwargs)
     if y is None and model.target_metric is None and not model.densmap and not model.output_dens:
-        if _is_sparse(data):
-            model._reject_unsupported(data, y)
+        csr = _maybe_as_csr_parts(data, "data")
+        if csr is not None:
+            indptr, indices, values, _, n_cols = csr
+            return model._core.fit_transform_sparse_csr_stateless(indptr, indices, values, n_cols)
         return model._core.fit_transform_stateless(_f32_matrix(data, "data"))
     return model.fit_transform(data, y=y)

@@ -210,6 +210,13 @@ SIGNATURES = {
         [_vp, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _i32, _i32, _vp],
     ),
     "umapb_transform": (_i32, [_vp, _vp, _i64, _i64, _vp]),
+    "umapb_fit_csr": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64]),
+    "umapb_fit_transform_csr": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _vp]),
+    "umapb_fit_transform_csr_stateless": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _vp]),
+    "umapb_transform_csr": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _vp]),
+    "umapb_knn_csr": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _i32, _vp, _vp]),
+    "umapb_knn_csr_query": (
+        _i32, [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _i32, _vp, _vp]),
     "umapb_profile_fit_transform": (
         _i32,
         [_vp, _vp, _i64, _i64, _vp, ctypes.POINTER(Timings), ctypes.POINTER(FitInfo)],

@@ -19,8 +19,6 @@ from . import _lib
 
 __version__ = "1.1.4"
 
-_SPARSE_MSG = "sparse CSR input is not supported by the B200 engine (dense float32 only)"
-
 
 def _parse_metric(metric: str, metric_p: float | None) -> tuple[int, float]:
     """parse_metric (umap_rs/src/lib.rs:22-48)."""
@@ -76,6 +74,40 @@ def _check_out(out: np.ndarray, shape: tuple[int, int]) -> None:
         )
     if out.dtype != np.float32 or not out.flags.c_contiguous or not out.flags.writeable:
         raise ValueError("output buffer must be a writeable C-contiguous float32 array")
+
+
+def _nonneg_i64(x: Any, name: str) -> np.ndarray:
+    """i64_slice_to_usize_vec (umap_rs/src/lib.rs:242-260)."""
+    arr = np.ascontiguousarray(np.asarray(x, dtype=np.int64))
+    if arr.ndim != 1:
+        raise ValueError(f"{name} must be a 1D array")
+    if arr.size and int(arr.min()) < 0:
+        raise ValueError(f"{name} must contain non-negative integers")
+    return arr
+
+
+def _csr_arrays(indptr: Any, indices: Any, data: Any, n_cols: int):
+    """sparse_csr_from_py (umap_rs/src/lib.rs:337-351) and the length checks
+    of SparseCsrMatrix::new (rust_umap/src/sparse.rs:20-56); the per-row
+    checks run in the engine."""
+    ip = _nonneg_i64(indptr, "indptr")
+    ix = _nonneg_i64(indices, "indices")
+    dv = np.ascontiguousarray(np.asarray(data, dtype=np.float32))
+    if dv.ndim != 1:
+        raise ValueError("data must be a 1D array")
+    if ip.shape[0] == 0:
+        raise ValueError("indptr cannot be empty")
+    n_rows = ip.shape[0] - 1
+    if int(n_cols) < 1:
+        raise ValueError("invalid parameter: csr n_cols must be >= 1")
+    if ip[0] != 0:
+        raise ValueError("invalid parameter: csr indptr must start from 0")
+    if ix.shape[0] != dv.shape[0]:
+        raise ValueError("invalid parameter: csr indices/data lengths must match")
+    if ip[n_rows] != ix.shape[0]:
+        raise ValueError(f"invalid parameter: csr indptr last value ({int(ip[n_rows])}) must "
+                         f"equal nnz ({ix.shape[0]})")
+    return ip, ix, dv, n_rows, int(n_cols)
 
 
 class UmapCore:
@@ -268,18 +300,6 @@ class UmapCore:
     def fit_transform_supervised_into(self, *args: Any, **kwargs: Any) -> None:
         raise ValueError("categorical supervised UMAP is not supported by the B200 engine")
 
-    def fit_sparse_csr(self, *args: Any, **kwargs: Any) -> None:
-        raise ValueError(_SPARSE_MSG)
-
-    def fit_transform_sparse_csr(self, *args: Any, **kwargs: Any) -> np.ndarray:
-        raise ValueError(_SPARSE_MSG)
-
-    def fit_transform_sparse_csr_stateless(self, *args: Any, **kwargs: Any) -> np.ndarray:
-        raise ValueError(_SPARSE_MSG)
-
-    def fit_transform_sparse_csr_into(self, *args: Any, **kwargs: Any) -> None:
-        raise ValueError(_SPARSE_MSG)
-
     # ----------------------------------------------------------- transform
     def transform(self, query: Any) -> np.ndarray:
         arr = _matrix(query, "query")
@@ -299,6 +319,54 @@ class UmapCore:
                 self._handle, _lib.ptr(arr), arr.shape[0], arr.shape[1], _lib.ptr(out)
             )
         )
+
+    # --------------------------------------------------------- CSR input
+    # fit_sparse_csr / fit_transform_sparse_csr[_into|_stateless] /
+    # transform_sparse_csr[_into] (umap_rs/src/lib.rs:674-686, 869-915,
+    # 1198-1227).
+    def fit_sparse_csr(self, indptr: Any, indices: Any, data: Any, n_cols: int) -> None:
+        ip, ix, dv, n, d = _csr_arrays(indptr, indices, data, n_cols)
+        _lib.check(self._lib.umapb_fit_csr(self._handle, _lib.ptr(ip), _lib.ptr(ix),
+                                           _lib.ptr(dv), n, d))
+
+    def fit_transform_sparse_csr(self, indptr: Any, indices: Any, data: Any,
+                                 n_cols: int) -> np.ndarray:
+        ip, ix, dv, n, d = _csr_arrays(indptr, indices, data, n_cols)
+        out = np.empty((n, self.n_components), dtype=np.float32)
+        _lib.check(self._lib.umapb_fit_transform_csr(self._handle, _lib.ptr(ip), _lib.ptr(ix),
+                                                     _lib.ptr(dv), n, d, _lib.ptr(out)))
+        return out
+
+    def fit_transform_sparse_csr_into(self, indptr: Any, indices: Any, data: Any, n_cols: int,
+                                      out: np.ndarray) -> None:
+        ip, ix, dv, n, d = _csr_arrays(indptr, indices, data, n_cols)
+        _check_out(out, (n, self.n_components))
+        _lib.check(self._lib.umapb_fit_transform_csr(self._handle, _lib.ptr(ip), _lib.ptr(ix),
+                                                     _lib.ptr(dv), n, d, _lib.ptr(out)))
+
+    def fit_transform_sparse_csr_stateless(self, indptr: Any, indices: Any, data: Any,
+                                           n_cols: int) -> np.ndarray:
+        ip, ix, dv, n, d = _csr_arrays(indptr, indices, data, n_cols)
+        out = np.empty((n, self.n_components), dtype=np.float32)
+        _lib.check(self._lib.umapb_fit_transform_csr_stateless(
+            ctypes.byref(self._params), _lib.ptr(ip), _lib.ptr(ix), _lib.ptr(dv), n, d,
+            _lib.ptr(out)))
+        return out
+
+    def transform_sparse_csr(self, indptr: Any, indices: Any, data: Any,
+                             n_cols: int) -> np.ndarray:
+        ip, ix, dv, n, d = _csr_arrays(indptr, indices, data, n_cols)
+        out = np.empty((n, self.n_components), dtype=np.float32)
+        _lib.check(self._lib.umapb_transform_csr(self._handle, _lib.ptr(ip), _lib.ptr(ix),
+                                                 _lib.ptr(dv), n, d, _lib.ptr(out)))
+        return out
+
+    def transform_sparse_csr_into(self, indptr: Any, indices: Any, data: Any, n_cols: int,
+                                  out: np.ndarray) -> None:
+        ip, ix, dv, n, d = _csr_arrays(indptr, indices, data, n_cols)
+        _check_out(out, (n, self.n_components))
+        _lib.check(self._lib.umapb_transform_csr(self._handle, _lib.ptr(ip), _lib.ptr(ix),
+                                                 _lib.ptr(dv), n, d, _lib.ptr(out)))
 
     # ------------------------------------------------- learned surrogate
     # No reference counterpart (the reference's ParametricUmapCore is a
@@ -347,12 +415,6 @@ class UmapCore:
         _lib.check(self._lib.umapb_surrogate_loss_history(self._handle, _lib.ptr(buf), buf.size,
                                                           ctypes.byref(n)))
         return buf[: n.value].copy()
-
-    def transform_sparse_csr(self, *args: Any, **kwargs: Any) -> np.ndarray:
-        raise ValueError(_SPARSE_MSG)
-
-    def transform_sparse_csr_into(self, *args: Any, **kwargs: Any) -> None:
-        raise ValueError(_SPARSE_MSG)
 
     def inverse_transform(self, *args: Any, **kwargs: Any) -> np.ndarray:
         if self.n_features is None:

@@ -170,6 +170,45 @@ void check_engine_support(const umapb_params& p) {
     if (p.n_components > 16) invalid("n_components above 16 is not supported by the B200 engine");
 }
 
+// SparseCsrMatrix::new (rust_umap/src/sparse.rs:20-105) on host arrays:
+// indptr holds n_rows + 1 offsets, indices and data indptr[n_rows] entries.
+void validate_csr_host(const int64_t* indptr, const int64_t* indices, const float* data,
+                       int64_t n_rows, int64_t n_cols) {
+    if (n_cols <= 0) invalid("csr n_cols must be >= 1");
+    if (!indptr || (indptr[n_rows] > 0 && (!indices || !data))) invalid("null csr array");
+    if (indptr[0] != 0) invalid("csr indptr must start from 0");
+    for (int64_t row = 0; row < n_rows; ++row) {
+        if (indptr[row] > indptr[row + 1])
+            invalid("csr indptr must be non-decreasing, got indptr[" + std::to_string(row) +
+                    "]=" + std::to_string(indptr[row]) + " > indptr[" + std::to_string(row + 1) +
+                    "]=" + std::to_string(indptr[row + 1]));
+        for (int64_t e = indptr[row] + 1; e < indptr[row + 1]; ++e)
+            if (indices[e - 1] >= indices[e])
+                invalid("csr row " + std::to_string(row) + " indices must be strictly increasing");
+        for (int64_t e = indptr[row]; e < indptr[row + 1]; ++e)
+            if (indices[e] < 0 || indices[e] >= n_cols)
+                invalid("csr row " + std::to_string(row) + " has column index " +
+                        std::to_string(indices[e]) + " out of bounds for n_cols=" +
+                        std::to_string(n_cols));
+    }
+    for (int64_t e = 0; e < indptr[n_rows]; ++e)
+        if (!std::isfinite(data[e])) invalid("csr data must be finite");
+    if (indptr[n_rows] > 0x7FFFFFFFll) invalid("csr input above 2^31 nonzeros is not supported");
+}
+
+// validate_sparse_metric and validate_sparse_density_params
+// (lib.rs:2241-2258), then the B200 sparse kNN's own limits.
+void check_sparse_support(const umapb_params& p) {
+    if (p.metric == UMAPB_METRIC_CANBERRA || p.metric == UMAPB_METRIC_BRAYCURTIS)
+        invalid(std::string(metric_debug_name(p.metric)) +
+                " metric is currently supported for dense input only");
+    if (p.densmap || p.output_dens)
+        invalid("densmap and output_dens are currently supported for dense input only");
+    check_engine_support(p);
+    if (p.n_neighbors > 32)
+        invalid("n_neighbors above 32 is not supported by the B200 sparse kNN");
+}
+
 // should_use_approximate_knn (lib.rs:2285-2311).
 bool should_use_approximate_knn(const umapb_params& p, int64_t n, int64_t d) {
     if (!p.use_approximate_knn || n <= p.approx_knn_threshold) return false;
@@ -219,7 +258,10 @@ struct umapb_model {
     float a = 0.0f, b = 0.0f;
     bool fitted = false;
     int64_t n_fit = 0, d_fit = 0;
-    DevBuf<float> X;    // training rows, n_fit x d_fit
+    DevBuf<float> X;    // training rows, n_fit x d_fit (dense fits)
+    umapb::CsrDevice csr;      // training rows of a sparse fit
+    umapb::CsrIndex csr_idx;   // their kNN index (tiles by column, norm order)
+    bool sparse = false;       // fitted from CSR rows
     DevBuf<float> emb;  // fitted embedding, n_fit x n_components
     Graph graph;        // the fit's fuzzy graph (CSR by head), the surrogate's edge loss
     DevBuf<float> radii_orig, radii_emb;  // densMAP / output_dens radii (n_fit each)
@@ -251,6 +293,9 @@ struct umapb_model {
         radii_emb.release();
         emb.release();
         X.release();
+        csr = umapb::CsrDevice();
+        csr_idx = umapb::CsrIndex();
+        sparse = false;
     }
     void resolve_ab() {
         // resolve_ab_params (lib.rs:613-622): computed once, reused by later fits
@@ -313,7 +358,8 @@ void knn_exact_device(const float* Q, int64_t nq, const float* R, int64_t nr, in
 // build_dense_fit_artifacts (lib.rs:1367-1464) from a device kNN graph;
 // writes the embedding into model->emb.
 void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const int32_t* idx,
-                  const float* dist, int k, FitOutputs* out, StageClock& clk) {
+                  const float* dist, int k, FitOutputs* out, StageClock& clk,
+                  const CsrDevice* csr = nullptr) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int64_t n_epochs = default_epochs(p, n);
@@ -348,7 +394,7 @@ void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const i
     bool spectral_ok = false;
     if (p.init == UMAPB_INIT_SPECTRAL) {
         const SpectralResult r =
-            spectral_init(Xd, n, static_cast<int>(d), g, dim, p.random_seed, emb.get(), s);
+            spectral_init(Xd, n, static_cast<int>(d), g, dim, p.random_seed, emb.get(), s, csr);
         spectral_ok = r.used_spectral;
         if (out) out->info.n_components_graph = r.n_components;
     }
@@ -459,6 +505,38 @@ void fit_host(umapb_model* m, const float* data, int64_t n, int64_t d, FitOutput
     }
 }
 
+// fit_sparse_csr / fit_transform_sparse_csr (lib.rs:998-1036, 1479-1549):
+// exact sparse kNN, then the dense pipeline from the kNN table with the
+// centroids of a disconnected graph taken from the CSR rows.
+void fit_csr_host(umapb_model* m, const int64_t* indptr, const int64_t* indices,
+                  const float* data, int64_t n, int64_t d, float* emb_out) {
+    validate_csr_host(indptr, indices, data, n, d);
+    if (n == 0) throw Error(UMAPB_ERR_EMPTY_DATA, "input data is empty");
+    if (n < 2) throw Error(UMAPB_ERR_NEED_TWO_SAMPLES, "need at least two samples");
+    validate_params(m->p, n);
+    check_sparse_support(m->p);
+    m->ensure_device();
+    cudaStream_t s = m->stream;
+    m->begin_fit();
+    CsrDevice csr;
+    csr_upload(indptr, indices, data, n, d, csr, s);
+    CsrIndex ci;
+    csr_index(csr, ci, s);
+    const int k = static_cast<int>(m->p.n_neighbors);
+    DevBuf<int32_t> idx(n * k, s);
+    DevBuf<float> dist(n * k, s);
+    knn_sparse(csr, csr, ci, true, k, m->p.metric, idx.get(), dist.get(), s);
+    StageClock clk(s, false);
+    fit_from_knn(m, nullptr, n, d, idx.get(), dist.get(), k, nullptr, clk, &csr);
+    m->csr = std::move(csr);
+    m->csr_idx = std::move(ci);
+    m->sparse = true;
+    m->n_fit = n;
+    m->d_fit = d;
+    m->fitted = true;
+    if (emb_out) copy_embedding_out(m, emb_out);
+}
+
 // validate_and_trim_precomputed_knn (lib.rs:1968-2040) on host arrays that
 // already passed the shape checks; writes the trimmed k columns.
 void trim_precomputed(const int64_t* idx, const float* dist, int64_t n, int64_t cols, int64_t k,
@@ -494,29 +572,47 @@ void trim_precomputed(const int64_t* idx, const float* dist, int64_t n, int64_t 
     }
 }
 
-// transform_dense (lib.rs:1593-1685) on device rows.  The default epoch
-// count follows the size of the whole request, `epoch_rows` (lib.rs:1650-1657).
+// transform_from_knn (lib.rs:1738-1780) on a device kNN table: bipartite
+// membership, weighted init and the per-query SGD.  The default epoch count
+// follows the size of the whole request, `epoch_rows` (lib.rs:1650-1657).
+void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* dist, int64_t nq,
+                               int k, int64_t epoch_rows, float* out_dev) {
+    cudaStream_t s = m->stream;
+    const umapb_params& p = m->p;
+    const int dim = static_cast<int>(p.n_components);
+    const int64_t n_epochs = p.n_epochs >= 0 ? std::max<int64_t>(p.n_epochs, 1)
+                                             : (epoch_rows <= 10000 ? 100 : 30);
+    DevBuf<float> sig(nq, s), rho(nq, s);
+    const float lc = std::max(p.local_connectivity - 1.0f, 0.0f);
+    smooth_knn(dist, nq, k, static_cast<float>(k), lc, 1.0f, false, sig.get(), rho.get(), s);
+    Graph g;
+    bipartite_graph(idx, dist, sig.get(), rho.get(), nq, k, n_epochs, g, s);
+    transform_layout(out_dev, nq, dim, m->emb.get(), m->n_fit, g, n_epochs, m->a, m->b,
+                     p.learning_rate / 4.0f, p.negative_sample_rate, p.repulsion_strength,
+                     p.random_seed ^ 0xA24BAED40B53C117ULL, s);
+}
+
+// transform_dense (lib.rs:1593-1685) on device rows.  A model fitted on CSR
+// rows takes the dense queries' nonzeros as CSR rows
+// (exact_nearest_neighbors_dense_query, sparse.rs:753-910, gives the same
+// distances).
 void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out_dev,
                       int64_t epoch_rows = -1) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
-    const int dim = static_cast<int>(p.n_components);
     const int k = static_cast<int>(std::min<int64_t>(p.n_neighbors, m->n_fit));
     if (epoch_rows < 0) epoch_rows = nq;
-    const int64_t n_epochs = p.n_epochs >= 0 ? std::max<int64_t>(p.n_epochs, 1)
-                                             : (epoch_rows <= 10000 ? 100 : 30);
     DevBuf<int32_t> idx(nq * k, s);
     DevBuf<float> dist(nq * k, s);
-    knn_exact_device(Qd, nq, m->X.get(), m->n_fit, static_cast<int>(d), k, p.metric,
-                     p.knn_backend, idx.get(), dist.get(), nullptr, nullptr, nullptr, s);
-    DevBuf<float> sig(nq, s), rho(nq, s);
-    const float lc = std::max(p.local_connectivity - 1.0f, 0.0f);
-    smooth_knn(dist.get(), nq, k, static_cast<float>(k), lc, 1.0f, false, sig.get(), rho.get(), s);
-    Graph g;
-    bipartite_graph(idx.get(), dist.get(), sig.get(), rho.get(), nq, k, n_epochs, g, s);
-    transform_layout(out_dev, nq, dim, m->emb.get(), m->n_fit, g, n_epochs, m->a, m->b,
-                     p.learning_rate / 4.0f, p.negative_sample_rate, p.repulsion_strength,
-                     p.random_seed ^ 0xA24BAED40B53C117ULL, s);
+    if (m->sparse) {
+        CsrDevice q;
+        csr_from_dense(Qd, nq, d, q, s);
+        knn_sparse(q, m->csr, m->csr_idx, false, k, p.metric, idx.get(), dist.get(), s);
+    } else {
+        knn_exact_device(Qd, nq, m->X.get(), m->n_fit, static_cast<int>(d), k, p.metric,
+                         p.knn_backend, idx.get(), dist.get(), nullptr, nullptr, nullptr, s);
+    }
+    transform_from_knn_device(m, idx.get(), dist.get(), nq, k, epoch_rows, out_dev);
 }
 
 // Surrogate transform of device rows: network outputs for every row, then
@@ -653,6 +749,65 @@ int32_t umapb_fit_transform(umapb_model* m, const float* data, int64_t n_rows, i
     return guarded([&] {
         std::lock_guard<std::mutex> lk(m->mu);
         fit_host(m, data, n_rows, n_cols, nullptr, out);
+    });
+}
+
+int32_t umapb_fit_csr(umapb_model* m, const int64_t* indptr, const int64_t* indices,
+                      const float* data, int64_t n_rows, int64_t n_cols) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        fit_csr_host(m, indptr, indices, data, n_rows, n_cols, nullptr);
+    });
+}
+
+int32_t umapb_fit_transform_csr(umapb_model* m, const int64_t* indptr, const int64_t* indices,
+                                const float* data, int64_t n_rows, int64_t n_cols, float* out) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        fit_csr_host(m, indptr, indices, data, n_rows, n_cols, out);
+    });
+}
+
+int32_t umapb_fit_transform_csr_stateless(const umapb_params* params, const int64_t* indptr,
+                                          const int64_t* indices, const float* data,
+                                          int64_t n_rows, int64_t n_cols, float* out) {
+    umapb_model* m = nullptr;
+    int32_t st = umapb_create(params, &m);
+    if (st != UMAPB_OK) return st;
+    st = umapb_fit_transform_csr(m, indptr, indices, data, n_rows, n_cols, out);
+    const std::string err = g_last_error;
+    umapb_destroy(m);
+    g_last_error = err;
+    return st;
+}
+
+int32_t umapb_transform_csr(umapb_model* m, const int64_t* indptr, const int64_t* indices,
+                            const float* data, int64_t n_rows, int64_t n_cols, float* out) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        validate_csr_host(indptr, indices, data, n_rows, n_cols);
+        // transform_sparse_csr (lib.rs:1687-1736)
+        if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        if (n_cols != m->d_fit)
+            throw Error(UMAPB_ERR_FEATURE_MISMATCH,
+                        "feature mismatch: expected " + std::to_string(m->d_fit) + ", got " +
+                            std::to_string(n_cols));
+        if (!m->sparse)
+            invalid("sparse query transform is supported only for sparse-fitted models");
+        if (n_rows == 0) return;
+        m->ensure_device();
+        cudaStream_t s = m->stream;
+        CsrDevice q;
+        csr_upload(indptr, indices, data, n_rows, n_cols, q, s);
+        const int k = static_cast<int>(std::min<int64_t>(m->p.n_neighbors, m->n_fit));
+        DevBuf<int32_t> idx(n_rows * k, s);
+        DevBuf<float> dist(n_rows * k, s);
+        knn_sparse(q, m->csr, m->csr_idx, false, k, m->p.metric, idx.get(), dist.get(), s);
+        DevBuf<float> outd(n_rows * m->p.n_components, s);
+        transform_from_knn_device(m, idx.get(), dist.get(), n_rows, k, n_rows, outd.get());
+        UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * m->p.n_components * 4,
+                                   cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
     });
 }
 
@@ -922,6 +1077,61 @@ int32_t umapb_knn_query(const float* query, int64_t nq, const float* reference, 
     });
 }
 
+int32_t umapb_knn_csr(const int64_t* indptr, const int64_t* indices, const float* data,
+                      int64_t n_rows, int64_t n_cols, int64_t k, int32_t metric,
+                      int64_t* out_idx, float* out_dist) {
+    return guarded([&] {
+        validate_csr_host(indptr, indices, data, n_rows, n_cols);
+        if (n_rows == 0) return;
+        if (k < 1 || k > n_rows) invalid("k must be in [1, n_rows]");
+        ScopedStream ss;
+        CsrDevice csr;
+        csr_upload(indptr, indices, data, n_rows, n_cols, csr, ss.s);
+        CsrIndex ci;
+        csr_index(csr, ci, ss.s);
+        DevBuf<int32_t> idx(n_rows * k, ss.s);
+        DevBuf<float> dist(n_rows * k, ss.s);
+        knn_sparse(csr, csr, ci, true, static_cast<int>(k), metric, idx.get(), dist.get(), ss.s);
+        std::vector<int32_t> ih(n_rows * k);
+        UMAPB_CUDA(cudaMemcpyAsync(ih.data(), idx.get(), n_rows * k * 4, cudaMemcpyDeviceToHost,
+                                   ss.s));
+        UMAPB_CUDA(cudaMemcpyAsync(out_dist, dist.get(), n_rows * k * 4, cudaMemcpyDeviceToHost,
+                                   ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        to_i64(ih, out_idx);
+    });
+}
+
+int32_t umapb_knn_csr_query(const int64_t* q_indptr, const int64_t* q_indices,
+                            const float* q_data, int64_t n_q, const int64_t* r_indptr,
+                            const int64_t* r_indices, const float* r_data, int64_t n_r,
+                            int64_t n_cols, int64_t k, int32_t metric, int64_t* out_idx,
+                            float* out_dist) {
+    return guarded([&] {
+        validate_csr_host(q_indptr, q_indices, q_data, n_q, n_cols);
+        validate_csr_host(r_indptr, r_indices, r_data, n_r, n_cols);
+        if (n_q == 0) return;
+        if (k < 1 || k > n_r) invalid("k must be in [1, n_reference]");
+        ScopedStream ss;
+        CsrDevice q, r;
+        csr_upload(q_indptr, q_indices, q_data, n_q, n_cols, q, ss.s);
+        csr_upload(r_indptr, r_indices, r_data, n_r, n_cols, r, ss.s);
+        CsrIndex ri;
+        csr_index(r, ri, ss.s);
+        DevBuf<int32_t> idx(n_q * k, ss.s);
+        DevBuf<float> dist(n_q * k, ss.s);
+        knn_sparse(q, r, ri, false, static_cast<int>(k), metric, idx.get(), dist.get(), ss.s);
+        std::vector<int32_t> ih(n_q * k);
+        UMAPB_CUDA(cudaMemcpyAsync(ih.data(), idx.get(), n_q * k * 4, cudaMemcpyDeviceToHost,
+                                   ss.s));
+        UMAPB_CUDA(cudaMemcpyAsync(out_dist, dist.get(), n_q * k * 4, cudaMemcpyDeviceToHost,
+                                   ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        to_i64(ih, out_idx);
+    });
+}
+
+
 int32_t umapb_nndescent(const float* data, int64_t n, int64_t d, int64_t k, int32_t metric,
                         int64_t candidate_pool, int64_t n_iters, uint64_t seed, int64_t* indices,
                         float* dists, int64_t* iters_run) {
@@ -1084,6 +1294,7 @@ int32_t umapb_surrogate_fit(umapb_model* m, const umapb_surrogate_params* params
         if (!m) invalid("null model");
         std::lock_guard<std::mutex> lk(m->mu);
         if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        if (m->sparse) invalid("the transform surrogate needs a model fitted on dense rows");
         if (!m->X.get() || !m->graph.row_ptr.get())
             invalid("the surrogate needs a model fitted on rows (not a stateless fit)");
         umapb_surrogate_params p;

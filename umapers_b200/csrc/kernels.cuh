@@ -46,6 +46,43 @@ bool knn_tc_supported(int d, int k, int metric);
 void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int k, int metric,
             int32_t* out_idx, float* out_dist, TcKnnStats* stats, cudaStream_t s);
 
+// --------------------------------------------------------- knn_sparse.cu
+// A CSR matrix on the device: indptr (n_rows + 1), int32 column indices
+// strictly increasing within a row, FP32 values, and the per-row squared and
+// L2 norms of SparseCsrMatrix (rust_umap/src/sparse.rs:90-97: sum of v * v in
+// stored order, and its square root).
+struct CsrDevice {
+    int64_t n_rows = 0, n_cols = 0, nnz = 0;
+    DevBuf<int64_t> indptr;
+    DevBuf<int32_t> indices;
+    DevBuf<float> values;
+    DevBuf<float> sq, l2;
+};
+
+// Uploads host CSR arrays (already validated) and computes the norms.
+void csr_upload(const int64_t* indptr, const int64_t* indices, const float* values,
+                int64_t n_rows, int64_t n_cols, CsrDevice& out, cudaStream_t s);
+// The nonzeros of dense device rows (n x d) as CSR rows, with their norms.
+void csr_from_dense(const float* X, int64_t n, int64_t d, CsrDevice& out, cudaStream_t s);
+
+// The reference side of a sparse kNN: its nonzeros regrouped by (tile of
+// 4096 rows, column), rows ascending within a group, and its rows ordered by
+// (squared norm, index).
+struct CsrIndex {
+    int64_t n_tiles = 0;
+    DevBuf<int64_t> tile_colptr;  // n_tiles * n_cols + 1 offsets
+    DevBuf<int32_t> tile_rows;    // row within its tile
+    DevBuf<float> tile_vals;
+    DevBuf<int32_t> norm_order;
+};
+void csr_index(const CsrDevice& r, CsrIndex& out, cudaStream_t s);
+
+// Exact kNN of the rows of q against the rows of r (euclidean or cosine,
+// k <= 32), the result of exact_nearest_neighbors (self = true, q = r) or
+// exact_nearest_neighbors_sparse_query (sparse.rs:605-657) bit for bit.
+void knn_sparse(const CsrDevice& q, const CsrDevice& r, const CsrIndex& ri, bool self, int k,
+                int metric, int32_t* out_idx, float* out_dist, cudaStream_t s);
+
 // ------------------------------------------------------------ gemm_tc.cu
 // C[M x N] = A[M x K] B[N x K]^T on tcgen05 tensor cores: BF16 operands
 // (row-major, K contiguous, K % 64 == 0, 16-byte aligned), FP32 accumulation
@@ -132,8 +169,11 @@ struct SpectralResult {
     int64_t n_components = 0;
 };
 // initialize_embedding with InitMethod::Spectral (rust_umap/src/lib.rs:3841-3888).
+// The input rows serve only the centroids of a disconnected graph's meta
+// layout: dense X (n x d), or the CSR rows when csr is given.
 SpectralResult spectral_init(const float* X, int64_t n, int d, const Graph& g, int dim,
-                             uint64_t seed, float* out, cudaStream_t s);
+                             uint64_t seed, float* out, cudaStream_t s,
+                             const CsrDevice* csr = nullptr);
 
 // random_init (rust_umap/src/lib.rs:3824-3839) with counter-based uniforms.
 void random_init(int64_t n, int dim, uint64_t seed, float low, float high, float* out,

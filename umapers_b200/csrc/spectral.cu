@@ -423,6 +423,22 @@ __global__ void centroid_kernel(const Chunk* __restrict__ chunks, const int32_t*
     }
 }
 
+// the same sums from CSR rows (component_centroids_sparse, lib.rs:4487-4505)
+__global__ void centroid_csr_kernel(const Chunk* __restrict__ chunks,
+                                    const int32_t* __restrict__ nodes,
+                                    const int64_t* __restrict__ indptr,
+                                    const int32_t* __restrict__ indices,
+                                    const float* __restrict__ values, int d,
+                                    double* __restrict__ cent) {
+    const Chunk ch = chunks[blockIdx.x];
+    for (int r = ch.start + static_cast<int>(threadIdx.x); r < ch.end; r += blockDim.x) {
+        const int64_t v = nodes[r];
+        for (int64_t e = indptr[v]; e < indptr[v + 1]; ++e)
+            atomicAdd(&cent[static_cast<int64_t>(ch.slot) * d + indices[e]],
+                      static_cast<double>(values[e]));
+    }
+}
+
 // ------------------------------------------------------------ host side --
 using HostCoords = std::vector<float>;  // row-major n x dim
 
@@ -726,7 +742,7 @@ void random_init(int64_t n, int dim, uint64_t seed, float low, float high, float
 }
 
 SpectralResult spectral_init(const float* X, int64_t n, int d, const Graph& g, int dim,
-                             uint64_t seed, float* out, cudaStream_t s) {
+                             uint64_t seed, float* out, cudaStream_t s, const CsrDevice* csr) {
     SpectralResult res;
     const int64_t m = g.n_edges;
     if (n <= dim + 1 || m == 0) return res;
@@ -825,8 +841,13 @@ SpectralResult spectral_init(const float* X, int64_t n, int d, const Graph& g, i
             UMAPB_CUDA(cudaMemcpyAsync(dch.get(), chunks.data(), chunks.size() * sizeof(Chunk),
                                        cudaMemcpyHostToDevice, s));
             UMAPB_CUDA(cudaMemsetAsync(dcent.get(), 0, n_comp * d * 8, s));
-            centroid_kernel<<<static_cast<unsigned>(chunks.size()), 128, 0, s>>>(
-                dch.get(), order.get(), X, d, dcent.get());
+            if (csr)
+                centroid_csr_kernel<<<static_cast<unsigned>(chunks.size()), 128, 0, s>>>(
+                    dch.get(), order.get(), csr->indptr.get(), csr->indices.get(),
+                    csr->values.get(), d, dcent.get());
+            else
+                centroid_kernel<<<static_cast<unsigned>(chunks.size()), 128, 0, s>>>(
+                    dch.get(), order.get(), X, d, dcent.get());
             UMAPB_LAUNCH_CHECK();
             cents.resize(n_comp * d);
             UMAPB_CUDA(cudaMemcpyAsync(cents.data(), dcent.get(), n_comp * d * 8,

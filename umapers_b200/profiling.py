@@ -3,6 +3,7 @@
     python -m umapers_b200.profiling knn_tc [--rows 262144] [--dim 64]
     python -m umapers_b200.profiling surrogate [--rows 262144]
     python -m umapers_b200.profiling fit [--rows 262144] [--dim 64]
+    python -m umapers_b200.profiling sparse [--rows 200000] [--dim 2000]
 
 Each case runs once untimed, then once inside an NVTX range named after the
 case, so a profiler can be limited to the measured launches, e.g.
@@ -93,6 +94,27 @@ def case_surrogate(rows: int) -> None:
     print(f"surrogate transform rows={rows}: {r.dt:.4f} s, gated rows {nf.value}")
 
 
+def case_sparse(rows: int, dim: int) -> None:
+    """Exact cosine kNN (k = 30) of `rows` CSR rows with about 20 LogNormal
+    values each among `dim` columns."""
+    x = workloads.sparse_lognormal_csr(rows, dim, 20, seed=3)
+    lib = _lib.load()
+    ip = np.ascontiguousarray(x.indptr, np.int64)
+    ix = np.ascontiguousarray(x.indices, np.int64)
+    dv = np.ascontiguousarray(x.data, np.float32)
+    idx = np.empty((rows, 30), np.int64)
+    dist = np.empty((rows, 30), np.float32)
+
+    def run():
+        _lib.check(lib.umapb_knn_csr(ip.ctypes.data, ix.ctypes.data, dv.ctypes.data, rows, dim,
+                                     30, 2, idx.ctypes.data, dist.ctypes.data))
+
+    run()
+    with _Range("sparse") as r:
+        run()
+    print(f"sparse kNN rows={rows} dim={dim} nnz={x.nnz}: {r.dt:.4f} s")
+
+
 def case_fit(rows: int, dim: int) -> None:
     """One complete fit (exact kNN, spectral init, 200 epochs)."""
     from umapers import Umap
@@ -107,14 +129,18 @@ def case_fit(rows: int, dim: int) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser(description="profiling cases of libumapb200")
-    ap.add_argument("case", choices=["knn_tc", "surrogate", "fit"])
+    ap.add_argument("case", choices=["knn_tc", "surrogate", "fit", "sparse"])
     ap.add_argument("--rows", type=int, default=262_144)
-    ap.add_argument("--dim", type=int, default=64)
+    ap.add_argument("--dim", type=int, default=None)
     a = ap.parse_args()
+    if a.dim is None:
+        a.dim = 2000 if a.case == "sparse" else 64
     if a.case == "knn_tc":
         case_knn_tc(a.rows, a.dim)
     elif a.case == "surrogate":
         case_surrogate(a.rows)
+    elif a.case == "sparse":
+        case_sparse(a.rows, a.dim)
     else:
         case_fit(a.rows, a.dim)
 

@@ -93,3 +93,22 @@ def three_centres(n_samples: int = 180, n_features: int = 12, seed: int = 42) ->
     x -= x.mean(axis=0, keepdims=True)
     x /= x.std(axis=0, keepdims=True) + 1e-6
     return x.astype(np.float32)
+
+
+def sparse_lognormal_csr(n: int = 200_000, d: int = 2000, nnz_row: int = 20, seed: int = 3):
+    """CSR rows with about `nnz_row` stored values each: column positions
+    drawn uniformly per row (repeats merged, so a row holds at most
+    `nnz_row`), sorted, values LogNormal(0, 1) (the sparse text-like
+    configuration, 200,000 x 2,000 at 1%)."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    cols = np.sort(rng.integers(0, d, size=(n, nnz_row)), axis=1)
+    keep = np.ones_like(cols, dtype=bool)
+    keep[:, 1:] = cols[:, 1:] != cols[:, :-1]
+    counts = keep.sum(axis=1)
+    indptr = np.zeros(n + 1, np.int64)
+    np.cumsum(counts, out=indptr[1:])
+    indices = cols[keep].astype(np.int64)
+    data = rng.lognormal(0.0, 1.0, size=indices.shape[0]).astype(np.float32)
+    return sp.csr_matrix((data, indices, indptr), shape=(n, d))
