@@ -18,9 +18,11 @@
 //    tile the warp walks the query's columns in ascending order and adds
 //    q_c * v_jc into a per-warp shared-memory accumulator of the tile's rows.
 //    Every row's products therefore arrive in ascending column order, the
-//    reference's summation order.  A second walk over the same columns turns
-//    each touched row's dot into a distance, offers its key to the warp's
-//    sorted list of the 32 smallest keys, and resets the accumulator entry.
+//    reference's summation order.  The first entries of four columns are
+//    loaded together, and rows touched for the first time are appended to a
+//    per-warp list.  The list is then walked once: each touched row's dot
+//    becomes a distance, its key is offered to the warp's sorted list of the
+//    32 smallest keys, and its accumulator entry is reset.
 // 2. Untouched rows (dot = 0).  Their distances depend only on the other
 //    row's norm: cosine gives 1 for all of them (or 0 / 1 for an empty
 //    query), euclidean sqrt(|x|^2 + |y|^2), non-decreasing in |y|^2.  The
@@ -156,10 +158,31 @@ struct SparseArgs {
     float* out_dist;
 };
 
+// Adds q * v of one stored entry (valid lanes) into the warp's accumulator and
+// appends rows touched for the first time to the warp's list of touched rows.
+__device__ __forceinline__ void accumulate(float* acc, uint16_t* touched, int& n_touched,
+                                           bool valid, int32_t jl, float prod) {
+    bool first = false;
+    if (valid) {
+        const float a = acc[jl];
+        first = __float_as_uint(a) == kUnset;
+        acc[jl] = __fadd_rn(first ? 0.0f : a, prod);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, first);
+    if (first)
+        touched[n_touched + __popc(m & ((1u << (threadIdx.x & 31)) - 1u))] =
+            static_cast<uint16_t>(jl);
+    n_touched += __popc(m);
+}
+
+constexpr int kColBatch = 4;   // query columns whose first entries load together
+constexpr int kEvalBatch = 4;  // chunks of touched rows whose norms load together
+
 __global__ void __launch_bounds__(kWarps * 32) knn_sparse_kernel(SparseArgs p) {
     extern __shared__ float acc_all[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* acc = acc_all + warp * kTileRows;
+    uint16_t* touched = reinterpret_cast<uint16_t*>(acc_all + kWarps * kTileRows) + warp * kTileRows;
     for (int j = lane; j < kTileRows; j += 32) acc[j] = __uint_as_float(kUnset);
     __syncwarp();
     const int64_t wstride = static_cast<int64_t>(gridDim.x) * kWarps;
@@ -172,42 +195,92 @@ __global__ void __launch_bounds__(kWarps * 32) knn_sparse_kernel(SparseArgs p) {
         // ---- 1. rows sharing a column with the query, tile by tile
         for (int64_t t = 0; t < p.n_tiles; ++t) {
             const int64_t* cp = p.tile_colptr + t * p.n_cols;
-            for (int64_t e = q0; e < q1; ++e) {
-                const int32_t c = p.qidx[e];
-                const float qv = p.qval[e];
-                const int64_t b0 = cp[c], b1 = cp[c + 1];
-                for (int64_t b = b0 + lane; b < b1; b += 32) {
-                    const int32_t jl = p.tile_rows[b];
-                    const float prod = __fmul_rn(qv, p.tile_vals[b]);
-                    const float a = acc[jl];
-                    acc[jl] = __fadd_rn(__float_as_uint(a) == kUnset ? 0.0f : a, prod);
+            int n_touched = 0;
+            for (int64_t e0 = q0; e0 < q1; e0 += 32) {
+                const int ne = static_cast<int>(q1 - e0 < 32 ? q1 - e0 : 32);
+                // lane u holds query column u of this chunk: value and entry range
+                int64_t mb0 = 0, mb1 = 0;
+                float mqv = 0.0f;
+                if (lane < ne) {
+                    const int32_t c = p.qidx[e0 + lane];
+                    mqv = p.qval[e0 + lane];
+                    mb0 = cp[c];
+                    mb1 = cp[c + 1];
                 }
-                __syncwarp();
-            }
-            const int64_t row0 = t << kTileShift;
-            for (int64_t e = q0; e < q1; ++e) {
-                const int32_t c = p.qidx[e];
-                const int64_t b0 = cp[c], b1 = cp[c + 1];
-                for (int64_t base = b0; base < b1; base += 32) {
-                    const int64_t b = base + lane;
-                    uint64_t key = ~0ull;
-                    if (b < b1) {
-                        const int32_t jl = p.tile_rows[b];
-                        const float a = acc[jl];
-                        if (__float_as_uint(a) != kUnset) {
-                            acc[jl] = __uint_as_float(kUnset);
-                            const int64_t j = row0 + jl;
-                            if (!(p.self && j == i)) {
-                                const float d = csr_distance_from_dot(a, qsq, ql2, p.rsq[j],
-                                                                      p.rl2[j], p.metric);
-                                key = knn_key(d, static_cast<uint32_t>(j));
-                            }
+                for (int ub = 0; ub < ne; ub += kColBatch) {
+                    // the first 32 entries of kColBatch columns load together; the
+                    // products still enter the accumulator in column order
+                    int32_t jl[kColBatch];
+                    float pv[kColBatch], qv[kColBatch];
+                    bool ok[kColBatch];
+                    int64_t b0[kColBatch], b1[kColBatch];
+#pragma unroll
+                    for (int r = 0; r < kColBatch; ++r) {
+                        const int u = ub + r < ne ? ub + r : ne - 1;
+                        b0[r] = __shfl_sync(0xffffffffu, mb0, u);
+                        b1[r] = __shfl_sync(0xffffffffu, mb1, u);
+                        qv[r] = __shfl_sync(0xffffffffu, mqv, u);
+                        const int64_t b = b0[r] + lane;
+                        ok[r] = ub + r < ne && b < b1[r];
+                        jl[r] = 0;
+                        pv[r] = 0.0f;
+                        if (ok[r]) {
+                            jl[r] = p.tile_rows[b];
+                            pv[r] = p.tile_vals[b];
                         }
+                    }
+#pragma unroll
+                    for (int r = 0; r < kColBatch; ++r) {
+                        if (ub + r >= ne) break;
+                        accumulate(acc, touched, n_touched, ok[r], jl[r],
+                                   __fmul_rn(qv[r], pv[r]));
+                        for (int64_t base = b0[r] + 32; base < b1[r]; base += 32) {
+                            const int64_t b = base + lane;
+                            const bool v = b < b1[r];
+                            const int32_t j2 = v ? p.tile_rows[b] : 0;
+                            const float x2 = v ? p.tile_vals[b] : 0.0f;
+                            accumulate(acc, touched, n_touched, v, j2, __fmul_rn(qv[r], x2));
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+            // every touched row: its distance, its key offered, its entry reset;
+            // the norms of kEvalBatch chunks of 32 rows load together
+            const int64_t row0 = t << kTileShift;
+            const bool cosine = p.metric == UMAPB_METRIC_COSINE;
+            for (int base = 0; base < n_touched; base += 32 * kEvalBatch) {
+                float dot[kEvalBatch], nrm[kEvalBatch];
+                int64_t jj[kEvalBatch];
+#pragma unroll
+                for (int r = 0; r < kEvalBatch; ++r) {
+                    const int at = base + 32 * r + lane;
+                    jj[r] = -1;
+                    dot[r] = 0.0f;
+                    nrm[r] = 0.0f;
+                    if (at < n_touched) {
+                        const int32_t jl = touched[at];
+                        dot[r] = acc[jl];
+                        acc[jl] = __uint_as_float(kUnset);
+                        jj[r] = row0 + jl;
+                        nrm[r] = cosine ? p.rl2[jj[r]] : p.rsq[jj[r]];
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kEvalBatch; ++r) {
+                    if (base + 32 * r >= n_touched) break;
+                    uint64_t key = ~0ull;
+                    if (jj[r] >= 0 && !(p.self && jj[r] == i)) {
+                        const float d = cosine ? csr_distance_from_dot(dot[r], qsq, ql2, 0.0f,
+                                                                       nrm[r], p.metric)
+                                               : csr_distance_from_dot(dot[r], qsq, ql2, nrm[r],
+                                                                       0.0f, p.metric);
+                        key = knn_key(d, static_cast<uint32_t>(jj[r]));
                     }
                     offer(list, key);
                 }
-                __syncwarp();
             }
+            __syncwarp();
         }
         // ---- 2. rows sharing no column with the query (dot = +0.0)
         const bool by_norm = p.metric != UMAPB_METRIC_COSINE;
@@ -490,7 +563,8 @@ void knn_sparse(const CsrDevice& q, const CsrDevice& r, const CsrIndex& ri, bool
     a.self = self ? 1 : 0;
     a.out_idx = out_idx;
     a.out_dist = out_dist;
-    const size_t smem = static_cast<size_t>(kWarps) * kTileRows * sizeof(float);
+    // per warp: the FP32 accumulator and the list of touched rows (uint16)
+    const size_t smem = static_cast<size_t>(kWarps) * kTileRows * (sizeof(float) + sizeof(uint16_t));
     UMAPB_CUDA(cudaFuncSetAttribute(knn_sparse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
     int dev = 0, sms = 0;
