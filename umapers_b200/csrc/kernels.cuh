@@ -66,7 +66,7 @@ void csr_upload(const int64_t* indptr, const int64_t* indices, const float* valu
 void csr_from_dense(const float* X, int64_t n, int64_t d, CsrDevice& out, cudaStream_t s);
 
 // The reference side of a sparse kNN: its nonzeros regrouped by (tile of
-// 4096 rows, column), rows ascending within a group, and its rows ordered by
+// 2048 rows, column), rows ascending within a group, and its rows ordered by
 // (squared norm, index).
 struct CsrIndex {
     int64_t n_tiles = 0;

@@ -13,7 +13,7 @@
 // stored column with the query has dot = +0.0 exactly.
 //
 // Here one warp serves one query row:
-// 1. Touched rows.  The reference rows are regrouped once into tiles of 4096
+// 1. Touched rows.  The reference rows are regrouped once into tiles of 2048
 //    rows, and within a tile by column (CSC order, rows ascending).  For each
 //    tile the warp walks the query's columns in ascending order and adds
 //    q_c * v_jc into a per-warp shared-memory accumulator of the tile's rows.
@@ -39,9 +39,9 @@
 namespace umapb {
 namespace {
 
-constexpr int kTileRows = 4096;             // reference rows per accumulator tile
-constexpr int kTileShift = 12;
-constexpr int kWarps = 8;                   // warps (queries in flight) per block
+constexpr int kTileRows = 2048;             // reference rows per accumulator tile
+constexpr int kTileShift = 11;
+constexpr int kWarps = 16;                  // warps (queries in flight) per block
 constexpr int kList = 32;                   // list length: k <= 32
 constexpr uint32_t kUnset = 0x7fc00001u;    // accumulator entry not touched yet
 
