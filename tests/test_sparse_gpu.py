@@ -4,7 +4,7 @@ The exact sparse kNN is pinned bit for bit against the oracle's restatement
 of sparse::exact_nearest_neighbors / exact_nearest_neighbors_sparse_query
 (rust_umap/src/sparse.rs:605-657): indices and FP32 distances, euclidean and
 cosine, on inputs with negative values, empty rows, duplicate rows and rows
-of equal norm, over more than one 4096-row tile.  The fit and transform follow
+of equal norm, over more than one 2048-row tile.  The fit and transform follow
 the reference's sparse tests (rust_umap/src/lib.rs:6376-6660, 7568-7740):
 sparse kNN equals the dense kNN of the same matrix, sparse and dense queries
 of a sparse model transform alike, sparse queries need a sparse model, and a
