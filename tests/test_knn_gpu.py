@@ -109,6 +109,20 @@ def test_tensor_knn_mixture_20000x192_sampled_rows(orc):
     assert fb <= 1000
 
 
+def test_tensor_knn_in_cell_order_matches_plain():
+    # at least one wave of query groups: the rows are regrouped by nearest
+    # pivot and each group starts at its own cell; the result keeps original
+    # row numbers and the lower-index tie rule, duplicates across cells included
+    x = workloads.anisotropic_mixture(60_000, 64, 50, seed=3)
+    x[59_000:59_020] = x[17]
+    x[123] = x[40_000]
+    ti, td, fb = gu.knn_exact(x, 15, backend="tensor")
+    pi, pd, _ = gu.knn_exact(x, 15, backend="plain")
+    np.testing.assert_array_equal(ti, pi)
+    np.testing.assert_array_equal(td, pd)
+    assert fb <= 600
+
+
 def test_tensor_knn_1m_x_64_sampled_rows(orc):
     x = workloads.anisotropic_mixture(1_000_000, 64, 50, seed=11)
     ti, td, fb = gu.knn_exact(x, 15, backend="tensor")

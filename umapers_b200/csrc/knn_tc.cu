@@ -26,7 +26,10 @@
 //    scratch and its qualifying keys are inserted cooperatively (one list
 //    entry per lane), while the next pending row's list is already being
 //    loaded.  When the query tiles are fewer than the SMs, the candidate
-//    tiles are split too (one wave of units), with lists per split.
+//    tiles are split too (one wave of units), with lists per split.  A self
+//    kNN over at least one wave of query groups first regroups its rows by
+//    nearest pivot ("cell order" below), and each group starts its candidate
+//    walk at its own cell, so the lists fill with near candidates first.
 // 3. rerank: one warp per row recomputes exact FP32 distances in the
 //    reference's summation order and keeps the k smallest (distance, index)
 //    keys.  With U_j = L_j + 2 e_j and B the smallest largest-L of the full
@@ -38,9 +41,11 @@
 //
 // Every wait on an mbarrier is bounded by a %globaltimer deadline; a timeout
 // sets an error word, stops all roles, drains in-flight copies and frees TMEM.
+#include <cub/cub.cuh>
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -149,11 +154,14 @@ struct TcArgs {
     int64_t n_ctiles;     // candidate tiles
     uint64_t* lists;      // n_q x n_split x 2 x S keys (L order-mapped << 32 | index), one
                           // list per (row, candidate split, half of each tile's columns)
+    const int32_t* start_tile;  // per query group, the first candidate tile to visit (rows in
+                                // cell order, one split), or null for the staggered start
     int* err;
 };
 
 // Work unit u covers query group u / n_split and the candidate tiles of
 // split u % n_split, visited from tile begin + rot onwards (cyclically).
+// With rows in cell order a group starts at its own cell's first tile.
 struct Unit {
     int32_t group, split, begin, len, rot;  // tile counts stay far below 2^31
 };
@@ -163,8 +171,9 @@ __device__ __forceinline__ Unit unit_of(const TcArgs& p, int64_t u) {
     r.split = static_cast<int32_t>(u - static_cast<int64_t>(r.group) * p.n_split);
     r.begin = r.split * static_cast<int32_t>(p.split_tiles);
     r.len = static_cast<int32_t>(min(p.split_tiles, p.n_ctiles - r.begin));
-    r.rot = static_cast<int32_t>(blockIdx.x % kStaggerGroups) * kStaggerStep;
-    if (r.rot >= r.len) r.rot = 0;
+    r.rot = p.start_tile != nullptr ? p.start_tile[r.group]
+                                    : static_cast<int32_t>(blockIdx.x % kStaggerGroups) * kStaggerStep;
+    if (r.rot >= r.len || r.rot < 0) r.rot = 0;
     return r;
 }
 
@@ -172,6 +181,22 @@ __device__ __forceinline__ Unit unit_of(const TcArgs& p, int64_t u) {
 __device__ __forceinline__ int32_t tile_at(int32_t t, const Unit& w) {
     const int32_t c = t + w.rot;
     return w.begin + (c >= w.len ? c - w.len : c);
+}
+
+// One k-block's MMAs for every query tile, fully unrolled: NKS k-steps of 16
+// columns, `first` zeroing the accumulators at the tile's first k-step.  One
+// thread issues all MMAs, and a loop with a runtime trip count issues them
+// more slowly than the tensor pipe retires 128 x 128 x 16 steps (64 cycles).
+constexpr uint32_t kTileDesc = kTileBytes >> 4;  // one 16 KiB tile in descriptor units
+template <int NKS, int MT>
+__device__ __forceinline__ void issue_kblock(uint32_t dcol, uint64_t da, uint32_t da_tile,
+                                             uint64_t db, bool first) {
+#pragma unroll
+    for (int ks = 0; ks < NKS; ++ks)
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt)
+            umma_bf16(dcol + mt * BN, da + mt * da_tile + 2 * ks, db + 2 * ks, kIdesc,
+                      (first && ks == 0) ? 0u : 1u);
 }
 
 // Threads: warp 0 TMA, warp 1 MMA, then 8 epilogue warps per query tile.
@@ -272,6 +297,9 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
             uint64_t it = 0, cg = 0;
             int64_t u_iter = 0;
             bool ok = true;
+            // descriptors advance by address / 16: per k-block, per ring stage, per query tile
+            const uint64_t dA0 = desc_sw128(sA), dB0 = desc_sw128(sB);
+            const uint32_t dA_tile = static_cast<uint32_t>(KB) * kTileDesc;
             for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x, ++u_iter) {
                 if (!mbar_wait(b_afull, static_cast<uint32_t>(u_iter & 1), abort_flag)) {
                     fail(3);
@@ -298,19 +326,19 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
                             break;
                         }
                         fence_after();
-                        const uint64_t db0 = desc_sw128(sB + stage * kTileBytes);
+                        const uint64_t da = dA0 + static_cast<uint64_t>(kb) * kTileDesc;
+                        const uint64_t db = dB0 + static_cast<uint64_t>(stage) * kTileDesc;
                         // the columns past 3d + 7 are zero: their k-steps are skipped
                         const int n_ks = kb == KB - 1 ? p.ks_last : BK / UK;
-#pragma unroll 4
-                        for (int ks = 0; ks < n_ks; ++ks) {
-#pragma unroll
-                            for (int mt = 0; mt < MT; ++mt) {
-                                const uint64_t da =
-                                    desc_sw128(sA + (mt * KB + kb) * kTileBytes) + 2 * ks;
-                                umma_bf16(dcol + mt * BN, da, db0 + 2 * ks, kIdesc,
-                                         (kb | ks) != 0 ? 1u : 0u);
-                            }
-                        }
+                        const bool first = kb == 0;
+                        if (n_ks == 4)
+                            issue_kblock<4, MT>(dcol, da, dA_tile, db, first);
+                        else if (n_ks == 3)
+                            issue_kblock<3, MT>(dcol, da, dA_tile, db, first);
+                        else if (n_ks == 2)
+                            issue_kblock<2, MT>(dcol, da, dA_tile, db, first);
+                        else
+                            issue_kblock<1, MT>(dcol, da, dA_tile, db, first);
                         umma_commit(b_empty + 8 * stage);
                     }
                     if (ok) umma_commit(b_tfull + 8 * buf);
@@ -544,12 +572,16 @@ __device__ __forceinline__ float sqdist_ref(const float* __restrict__ x, const f
 __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restrict__ R,
                               const float* __restrict__ qsq, const float* __restrict__ rsq,
                               const uint64_t* __restrict__ lists, int n_lists, int64_t n_q,
-                              int d, int k, double c1, double c2, int32_t* __restrict__ out_idx,
+                              int d, int k, double c1, double c2,
+                              const int32_t* __restrict__ perm, int32_t* __restrict__ out_idx,
                               float* __restrict__ out_dist, int* __restrict__ fb_count,
                               int32_t* __restrict__ fb_rows) {
     const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n_q) return;
+    // rows in cell order (perm non-null): position -> original row; keys, outputs
+    // and fallback rows use original indices, so ties break as in the reference
+    const int64_t orow = perm != nullptr ? perm[row] : row;
     const uint64_t* rl = lists + row * n_lists * S;
     // The smallest bound a candidate missing from every list can have: a full
     // list left out only candidates with L >= its largest entry, a list that
@@ -607,15 +639,16 @@ __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restri
         uint64_t key = ~0ull;
         if (take) {
             const uint32_t j = static_cast<uint32_t>(lk);
-            key = knn_key(sqdist_ref(Q + row * d, R + static_cast<int64_t>(j) * d, d), j);
+            key = knn_key(sqdist_ref(Q + row * d, R + static_cast<int64_t>(j) * d, d),
+                          perm != nullptr ? static_cast<uint32_t>(perm[j]) : j);
         }
         top = warp_merge_keys(top, key);
     }
     if (lane < k) {
-        out_idx[row * k + lane] = static_cast<int32_t>(key_index(top));
-        out_dist[row * k + lane] = __fsqrt_rn(key_dist(top));
+        out_idx[orow * k + lane] = static_cast<int32_t>(key_index(top));
+        out_dist[orow * k + lane] = __fsqrt_rn(key_dist(top));
     }
-    if (below < k && lane == 0) fb_rows[atomicAdd(fb_count, 1)] = static_cast<int32_t>(row);
+    if (below < k && lane == 0) fb_rows[atomicAdd(fb_count, 1)] = static_cast<int32_t>(orow);
 }
 
 // --------------------------------------------------------------- host ----
@@ -670,6 +703,178 @@ TcArgs plan(int64_t n_q, int64_t n_r, int d, bool allow_split) {
     return a;
 }
 
+// ------------------------------------------------------------ cell order --
+// A self kNN over at least one wave of query groups runs on its rows
+// regrouped by cell.
+// - Every row joins the nearest of C pivot rows (rows p * (n / C)).
+// - The rows are stably sorted by cell.
+// - Each query group starts its candidate walk at its own cell's first tile.
+// The shortlists then fill with near candidates in the first tiles. Their
+// thresholds drop early, and later tiles rarely hold a qualifying key.
+// The groups of one wave start within a few hundred tiles of each other, so
+// they still stream the candidate operand in step through L2.
+// The result does not change: the certificate does not depend on the
+// visiting order, and the re-rank maps positions back to original rows.
+constexpr int kMaxCells = 256;
+constexpr int64_t kCellPivotFloats = 16384;  // 64 KiB of pivots in shared memory
+
+// Cells: 32, 64, 128 or 256, as many as keep at least 2,048 rows per cell
+// (512 at 32 cells) and the pivots within 64 KiB; 0 = rows stay in order.
+int cell_count(int64_t n, int d) {
+    int c = kMaxCells;
+    while (c > 32 && (c * static_cast<int64_t>(d) > kCellPivotFloats || c * int64_t{2048} > n))
+        c >>= 1;
+    if (c * static_cast<int64_t>(d) > kCellPivotFloats || c * int64_t{512} > n) return 0;
+    return c;
+}
+
+// One warp per row: lane l scores pivots l + 32 q (q < PPL) from shared
+// memory ([d][C], conflict-free), the row's values broadcast by shuffle, and
+// the warp keeps the pivot with the smallest |p|^2 - 2 x.p (lower on ties).
+template <int PPL>
+__global__ void __launch_bounds__(256) cell_assign_kernel(const float* __restrict__ X, int64_t n,
+                                                          int d, int64_t stride,
+                                                          uint8_t* __restrict__ cell,
+                                                          int32_t* __restrict__ iota) {
+    constexpr int C = 32 * PPL;
+    extern __shared__ float piv[];
+    float* pn = piv + static_cast<int64_t>(d) * C;
+    for (int i = threadIdx.x; i < C * d; i += blockDim.x) {
+        const int pc = i / d, t = i - pc * d;
+        piv[t * C + pc] = X[static_cast<int64_t>(pc) * stride * d + t];
+    }
+    __syncthreads();
+    for (int pc = threadIdx.x; pc < C; pc += blockDim.x) {
+        float sq = 0.0f;
+        for (int t = 0; t < d; ++t) sq = fmaf(piv[t * C + pc], piv[t * C + pc], sq);
+        pn[pc] = sq;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; row < n;
+         row += warps) {
+        const float* x = X + row * d;
+        float acc[PPL];
+#pragma unroll
+        for (int q = 0; q < PPL; ++q) acc[q] = 0.0f;
+        for (int t0 = 0; t0 < d; t0 += 32) {
+            const float xv = t0 + lane < d ? x[t0 + lane] : 0.0f;
+            const int tn = min(32, d - t0);
+            for (int j = 0; j < tn; ++j) {
+                const float xj = __shfl_sync(0xffffffffu, xv, j);
+                const float* pr = piv + (t0 + j) * C + lane;
+#pragma unroll
+                for (int q = 0; q < PPL; ++q) acc[q] = fmaf(xj, pr[32 * q], acc[q]);
+            }
+        }
+        float best = INFINITY;
+        int bi = C;
+#pragma unroll
+        for (int q = 0; q < PPL; ++q) {
+            const float sc = pn[lane + 32 * q] - 2.0f * acc[q];
+            if (sc < best) {
+                best = sc;
+                bi = lane + 32 * q;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ob < best || (ob == best && oi < bi)) {
+                best = ob;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            cell[row] = static_cast<uint8_t>(bi < C ? bi : 0);
+            iota[row] = static_cast<int32_t>(row);
+        }
+    }
+}
+
+// First candidate tile of each query group: the tile holding the first row
+// of the cell that the group's first row belongs to (binary search in the
+// sorted cell keys).
+__global__ void group_start_kernel(const uint8_t* __restrict__ skey, int64_t groups,
+                                   int rows_per_group, int32_t* __restrict__ start_tile) {
+    const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= groups) return;
+    const int64_t r0 = g * rows_per_group;
+    const uint8_t c = skey[r0];
+    int64_t lo = 0, hi = r0;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (skey[mid] < c)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    start_tile[g] = static_cast<int32_t>(lo / BN);
+}
+
+__global__ void gather_rows_kernel(const float* __restrict__ X, const int32_t* __restrict__ perm,
+                                   int64_t n, int d, float* __restrict__ out) {
+    const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* src = X + static_cast<int64_t>(perm[row]) * d;
+    float* dst = out + row * d;
+    for (int t = lane; t < d; t += 32) dst[t] = src[t];
+}
+
+struct CellOrder {
+    DevBuf<float> rows;          // the rows in cell order
+    DevBuf<int32_t> perm;        // position -> original row
+    DevBuf<int32_t> start_tile;  // per query group
+};
+
+template <int PPL>
+void launch_assign(const float* X, int64_t n, int d, uint8_t* cell, int32_t* iota,
+                   cudaStream_t s) {
+    constexpr int C = 32 * PPL;
+    const size_t smem = (static_cast<size_t>(C) * d + C) * sizeof(float);
+    auto kern = cell_assign_kernel<PPL>;
+    UMAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+    int dev = 0, sms = 0;
+    UMAPB_CUDA(cudaGetDevice(&dev));
+    UMAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 8), static_cast<int64_t>(sms) * 3);
+    kern<<<static_cast<unsigned>(blocks), 256, smem, s>>>(X, n, d, n / C, cell, iota);
+    UMAPB_LAUNCH_CHECK();
+}
+
+void cell_order(const float* X, int64_t n, int d, int cells, int rows_per_group, int64_t groups,
+                CellOrder& co, cudaStream_t s) {
+    DevBuf<uint8_t> key(n, s), skey(n, s);
+    DevBuf<int32_t> iota(n, s);
+    co.perm.alloc(n, s);
+    switch (cells) {
+        case 32: launch_assign<1>(X, n, d, key.get(), iota.get(), s); break;
+        case 64: launch_assign<2>(X, n, d, key.get(), iota.get(), s); break;
+        case 128: launch_assign<4>(X, n, d, key.get(), iota.get(), s); break;
+        default: launch_assign<8>(X, n, d, key.get(), iota.get(), s); break;
+    }
+    size_t tmp_bytes = 0;
+    UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key.get(), skey.get(),
+                                               iota.get(), co.perm.get(), static_cast<int>(n), 0,
+                                               8, s));
+    DevBuf<uint8_t> tmp(tmp_bytes, s);
+    UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmp_bytes, key.get(), skey.get(),
+                                               iota.get(), co.perm.get(), static_cast<int>(n), 0,
+                                               8, s));
+    co.start_tile.alloc(groups, s);
+    group_start_kernel<<<static_cast<unsigned>(ceil_div(groups, 256)), 256, 0, s>>>(
+        skey.get(), groups, rows_per_group, co.start_tile.get());
+    UMAPB_LAUNCH_CHECK();
+    co.rows.alloc(static_cast<size_t>(n) * d, s);
+    gather_rows_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
+        X, co.perm.get(), n, d, co.rows.get());
+    UMAPB_LAUNCH_CHECK();
+}
+
 }  // namespace
 
 bool knn_tc_supported(int d, int k, int metric) {
@@ -686,10 +891,21 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     if (n_q == 0) return;
     if (k > n_r) invalid("kNN needs k <= number of reference rows");
     const bool self = Q == R && n_q == n_r;
+    const float* const Q0 = Q;  // original rows: the fallback recomputes rows of these
+    const float* const R0 = R;
     const int kp = padded_k(d);
     const int kb = kp / BK;
     const double c1 = kBoundC1;
     const double c2 = bound_c2(d);
+    TcArgs a = plan(n_q, n_r, d, true);
+    const int mt = query_tiles_for(kb);
+    CellOrder co;
+    const int cells = self && a.n_split == 1 ? cell_count(n_q, d) : 0;
+    if (cells > 0) {
+        cell_order(Q, n_q, d, cells, mt * BM, ceil_div(n_q, static_cast<int64_t>(BM) * mt), co, s);
+        Q = R = co.rows.get();
+        a.start_tile = co.start_tile.get();
+    }
     DevBuf<float> qsq(n_q, s), rsq;
     row_norms(Q, n_q, d, nullptr, qsq.get(), s);
     if (!self) {
@@ -704,8 +920,6 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     prep_kernel<<<static_cast<unsigned>(ceil_div(n_r * 32, 256)), 256, 0, s>>>(
         R, rsq_p, n_r, d, kp, static_cast<float>(c1), static_cast<float>(c2), false, B.get());
     UMAPB_LAUNCH_CHECK();
-    TcArgs a = plan(n_q, n_r, d, true);
-    const int mt = query_tiles_for(kb);
     const int n_lists = 2 * a.n_split;
     DevBuf<uint64_t> lists(n_q * n_lists * S, s);
     UMAPB_CUDA(cudaMemsetAsync(lists.get(), 0xFF, n_q * n_lists * S * 8, s));
@@ -738,13 +952,13 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
                         std::to_string(err_h) + ")");
     DevBuf<int32_t> fb_rows(n_q, s);
     rerank_kernel<<<static_cast<unsigned>(ceil_div(n_q * 32, 256)), 256, 0, s>>>(
-        Q, R, qsq.get(), rsq_p, lists.get(), n_lists, n_q, d, k, c1, c2, out_idx, out_dist,
-        fb_count.get(), fb_rows.get());
+        Q, R, qsq.get(), rsq_p, lists.get(), n_lists, n_q, d, k, c1, c2,
+        cells > 0 ? co.perm.get() : nullptr, out_idx, out_dist, fb_count.get(), fb_rows.get());
     UMAPB_LAUNCH_CHECK();
     int fb = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&fb, fb_count.get(), 4, cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
-    if (fb > 0) knn_plain(Q, fb_rows.get(), fb, R, n_r, d, k, metric, nullptr, nullptr, out_idx,
+    if (fb > 0) knn_plain(Q0, fb_rows.get(), fb, R0, n_r, d, k, metric, nullptr, nullptr, out_idx,
                           out_dist, s);
     if (stats) {
         stats->fallback_rows = fb;
@@ -863,7 +1077,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
         throw Error(UMAPB_ERR_CUDA, "tensor-core kNN kernel stopped on a wait timeout (code " +
                                         std::to_string(flags_h[0]) + ")");
     rerank_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
-        X, X, sq, sq, lists, 2, n, d, k, c1, c2, out_idx, out_dist, flags + 1, fb_rows);
+        X, X, sq, sq, lists, 2, n, d, k, c1, c2, nullptr, out_idx, out_dist, flags + 1, fb_rows);
     UMAPB_LAUNCH_CHECK();
     UMAPB_CUDA(cudaMemcpyAsync(flags_h, flags, 8, cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
