@@ -374,6 +374,10 @@ def run_gpu(args) -> None:
                                                              "symmetrize_sec", "prune_sec",
                                                              "init_sec", "optimize_sec")]
                                 for st in stage],
+            # the tensor kNN kernel alone, CUDA events on the engine's stream: a
+            # step whose kNN stage is long while this stays flat lost its time
+            # outside the kernel
+            "step_knn_kernel_sec": [round(t, 4) for t in knn_sec],
             "pool_reserved_gb": [pool0] + pool,
         }
         if transform is not None:
