@@ -496,6 +496,26 @@ def knn_legs(args, lib, x: np.ndarray) -> dict:
                                    ed.ctypes.data, None))
     rows = np.random.default_rng(3).choice(n, 2000, replace=False)
     recall = float(np.mean([len(set(ni[r]) & set(ei[r])) / K for r in rows]))
+    # the fit's ratio to the plain FP32 CUDA-core path: its exact kNN (the same
+    # sets as the tensor path's, checked in full) and one fit on it
+    pi = np.empty((n, K), np.int64)
+    pd = np.empty((n, K), np.float32)
+    t0 = time.perf_counter()
+    _lib.check(lib.umapb_knn_exact(x.ctypes.data, n, x.shape[1], K, 0, 2, pi.ctypes.data,
+                                   pd.ctypes.data, None))
+    t_plain_knn = time.perf_counter() - t0
+    mp = Umap(n_neighbors=K, n_epochs=EPOCHS, ann_mode="exact", knn_backend="plain")
+    t0 = time.perf_counter()
+    emb_p = mp.fit_transform(x)
+    t_plain_fit = time.perf_counter() - t0
+    qp = diagnostics.quality(x, emb_p, sample=10_000, seed=11)
+    out["plain_1m_x64"] = {
+        "knn_s_plain": round(t_plain_knn, 3), "fit_s_plain": round(t_plain_fit, 3),
+        "identical_indices": bool(np.array_equal(pi, ei)),
+        "identical_distances": bool(np.array_equal(pd, ed)),
+        "trust15_plain": round(qp["trustworthiness"], 4),
+        "note": "host API from a host array (the 256 MB upload inside), one fit; compare with "
+                "the headline's e2e and quality"}
     out["sparse_cosine_200000x2000"] = sparse_leg(args, lib)
     out["nndescent_1m_x64"] = {
         "knn_s": round(t_nd, 4), "iters": int(ran.value), "recall_at_15": round(recall, 4),
