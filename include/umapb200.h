@@ -177,6 +177,25 @@ int32_t umapb_fit_transform(umapb_model* model, const float* data, int64_t n_row
 int32_t umapb_fit_transform_stateless(const umapb_params* params, const float* data,
                                       int64_t n_rows, int64_t n_cols, float* out);
 
+/* ---- categorical supervision ----------------------------------------------
+ * UmapCore.fit_supervised / fit_transform_supervised[_into]
+ * (umap_rs/src/lib.rs:647-673, 746-779, 835-868) -> UmapModel::fit_dense_supervised /
+ * fit_transform_dense_supervised (rust_umap/src/lib.rs:722-767).  `labels` holds
+ * n_labels int64 class labels (-1 = unlabelled), checked against n_rows by
+ * validate_supervised_target (lib.rs:2260-2283) with its messages, as are
+ * target_weight in [0, 1] and target_n_neighbors (>= 1, or < 0 for none; the
+ * production path does not use it).  After the fuzzy union, each edge is scaled by
+ * label agreement, every head's row is renormalised by its largest weight, and the
+ * graph is unioned again (apply_categorical_target_intersection, lib.rs:3694-3760).
+ * A target_weight of 0 leaves the graph as the unsupervised fit's. */
+int32_t umapb_fit_supervised(umapb_model* model, const float* data, int64_t n_rows,
+                             int64_t n_cols, const int64_t* labels, int64_t n_labels,
+                             float target_weight, int64_t target_n_neighbors);
+int32_t umapb_fit_transform_supervised(umapb_model* model, const float* data, int64_t n_rows,
+                                       int64_t n_cols, const int64_t* labels, int64_t n_labels,
+                                       float target_weight, int64_t target_n_neighbors,
+                                       float* out);
+
 /* ---- CSR input -----------------------------------------------------------
  * indptr holds n_rows + 1 int64 offsets starting at 0; indices (int64) and
  * data (float32) hold indptr[n_rows] entries, column indices strictly
@@ -339,6 +358,15 @@ int32_t umapb_fuzzy_graph(const int64_t* indices, const float* dists, int64_t n_
                           int64_t k, float set_op_mix_ratio, float local_connectivity,
                           int64_t n_epochs, int32_t* heads, int32_t* tails, float* weights,
                           int64_t capacity, int64_t* n_edges, float* sigmas, float* rhos);
+
+/* umapb_fuzzy_graph followed by apply_categorical_target_intersection
+ * (rust_umap/src/lib.rs:1426-1431, 3694-3760) for n_rows int64 `labels` at
+ * `target_weight` > 0, then prune_edges when n_epochs > 0. */
+int32_t umapb_fuzzy_graph_supervised(const int64_t* indices, const float* dists, int64_t n_rows,
+                                     int64_t k, float set_op_mix_ratio, float local_connectivity,
+                                     int64_t n_epochs, const int64_t* labels, float target_weight,
+                                     int32_t* heads, int32_t* tails, float* weights,
+                                     int64_t capacity, int64_t* n_edges);
 
 /* spectral_init (rust_umap/src/lib.rs:3871-3888, connected and
  * multi-component); `data` (n_rows x n_cols) feeds the component centroids

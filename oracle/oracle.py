@@ -43,6 +43,8 @@ _SIGS = {
         _i64,
         [_vp, _vp, _i64, _i64, _f32, _f32, _i64, _vp, _vp, _vp, _i64, _vp, _vp],
     ),
+    "orc_categorical_intersection": (
+        _i64, [_vp, _vp, _vp, _i64, _vp, _i64, _f32, _i64, _vp, _vp, _vp, _i64]),
     "orc_spectral_init": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _i64, _i64, _u64, _vp, _vp]),
     "orc_random_init": (None, [_i64, _i64, _u64, _f32, _f32, _vp]),
     "orc_optimize_layout": (
@@ -230,6 +232,24 @@ def fuzzy_graph(idx, dist, mix: float = 1.0, local_connectivity: float = 1.0, n_
     ne = load().orc_fuzzy_graph(_p(idx), _p(dist), n, k, mix, local_connectivity, n_epochs,
                                 _p(h), _p(t), _p(w), cap, _p(sig), _p(rho))
     return h[:ne].copy(), t[:ne].copy(), w[:ne].copy(), sig, rho
+
+
+def categorical_intersection(heads, tails, weights, labels, weight: float, n_epochs: int = 0):
+    """apply_categorical_target_intersection (lib.rs:3694-3760) of an edge
+    list, then prune_edges when n_epochs > 0."""
+    heads = np.ascontiguousarray(heads, np.int32)
+    tails = np.ascontiguousarray(tails, np.int32)
+    weights = _f32m(weights)
+    labels = np.ascontiguousarray(labels, np.int64)
+    m = heads.shape[0]
+    cap = max(m, 1)
+    h = np.empty(cap, np.int32)
+    t = np.empty(cap, np.int32)
+    w = np.empty(cap, np.float32)
+    ne = load().orc_categorical_intersection(_p(heads), _p(tails), _p(weights), m, _p(labels),
+                                             labels.shape[0], weight, n_epochs, _p(h), _p(t),
+                                             _p(w), cap)
+    return h[:ne].copy(), t[:ne].copy(), w[:ne].copy()
 
 
 def spectral_init(x, heads, tails, weights, dim: int, seed: int):

@@ -677,6 +677,41 @@ void prune_edges(std::vector<Edge>& edges, size_t n_epochs) {
     edges.swap(kept);
 }
 
+// apply_categorical_target_intersection + reset_local_connectivity_edges
+// (lib.rs:3694-3760): every edge's weight times 1 (same label), exp(-1)
+// (either label -1) or exp(-far_dist) (different labels), with
+// far_dist = 2.5 / (1 - weight) (1e12 at weight 1), all in FP32; edges whose
+// product is not positive and finite are dropped; each head's edges are
+// divided by its largest weight; the result is the fuzzy union (mix 1) of
+// those directed edges.  A weight <= 0 or an empty graph returns the input.
+std::vector<Edge> categorical_intersection(const std::vector<Edge>& edges, const int64_t* labels,
+                                           size_t n, float weight) {
+    if (weight <= 0.0f || edges.empty()) return edges;
+    const float far_dist = weight < 1.0f ? 2.5f / (1.0f - weight) : 1.0e12f;
+    const float unknown_scale = std::exp(-1.0f);
+    const float far_scale = std::exp(-far_dist);
+    std::vector<Edge> scaled;
+    scaled.reserve(edges.size());
+    for (const auto& e : edges) {
+        const int64_t lhs = labels[e.head], rhs = labels[e.tail];
+        const float scale =
+            (lhs == -1 || rhs == -1) ? unknown_scale : (lhs != rhs ? far_scale : 1.0f);
+        const float w = e.weight * scale;
+        if (w > 0.0f && std::isfinite(w)) scaled.push_back({e.head, e.tail, w});
+    }
+    if (scaled.empty()) return {};
+    std::vector<float> row_max(n, 0.0f);
+    for (const auto& e : scaled) row_max[e.head] = std::max(row_max[e.head], e.weight);
+    std::vector<Edge> directed;
+    directed.reserve(scaled.size());
+    for (const auto& e : scaled) {
+        const float mx = row_max[e.head];
+        if (mx <= 0.0f || !std::isfinite(mx)) continue;
+        directed.push_back({e.head, e.tail, e.weight / mx});
+    }
+    return symmetrize(directed, 1.0f);
+}
+
 // random_init (lib.rs:3824-3839).
 std::vector<std::vector<float>> random_init(size_t n, size_t dim, uint64_t seed, float low,
                                             float high) {
@@ -1875,6 +1910,26 @@ int64_t orc_fuzzy_graph(const int64_t* idx, const float* dist, int64_t n, int64_
     if (sig_out) std::memcpy(sig_out, sig.data(), sizeof(float) * n);
     if (rho_out) std::memcpy(rho_out, rho.data(), sizeof(float) * n);
     return static_cast<int64_t>(edges.size());
+}
+
+// The categorical target intersection (lib.rs:1426-1431) of an edge list,
+// then prune_edges when n_epochs > 0.
+int64_t orc_categorical_intersection(const int32_t* heads, const int32_t* tails,
+                                     const float* weights, int64_t m, const int64_t* labels,
+                                     int64_t n, float weight, int64_t n_epochs, int32_t* out_h,
+                                     int32_t* out_t, float* out_w, int64_t capacity) {
+    std::vector<Edge> edges(static_cast<size_t>(m));
+    for (int64_t e = 0; e < m; ++e)
+        edges[e] = {static_cast<size_t>(heads[e]), static_cast<size_t>(tails[e]), weights[e]};
+    auto out = categorical_intersection(edges, labels, static_cast<size_t>(n), weight);
+    if (n_epochs > 0) prune_edges(out, static_cast<size_t>(n_epochs));
+    if (static_cast<int64_t>(out.size()) > capacity) return -1;
+    for (size_t e = 0; e < out.size(); ++e) {
+        out_h[e] = static_cast<int32_t>(out[e].head);
+        out_t[e] = static_cast<int32_t>(out[e].tail);
+        out_w[e] = out[e].weight;
+    }
+    return static_cast<int64_t>(out.size());
 }
 
 // spectral_init with the random-init fallback of initialize_embedding.

@@ -74,6 +74,24 @@ def fuzzy_graph(idx, dist, mix=1.0, local_connectivity=1.0, n_epochs=0):
     return h[:m].copy(), t[:m].copy(), w[:m].copy(), sig, rho
 
 
+def fuzzy_graph_supervised(idx, dist, labels, target_weight, mix=1.0, local_connectivity=1.0,
+                           n_epochs=0):
+    idx = np.ascontiguousarray(idx, np.int64)
+    dist = np.ascontiguousarray(dist, np.float32)
+    labels = np.ascontiguousarray(labels, np.int64)
+    n, k = idx.shape
+    cap = 2 * n * k
+    h = np.empty(cap, np.int32)
+    t = np.empty(cap, np.int32)
+    w = np.empty(cap, np.float32)
+    ne = ctypes.c_int64(0)
+    _lib.check(_lib.load().umapb_fuzzy_graph_supervised(
+        _p(idx), _p(dist), n, k, mix, local_connectivity, n_epochs, _p(labels), target_weight,
+        _p(h), _p(t), _p(w), cap, ctypes.byref(ne)))
+    m = ne.value
+    return h[:m].copy(), t[:m].copy(), w[:m].copy()
+
+
 def spectral_init(x, h, t, w, dim, seed):
     x = np.ascontiguousarray(x, np.float32)
     n, d = x.shape

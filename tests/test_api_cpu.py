@@ -172,8 +172,6 @@ def test_sparse_input_checks_run_before_the_device():
         Umap(densmap=True).fit(x)
     with pytest.raises(ValueError, match="categorical supervised UMAP currently supports dense"):
         Umap(target_metric="categorical").fit(x, y=np.zeros(50))
-    with pytest.raises(ValueError, match="supervised"):
-        Umap(target_metric="categorical").fit(np.zeros((50, 3), np.float32), y=np.zeros(50))
     core = UmapCore(n_neighbors=5)
     ip = np.array([0, 2, 3], np.int64)
     with pytest.raises(ValueError, match="indices must contain non-negative integers"):
@@ -200,6 +198,28 @@ def test_sparse_input_checks_run_before_the_device():
         Umap(metric="canberra", n_neighbors=5).fit(x)
     with pytest.raises(ValueError, match="n_neighbors above 32"):
         Umap(n_neighbors=40).fit(x)
+
+
+def test_supervised_target_checks_run_before_the_device():
+    # validate_supervised_target (rust_umap/src/lib.rs:2260-2283) and the
+    # facade's label conversion (_api.py:127-131), before any device work
+    x = np.zeros((50, 3), np.float32)
+    with pytest.raises(ValueError, match=r"target label length \(49\) must match number of "
+                                         r"samples \(50\)"):
+        Umap(target_metric="categorical").fit(x, y=np.zeros(49))
+    with pytest.raises(ValueError, match="y must be a 1D label array, got ndim=2"):
+        Umap(target_metric="categorical").fit_transform(x, y=np.zeros((50, 1)))
+    core = UmapCore(n_neighbors=5)
+    with pytest.raises(ValueError, match=r"target_weight must be finite and in \[0, 1\]"):
+        core.fit_supervised(x, np.zeros(50), 1.5)
+    with pytest.raises(ValueError, match=r"target_weight must be finite and in \[0, 1\]"):
+        core.fit_transform_supervised(x, np.zeros(50), float("nan"))
+    with pytest.raises(ValueError, match="target_n_neighbors must be >= 1 when provided"):
+        core.fit_supervised(x, np.zeros(50), 0.5, 0)
+    with pytest.raises(OverflowError):
+        core.fit_supervised(x, np.zeros(50), 0.5, -3)
+    with pytest.raises(ValueError, match="target_weight must be finite and in"):
+        Umap(target_metric="categorical", target_weight=2.0)
 
 
 def test_metrics_outside_the_engine_are_rejected_at_fit():

@@ -210,3 +210,42 @@ def test_sparse_knn_follows_the_reference_formulas(orc):
     np.testing.assert_array_equal(dist[1], [0.0, 1.0, 1.0, 1.0])
     # row 3 shares no column with rows 0 / 2: cosine 1
     assert dist[3][1] == f(1.0)
+
+
+def test_categorical_intersection_pins_the_reference_test(orc):
+    # categorical_target_intersection_modulates_existing_feature_edges
+    # (rust_umap/src/lib.rs:7256-7335): the same ten data edges, labels
+    # [0, 0, 1, 1], target weight 0.6
+    pairs = [(0, 1, 0.8), (1, 0, 0.8), (0, 2, 0.7), (2, 0, 0.7), (1, 2, 0.4), (2, 1, 0.4),
+             (2, 3, 0.8), (3, 2, 0.8), (0, 3, 0.6), (3, 0, 0.6)]
+    h = np.array([p[0] for p in pairs], np.int32)
+    t = np.array([p[1] for p in pairs], np.int32)
+    w = np.array([p[2] for p in pairs], np.float32)
+    labels = np.array([0, 0, 1, 1], np.int64)
+    oh, ot, ow = orc.categorical_intersection(h, t, w, labels, 0.6)
+    assert set(zip(oh.tolist(), ot.tolist())) <= set(zip(h.tolist(), t.tolist()))
+    weight = {(a, b): c for a, b, c in zip(oh.tolist(), ot.tolist(), ow.tolist())}
+    wt = lambda a, b: weight.get((a, b), 0.0)  # noqa: E731
+    assert wt(0, 1) > wt(0, 2) and wt(1, 0) > wt(1, 2)
+    assert wt(2, 3) > wt(2, 0) and wt(3, 2) > wt(3, 0)
+    # the same steps written out in float32: scale, divide by the head's
+    # largest weight, fuzzy union with mix 1
+    far = np.float32(np.exp(-np.float32(2.5) / (np.float32(1.0) - np.float32(0.6))))
+    scaled = {(a, b): np.float32(c) * (np.float32(1.0) if labels[a] == labels[b] else far)
+              for a, b, c in pairs}
+    row_max = {i: max(v for (a, _), v in scaled.items() if a == i) for i in range(4)}
+    directed = {(a, b): np.float32(v / row_max[a]) for (a, b), v in scaled.items()}
+    for (a, b), v in directed.items():
+        u = directed[(b, a)]
+        expect = np.float32(np.float32(v + u) - np.float32(v * u))
+        assert np.float32(wt(a, b)) == expect, (a, b)
+    # weight 0 leaves the graph unchanged; weight 1 drops the cross-label edges
+    zh, zt, zw = orc.categorical_intersection(h, t, w, labels, 0.0)
+    np.testing.assert_array_equal(zw, w)
+    ah, at, aw = orc.categorical_intersection(h, t, w, labels, 1.0)
+    assert all(labels[a] == labels[b] for a, b in zip(ah.tolist(), at.tolist()))
+    # an unlabelled end scales by exp(-1), far less than a label mismatch
+    lab_u = np.array([0, -1, 1, 1], np.int64)
+    uh, ut, uw = orc.categorical_intersection(h, t, w, lab_u, 0.6)
+    uwt = {(a, b): c for a, b, c in zip(uh.tolist(), ut.tolist(), uw.tolist())}
+    assert uwt[(1, 2)] > 100 * wt(1, 2)

@@ -6,10 +6,11 @@ _api.py:324-873, 1054-1094): keyword arguments and defaults, sklearn-style
 int64 kNN indices), ``out=`` buffers, the ``ann_mode`` shortcut, and the
 fitted attributes ``embedding_``, ``n_features_in_``, ``n_samples_fit_``.
 Compute runs on one B200 through ``UmapCore`` (libumapb200.so), densMAP and
-``output_dens`` (dense input) and CSR sparse input (scipy csr/csc/coo)
-included.  Inputs the engine does not cover (supervised targets,
-inverse_transform, metrics other than euclidean/cosine, sparse input with
-n_neighbors above 32) raise ValueError.
+``output_dens`` (dense input), categorical supervision (``target_metric=
+"categorical"`` with ``y``, dense input) and CSR sparse input (scipy
+csr/csc/coo) included.  Inputs the engine does not cover (inverse_transform,
+metrics other than euclidean/cosine, sparse input with n_neighbors above 32)
+raise ValueError.
 """
 from __future__ import annotations
 
@@ -202,6 +203,14 @@ def _ann_mode(ann_mode: Any, use_approx: bool, threshold: int) -> tuple[str, boo
     if mode == "approximate":
         return mode, True, 0
     raise ValueError(f"unsupported ann_mode '{ann_mode}', expected auto|exact|approximate")
+
+
+def _as_labels(x: Any, name: str) -> np.ndarray:
+    """Class labels as a C-contiguous int64 vector (_api.py:127-131)."""
+    arr = np.asarray(x, dtype=np.int64, order="C")
+    if arr.ndim != 1:
+        raise ValueError(f"{name} must be a 1D label array, got ndim={arr.ndim}")
+    return arr
 
 
 def _target_metric(target_metric: Any) -> str | None:
@@ -462,10 +471,6 @@ class Umap:
         if self.target_metric == "categorical" and y is not None:
             raise ValueError("categorical supervised UMAP currently supports dense input only")
 
-    def _reject_unsupported(self, data: Any, y: Any) -> None:
-        if self.target_metric == "categorical" and y is not None:
-            raise ValueError("categorical supervised UMAP is not supported by the B200 engine")
-
     # ---------------------------------------------------------------- fit
     def fit(self, data: Any, y: Any | None = None) -> "Umap":
         """Fit the model and return ``self``.
@@ -491,8 +496,12 @@ class Umap:
             self._core.fit_sparse_csr(indptr, indices, values, n_cols)
             self._set_fitted(self._core.embedding, n_cols, n_rows)
             return self
-        self._reject_unsupported(data, y)
         arr = _f32_matrix(data, "data")
+        if self.target_metric == "categorical" and y is not None:
+            labels = _as_labels(y, "y")
+            self._core.fit_supervised(arr, labels, self.target_weight, self.target_n_neighbors)
+            self._set_fitted(self._core.embedding, arr.shape[1], arr.shape[0])
+            return self
         self._core.fit(arr)
         self._set_fitted(self._core.embedding, arr.shape[1], arr.shape[0])
         return self
@@ -536,10 +545,23 @@ class Umap:
             self._core.fit_transform_sparse_csr_into(indptr, indices, values, n_cols, buf)
             self._set_fitted(buf, n_cols, n_rows)
             return buf
-        self._reject_unsupported(data, y)
         arr = _f32_matrix(data, "data")
         if out is not None and self.output_dens:
             raise ValueError("out cannot be used when output_dens=True")
+        if self.target_metric == "categorical" and y is not None:
+            labels = _as_labels(y, "y")
+            if out is None:
+                emb = self._core.fit_transform_supervised(arr, labels, self.target_weight,
+                                                          self.target_n_neighbors)
+                self._set_fitted(emb, arr.shape[1], arr.shape[0])
+                if self.output_dens:
+                    return emb, self.radii_original_, self.radii_embedding_
+                return emb
+            buf = _out_buffer(out, (arr.shape[0], self.n_components))
+            self._core.fit_transform_supervised_into(arr, labels, buf, self.target_weight,
+                                                     self.target_n_neighbors)
+            self._set_fitted(buf, arr.shape[1], arr.shape[0])
+            return buf
         if out is None:
             emb = self._core.fit_transform(arr)
             self._set_fitted(emb, arr.shape[1], arr.shape[0])

@@ -204,6 +204,8 @@ SIGNATURES = {
     "umapb_destroy": (None, [_vp]),
     "umapb_fit": (_i32, [_vp, _vp, _i64, _i64]),
     "umapb_fit_transform": (_i32, [_vp, _vp, _i64, _i64, _vp]),
+    "umapb_fit_supervised": (_i32, [_vp, _vp, _i64, _i64, _vp, _i64, _f32, _i64]),
+    "umapb_fit_transform_supervised": (_i32, [_vp, _vp, _i64, _i64, _vp, _i64, _f32, _i64, _vp]),
     "umapb_fit_transform_stateless": (_i32, [ctypes.POINTER(Params), _vp, _i64, _i64, _vp]),
     "umapb_fit_transform_with_knn": (
         _i32,
@@ -243,6 +245,10 @@ SIGNATURES = {
     "umapb_fuzzy_graph": (
         _i32,
         [_vp, _vp, _i64, _i64, _f32, _f32, _i64, _vp, _vp, _vp, _i64, _i64p, _vp, _vp],
+    ),
+    "umapb_fuzzy_graph_supervised": (
+        _i32,
+        [_vp, _vp, _i64, _i64, _f32, _f32, _i64, _vp, _f32, _vp, _vp, _vp, _i64, _i64p],
     ),
     "umapb_spectral_init": (
         _i32,

@@ -207,6 +207,61 @@ class UmapCore:
             )
         )
 
+    # ------------------------------------------- categorical supervision
+    @staticmethod
+    def _target(y: Any, target_weight: float, target_n_neighbors: int | None):
+        """Labels as int64 (PyReadonlyArray1<i64>), the weight as f32 and
+        target_n_neighbors as Option<usize> (-1 for none) of the reference's
+        supervised_target_from_py (umap_rs/src/lib.rs:324-335)."""
+        labels = np.ascontiguousarray(y, dtype=np.int64)
+        if labels.ndim != 1:
+            raise ValueError(f"y must be a 1D label array, got ndim={labels.ndim}")
+        if target_n_neighbors is None:
+            tnn = -1
+        else:
+            tnn = int(target_n_neighbors)
+            if tnn < 0:
+                raise OverflowError("can't convert negative int to unsigned")
+        return labels, float(target_weight), tnn
+
+    def fit_supervised(self, data: Any, y: Any, target_weight: float,
+                       target_n_neighbors: int | None = None) -> None:
+        """UmapCore.fit_supervised (umap_rs/src/lib.rs:647-673)."""
+        arr = _matrix(data, "data")
+        labels, weight, tnn = self._target(y, target_weight, target_n_neighbors)
+        _lib.check(
+            self._lib.umapb_fit_supervised(self._handle, _lib.ptr(arr), arr.shape[0], arr.shape[1],
+                                           _lib.ptr(labels), labels.shape[0], weight, tnn)
+        )
+
+    def fit_transform_supervised(self, data: Any, y: Any, target_weight: float,
+                                 target_n_neighbors: int | None = None) -> np.ndarray:
+        """UmapCore.fit_transform_supervised (umap_rs/src/lib.rs:746-779)."""
+        arr = _matrix(data, "data")
+        labels, weight, tnn = self._target(y, target_weight, target_n_neighbors)
+        out = np.empty((arr.shape[0], self.n_components), dtype=np.float32)
+        _lib.check(
+            self._lib.umapb_fit_transform_supervised(
+                self._handle, _lib.ptr(arr), arr.shape[0], arr.shape[1], _lib.ptr(labels),
+                labels.shape[0], weight, tnn, _lib.ptr(out)
+            )
+        )
+        return out
+
+    def fit_transform_supervised_into(self, data: Any, y: Any, out: np.ndarray,
+                                      target_weight: float,
+                                      target_n_neighbors: int | None = None) -> None:
+        """UmapCore.fit_transform_supervised_into (umap_rs/src/lib.rs:835-868)."""
+        arr = _matrix(data, "data")
+        labels, weight, tnn = self._target(y, target_weight, target_n_neighbors)
+        _check_out(out, (arr.shape[0], self.n_components))
+        _lib.check(
+            self._lib.umapb_fit_transform_supervised(
+                self._handle, _lib.ptr(arr), arr.shape[0], arr.shape[1], _lib.ptr(labels),
+                labels.shape[0], weight, tnn, _lib.ptr(out)
+            )
+        )
+
     def fit_transform_stateless(self, data: Any) -> np.ndarray:
         arr = _matrix(data, "data")
         out = np.empty((arr.shape[0], self.n_components), dtype=np.float32)
@@ -290,15 +345,6 @@ class UmapCore:
     ) -> None:
         _check_out(out, (np.shape(data)[0], self.n_components))
         self._with_knn(data, knn_indices, knn_dists, out, knn_metric, validate_precomputed)
-
-    def fit_supervised(self, *args: Any, **kwargs: Any) -> None:
-        raise ValueError("categorical supervised UMAP is not supported by the B200 engine")
-
-    def fit_transform_supervised(self, *args: Any, **kwargs: Any) -> np.ndarray:
-        raise ValueError("categorical supervised UMAP is not supported by the B200 engine")
-
-    def fit_transform_supervised_into(self, *args: Any, **kwargs: Any) -> None:
-        raise ValueError("categorical supervised UMAP is not supported by the B200 engine")
 
     # ----------------------------------------------------------- transform
     def transform(self, query: Any) -> np.ndarray:

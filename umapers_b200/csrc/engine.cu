@@ -359,7 +359,7 @@ void knn_exact_device(const float* Q, int64_t nq, const float* R, int64_t nr, in
 // writes the embedding into model->emb.
 void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const int32_t* idx,
                   const float* dist, int k, FitOutputs* out, StageClock& clk,
-                  const CsrDevice* csr = nullptr) {
+                  const CsrDevice* csr = nullptr, const CategoricalTarget* target = nullptr) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int64_t n_epochs = default_epochs(p, n);
@@ -381,7 +381,7 @@ void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const i
     Graph g;
     double phases[3] = {0.0, 0.0, 0.0};
     fuzzy_union(idx, dist, sig.get(), rho.get(), n, k, p.set_op_mix_ratio, n_epochs, g, s,
-                out ? phases : nullptr);
+                out ? phases : nullptr, target);
     if (out) {
         clk.lap();
         out->t.membership_sec = phases[0];
@@ -429,7 +429,7 @@ void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const i
 
 // Full dense fit on device-resident rows `Xd` (owned copy is taken).
 void fit_device(umapb_model* m, const float* Xd, int64_t n, int64_t d, bool copy_rows,
-                FitOutputs* out, StageClock& clk) {
+                FitOutputs* out, StageClock& clk, const CategoricalTarget* target = nullptr) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int k = static_cast<int>(p.n_neighbors);
@@ -462,7 +462,7 @@ void fit_device(umapb_model* m, const float* Xd, int64_t n, int64_t d, bool copy
         }
     }
     if (out) out->t.knn_sec = clk.lap();
-    fit_from_knn(m, X, n, d, idx.get(), dist.get(), k, out, clk);
+    fit_from_knn(m, X, n, d, idx.get(), dist.get(), k, out, clk, nullptr, target);
     if (copy_rows) m->X = std::move(Xown);
     m->n_fit = n;
     m->d_fit = d;
@@ -503,6 +503,59 @@ void fit_host(umapb_model* m, const float* data, int64_t n, int64_t d, FitOutput
         out->info.n_samples = n;
         out->info.n_features = d;
     }
+}
+
+// validate_supervised_target (lib.rs:2260-2283), with its messages.
+// `target_n_neighbors` < 0 means none; the production path does not use it
+// (only the reference's test-only target graph does, lib.rs:3651-3692).
+void validate_supervised_target(int64_t n_labels, float weight, int64_t target_n_neighbors,
+                                int64_t n_samples) {
+    if (n_labels != n_samples)
+        invalid("target label length (" + std::to_string(n_labels) +
+                ") must match number of samples (" + std::to_string(n_samples) + ")");
+    if (!std::isfinite(weight) || !(weight >= 0.0f && weight <= 1.0f))
+        invalid("target_weight must be finite and in [0, 1]");
+    if (target_n_neighbors == 0) invalid("target_n_neighbors must be >= 1 when provided");
+}
+
+// The scales of apply_categorical_target_intersection (lib.rs:3702-3708),
+// FP32 as in the reference: exp(-1) for an unlabelled end, exp(-far_dist)
+// with far_dist = 2.5 / (1 - weight) (1e12 at weight 1) for different labels.
+void categorical_scales(float weight, float* unknown_scale, float* far_scale) {
+    const float far_dist = weight < 1.0f ? 2.5f / (1.0f - weight) : 1.0e12f;
+    *unknown_scale = std::exp(-1.0f);
+    *far_scale = std::exp(-far_dist);
+}
+
+// fit_dense_supervised / fit_transform_dense_supervised (lib.rs:722-767,
+// 1367-1431): the dense fit with the categorical target intersection between
+// the fuzzy union and prune.  A weight of 0 leaves the graph as it is.
+void fit_supervised_host(umapb_model* m, const float* data, int64_t n, int64_t d,
+                         const int64_t* labels, int64_t n_labels, float weight,
+                         int64_t target_n_neighbors, float* emb_out) {
+    validate_data_host(data, n, d);
+    validate_params(m->p, n);
+    validate_supervised_target(n_labels, weight, target_n_neighbors, n);
+    check_engine_support(m->p);
+    m->ensure_device();
+    cudaStream_t s = m->stream;
+    StageClock clk(s, false);
+    m->begin_fit();
+    DevBuf<float> X;
+    upload(X, data, n * d, s);
+    DevBuf<int64_t> lab;
+    CategoricalTarget target;
+    if (weight > 0.0f) {
+        lab.alloc(n, s);
+        UMAPB_CUDA(cudaMemcpyAsync(lab.get(), labels, n * 8, cudaMemcpyHostToDevice, s));
+        target.labels = lab.get();
+        target.weight = weight;
+        categorical_scales(weight, &target.unknown_scale, &target.far_scale);
+    }
+    fit_device(m, X.get(), n, d, false, nullptr, clk, weight > 0.0f ? &target : nullptr);
+    m->X = std::move(X);
+    if (emb_out) copy_embedding_out(m, emb_out);
+    UMAPB_CUDA(cudaStreamSynchronize(s));
 }
 
 // fit_sparse_csr / fit_transform_sparse_csr (lib.rs:998-1036, 1479-1549):
@@ -749,6 +802,27 @@ int32_t umapb_fit_transform(umapb_model* m, const float* data, int64_t n_rows, i
     return guarded([&] {
         std::lock_guard<std::mutex> lk(m->mu);
         fit_host(m, data, n_rows, n_cols, nullptr, out);
+    });
+}
+
+int32_t umapb_fit_supervised(umapb_model* m, const float* data, int64_t n_rows, int64_t n_cols,
+                             const int64_t* labels, int64_t n_labels, float target_weight,
+                             int64_t target_n_neighbors) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        fit_supervised_host(m, data, n_rows, n_cols, labels, n_labels, target_weight,
+                            target_n_neighbors, nullptr);
+    });
+}
+
+int32_t umapb_fit_transform_supervised(umapb_model* m, const float* data, int64_t n_rows,
+                                       int64_t n_cols, const int64_t* labels, int64_t n_labels,
+                                       float target_weight, int64_t target_n_neighbors,
+                                       float* out) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        fit_supervised_host(m, data, n_rows, n_cols, labels, n_labels, target_weight,
+                            target_n_neighbors, out);
     });
 }
 
@@ -1202,6 +1276,48 @@ int32_t umapb_fuzzy_graph(const int64_t* indices, const float* dists, int64_t n,
         }
         if (sigmas) UMAPB_CUDA(cudaMemcpyAsync(sigmas, sg.get(), n * 4, cudaMemcpyDeviceToHost, ss.s));
         if (rhos) UMAPB_CUDA(cudaMemcpyAsync(rhos, rh.get(), n * 4, cudaMemcpyDeviceToHost, ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        *n_edges = g.n_edges;
+    });
+}
+
+int32_t umapb_fuzzy_graph_supervised(const int64_t* indices, const float* dists, int64_t n,
+                                     int64_t k, float set_op_mix_ratio, float local_connectivity,
+                                     int64_t n_epochs, const int64_t* labels, float target_weight,
+                                     int32_t* heads, int32_t* tails, float* weights,
+                                     int64_t capacity, int64_t* n_edges) {
+    return guarded([&] {
+        if (n <= 0 || k <= 0) invalid("empty kNN graph");
+        if (capacity < 2 * n * k) invalid("capacity must be >= 2 * n_rows * k");
+        validate_supervised_target(n, target_weight, -1, n);
+        ScopedStream ss;
+        std::vector<int32_t> ih(n * k);
+        for (int64_t i = 0; i < n * k; ++i) {
+            if (indices[i] < 0 || indices[i] >= n) invalid("kNN index out of range");
+            ih[i] = static_cast<int32_t>(indices[i]);
+        }
+        DevBuf<int32_t> idx(n * k, ss.s);
+        DevBuf<float> dist;
+        UMAPB_CUDA(cudaMemcpyAsync(idx.get(), ih.data(), n * k * 4, cudaMemcpyHostToDevice, ss.s));
+        upload(dist, dists, n * k, ss.s);
+        DevBuf<int64_t> lab(n, ss.s);
+        UMAPB_CUDA(cudaMemcpyAsync(lab.get(), labels, n * 8, cudaMemcpyHostToDevice, ss.s));
+        CategoricalTarget target;
+        target.labels = lab.get();
+        target.weight = target_weight;
+        categorical_scales(target_weight, &target.unknown_scale, &target.far_scale);
+        const bool self = knn_includes_self(idx.get(), dist.get(), n, static_cast<int>(k), ss.s);
+        DevBuf<float> sg(n, ss.s), rh(n, ss.s);
+        smooth_knn(dist.get(), n, static_cast<int>(k), static_cast<float>(k), local_connectivity,
+                   1.0f, self, sg.get(), rh.get(), ss.s);
+        Graph g;
+        fuzzy_union(idx.get(), dist.get(), sg.get(), rh.get(), n, static_cast<int>(k),
+                    set_op_mix_ratio, n_epochs, g, ss.s, nullptr, &target);
+        if (g.n_edges > 0) {
+            UMAPB_CUDA(cudaMemcpyAsync(heads, g.heads.get(), g.n_edges * 4, cudaMemcpyDeviceToHost, ss.s));
+            UMAPB_CUDA(cudaMemcpyAsync(tails, g.tails.get(), g.n_edges * 4, cudaMemcpyDeviceToHost, ss.s));
+            UMAPB_CUDA(cudaMemcpyAsync(weights, g.weights.get(), g.n_edges * 4, cudaMemcpyDeviceToHost, ss.s));
+        }
         UMAPB_CUDA(cudaStreamSynchronize(ss.s));
         *n_edges = g.n_edges;
     });

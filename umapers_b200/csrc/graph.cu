@@ -256,6 +256,60 @@ __global__ void gather_sel_kernel(const int64_t* __restrict__ sel, int64_t m,
     wout[p] = win[e];
 }
 
+// apply_categorical_target_intersection (lib.rs:3694-3731): each edge's
+// weight times 1 (same label), exp(-1) (either label -1) or exp(-far_dist)
+// (different labels), both scales computed on the host in FP32; a product
+// that is not positive and finite drops the edge (0).  Every head's largest
+// kept weight is kept as its bit pattern (positive floats order as uints).
+__global__ void target_scale_kernel(const int32_t* __restrict__ heads,
+                                    const int32_t* __restrict__ tails,
+                                    const float* __restrict__ w, int64_t m,
+                                    const int64_t* __restrict__ labels, float unknown_scale,
+                                    float far_scale, float* __restrict__ scaled,
+                                    unsigned* __restrict__ row_max) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= m) return;
+    const int64_t lhs = labels[heads[e]], rhs = labels[tails[e]];
+    const float scale = (lhs == -1 || rhs == -1) ? unknown_scale : (lhs != rhs ? far_scale : 1.0f);
+    const float v = __fmul_rn(w[e], scale);
+    const bool keep = v > 0.0f && isfinite(v);
+    scaled[e] = keep ? v : 0.0f;
+    if (keep) atomicMax(row_max + heads[e], __float_as_uint(v));
+}
+
+// reset_local_connectivity_edges (lib.rs:3733-3760): every kept edge divided
+// by its head's largest kept weight, as a directed edge keyed for the fuzzy
+// union (min << (b+1) | max << 1 | head > tail); dropped edges get the
+// invalid key.
+__global__ void target_keys_kernel(const int32_t* __restrict__ heads,
+                                   const int32_t* __restrict__ tails,
+                                   const float* __restrict__ scaled, int64_t m,
+                                   const unsigned* __restrict__ row_max, int b,
+                                   uint64_t invalid_key, uint64_t* __restrict__ keys,
+                                   float* __restrict__ vals,
+                                   unsigned long long* __restrict__ n_valid) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    bool valid = false;
+    if (e < m) {
+        const int64_t i = heads[e], j = tails[e];
+        const float v = scaled[e];
+        const float mx = __uint_as_float(row_max[i]);
+        if (v > 0.0f && i != j && mx > 0.0f && isfinite(mx)) {
+            const uint64_t lo = static_cast<uint64_t>(i < j ? i : j);
+            const uint64_t hi = static_cast<uint64_t>(i < j ? j : i);
+            keys[e] = (lo << (b + 1)) | (hi << 1) | static_cast<uint64_t>(i > j);
+            vals[e] = __fdiv_rn(v, mx);
+            valid = true;
+        } else {
+            keys[e] = invalid_key;
+            vals[e] = 0.0f;
+        }
+    }
+    const unsigned ballot = __ballot_sync(0xffffffffu, valid);
+    if ((threadIdx.x & 31) == 0 && ballot)
+        atomicAdd(n_valid, static_cast<unsigned long long>(__popc(ballot)));
+}
+
 inline unsigned grid_for(int64_t n, int threads = 256) {
     return static_cast<unsigned>(ceil_div(std::max<int64_t>(n, 1), threads));
 }
@@ -330,7 +384,7 @@ void build_row_ptr(const int32_t* heads, int64_t m, int64_t n, int32_t* row_ptr,
 
 void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, const float* rhos,
                  int64_t n, int k, float mix, int64_t n_epochs, Graph& g, cudaStream_t s,
-                 double* phase_sec) {
+                 double* phase_sec, const CategoricalTarget* target) {
     // phase clock of FitTimingBreakdown's membership / symmetrize / prune
     // fields (lib.rs:51-68); it synchronises only when asked for
     auto t_last = std::chrono::steady_clock::now();
@@ -345,56 +399,98 @@ void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, con
     const int b = bits_for(n);
     const int key_bits = 2 * b + 1;
     const uint64_t invalid_key = (key_bits >= 64) ? ~0ULL : ((uint64_t(1) << key_bits) - 1);
-    DevBuf<uint64_t> keys(m, s), keys2(m, s);
-    DevBuf<float> vals(m, s), vals2(m, s);
-    DevBuf<unsigned long long> nvalid(1, s);
-    UMAPB_CUDA(cudaMemsetAsync(nvalid.get(), 0, 8, s));
-    membership_keys_kernel<<<grid_for(m), 256, 0, s>>>(idx, dist, sigmas, rhos, n, k, b,
-                                                       invalid_key, keys.get(), vals.get(),
-                                                       nvalid.get());
-    UMAPB_LAUNCH_CHECK();
-    {
-        size_t tmp_bytes = 0;
-        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys.get(), keys2.get(),
-                                                   vals.get(), vals2.get(), m, 0, key_bits, s));
-        DevBuf<unsigned char> tmp(tmp_bytes, s);
-        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmp_bytes, keys.get(), keys2.get(),
-                                                   vals.get(), vals2.get(), m, 0, key_bits, s));
-    }
-    phase(0);
-    DevBuf<int> cnt(1, s);
-    UMAPB_CUDA(cudaMemsetAsync(cnt.get(), 0, 4, s));
-    DevBuf<uint64_t> sym_keys(2 * m + 2, s), sym_keys2(2 * m + 2, s);
-    DevBuf<float> sym_w(2 * m + 2, s), sym_w2(2 * m + 2, s);
-    // valid keys form the sorted prefix
-    unsigned long long valid_h = 0;
-    UMAPB_CUDA(cudaMemcpyAsync(&valid_h, nvalid.get(), 8, cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
-    const int64_t valid = static_cast<int64_t>(valid_h);
-    if (valid > 0) {
-        merge_pairs_kernel<<<grid_for(valid), 256, 0, s>>>(keys2.get(), vals2.get(), valid, b, mix,
-                                                           cnt.get(), sym_keys.get(), sym_w.get());
-        UMAPB_LAUNCH_CHECK();
-    }
+    // The symmetric graph: (head << 32 | tail) keys sorted, weights, heads, tails.
+    DevBuf<uint64_t> sym_keys2;
+    DevBuf<float> sym_w2;
+    DevBuf<int32_t> heads, tails;
     int n_sym = 0;
-    UMAPB_CUDA(cudaMemcpyAsync(&n_sym, cnt.get(), 4, cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
-    if (n_sym > 0) {
-        size_t tmp_bytes = 0;
-        const int end_bit = 32 + b;
-        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, sym_keys.get(),
-                                                   sym_keys2.get(), sym_w.get(), sym_w2.get(),
-                                                   n_sym, 0, end_bit, s));
-        DevBuf<unsigned char> tmp(tmp_bytes, s);
-        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmp_bytes, sym_keys.get(),
-                                                   sym_keys2.get(), sym_w.get(), sym_w2.get(),
-                                                   n_sym, 0, end_bit, s));
-    }
-    DevBuf<int32_t> heads(std::max(n_sym, 1), s), tails(std::max(n_sym, 1), s);
-    if (n_sym > 0) {
-        split_keys_kernel<<<grid_for(n_sym), 256, 0, s>>>(sym_keys2.get(), n_sym, heads.get(),
-                                                          tails.get());
+    // symmetrize_fuzzy_graph (lib.rs:3597-3649) of `mm` directed edges given
+    // as (min, max, head > tail) keys (invalid ones sort last, `nv` counts the
+    // rest): sort, merge each pair, sort by (head, tail), split.
+    auto union_keys = [&](DevBuf<uint64_t>& kin, DevBuf<float>& vin, int64_t mm,
+                          DevBuf<unsigned long long>& nv, float mixv, bool timed) {
+        DevBuf<uint64_t> ksorted(mm, s);
+        DevBuf<float> vsorted(mm, s);
+        {
+            size_t tmp_bytes = 0;
+            UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, kin.get(),
+                                                       ksorted.get(), vin.get(), vsorted.get(),
+                                                       mm, 0, key_bits, s));
+            DevBuf<unsigned char> tmp(tmp_bytes, s);
+            UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmp_bytes, kin.get(),
+                                                       ksorted.get(), vin.get(), vsorted.get(),
+                                                       mm, 0, key_bits, s));
+        }
+        if (timed) phase(0);
+        DevBuf<int> cnt(1, s);
+        UMAPB_CUDA(cudaMemsetAsync(cnt.get(), 0, 4, s));
+        DevBuf<uint64_t> sym_keys(2 * mm + 2, s);
+        DevBuf<float> sym_w(2 * mm + 2, s);
+        sym_keys2.alloc(2 * mm + 2, s);
+        sym_w2.alloc(2 * mm + 2, s);
+        // valid keys form the sorted prefix
+        unsigned long long valid_h = 0;
+        UMAPB_CUDA(cudaMemcpyAsync(&valid_h, nv.get(), 8, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        const int64_t valid = static_cast<int64_t>(valid_h);
+        if (valid > 0) {
+            merge_pairs_kernel<<<grid_for(valid), 256, 0, s>>>(ksorted.get(), vsorted.get(), valid,
+                                                               b, mixv, cnt.get(), sym_keys.get(),
+                                                               sym_w.get());
+            UMAPB_LAUNCH_CHECK();
+        }
+        UMAPB_CUDA(cudaMemcpyAsync(&n_sym, cnt.get(), 4, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        if (n_sym > 0) {
+            size_t tmp_bytes = 0;
+            const int end_bit = 32 + b;
+            UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, sym_keys.get(),
+                                                       sym_keys2.get(), sym_w.get(), sym_w2.get(),
+                                                       n_sym, 0, end_bit, s));
+            DevBuf<unsigned char> tmp(tmp_bytes, s);
+            UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmp_bytes, sym_keys.get(),
+                                                       sym_keys2.get(), sym_w.get(), sym_w2.get(),
+                                                       n_sym, 0, end_bit, s));
+        }
+        heads.alloc(std::max(n_sym, 1), s);
+        tails.alloc(std::max(n_sym, 1), s);
+        if (n_sym > 0) {
+            split_keys_kernel<<<grid_for(n_sym), 256, 0, s>>>(sym_keys2.get(), n_sym, heads.get(),
+                                                              tails.get());
+            UMAPB_LAUNCH_CHECK();
+        }
+    };
+    {
+        DevBuf<uint64_t> keys(m, s);
+        DevBuf<float> vals(m, s);
+        DevBuf<unsigned long long> nvalid(1, s);
+        UMAPB_CUDA(cudaMemsetAsync(nvalid.get(), 0, 8, s));
+        membership_keys_kernel<<<grid_for(m), 256, 0, s>>>(idx, dist, sigmas, rhos, n, k, b,
+                                                           invalid_key, keys.get(), vals.get(),
+                                                           nvalid.get());
         UMAPB_LAUNCH_CHECK();
+        union_keys(keys, vals, m, nvalid, mix, true);
+    }
+    if (target != nullptr && target->weight > 0.0f && n_sym > 0) {
+        // apply_categorical_target_intersection (lib.rs:1426-1431, 3694-3760):
+        // label-scaled weights, each head's row divided by its largest kept
+        // weight, and the fuzzy union of those directed edges with mix 1
+        DevBuf<float> scaled(n_sym, s);
+        DevBuf<unsigned> row_max(n, s);
+        UMAPB_CUDA(cudaMemsetAsync(row_max.get(), 0, n * 4, s));
+        target_scale_kernel<<<grid_for(n_sym), 256, 0, s>>>(
+            heads.get(), tails.get(), sym_w2.get(), n_sym, target->labels, target->unknown_scale,
+            target->far_scale, scaled.get(), row_max.get());
+        UMAPB_LAUNCH_CHECK();
+        DevBuf<uint64_t> keys(n_sym, s);
+        DevBuf<float> vals(n_sym, s);
+        DevBuf<unsigned long long> nvalid(1, s);
+        UMAPB_CUDA(cudaMemsetAsync(nvalid.get(), 0, 8, s));
+        target_keys_kernel<<<grid_for(n_sym), 256, 0, s>>>(heads.get(), tails.get(), scaled.get(),
+                                                           n_sym, row_max.get(), b, invalid_key,
+                                                           keys.get(), vals.get(), nvalid.get());
+        UMAPB_LAUNCH_CHECK();
+        union_keys(keys, vals, n_sym, nvalid, 1.0f, false);
     }
     g.n = n;
     phase(1);

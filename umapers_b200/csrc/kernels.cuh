@@ -142,13 +142,25 @@ bool knn_includes_self(const int32_t* idx, const float* dist, int64_t n, int k, 
 void smooth_knn(const float* dist, int64_t n, int k, float k_f, float local_conn, float bandwidth,
                 bool include_self, float* sigmas, float* rhos, cudaStream_t s);
 
-// compute_membership_strengths + symmetrize_fuzzy_graph (+ prune_edges when
+// A categorical supervision target (SupervisedTarget, rust_umap/src/lib.rs:
+// 109-125) on the device: int64 labels (-1 = unlabelled), the target weight
+// and the two scales of apply_categorical_target_intersection, exp(-1) and
+// exp(-far_dist), computed on the host in FP32.
+struct CategoricalTarget {
+    const int64_t* labels = nullptr;
+    float weight = 0.0f;
+    float unknown_scale = 0.0f;
+    float far_scale = 0.0f;
+};
+
+// compute_membership_strengths + symmetrize_fuzzy_graph (+ the categorical
+// target intersection when `target` has a positive weight, + prune_edges when
 // n_epochs > 0): the symmetric graph sorted by (head, tail).
 // `phase_sec` (nullable, 3 values): seconds of membership, symmetrisation
 // and prune + CSR offsets, with a stream synchronisation after each.
 void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, const float* rhos,
                  int64_t n, int k, float mix, int64_t n_epochs, Graph& g, cudaStream_t s,
-                 double* phase_sec = nullptr);
+                 double* phase_sec = nullptr, const CategoricalTarget* target = nullptr);
 
 // Bipartite membership + prune for transform (rust_umap/src/lib.rs:1738-1761):
 // edges grouped by query in kNN order; returns the edge count.
