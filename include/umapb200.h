@@ -196,6 +196,14 @@ int32_t umapb_fit_transform_supervised(umapb_model* model, const float* data, in
                                        float target_weight, int64_t target_n_neighbors,
                                        float* out);
 
+/* UmapCore.inverse_transform[_into] (umap_rs/src/lib.rs:1229-1290) ->
+ * UmapModel::inverse_transform_dense (rust_umap/src/lib.rs:1789-1915).
+ * `embedded_query` is n_rows x n_cols float32 (n_cols must equal
+ * n_components); `out` is n_rows x n_features.  Dense-fitted models only;
+ * n_components <= 16 and n_neighbors <= 32 on this path. */
+int32_t umapb_inverse_transform(umapb_model* model, const float* embedded_query, int64_t n_rows,
+                                int64_t n_cols, float* out);
+
 /* ---- CSR input -----------------------------------------------------------
  * indptr holds n_rows + 1 int64 offsets starting at 0; indices (int64) and
  * data (float32) hold indptr[n_rows] entries, column indices strictly

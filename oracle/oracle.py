@@ -43,6 +43,9 @@ _SIGS = {
         _i64,
         [_vp, _vp, _i64, _i64, _f32, _f32, _i64, _vp, _vp, _vp, _i64, _vp, _vp],
     ),
+    "orc_inverse_transform": (
+        _i32, [_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _i64, _i64, _f32, _f32, _f32,
+               _i64, _f32, _u64, _vp]),
     "orc_categorical_intersection": (
         _i64, [_vp, _vp, _vp, _i64, _vp, _i64, _f32, _i64, _vp, _vp, _vp, _i64]),
     "orc_spectral_init": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _i64, _i64, _u64, _vp, _vp]),
@@ -250,6 +253,25 @@ def categorical_intersection(heads, tails, weights, labels, weight: float, n_epo
                                              labels.shape[0], weight, n_epochs, _p(h), _p(t),
                                              _p(w), cap)
     return h[:ne].copy(), t[:ne].copy(), w[:ne].copy()
+
+
+def inverse_transform(x, emb, sigmas, rhos, query, n_neighbors: int = 15, n_epochs=None,
+                      a: float = 1.0, b: float = 1.0, lr: float = 1.0, neg_rate: int = 5,
+                      repulsion: float = 1.0, seed: int = 42):
+    """inverse_transform_rows (lib.rs:1800-1915) of a model given by its
+    rows, embedding and the fit's sigmas / rhos; the SGD seed is the model
+    seed ^ 0xD1B54A32D192ED03 as in the reference."""
+    x, emb, query = _f32m(x), _f32m(emb), _f32m(query)
+    sig = np.ascontiguousarray(sigmas, np.float32)
+    rho = np.ascontiguousarray(rhos, np.float32)
+    n, d = x.shape
+    nq, low = query.shape
+    out = np.empty((nq, d), np.float32)
+    load().orc_inverse_transform(_p(x), n, d, _p(emb), low, _p(sig), _p(rho), _p(query), nq,
+                                 n_neighbors, -1 if n_epochs is None else n_epochs, a, b, lr,
+                                 neg_rate, repulsion, (seed ^ 0xD1B54A32D192ED03) & (2**64 - 1),
+                                 _p(out))
+    return out
 
 
 def spectral_init(x, heads, tails, weights, dim: int, seed: int):

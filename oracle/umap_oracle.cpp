@@ -1912,6 +1912,185 @@ int64_t orc_fuzzy_graph(const int64_t* idx, const float* dist, int64_t n, int64_
     return static_cast<int64_t>(edges.size());
 }
 
+// inverse_transform_rows (lib.rs:1800-1915) for a model given by its rows X
+// (n x D), embedding E (n x L) and the fit's sigmas / rhos: exact kNN of the
+// queries among E, weights 1 / (1 + a d^(2b)), init_inverse_points
+// (lib.rs:4838-4935, with an LU of partial pivoting for the L x L system) and
+// optimize_layout_inverse (lib.rs:5547-5645, one SmallRng over all edges in
+// order).  n_epochs_param < 0 is None.
+int32_t orc_inverse_transform(const float* X, int64_t n, int64_t D, const float* E, int64_t L,
+                              const float* sig, const float* rho, const float* Z, int64_t nq,
+                              int64_t n_neighbors, int64_t n_epochs_param, float a, float b,
+                              float lr, int64_t neg_rate, float repulsion, uint64_t seed,
+                              float* out) {
+    if (nq == 0) return 0;
+    const size_t k = static_cast<size_t>(std::max<int64_t>(1, std::min<int64_t>(n_neighbors, n)));
+    const size_t n_epochs = n_epochs_param < 0 ? (nq <= 10000 ? 100 : 30)
+                                               : static_cast<size_t>(std::max<int64_t>(n_epochs_param / 3, 1));
+    const Knn knn = exact_knn_query(Z, nq, E, n, L, k, UMAPB_METRIC_EUCLIDEAN);
+    std::vector<Edge> edges;
+    std::vector<std::vector<float>> init_w(nq, std::vector<float>(k, 0.0f));
+    std::vector<char> fixed(nq, 0);
+    for (int64_t i = 0; i < nq; ++i) {
+        float row_sum = 0.0f;
+        for (size_t j = 0; j < k; ++j) {
+            const float w = 1.0f / (1.0f + a * std::pow(knn.dist[i][j], 2.0f * b));
+            if (w > 0.0f && std::isfinite(w)) {
+                init_w[i][j] = w;
+                row_sum += w;
+                edges.push_back({static_cast<size_t>(i), knn.idx[i][j], w});
+            }
+        }
+        if (row_sum > 0.0f)
+            for (auto& w : init_w[i]) w /= row_sum;
+        fixed[i] = knn.dist[i][0] <= 1e-6f;
+    }
+    std::vector<std::vector<float>> pts(nq, std::vector<float>(D, 0.0f));
+    for (int64_t i = 0; i < nq; ++i) {
+        auto& res = pts[i];
+        if (fixed[i]) {
+            std::copy(X + knn.idx[i][0] * D, X + knn.idx[i][0] * D + D, res.begin());
+            continue;
+        }
+        std::vector<float> zbar(L, 0.0f), xbar(D, 0.0f);
+        float wsum = 0.0f;
+        for (size_t j = 0; j < k; ++j) {
+            const float w = init_w[i][j];
+            if (w <= 0.0f || !std::isfinite(w)) continue;
+            wsum += w;
+            const size_t id = knn.idx[i][j];
+            for (int64_t c = 0; c < L; ++c) zbar[c] += w * E[id * L + c];
+            for (int64_t d = 0; d < D; ++d) xbar[d] += w * X[id * D + d];
+        }
+        if (wsum <= 0.0f) {
+            std::fill(res.begin(), res.end(), std::numeric_limits<float>::quiet_NaN());
+            continue;
+        }
+        std::vector<float> g(L * L, 0.0f), rhs(L * D, 0.0f);
+        size_t non_zero = 0;
+        for (size_t j = 0; j < k; ++j) {
+            const float w = init_w[i][j];
+            if (w <= 0.0f || !std::isfinite(w)) continue;
+            ++non_zero;
+            const size_t id = knn.idx[i][j];
+            for (int64_t aa = 0; aa < L; ++aa) {
+                const float za = E[id * L + aa] - zbar[aa];
+                for (int64_t bb = 0; bb < L; ++bb) g[aa * L + bb] += w * za * (E[id * L + bb] - zbar[bb]);
+                for (int64_t d = 0; d < D; ++d) rhs[aa * D + d] += w * za * (X[id * D + d] - xbar[d]);
+            }
+        }
+        for (int64_t c = 0; c < L; ++c) g[c * L + c] += 1e-3f;
+        res = xbar;
+        if (non_zero > static_cast<size_t>(L)) {
+            // LU with partial pivoting; a zero pivot leaves x_bar
+            std::vector<int64_t> perm(L);
+            for (int64_t c = 0; c < L; ++c) perm[c] = c;
+            bool ok = true;
+            for (int64_t c = 0; c < L && ok; ++c) {
+                int64_t piv = c;
+                float best = std::fabs(g[c * L + c]);
+                for (int64_t r = c + 1; r < L; ++r)
+                    if (std::fabs(g[r * L + c]) > best) {
+                        best = std::fabs(g[r * L + c]);
+                        piv = r;
+                    }
+                if (best == 0.0f) {
+                    ok = false;
+                    break;
+                }
+                if (piv != c) {
+                    for (int64_t cc = 0; cc < L; ++cc) std::swap(g[c * L + cc], g[piv * L + cc]);
+                    std::swap(perm[c], perm[piv]);
+                }
+                for (int64_t r = c + 1; r < L; ++r) {
+                    const float f = g[r * L + c] / g[c * L + c];
+                    g[r * L + c] = f;
+                    for (int64_t cc = c + 1; cc < L; ++cc) g[r * L + cc] -= f * g[c * L + cc];
+                }
+            }
+            if (ok) {
+                std::vector<float> pred(D);
+                bool valid = true;
+                std::vector<float> y(L), beta(L);
+                for (int64_t d = 0; d < D && valid; ++d) {
+                    for (int64_t r = 0; r < L; ++r) {
+                        float v = rhs[perm[r] * D + d];
+                        for (int64_t c = 0; c < r; ++c) v -= g[r * L + c] * y[c];
+                        y[r] = v;
+                    }
+                    for (int64_t r = L - 1; r >= 0; --r) {
+                        float v = y[r];
+                        for (int64_t c = r + 1; c < L; ++c) v -= g[r * L + c] * beta[c];
+                        beta[r] = v / g[r * L + r];
+                    }
+                    float v = xbar[d];
+                    for (int64_t c = 0; c < L; ++c) v += (Z[i * L + c] - zbar[c]) * beta[c];
+                    if (!std::isfinite(v)) valid = false;
+                    pred[d] = v;
+                }
+                if (valid) res = pred;
+            }
+        }
+    }
+    // optimize_layout_inverse
+    if (!edges.empty() && n_epochs > 0) {
+        std::vector<float> w(edges.size());
+        for (size_t e = 0; e < edges.size(); ++e) w[e] = edges[e].weight;
+        const std::vector<float> eps = epochs_per_sample(w, n_epochs);
+        std::vector<float> next = eps, eps_neg(eps.size()), next_neg;
+        for (size_t e = 0; e < eps.size(); ++e) eps_neg[e] = eps[e] / static_cast<float>(neg_rate);
+        next_neg = eps_neg;
+        SmallRng rng(seed);
+        const float alpha0 = lr / 4.0f;
+        auto dist_denom = [&](const std::vector<float>& x, const float* y, float* dist) {
+            float sq = 0.0f;
+            for (int64_t d = 0; d < D; ++d) {
+                const float df = x[d] - y[d];
+                sq += df * df;
+            }
+            *dist = std::sqrt(sq);
+            return 1e-6f + *dist;
+        };
+        for (size_t epoch = 0; epoch < n_epochs; ++epoch) {
+            const float alpha = alpha0 * (1.0f - static_cast<float>(epoch) / static_cast<float>(n_epochs));
+            for (size_t e = 0; e < edges.size(); ++e) {
+                if (next[e] > static_cast<float>(epoch)) continue;
+                const size_t head = edges[e].head, tail = edges[e].tail;
+                auto& cur = pts[head];
+                bool finite = true;
+                for (float v : cur) finite = finite && std::isfinite(v);
+                if (fixed[head] || !finite) continue;
+                float dd;
+                const float denom = dist_denom(cur, X + tail * D, &dd);
+                const float gc = -(1.0f / (edges[e].weight * sig[tail] + 1e-6f));
+                for (int64_t d = 0; d < D; ++d) {
+                    const float gd = clip4(gc * ((cur[d] - X[tail * D + d]) / denom));
+                    cur[d] += gd * alpha;
+                }
+                next[e] += eps[e];
+                const float en = eps_neg[e];
+                if (!std::isfinite(en) || en <= 0.0f) continue;
+                const float f = std::floor((static_cast<float>(epoch) - next_neg[e]) / en);
+                const size_t n_neg = f > 0.0f ? static_cast<size_t>(f) : 0;
+                for (size_t s_ = 0; s_ < n_neg; ++s_) {
+                    const size_t neg = rng.gen_range(0, static_cast<uint64_t>(n));
+                    float dn;
+                    const float den2 = dist_denom(cur, X + neg * D, &dn);
+                    const float wh = std::exp(-std::max(dn - rho[neg], 1e-6f) / (sig[neg] + 1e-6f));
+                    const float g2 = -repulsion * ((0.0f - wh) / ((1.0f - wh) * sig[neg] + 1e-6f));
+                    for (int64_t d = 0; d < D; ++d) {
+                        const float gd = clip4(g2 * ((cur[d] - X[neg * D + d]) / den2));
+                        cur[d] += gd * alpha;
+                    }
+                }
+                next_neg[e] += static_cast<float>(n_neg) * en;
+            }
+        }
+    }
+    for (int64_t i = 0; i < nq; ++i) std::copy(pts[i].begin(), pts[i].end(), out + i * D);
+    return 0;
+}
+
 // The categorical target intersection (lib.rs:1426-1431) of an edge list,
 // then prune_edges when n_epochs > 0.
 int64_t orc_categorical_intersection(const int32_t* heads, const int32_t* tails,

@@ -249,3 +249,24 @@ def test_categorical_intersection_pins_the_reference_test(orc):
     uh, ut, uw = orc.categorical_intersection(h, t, w, lab_u, 0.6)
     uwt = {(a, b): c for a, b, c in zip(uh.tolist(), ut.tolist(), uw.tolist())}
     assert uwt[(1, 2)] > 100 * wt(1, 2)
+
+
+def test_inverse_transform_restatement_basics(orc):
+    # inverse_transform_workflow (rust_umap/src/lib.rs:6271-6293) on the
+    # oracle: shape, finiteness, and an embedded point that is a fitted point
+    # (distance 0 <= 1e-6) maps back to that row exactly (lib.rs:1890, 4856)
+    x = workloads.reference_synthetic(140, 6)
+    idx, dist = orc.exact_knn(x, 15)
+    _, _, _, sig, rho = orc.fuzzy_graph(idx, dist)
+    rng = np.random.default_rng(0)
+    emb = (x[:, :2] + 0.01 * rng.normal(size=(140, 2))).astype(np.float32)
+    a, b = orc.find_ab_params(1.0, 0.1)
+    rec = orc.inverse_transform(x, emb, sig, rho, emb[130:], n_neighbors=15, n_epochs=90, a=a, b=b)
+    assert rec.shape == (10, 6) and np.all(np.isfinite(rec))
+    np.testing.assert_array_equal(rec, x[130:])
+    # points between fitted points land near the local linear model's prediction
+    mid = ((emb[:10] + emb[10:20]) / 2).astype(np.float32)
+    rm = orc.inverse_transform(x, emb, sig, rho, mid, n_neighbors=15, n_epochs=90, a=a, b=b)
+    assert np.all(np.isfinite(rm))
+    assert np.mean(np.linalg.norm(rm - (x[:10] + x[10:20]) / 2, axis=1)) < \
+        np.mean(np.linalg.norm(x - x.mean(0), axis=1))

@@ -8,9 +8,9 @@ fitted attributes ``embedding_``, ``n_features_in_``, ``n_samples_fit_``.
 Compute runs on one B200 through ``UmapCore`` (libumapb200.so), densMAP and
 ``output_dens`` (dense input), categorical supervision (``target_metric=
 "categorical"`` with ``y``, dense input) and CSR sparse input (scipy
-csr/csc/coo) included.  Inputs the engine does not cover (inverse_transform,
-metrics other than euclidean/cosine, sparse input with n_neighbors above 32)
-raise ValueError.
+csr/csc/coo) included, and ``inverse_transform`` of dense-fitted models.
+Inputs the engine does not cover (metrics other than euclidean/cosine, sparse
+input with n_neighbors above 32) raise ValueError.
 """
 from __future__ import annotations
 
@@ -686,11 +686,31 @@ class Umap:
         return buf
 
     def inverse_transform(self, embedded_query: Any, *, out: np.ndarray | None = None) -> np.ndarray:
-        """Not provided by the B200 engine (raises after the fitted check)."""
-        _f32_matrix(embedded_query, "embedded_query")
-        if out is not None and self._core.n_features is None:
+        """Map embedded samples back to the feature space (_api.py:838-873).
+
+        Parameters
+        ----------
+        embedded_query:
+            Dense embedding of shape ``(n_samples, n_components)``, converted
+            to ``float32``.
+        out:
+            Optional writable ``float32`` buffer of shape
+            ``(n_samples, n_features)``; the model must be fit first.
+
+        Returns
+        -------
+        numpy.ndarray
+            The reconstructed samples, shape ``(n_samples, n_features)``.
+        """
+        arr = _f32_matrix(embedded_query, "embedded_query")
+        if out is None:
+            return self._core.inverse_transform(arr)
+        n_features = self._core.n_features
+        if n_features is None:
             raise RuntimeError("model must be fit before inverse_transform(out=...)")
-        return self._core.inverse_transform(embedded_query)
+        buf = _out_buffer(out, (arr.shape[0], n_features))
+        self._core.inverse_transform_into(arr, buf)
+        return buf
 
 
 class ParametricUmap:

@@ -205,6 +205,7 @@ SIGNATURES = {
     "umapb_fit": (_i32, [_vp, _vp, _i64, _i64]),
     "umapb_fit_transform": (_i32, [_vp, _vp, _i64, _i64, _vp]),
     "umapb_fit_supervised": (_i32, [_vp, _vp, _i64, _i64, _vp, _i64, _f32, _i64]),
+    "umapb_inverse_transform": (_i32, [_vp, _vp, _i64, _i64, _vp]),
     "umapb_fit_transform_supervised": (_i32, [_vp, _vp, _i64, _i64, _vp, _i64, _f32, _i64, _vp]),
     "umapb_fit_transform_stateless": (_i32, [ctypes.POINTER(Params), _vp, _i64, _i64, _vp]),
     "umapb_fit_transform_with_knn": (

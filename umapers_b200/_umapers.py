@@ -462,13 +462,27 @@ class UmapCore:
                                                           ctypes.byref(n)))
         return buf[: n.value].copy()
 
-    def inverse_transform(self, *args: Any, **kwargs: Any) -> np.ndarray:
-        if self.n_features is None:
-            raise RuntimeError("model is not fitted yet")
-        raise ValueError("inverse_transform is not supported by the B200 engine")
+    def inverse_transform(self, embedded_query: Any) -> np.ndarray:
+        """UmapCore.inverse_transform (umap_rs/src/lib.rs:1229-1252): rows of
+        the embedding mapped back to the feature space."""
+        arr = _matrix(embedded_query, "embedded_query")
+        out = np.empty((arr.shape[0], self.n_features or 0), dtype=np.float32)
+        _lib.check(
+            self._lib.umapb_inverse_transform(
+                self._handle, _lib.ptr(arr), arr.shape[0], arr.shape[1], _lib.ptr(out)
+            )
+        )
+        return out
 
-    def inverse_transform_into(self, *args: Any, **kwargs: Any) -> None:
-        self.inverse_transform()
+    def inverse_transform_into(self, embedded_query: Any, out: np.ndarray) -> None:
+        """UmapCore.inverse_transform_into (umap_rs/src/lib.rs:1254-1290)."""
+        arr = _matrix(embedded_query, "embedded_query")
+        _check_out(out, (arr.shape[0], self.n_features or 0))
+        _lib.check(
+            self._lib.umapb_inverse_transform(
+                self._handle, _lib.ptr(arr), arr.shape[0], arr.shape[1], _lib.ptr(out)
+            )
+        )
 
     # --------------------------------------------------------- diagnostics
     def knn_recall_diagnostics(self, data: Any) -> dict[str, Any]:

@@ -263,6 +263,7 @@ struct umapb_model {
     umapb::CsrIndex csr_idx;   // their kNN index (tiles by column, norm order)
     bool sparse = false;       // fitted from CSR rows
     DevBuf<float> emb;  // fitted embedding, n_fit x n_components
+    DevBuf<float> fit_sig, fit_rho;  // the fit's smooth_knn_dist sigmas / rhos (inverse_transform)
     Graph graph;        // the fit's fuzzy graph (CSR by head), the surrogate's edge loss
     DevBuf<float> radii_orig, radii_emb;  // densMAP / output_dens radii (n_fit each)
     SurrogatePtr surrogate;
@@ -291,6 +292,8 @@ struct umapb_model {
         graph = Graph();
         radii_orig.release();
         radii_emb.release();
+        fit_sig.release();
+        fit_rho.release();
         emb.release();
         X.release();
         csr = umapb::CsrDevice();
@@ -421,6 +424,8 @@ void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const i
         out->info.n_epochs = n_epochs;
     }
     m->emb = std::move(emb);
+    m->fit_sig = std::move(sig);
+    m->fit_rho = std::move(rho);
     g.heads.release();
     m->graph = std::move(g);
     m->surrogate.reset();
@@ -555,6 +560,48 @@ void fit_supervised_host(umapb_model* m, const float* data, int64_t n, int64_t d
     fit_device(m, X.get(), n, d, false, nullptr, clk, weight > 0.0f ? &target : nullptr);
     m->X = std::move(X);
     if (emb_out) copy_embedding_out(m, emb_out);
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+}
+
+// inverse_transform_dense (lib.rs:1789-1915): checks in the reference's
+// order, exact kNN of the embedded queries among the fitted embedding
+// (exact_nearest_neighbors_to_reference, euclidean), then init_inverse_points
+// and optimize_layout_inverse on the device.  `out` is nq x n_features.
+void inverse_transform_host(umapb_model* m, const float* zq, int64_t nq, int64_t L, float* out) {
+    if (m->fitted && m->sparse)
+        invalid("inverse_transform is not supported for sparse-trained models yet");
+    if (!m->fitted || m->fit_sig.get() == nullptr)
+        throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+    if (nq == 0) return;
+    if (L != m->p.n_components)
+        throw Error(UMAPB_ERR_EMBEDDING_DIM_MISMATCH,
+                    "embedding dimension mismatch: expected " + std::to_string(m->p.n_components) +
+                        ", got " + std::to_string(L));
+    for (int64_t i = 0; i < nq; ++i)
+        for (int64_t c = 0; c < L; ++c)
+            if (!std::isfinite(zq[i * L + c]))
+                invalid("input contains non-finite value at row " + std::to_string(i));
+    const umapb_params& p = m->p;
+    cudaStream_t s = m->stream;
+    UMAPB_CUDA(cudaSetDevice(m->device));
+    const int64_t n = m->n_fit;
+    const int64_t D = m->d_fit;
+    // inverse_neighbor_count (lib.rs:3420-3422)
+    const int k = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(p.n_neighbors, n)));
+    const int64_t n_epochs = p.n_epochs < 0 ? (nq <= 10000 ? 100 : 30)
+                                            : std::max<int64_t>(p.n_epochs / 3, 1);
+    DevBuf<float> Z;
+    upload(Z, zq, nq * L, s);
+    DevBuf<int32_t> idx(nq * k, s);
+    DevBuf<float> dist(nq * k, s);
+    knn_exact_device(Z.get(), nq, m->emb.get(), n, static_cast<int>(L), k, UMAPB_METRIC_EUCLIDEAN,
+                     UMAPB_KNN_PLAIN, idx.get(), dist.get(), nullptr, nullptr, nullptr, s);
+    DevBuf<float> o(nq * D, s);
+    inverse_layout(Z.get(), nq, static_cast<int>(L), idx.get(), dist.get(), k, m->emb.get(),
+                   m->X.get(), n, static_cast<int>(D), m->fit_sig.get(), m->fit_rho.get(), m->a,
+                   m->b, n_epochs, p.learning_rate, p.negative_sample_rate, p.repulsion_strength,
+                   p.random_seed ^ 0xD1B54A32D192ED03ULL, o.get(), s);
+    UMAPB_CUDA(cudaMemcpyAsync(out, o.get(), nq * D * 4, cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -823,6 +870,14 @@ int32_t umapb_fit_transform_supervised(umapb_model* m, const float* data, int64_
         std::lock_guard<std::mutex> lk(m->mu);
         fit_supervised_host(m, data, n_rows, n_cols, labels, n_labels, target_weight,
                             target_n_neighbors, out);
+    });
+}
+
+int32_t umapb_inverse_transform(umapb_model* m, const float* embedded_query, int64_t n_rows,
+                                int64_t n_cols, float* out) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        inverse_transform_host(m, embedded_query, n_rows, n_cols, out);
     });
 }
 

@@ -175,6 +175,15 @@ void build_row_ptr(const int32_t* heads, int64_t n_edges, int64_t n, int32_t* ro
 // max over weights
 float max_weight(const float* w, int64_t n, cudaStream_t s);
 
+// init_inverse_points + optimize_layout_inverse (rust_umap/src/lib.rs:
+// 4838-4935, 5547-5645) for nq embedded queries zq (nq x L) whose k
+// neighbours in the fitted embedding are idx/dist: writes nq x D points.
+void inverse_layout(const float* zq, int64_t nq, int L, const int32_t* idx, const float* dist,
+                    int k, const float* emb, const float* X, int64_t n, int D, const float* sig,
+                    const float* rho, float a, float b, int64_t n_epochs, float lr,
+                    int64_t neg_rate, float repulsion, uint64_t seed, float* out,
+                    cudaStream_t s);
+
 // ----------------------------------------------------------- spectral.cu
 struct SpectralResult {
     bool used_spectral = false;

@@ -791,6 +791,275 @@ __global__ void __launch_bounds__(kTransformThreads) transform_kernel(TransformA
     for (int c = 0; c < dim; ++c) p.out[q * dim + c] = cur[c];
 }
 
+// ------------------------------------------------------ inverse transform --
+// inverse_transform_rows (rust_umap/src/lib.rs:1800-1915): every embedded
+// query q gets k neighbours among the fitted embedding's rows, edge weights
+// 1 / (1 + a d^(2b)), an initial point in data space (init_inverse_points,
+// lib.rs:4838-4935), then per-query SGD against the fitted rows
+// (optimize_layout_inverse, lib.rs:5547-5645).  One warp per query; lanes
+// split the data dimensions.
+constexpr int kInvMaxLow = 16;  // n_components
+constexpr int kInvMaxK = 32;    // neighbours per query
+
+struct InverseArgs {
+    const float* zq;      // nq x L embedded queries
+    const int32_t* idx;   // nq x k neighbours in the fitted embedding
+    const float* dist;    // nq x k
+    const float* emb;     // n x L fitted embedding
+    const float* X;       // n x D fitted rows
+    const float* sig;     // n: the fit's sigmas
+    const float* rho;     // n: the fit's rhos
+    float* out;           // nq x D
+    float* w;             // nq x k edge weights, 0 where the reference adds no edge
+    uint8_t* fixed;       // nq: first neighbour within 1e-6
+    int64_t nq, n;
+    int L, D, k;
+    float a, b;
+    // optimize_layout_inverse
+    float max_w;          // largest edge weight of the whole inverse graph
+    int64_t n_epochs;
+    float alpha0, neg_rate_f, rep;
+    uint64_t seed;
+};
+
+// Partial-pivoting LU of the L x L matrix g (row-major, in place) with the
+// row permutation in perm; false when a pivot is 0 (nalgebra's solve then
+// returns None).
+__device__ bool lu_factor(float* g, int L, int* perm) {
+    for (int i = 0; i < L; ++i) perm[i] = i;
+    for (int i = 0; i < L; ++i) {
+        int piv = i;
+        float best = fabsf(g[i * L + i]);
+        for (int r = i + 1; r < L; ++r)
+            if (fabsf(g[r * L + i]) > best) {
+                best = fabsf(g[r * L + i]);
+                piv = r;
+            }
+        if (best == 0.0f) return false;
+        if (piv != i) {
+            for (int c = 0; c < L; ++c) {
+                const float t = g[i * L + c];
+                g[i * L + c] = g[piv * L + c];
+                g[piv * L + c] = t;
+            }
+            const int t = perm[i];
+            perm[i] = perm[piv];
+            perm[piv] = t;
+        }
+        const float inv = g[i * L + i];
+        for (int r = i + 1; r < L; ++r) {
+            const float f = __fdiv_rn(g[r * L + i], inv);
+            g[r * L + i] = f;
+            for (int c = i + 1; c < L; ++c)
+                g[r * L + c] = __fsub_rn(g[r * L + c], __fmul_rn(f, g[i * L + c]));
+        }
+    }
+    return true;
+}
+
+// Solves LU x = P rhs for one right-hand side (x overwrites rhs).
+__device__ void lu_solve(const float* g, int L, const int* perm, float* rhs) {
+    float y[kInvMaxLow];
+    for (int i = 0; i < L; ++i) {
+        float v = rhs[perm[i]];
+        for (int c = 0; c < i; ++c) v = __fsub_rn(v, __fmul_rn(g[i * L + c], y[c]));
+        y[i] = v;
+    }
+    for (int i = L - 1; i >= 0; --i) {
+        float v = y[i];
+        for (int c = i + 1; c < L; ++c) v = __fsub_rn(v, __fmul_rn(g[i * L + c], rhs[c]));
+        rhs[i] = __fdiv_rn(v, g[i * L + i]);
+    }
+}
+
+__global__ void __launch_bounds__(256) inverse_init_kernel(InverseArgs p) {
+    const int64_t q = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (q >= p.nq) return;
+    const int L = p.L, D = p.D, k = p.k;
+    const int32_t* nb = p.idx + q * k;
+    float* out = p.out + q * D;
+    // edge weights in neighbour order (lib.rs:1871-1893)
+    float wj = 0.0f;
+    if (lane < k) {
+        const float d = p.dist[q * k + lane];
+        const float v = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(p.a, powf(d, __fmul_rn(2.0f, p.b)))));
+        wj = (v > 0.0f && isfinite(v)) ? v : 0.0f;
+        p.w[q * k + lane] = wj;
+    }
+    float row_sum = 0.0f;
+    for (int j = 0; j < k; ++j) row_sum = __fadd_rn(row_sum, __shfl_sync(0xffffffffu, wj, j));
+    const float nw = row_sum > 0.0f ? __fdiv_rn(wj, row_sum) : wj;  // normalised init weight
+    const bool fixed = p.dist[q * k] <= 1e-6f;
+    if (lane == 0) p.fixed[q] = fixed ? 1 : 0;
+    if (fixed) {
+        const float* src = p.X + static_cast<int64_t>(nb[0]) * D;
+        for (int d = lane; d < D; d += 32) out[d] = src[d];
+        return;
+    }
+    // weighted means of the neighbours' embedding and data rows (lib.rs:4859-4875)
+    float zbar[kInvMaxLow];
+    for (int c = 0; c < L; ++c) zbar[c] = 0.0f;
+    float wsum = 0.0f;
+    int non_zero = 0;
+    for (int j = 0; j < k; ++j) {
+        const float w = __shfl_sync(0xffffffffu, nw, j);
+        if (!(w > 0.0f) || !isfinite(w)) continue;
+        wsum = __fadd_rn(wsum, w);
+        ++non_zero;
+        const float* e = p.emb + static_cast<int64_t>(nb[j]) * L;
+        for (int c = 0; c < L; ++c) zbar[c] = __fadd_rn(zbar[c], __fmul_rn(w, e[c]));
+    }
+    if (wsum <= 0.0f) {
+        for (int d = lane; d < D; d += 32) out[d] = NAN;
+        return;
+    }
+    // gram = sum w z_a z_b, plus 1e-3 on the diagonal (lib.rs:4881-4902)
+    float g[kInvMaxLow * kInvMaxLow];
+    for (int c = 0; c < L * L; ++c) g[c] = 0.0f;
+    for (int j = 0; j < k; ++j) {
+        const float w = __shfl_sync(0xffffffffu, nw, j);
+        if (!(w > 0.0f) || !isfinite(w)) continue;
+        const float* e = p.emb + static_cast<int64_t>(nb[j]) * L;
+        for (int a = 0; a < L; ++a) {
+            const float za = __fsub_rn(e[a], zbar[a]);
+            for (int b = 0; b < L; ++b)
+                g[a * L + b] = __fadd_rn(g[a * L + b], __fmul_rn(__fmul_rn(w, za), __fsub_rn(e[b], zbar[b])));
+        }
+    }
+    for (int c = 0; c < L; ++c) g[c * L + c] = __fadd_rn(g[c * L + c], 1e-3f);
+    int perm[kInvMaxLow];
+    const bool solve = non_zero > L && lu_factor(g, L, perm);
+    const float* zq = p.zq + q * L;
+    // per data dimension: x_bar, the rhs column, beta = gram^-1 rhs, the
+    // prediction x_bar + (z - z_bar) beta (lib.rs:4870-4931)
+    bool ok = true;
+    for (int d0 = 0; d0 < D; d0 += 32) {
+        const int d = d0 + lane;
+        const bool in = d < D;
+        float xbar = 0.0f;
+        for (int j = 0; j < k; ++j) {
+            const float w = __shfl_sync(0xffffffffu, nw, j);
+            if (!(w > 0.0f) || !isfinite(w) || !in) continue;
+            xbar = __fadd_rn(xbar, __fmul_rn(w, p.X[static_cast<int64_t>(nb[j]) * D + d]));
+        }
+        float pred = xbar;
+        float rhs[kInvMaxLow];
+        for (int a = 0; a < L; ++a) rhs[a] = 0.0f;
+        for (int j = 0; j < k; ++j) {
+            // every lane takes part in the shuffle; only lanes with a column add
+            const float w = __shfl_sync(0xffffffffu, nw, j);
+            if (!(w > 0.0f) || !isfinite(w) || !in || !solve) continue;
+            const float* e = p.emb + static_cast<int64_t>(nb[j]) * L;
+            const float xd = __fsub_rn(p.X[static_cast<int64_t>(nb[j]) * D + d], xbar);
+            for (int a = 0; a < L; ++a)
+                rhs[a] = __fadd_rn(rhs[a], __fmul_rn(__fmul_rn(w, __fsub_rn(e[a], zbar[a])), xd));
+        }
+        if (solve && in) {
+            lu_solve(g, L, perm, rhs);
+            float v = xbar;
+            for (int a = 0; a < L; ++a) v = __fadd_rn(v, __fmul_rn(__fsub_rn(zq[a], zbar[a]), rhs[a]));
+            if (!isfinite(v)) ok = false;
+            pred = v;
+        }
+        if (in) out[d] = pred;
+    }
+    // a non-finite prediction anywhere keeps x_bar for the whole row
+    if (solve && __any_sync(0xffffffffu, !ok)) {
+        for (int d0 = 0; d0 < D; d0 += 32) {
+            const int d = d0 + lane;
+            float xbar = 0.0f;
+            for (int j = 0; j < k; ++j) {
+                const float w = __shfl_sync(0xffffffffu, nw, j);
+                if (!(w > 0.0f) || !isfinite(w) || d >= D) continue;
+                xbar = __fadd_rn(xbar, __fmul_rn(w, p.X[static_cast<int64_t>(nb[j]) * D + d]));
+            }
+            if (d < D) out[d] = xbar;
+        }
+    }
+}
+
+// Euclidean distance between a query row and a fitted row, reduced across
+// the warp: (distance, 1e-6 + distance) as euclidean_distance_with_grad_denom
+// (lib.rs:5035-5043).
+__device__ __forceinline__ float warp_dist(const float* x, const float* y, int D, int lane) {
+    float sq = 0.0f;
+    for (int d = lane; d < D; d += 32) {
+        const float df = __fsub_rn(x[d], y[d]);
+        sq = __fadd_rn(sq, __fmul_rn(df, df));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sq = __fadd_rn(sq, __shfl_xor_sync(0xffffffffu, sq, o));
+    return sqrtf(sq);
+}
+
+__global__ void __launch_bounds__(256) inverse_sgd_kernel(InverseArgs p) {
+    const int64_t q = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (q >= p.nq || p.fixed[q]) return;
+    const int D = p.D, k = p.k;
+    const int32_t* nb = p.idx + q * k;
+    float* cur = p.out + q * D;
+    // per-edge schedule, lane j for neighbour j (make_epochs_per_sample over
+    // the whole inverse graph, lib.rs:4937-4960)
+    const float wl = lane < k ? p.w[q * k + lane] : 0.0f;
+    const float nef = static_cast<float>(p.n_epochs);
+    float eps = INFINITY;
+    if (wl > 0.0f) {
+        const float ns = __fmul_rn(nef, __fdiv_rn(wl, p.max_w));
+        eps = ns > 0.0f ? __fdiv_rn(nef, ns) : INFINITY;
+    }
+    float next = eps;
+    const float eps_neg = __fdiv_rn(eps, p.neg_rate_f);
+    float next_neg = eps_neg;
+    const uint64_t qseed = mix64(p.seed ^ mix64(static_cast<uint64_t>(q)));
+    for (int64_t epoch = 0; epoch < p.n_epochs; ++epoch) {
+        const float alpha = __fmul_rn(p.alpha0, __fsub_rn(1.0f, __fdiv_rn(static_cast<float>(epoch), nef)));
+        const float ef = static_cast<float>(epoch);
+        for (int j = 0; j < k; ++j) {
+            const float wj = __shfl_sync(0xffffffffu, wl, j);
+            if (!(wj > 0.0f)) continue;  // no edge for this neighbour
+            if (__shfl_sync(0xffffffffu, next, j) > ef) continue;
+            bool fin = true;
+            for (int d = lane; d < D; d += 32) fin = fin && isfinite(cur[d]);
+            if (!__all_sync(0xffffffffu, fin)) continue;
+            const int32_t tail = nb[j];
+            const float* other = p.X + static_cast<int64_t>(tail) * D;
+            const float denom = __fadd_rn(1e-6f, warp_dist(cur, other, D, lane));
+            const float gc = -__fdiv_rn(1.0f, __fadd_rn(__fmul_rn(wj, p.sig[tail]), 1e-6f));
+            for (int d = lane; d < D; d += 32) {
+                const float gd = clip4(__fmul_rn(gc, __fdiv_rn(__fsub_rn(cur[d], other[d]), denom)));
+                cur[d] = __fadd_rn(cur[d], __fmul_rn(gd, alpha));
+            }
+            __syncwarp();
+            if (lane == j) next = __fadd_rn(next, eps);
+            const float en = __shfl_sync(0xffffffffu, eps_neg, j);
+            if (!isfinite(en) || en <= 0.0f) continue;
+            const float nn = __shfl_sync(0xffffffffu, next_neg, j);
+            const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(ef, nn), en));
+            for (uint32_t s = 0; s < n_neg; ++s) {
+                const uint64_t word = rng_word(qseed, static_cast<uint64_t>(j),
+                                               (static_cast<uint64_t>(epoch) << 32) | s);
+                const uint32_t neg = rng_below(word, static_cast<uint32_t>(p.n));
+                const float* o = p.X + static_cast<int64_t>(neg) * D;
+                const float dn = warp_dist(cur, o, D, lane);
+                const float sn = p.sig[neg];
+                const float wh = expf(__fdiv_rn(-fmaxf(__fsub_rn(dn, p.rho[neg]), 1e-6f),
+                                                __fadd_rn(sn, 1e-6f)));
+                const float g2 = __fmul_rn(-p.rep, __fdiv_rn(__fsub_rn(0.0f, wh),
+                                                              __fadd_rn(__fmul_rn(__fsub_rn(1.0f, wh), sn), 1e-6f)));
+                const float den2 = __fadd_rn(1e-6f, dn);
+                for (int d = lane; d < D; d += 32) {
+                    const float gd = clip4(__fmul_rn(g2, __fdiv_rn(__fsub_rn(cur[d], o[d]), den2)));
+                    cur[d] = __fadd_rn(cur[d], __fmul_rn(gd, alpha));
+                }
+                __syncwarp();
+            }
+            if (lane == j) next_neg = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), en));
+        }
+    }
+}
+
 }  // namespace
 
 void local_radii(const int32_t* idx, const float* dist, int64_t n, int k, float var_shift,
@@ -966,6 +1235,50 @@ void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_
     p.seed = seed;
     transform_kernel<<<static_cast<unsigned>(ceil_div(nq, static_cast<int64_t>(kTransformThreads))),
                        kTransformThreads, 0, s>>>(p);
+    UMAPB_LAUNCH_CHECK();
+}
+
+void inverse_layout(const float* zq, int64_t nq, int L, const int32_t* idx, const float* dist,
+                    int k, const float* emb, const float* X, int64_t n, int D, const float* sig,
+                    const float* rho, float a, float b, int64_t n_epochs, float lr,
+                    int64_t neg_rate, float repulsion, uint64_t seed, float* out,
+                    cudaStream_t s) {
+    if (nq == 0) return;
+    if (L > kInvMaxLow) invalid("inverse_transform supports n_components <= 16 on the GPU path");
+    if (k > kInvMaxK) invalid("inverse_transform supports n_neighbors <= 32 on the GPU path");
+    DevBuf<float> w(nq * k, s);
+    DevBuf<uint8_t> fixed(nq, s);
+    InverseArgs p{};
+    p.zq = zq;
+    p.idx = idx;
+    p.dist = dist;
+    p.emb = emb;
+    p.X = X;
+    p.sig = sig;
+    p.rho = rho;
+    p.out = out;
+    p.w = w.get();
+    p.fixed = fixed.get();
+    p.nq = nq;
+    p.n = n;
+    p.L = L;
+    p.D = D;
+    p.k = k;
+    p.a = a;
+    p.b = b;
+    const unsigned grid = static_cast<unsigned>(ceil_div(nq * 32, 256));
+    inverse_init_kernel<<<grid, 256, 0, s>>>(p);
+    UMAPB_LAUNCH_CHECK();
+    // optimize_layout_inverse returns at once for an empty graph or 0 epochs
+    const float mx = max_weight(w.get(), nq * k, s);
+    if (n_epochs == 0 || !(mx > 0.0f)) return;
+    p.max_w = mx;
+    p.n_epochs = n_epochs;
+    p.alpha0 = lr / 4.0f;
+    p.neg_rate_f = static_cast<float>(neg_rate);
+    p.rep = repulsion;
+    p.seed = seed;
+    inverse_sgd_kernel<<<grid, 256, 0, s>>>(p);
     UMAPB_LAUNCH_CHECK();
 }
 
