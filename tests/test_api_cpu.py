@@ -222,6 +222,17 @@ def test_supervised_target_checks_run_before_the_device():
         Umap(target_metric="categorical", target_weight=2.0)
 
 
+def test_inverse_transform_needs_a_fit():
+    # inverse_transform_requires_fit (rust_umap/src/lib.rs:6366-6374) and the
+    # facade's out= check (_api.py:866-871), before any device work
+    with pytest.raises(RuntimeError, match="model is not fitted yet"):
+        Umap().inverse_transform(np.array([[0.1, 0.2]], np.float32))
+    with pytest.raises(RuntimeError, match="model must be fit before inverse_transform"):
+        Umap().inverse_transform(np.zeros((1, 2), np.float32), out=np.zeros((1, 3), np.float32))
+    with pytest.raises(RuntimeError, match="model is not fitted yet"):
+        UmapCore().inverse_transform(np.zeros((1, 2), np.float32))
+
+
 def test_metrics_outside_the_engine_are_rejected_at_fit():
     x = workloads.reference_synthetic(40, 6)
     with pytest.raises(ValueError, match="not supported by the B200 engine"):
