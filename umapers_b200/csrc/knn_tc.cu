@@ -147,7 +147,6 @@ struct TcArgs {
     int64_t n_q;
     int64_t n_r;
     int kb;          // k-blocks of 64 columns
-    int ks_last;     // k-steps of 16 columns holding data in the last k-block
     int64_t n_units;      // work units: (group of MT query tiles, candidate split)
     int n_split;          // candidate splits per group (1 unless query tiles are few)
     int64_t split_tiles;  // candidate tiles per split (the last split may hold fewer)
@@ -183,21 +182,7 @@ __device__ __forceinline__ int32_t tile_at(int32_t t, const Unit& w) {
     return w.begin + (c >= w.len ? c - w.len : c);
 }
 
-// One k-block's MMAs for every query tile, fully unrolled: NKS k-steps of 16
-// columns, `first` zeroing the accumulators at the tile's first k-step.  One
-// thread issues all MMAs, and a loop with a runtime trip count issues them
-// more slowly than the tensor pipe retires 128 x 128 x 16 steps (64 cycles).
 constexpr uint32_t kTileDesc = kTileBytes >> 4;  // one 16 KiB tile in descriptor units
-template <int NKS, int MT>
-__device__ __forceinline__ void issue_kblock(uint32_t dcol, uint64_t da, uint32_t da_tile,
-                                             uint64_t db, bool first) {
-#pragma unroll
-    for (int ks = 0; ks < NKS; ++ks)
-#pragma unroll
-        for (int mt = 0; mt < MT; ++mt)
-            umma_bf16(dcol + mt * BN, da + mt * da_tile + 2 * ks, db + 2 * ks, kIdesc,
-                      (first && ks == 0) ? 0u : 1u);
-}
 
 // Threads: warp 0 TMA, warp 1 MMA, then 8 epilogue warps per query tile.
 template <int MT>
@@ -297,9 +282,8 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
             uint64_t it = 0, cg = 0;
             int64_t u_iter = 0;
             bool ok = true;
-            // descriptors advance by address / 16: per k-block, per ring stage, per query tile
-            const uint64_t dA0 = desc_sw128(sA), dB0 = desc_sw128(sB);
-            const uint32_t dA_tile = static_cast<uint32_t>(KB) * kTileDesc;
+            // ring-stage descriptors advance by address / 16
+            const uint64_t dB0 = desc_sw128(sB);
             for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x, ++u_iter) {
                 if (!mbar_wait(b_afull, static_cast<uint32_t>(u_iter & 1), abort_flag)) {
                     fail(3);
@@ -326,19 +310,20 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
                             break;
                         }
                         fence_after();
-                        const uint64_t da = dA0 + static_cast<uint64_t>(kb) * kTileDesc;
-                        const uint64_t db = dB0 + static_cast<uint64_t>(stage) * kTileDesc;
-                        // the columns past 3d + 7 are zero: their k-steps are skipped
-                        const int n_ks = kb == KB - 1 ? p.ks_last : BK / UK;
-                        const bool first = kb == 0;
-                        if (n_ks == 4)
-                            issue_kblock<4, MT>(dcol, da, dA_tile, db, first);
-                        else if (n_ks == 3)
-                            issue_kblock<3, MT>(dcol, da, dA_tile, db, first);
-                        else if (n_ks == 2)
-                            issue_kblock<2, MT>(dcol, da, dA_tile, db, first);
-                        else
-                            issue_kblock<1, MT>(dcol, da, dA_tile, db, first);
+                        // All four k-steps of every k-block, the zero columns past
+                        // 3d + 7 included (they add exact zeros): a loop of constant
+                        // trip count keeps the tensor pipe fed, skipping them does not.
+                        const uint64_t db0 = dB0 + static_cast<uint64_t>(stage) * kTileDesc;
+#pragma unroll
+                        for (int ks = 0; ks < BK / UK; ++ks) {
+#pragma unroll
+                            for (int mt = 0; mt < MT; ++mt) {
+                                const uint64_t da =
+                                    desc_sw128(sA + (mt * KB + kb) * kTileBytes) + 2 * ks;
+                                umma_bf16(dcol + mt * BN, da, db0 + 2 * ks, kIdesc,
+                                          (kb | ks) != 0 ? 1u : 0u);
+                            }
+                        }
                         umma_commit(b_empty + 8 * stage);
                     }
                     if (ok) umma_commit(b_tfull + 8 * buf);
@@ -684,7 +669,6 @@ TcArgs plan(int64_t n_q, int64_t n_r, int d, bool allow_split) {
     a.n_q = n_q;
     a.n_r = n_r;
     a.kb = kp / BK;
-    a.ks_last = static_cast<int>(ceil_div(3 * d + 7 - (a.kb - 1) * BK, UK));
     a.n_ctiles = ceil_div(n_r, BN);
     const int mt = query_tiles_for(a.kb);
     const int64_t groups = ceil_div(n_q, static_cast<int64_t>(BM) * mt);
@@ -935,7 +919,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     UMAPB_CUDA(cudaEventCreate(&e1));
     UMAPB_CUDA(cudaEventRecord(e0, s));
     if (mt == 2)
-        launch_tc<2, 5>(ma, mb, a, s);
+        launch_tc<2, 4>(ma, mb, a, s);
     else
         launch_tc<1, 3>(ma, mb, a, s);
     UMAPB_CUDA(cudaEventRecord(e1, s));
@@ -1067,7 +1051,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     a.lists = lists;
     a.err = flags;
     if (mt == 2)
-        launch_tc<2, 5>(ma, mb, a, s);
+        launch_tc<2, 4>(ma, mb, a, s);
     else
         launch_tc<1, 3>(ma, mb, a, s);
     int flags_h[2] = {0, 0};
