@@ -715,13 +715,15 @@ void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, fl
     transform_from_knn_device(m, idx.get(), dist.get(), nq, k, epoch_rows, out_dev);
 }
 
+void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
+                        const uint8_t* flags, int64_t nf);
+
 // Surrogate transform of device rows: network outputs for every row, then
 // (use_fallback) the plain transform for the rows the gate rejects.
 void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d,
                                 bool use_fallback, float* out, uint8_t* flags_out,
                                 int64_t* n_fallback) {
     cudaStream_t s = m->stream;
-    const int dim = static_cast<int>(m->p.n_components);
     DevBuf<uint8_t> own;
     uint8_t* flags = flags_out;
     if (!flags) {
@@ -730,7 +732,15 @@ void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int
     }
     const int64_t nf = surrogate_infer(*m->surrogate, Qd, nq, static_cast<int>(d), out, flags, s);
     if (n_fallback) *n_fallback = nf;
-    if (!use_fallback || nf == 0) return;
+    if (use_fallback) surrogate_fallback(m, Qd, nq, d, out, flags, nf);
+}
+
+// The plain transform for the `nf` rows the gate flagged, scattered into out.
+void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
+                        const uint8_t* flags, int64_t nf) {
+    if (nf == 0) return;
+    cudaStream_t s = m->stream;
+    const int dim = static_cast<int>(m->p.n_components);
     DevBuf<int32_t> ids(nf, s);
     select_flagged(flags, nq, ids.get(), s);
     DevBuf<float> sub(nf * d, s), sub_out(nf * dim, s);
@@ -753,6 +763,31 @@ void check_transform(umapb_model* m, int64_t n_cols) {
     if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
     (void)n_cols;
 }
+
+// Rows per upload chunk of a host surrogate transform (64 MB at 128 features).
+constexpr int64_t kUploadChunkRows = 131072;
+
+// A copy stream with one completion event per chunk.  Its destructor waits
+// for every copy issued on it, so buffers it writes outlive its work.
+struct CopyStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ready = nullptr;
+    std::vector<cudaEvent_t> done;
+    explicit CopyStream(int64_t n) : done(static_cast<size_t>(n), nullptr) {
+        UMAPB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        UMAPB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        for (auto& e : done) UMAPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    CopyStream(const CopyStream&) = delete;
+    CopyStream& operator=(const CopyStream&) = delete;
+    ~CopyStream() {
+        if (s) cudaStreamSynchronize(s);
+        for (auto e : done)
+            if (e) cudaEventDestroy(e);
+        if (ready) cudaEventDestroy(ready);
+        if (s) cudaStreamDestroy(s);
+    }
+};
 
 }  // namespace
 
@@ -1497,13 +1532,37 @@ int32_t umapb_surrogate_transform(umapb_model* m, const float* query, int64_t n_
         m->ensure_device();
         cudaStream_t s = m->stream;
         const int64_t dim = m->p.n_components;
-        DevBuf<float> Q, outd(n_rows * dim, s);
+        DevBuf<float> Q(n_rows * n_cols, s), outd(n_rows * dim, s);
         DevBuf<uint8_t> fl(n_rows, s);
-        upload(Q, query, n_rows * n_cols, s);
-        const int64_t bad = first_nonfinite_row(Q.get(), n_rows, static_cast<int>(n_cols), s);
-        if (bad != INT64_MAX) invalid("input contains non-finite value at row " + std::to_string(bad));
-        surrogate_transform_device(m, Q.get(), n_rows, n_cols, use_fallback != 0, outd.get(),
-                                   fl.get(), n_fallback);
+        // The rows go up in chunks on a second stream, and the model's stream
+        // checks and infers each chunk as soon as it has landed, so the copy
+        // of the next chunk overlaps the network on this one.  The guard
+        // waits for every copy before Q can be freed, errors included.
+        const int64_t chunk = n_rows >= 4 * kUploadChunkRows ? kUploadChunkRows : n_rows;
+        const int64_t n_chunks = ceil_div(n_rows, chunk);
+        CopyStream cs(n_chunks);
+        UMAPB_CUDA(cudaEventRecord(cs.ready, s));  // Q is allocated on s
+        UMAPB_CUDA(cudaStreamWaitEvent(cs.s, cs.ready, 0));
+        for (int64_t c = 0; c < n_chunks; ++c) {
+            const int64_t r0 = c * chunk, rows = std::min(chunk, n_rows - r0);
+            UMAPB_CUDA(cudaMemcpyAsync(Q.get() + r0 * n_cols, query + r0 * n_cols,
+                                       rows * n_cols * 4, cudaMemcpyHostToDevice, cs.s));
+            UMAPB_CUDA(cudaEventRecord(cs.done[c], cs.s));
+        }
+        int64_t nf = 0;
+        for (int64_t c = 0; c < n_chunks; ++c) {
+            const int64_t r0 = c * chunk, rows = std::min(chunk, n_rows - r0);
+            UMAPB_CUDA(cudaStreamWaitEvent(s, cs.done[c], 0));
+            const int64_t bad =
+                first_nonfinite_row(Q.get() + r0 * n_cols, rows, static_cast<int>(n_cols), s);
+            if (bad != INT64_MAX)
+                invalid("input contains non-finite value at row " + std::to_string(r0 + bad));
+            nf += surrogate_infer(*m->surrogate, Q.get() + r0 * n_cols, rows,
+                                  static_cast<int>(n_cols), outd.get() + r0 * dim,
+                                  fl.get() + r0, s);
+        }
+        if (n_fallback) *n_fallback = nf;
+        if (use_fallback != 0) surrogate_fallback(m, Q.get(), n_rows, n_cols, outd.get(), fl.get(), nf);
         UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * dim * 4, cudaMemcpyDeviceToHost, s));
         if (fallback)
             UMAPB_CUDA(cudaMemcpyAsync(fallback, fl.get(), n_rows, cudaMemcpyDeviceToHost, s));
