@@ -17,7 +17,9 @@ import re
 import sys
 from pathlib import Path
 
-ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    raise SystemExit("usage: python tests/golden/make_pins.py <reference checkout>")
+ref = Path(sys.argv[1])
 src = (ref / "rust_umap/src/lib.rs").read_text()
 lines = src.splitlines()
 

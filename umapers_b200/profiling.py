@@ -8,7 +8,8 @@
 Each case runs once untimed, then once inside an NVTX range named after the
 case, so a profiler can be limited to the measured launches, e.g.
 
-    ncu --nvtx --nvtx-include "knn_tc/" -k regex:tc_knn_kernel -c 1 ...
+    ncu --clock-control none --nvtx --nvtx-include "knn_tc/" \
+        -k regex:tc_knn_kernel -c 1 ...
 
 and prints the wall time of the measured run.  Inputs are the seeded
 synthetic mixtures of ``umapers_b200.workloads``; the cases are sized to stay
