@@ -30,7 +30,7 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define UMAPB_ABI_VERSION 1
+#define UMAPB_ABI_VERSION 2
 
 typedef enum umapb_status {
     UMAPB_OK = 0,
@@ -134,6 +134,7 @@ typedef struct umapb_fit_info {
     int64_t n_components_graph;   /* connected components of the fuzzy graph */
     double knn_kernel_sec;        /* dominant kNN kernel, CUDA events */
     double sgd_edge_samples;      /* attractive edge samples over all epochs */
+    int64_t knn_second_pass_rows; /* rows the first tensor-core pass could not certify */
 } umapb_fit_info;
 
 typedef struct umapb_model umapb_model;

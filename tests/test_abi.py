@@ -28,7 +28,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_and_defaults():
     lib = _lib.load()
-    assert lib.umapb_abi_version() == 1
+    assert lib.umapb_abi_version() == 2
     assert lib.umapb_version().decode().startswith("1.1.4")
     p = _lib.Params()
     lib.umapb_params_default(ctypes.byref(p))

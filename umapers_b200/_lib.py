@@ -109,6 +109,7 @@ class FitInfo(ctypes.Structure):
         ("n_components_graph", ctypes.c_int64),
         ("knn_kernel_sec", ctypes.c_double),
         ("sgd_edge_samples", ctypes.c_double),
+        ("knn_second_pass_rows", ctypes.c_int64),
     ]
 
 

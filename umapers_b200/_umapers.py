@@ -299,6 +299,7 @@ class UmapCore:
             "n_edges": int(info.n_edges),
             "knn_backend": backend,
             "knn_fallback_rows": int(info.knn_fallback_rows),
+            "knn_second_pass_rows": int(info.knn_second_pass_rows),
             "knn_kernel_sec": float(info.knn_kernel_sec),
             "n_graph_components": int(info.n_components_graph),
             "sgd_edge_samples": float(info.sgd_edge_samples),

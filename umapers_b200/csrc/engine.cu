@@ -317,7 +317,8 @@ struct FitOutputs {
 // Exact kNN on the device (exact_nearest_neighbors{,_to_reference}).
 void knn_exact_device(const float* Q, int64_t nq, const float* R, int64_t nr, int d, int k,
                       int metric, int backend, int32_t* idx, float* dist, int64_t* fallback,
-                      double* kernel_sec, int32_t* backend_used, cudaStream_t s) {
+                      double* kernel_sec, int32_t* backend_used, cudaStream_t s,
+                      int64_t* second_pass = nullptr) {
     const bool use_tc = backend == UMAPB_KNN_TENSOR ||
                         (backend == UMAPB_KNN_AUTO && knn_tc_supported(d, k, metric));
     if (backend == UMAPB_KNN_TENSOR && !knn_tc_supported(d, k, metric))
@@ -326,6 +327,7 @@ void knn_exact_device(const float* Q, int64_t nq, const float* R, int64_t nr, in
         TcKnnStats st;
         knn_tc(Q, nq, R, nr, d, k, metric, idx, dist, &st, s);
         if (fallback) *fallback = st.fallback_rows;
+        if (second_pass) *second_pass = st.second_pass_rows;
         if (kernel_sec) *kernel_sec = st.kernel_ms * 1e-3;
         if (backend_used) *backend_used = UMAPB_KNN_TENSOR;
         return;
@@ -354,6 +356,7 @@ void knn_exact_device(const float* Q, int64_t nq, const float* R, int64_t nr, in
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (fallback) *fallback = 0;
+    if (second_pass) *second_pass = 0;
     if (kernel_sec) *kernel_sec = ms * 1e-3;
     if (backend_used) *backend_used = UMAPB_KNN_PLAIN;
 }
@@ -455,13 +458,14 @@ void fit_device(umapb_model* m, const float* Xd, int64_t n, int64_t d, bool copy
                   dist.get(), s);
         if (out) out->info.knn_backend_used = -1;
     } else {
-        int64_t fb = 0;
+        int64_t fb = 0, second = 0;
         double ks = 0.0;
         int32_t used = 0;
         knn_exact_device(X, n, X, n, static_cast<int>(d), k, p.metric, p.knn_backend, idx.get(),
-                         dist.get(), &fb, &ks, &used, s);
+                         dist.get(), &fb, &ks, &used, s, &second);
         if (out) {
             out->info.knn_fallback_rows = fb;
+            out->info.knn_second_pass_rows = second;
             out->info.knn_kernel_sec = ks;
             out->info.knn_backend_used = used;
         }

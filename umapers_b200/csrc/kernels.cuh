@@ -32,17 +32,20 @@ void knn_plain(const float* Q, const int32_t* q_rows, int64_t n_q, const float* 
 
 // ------------------------------------------------------------- knn_tc.cu
 struct TcKnnStats {
-    int64_t fallback_rows = 0;
-    float kernel_ms = 0.0f;   // distance-GEMM + select kernel, CUDA events
+    int64_t fallback_rows = 0;     // rows recomputed on the plain path
+    int64_t second_pass_rows = 0;  // rows the first tensor-core pass could not certify
+    float kernel_ms = 0.0f;        // distance-GEMM + select kernels, CUDA events
     int64_t shortlist = 0;
 };
 
 // True when the tcgen05 path supports this shape on the current device.
 bool knn_tc_supported(int d, int k, int metric);
 
-// Exact kNN through BF16 split tensor-core tiles with a certified shortlist
-// and an FP32 re-rank in reference order; rows whose shortlist cannot be
-// certified are recomputed by knn_plain.  Q may equal R (self join).
+// Exact kNN (euclidean or cosine) through FP16 tensor-core tiles with a
+// certified shortlist and an FP32 re-rank in reference order; rows whose
+// shortlist cannot be certified run a second pass with more lists per row,
+// and rows that still fail are recomputed by knn_plain.  Q may equal R
+// (self join).
 void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int k, int metric,
             int32_t* out_idx, float* out_dist, TcKnnStats* stats, cudaStream_t s);
 

@@ -1,49 +1,60 @@
 // knn_tc.cu - exact kNN through tcgen05 tensor-core distance tiles.
 //
 // Replaces exact_nearest_neighbors{,_to_reference} (rust_umap/src/lib.rs:
-// 2863-2928, 3346-3399) for euclidean rows with the same result as the
-// reference, bit for bit, in three steps:
+// 2863-2928, 3346-3399) and exact_nearest_neighbors_cosine (lib.rs:2874-2889)
+// for dense rows with the same result as the reference, bit for bit:
 //
-// 1. prep: every row x becomes two BF16 operand rows of K' (a multiple of 64)
-//    columns.  With h = bf16(x), l = bf16(x - h), n = |x|^2 (FP32):
-//        A = [-2h | -2h | -2l | split3((1-c2) n) | 1 1 1 | bf16(-c1 sqrt n) | 0...]
-//        B = [  h |   l |   h | 1 1 1 | split3((1-c2) n) | bf16(sqrt n)     | 0...]
-//    so one GEMM gives L_ij = n_i + n_j - 2 x_i.x_j - e_ij, a certified lower
-//    bound of the reference's FP32 squared distance d_ij, where
-//    e_ij = c1 sqrt(n_i n_j) + c2 (n_i + n_j) bounds the BF16 split error
-//    (3.02 * 2^-16 per product, doubled), the FP32 accumulation of K' terms,
-//    and the reference's own FP32 rounding (see kBoundC1/kBoundC2 below).
+// 1. prep: every row becomes one FP16 operand row of K' = round_up(d + 6, 16)
+//    columns.  Euclidean rows are first multiplied by a power of two s (the
+//    same for every row, exact) that keeps the largest squared norm at or
+//    below 2^15; cosine rows are divided by their L2 norm.  With h = fp16(row)
+//    and a_i, b_j per-row terms split into three FP16 parts,
+//        A = [alpha h | 1 1 1 | split3(a_i) | 0...]
+//        B = [      h | split3(b_j) | 1 1 1 | 0...]
+//    one GEMM gives L_ij = alpha h_i.h_j + a_i + b_j (alpha = -2, a = (1-c) n -
+//    c0/2 for euclidean; alpha = -1, a = 1 - c0, b = 0 for cosine), a
+//    certified LOWER bound of the reference's FP32 distance (scaled by s^2).
+//    FP16 keeps 11 significant bits, so one product term h_i.h_j is within
+//    2^-10 |x||y| of x.y; c and c0 also cover FP32 accumulation, the FP32
+//    norms, the FP16 subnormal range and the reference's own rounding (see
+//    bound_for).  By |x||y| <= (|x|^2 + |y|^2) / 2 the bound separates into a
+//    row term and a column term, so it folds into the operands.
 // 2. tc_knn_kernel: a persistent, warp-specialised tcgen05 kernel.  A CTA
 //    keeps MT query tiles of 128 rows of A resident in shared memory, streams
-//    128-row candidate tiles of B through a TMA ring (SWIZZLE_128B, no
-//    multicast), and one thread issues tcgen05.mma (kind::f16, BF16 in, FP32
-//    accumulate) into double-buffered TMEM accumulators.  Eight epilogue
-//    warps per query tile each own 32 rows x 64 columns of the accumulator:
-//    they read it with tcgen05.ld and keep, per (row, column half), the
-//    S = 32 smallest (L, index) keys in a global list.  A per-list threshold
-//    skips a row's 64 columns with one vote in the common case; otherwise the
-//    row's values are transposed across the warp through a shared-memory
-//    scratch and its qualifying keys are inserted cooperatively (one list
-//    entry per lane), while the next pending row's list is already being
-//    loaded.  When the query tiles are fewer than the SMs, the candidate
-//    tiles are split too (one wave of units), with lists per split.  A self
-//    kNN over at least one wave of query groups first regroups its rows by
-//    nearest pivot ("cell order" below), and each group starts its candidate
-//    walk at its own cell, so the lists fill with near candidates first.
+//    BN-row candidate tiles of B through a TMA ring (SWIZZLE_128B, no
+//    multicast), and one thread issues 128 x BN x 16 tcgen05.mma (kind::f16,
+//    FP16 in, FP32 accumulate) into double-buffered TMEM accumulators.  One
+//    epilogue warp per (TMEM lane quarter, query tile, 64-column group) owns
+//    32 rows x 64 columns of the accumulator: it reads them with tcgen05.ld
+//    and keeps, per (row, 64-column group), the S = 32 smallest (L, index)
+//    keys in a global list.  A per-list threshold skips a row's 64 columns
+//    with one vote in the common case; otherwise the row's values are
+//    transposed across the warp through a shared-memory scratch and its
+//    qualifying keys are inserted cooperatively (one list entry per lane),
+//    while the next pending row's list is already being loaded.  When the
+//    query tiles are fewer than the SMs, the candidate tiles are split too
+//    (one wave of units), with lists per split.  A self kNN over at least one
+//    wave of query groups first regroups its rows by nearest pivot ("cell
+//    order" below), and each group starts its candidate walk at its own
+//    cell, so the lists fill with near candidates first.
 // 3. rerank: one warp per row recomputes exact FP32 distances in the
 //    reference's summation order and keeps the k smallest (distance, index)
 //    keys.  With U_j = L_j + 2 e_j and B the smallest largest-L of the full
 //    lists, every candidate missing from the lists has d >= B, so the row is
 //    certified when at least k candidates have U < B.  Only listed candidates
 //    with L <= T, T the k-th smallest U, can rank in the top k, so only they
-//    are recomputed.  Rows that fail (near-ties wider than the bound) are
-//    recomputed by knn_plain.
+//    are recomputed.
+// 4. Rows that fail (near-ties wider than the bound, or too few listed
+//    candidates below B) run a second pass as a query set with at least two
+//    candidate splits, i.e. twice as many lists per row; rows that still fail
+//    (duplicates beyond the lists, zero cosine rows) are recomputed by
+//    knn_plain.
 //
 // Every wait on an mbarrier is bounded by a %globaltimer deadline; a timeout
 // sets an error word, stops all roles, drains in-flight copies and frees TMEM.
 #include <cub/cub.cuh>
 #include <cuda.h>
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -58,23 +69,69 @@ namespace {
 using namespace tc;
 
 constexpr int BM = 128;     // query rows per tile (UMMA M)
-constexpr int BN = 128;     // candidate rows per tile (UMMA N)
-constexpr int BK = kBK;     // bf16 columns per k-block (one 128-byte swizzle row)
+constexpr int BK = kBK;     // FP16 columns per k-block (one 128-byte swizzle row)
 constexpr int UK = kUK;     // K of one tcgen05.mma kind::f16
-constexpr int S = 32;       // shortlist length per row
-constexpr int kTileBytes = BM * BK * 2;  // 16 KiB
-constexpr int kBarBytes = 256;           // mbarriers, TMEM address, abort flag
-constexpr int kScratchBytes = 256;       // per epilogue warp: one row's 64 values
-constexpr uint32_t kIdesc = idesc_bf16(BM, BN);
+constexpr int S = 32;       // shortlist length per list
+constexpr int kATileBytes = BM * BK * 2;  // 16 KiB: one query tile's k-block
+constexpr int kBarBytes = 256;            // mbarriers, TMEM address, abort flag
+constexpr int kScratchBytes = 256;        // per epilogue warp: one row's 64 values
+constexpr int kNormCols = 6;              // 3 + 3 FP16 columns of the folded row terms
+constexpr int kMaxStages = 8;
+constexpr size_t kSmemLimit = 227 * 1024;
 
-// Bound constants (see header comment).  c1 covers the split products
-// (2 * 3.02 * 2^-16) with 2% slack for the BF16 rounding of the bound term;
-// c2 = (K' + D + 8) * 2^-22 covers the FP32 accumulation of the GEMM and the
-// FP32 rounding of the norms and of the reference distance.
-constexpr double kBoundC1 = 1.02 * 2.0 * 3.02 / 65536.0;
+// Operand geometry for d features: K' columns used by the MMA (kmma), the
+// stored row length (at least one 64-column block), k-blocks, and the k-steps
+// of 16 columns issued in the last k-block.
+struct Geom {
+    int kmma, kst, kb, tail;
+};
+inline Geom geom(int d) {
+    Geom g;
+    g.kmma = ((d + kNormCols + UK - 1) / UK) * UK;
+    g.kst = std::max(g.kmma, BK);
+    g.kb = (g.kmma + BK - 1) / BK;
+    g.tail = (g.kmma - BK * (g.kb - 1)) / UK;
+    return g;
+}
 
-inline int padded_k(int d) { return ((3 * d + 7 + BK - 1) / BK) * BK; }
-inline double bound_c2(int d) { return (padded_k(d) + d + 8) * std::ldexp(1.0, -22); }
+// Error bound of one GEMM entry against the reference's FP32 distance, in
+// the scaled units of the GEMM: e_ij = c (n_i + n_j) + c0 for euclidean (n the
+// scaled FP32 squared norms), e = c0 for cosine.  Terms (u = 2^-11 the FP16
+// unit roundoff, eta = 2^-25 half the FP16 subnormal spacing):
+//   2u + u^2            the one-term FP16 product, |x||y| <= (n_i + n_j) / 2
+//   2.01 K' 2^-23       FP32 accumulation of K' terms (truncating adders)
+//   d 2^-24             the FP32 norms
+//   2 (d + 16) 2^-24    the reference's FP32 sum and subtractions (d <= 2(n_i + n_j))
+//   2 eta sqrt(d)       FP16 subnormals (absolute part in c0)
+//   2^-23               the FP32 rounding of the folded row terms
+// with 25% slack on the sum.
+struct Bound {
+    double c, c0;
+};
+inline Bound bound_for(int d, int kmma, bool cosine) {
+    const double u = std::ldexp(1.0, -11), eta = std::ldexp(1.0, -25);
+    const double sd = std::sqrt(static_cast<double>(d));
+    Bound b;
+    if (!cosine) {
+        b.c = 1.25 * (2.0 * u + u * u + 2.01 * kmma * std::ldexp(1.0, -23) +
+                      d * std::ldexp(1.0, -24) + 2.0 * (d + 16) * std::ldexp(1.0, -24) +
+                      2.0 * eta * sd * 1.01 + std::ldexp(1.0, -23));
+        b.c0 = 2.0 * (4.1 * eta * sd + 6.0 * eta);
+    } else {
+        // unit rows: |x^.y^ - cos| <= (2u + u^2)(1 + d 2^-23) + subnormals,
+        // |cos_ref - cos| <= (2d + 16) 2^-24 (dot, norms, product, division)
+        b.c = 0.0;
+        b.c0 = 1.25 * (2.0 * u + u * u + 4.0 * eta * sd +
+                       (3.0 * d + 2.01 * kmma + 16.0) * std::ldexp(1.0, -23)) +
+               12.0 * eta;
+    }
+    return b;
+}
+
+// The power-of-two scale of euclidean rows: s = 2^e, s^2 = 2^(2e).
+struct ScaleInfo {
+    float s, s2;
+};
 
 // order-preserving map of a float to uint32 (negative values included)
 __device__ __forceinline__ uint32_t f2o(float f) {
@@ -137,22 +194,23 @@ __device__ __forceinline__ uint64_t warp_merge_keys(uint64_t list, uint64_t keys
 // pass instead of key by key (about 6 sequential insertions cost as much).
 constexpr int kBulkMergeMin = 6;
 
-// CTAs begin their candidate range at staggered tiles (16 groups, 4 tiles
-// apart: a window of 4 MiB of B at K' = 256, L2-resident) so they do not all
-// request the same tile at once.  The shortlist certificate does not depend
-// on the visiting order.
-constexpr int32_t kStaggerGroups = 16, kStaggerStep = 4;
+// CTAs begin their candidate range at staggered tiles (16 groups, 2 tiles
+// apart) so they do not all request the same tile at once.  The shortlist
+// certificate does not depend on the visiting order.
+constexpr int32_t kStaggerGroups = 16, kStaggerStep = 2;
 
 struct TcArgs {
     int64_t n_q;
     int64_t n_r;
-    int kb;          // k-blocks of 64 columns
+    int kb;               // k-blocks of 64 columns
+    int tail;             // k-steps issued in the last k-block (1..4)
+    int st;               // stages of the candidate ring
     int64_t n_units;      // work units: (group of MT query tiles, candidate split)
     int n_split;          // candidate splits per group (1 unless query tiles are few)
     int64_t split_tiles;  // candidate tiles per split (the last split may hold fewer)
     int64_t n_ctiles;     // candidate tiles
-    uint64_t* lists;      // n_q x n_split x 2 x S keys (L order-mapped << 32 | index), one
-                          // list per (row, candidate split, half of each tile's columns)
+    uint64_t* lists;      // n_q x n_split x (BN / 64) x S keys (L order-mapped << 32 |
+                          // index), one list per (row, candidate split, 64-column group)
     const int32_t* start_tile;  // per query group, the first candidate tile to visit (rows in
                                 // cell order, one split), or null for the staggered start
     int* err;
@@ -182,23 +240,32 @@ __device__ __forceinline__ int32_t tile_at(int32_t t, const Unit& w) {
     return w.begin + (c >= w.len ? c - w.len : c);
 }
 
-constexpr uint32_t kTileDesc = kTileBytes >> 4;  // one 16 KiB tile in descriptor units
+// Kernel shapes: MT query tiles of 128 rows share each BN-row candidate tile;
+// 2 TMEM buffers of MT x BN columns; one epilogue warp per (TMEM lane quarter,
+// query tile, 64-column group).
+template <int MT, int BN>
+constexpr int epi_warps() { return 4 * MT * (BN / 64); }
+template <int MT, int BN>
+constexpr int tc_threads() { return 64 + 32 * epi_warps<MT, BN>(); }
 
-// Threads: warp 0 TMA, warp 1 MMA, then 8 epilogue warps per query tile.
-template <int MT>
-constexpr int tc_threads() { return 64 + 256 * MT; }
-
-template <int MT, int ST>
-__global__ void __launch_bounds__(tc_threads<MT>(), 1)
+template <int MT, int BN>
+__global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
     tc_knn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                   TcArgs p) {
+    static_assert(MT * BN <= 256 && (BN == 128 || BN == 256), "at most 512 TMEM columns");
+    constexpr int kEpiWarps = epi_warps<MT, BN>();
+    constexpr int kBTileBytes = BN * BK * 2;
+    constexpr uint32_t kIdesc = idesc_f16(BM, BN);
+    constexpr uint32_t kBDesc = kBTileBytes >> 4;  // one ring stage in descriptor units
+    constexpr int GPT = BN / 64;                   // lists per candidate tile
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-    const int KB = p.kb;
+    const int KB = p.kb, TAIL = p.tail, ST = p.st;
     const uint32_t sA = smem_u32(smem);
-    const uint32_t sB = sA + MT * KB * kTileBytes;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + MT * KB * kTileBytes + ST * kTileBytes);
+    const uint32_t sB = sA + MT * KB * kATileBytes;
+    uint64_t* bars =
+        reinterpret_cast<uint64_t*>(smem + MT * KB * kATileBytes + ST * kBTileBytes);
     const uint32_t b_full = smem_u32(bars);
     const uint32_t b_empty = b_full + 8 * ST;
     const uint32_t b_tfull = b_empty + 8 * ST;
@@ -210,7 +277,7 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_holder + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr uint32_t kTmemCols = MT == 2 ? 512 : 256;
+    constexpr uint32_t kTmemCols = 2 * MT * BN;  // 256 or 512: a power of two
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < ST; ++s) {
@@ -219,7 +286,7 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(b_tfull + 8 * b, 1);
-            mbar_init(b_tempty + 8 * b, 8 * MT);
+            mbar_init(b_tempty + 8 * b, kEpiWarps);
         }
         mbar_init(b_afull, 1);
         mbar_init(b_aempty, 1);
@@ -243,7 +310,8 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
     if (warp == 0) {
         // ------------------------------------------------ TMA producer
         if (lane == 0) {
-            uint64_t it = 0;
+            int stage = 0;
+            uint32_t phase = 0;
             int64_t u_iter = 0;
             for (int64_t unit = blockIdx.x; unit < p.n_units && !*abort_flag;
                  unit += gridDim.x, ++u_iter) {
@@ -253,24 +321,27 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
                     break;
                 }
                 const Unit w = unit_of(p, unit);
-                mbar_expect_tx(b_afull, MT * KB * kTileBytes);
+                mbar_expect_tx(b_afull, MT * KB * kATileBytes);
                 for (int mt = 0; mt < MT; ++mt)
                     for (int kb = 0; kb < KB; ++kb)
-                        tma_load_2d(sA + (mt * KB + kb) * kTileBytes, &tmA, b_afull, kb * BK,
+                        tma_load_2d(sA + (mt * KB + kb) * kATileBytes, &tmA, b_afull, kb * BK,
                                     static_cast<int>((w.group * MT + mt) * BM));
                 bool ok = true;
                 for (int32_t c = 0; c < w.len && ok; ++c) {
-                    for (int kb = 0; kb < KB; ++kb, ++it) {
-                        const int stage = static_cast<int>(it % ST);
-                        const uint32_t round = static_cast<uint32_t>(it / ST);
-                        if (!mbar_wait(b_empty + 8 * stage, (round & 1) ^ 1, abort_flag)) {
+                    const int ty = static_cast<int>(tile_at(c, w) * BN);
+                    for (int kb = 0; kb < KB; ++kb) {
+                        if (!mbar_wait(b_empty + 8 * stage, phase ^ 1, abort_flag)) {
                             fail(2);
                             ok = false;
                             break;
                         }
-                        mbar_expect_tx(b_full + 8 * stage, kTileBytes);
-                        tma_load_2d(sB + stage * kTileBytes, &tmB, b_full + 8 * stage, kb * BK,
-                                    static_cast<int>(tile_at(c, w) * BN));
+                        mbar_expect_tx(b_full + 8 * stage, kBTileBytes);
+                        tma_load_2d(sB + stage * kBTileBytes, &tmB, b_full + 8 * stage, kb * BK,
+                                    ty);
+                        if (++stage == ST) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                 }
                 if (!ok) break;
@@ -279,10 +350,11 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
     } else if (warp == 1) {
         // ------------------------------------------------- MMA issuer
         if (lane == 0) {
-            uint64_t it = 0, cg = 0;
+            int stage = 0;
+            uint32_t phase = 0;
+            uint64_t cg = 0;
             int64_t u_iter = 0;
             bool ok = true;
-            // ring-stage descriptors advance by address / 16
             const uint64_t dB0 = desc_sw128(sB);
             for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x, ++u_iter) {
                 if (!mbar_wait(b_afull, static_cast<uint32_t>(u_iter & 1), abort_flag)) {
@@ -301,30 +373,32 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
                     }
                     fence_after();
                     const uint32_t dcol = tmem_base + buf * (MT * BN);
-                    for (int kb = 0; kb < KB; ++kb, ++it) {
-                        const int stage = static_cast<int>(it % ST);
-                        if (!mbar_wait(b_full + 8 * stage, static_cast<uint32_t>((it / ST) & 1),
-                                       abort_flag)) {
+                    for (int kb = 0; kb < KB; ++kb) {
+                        if (!mbar_wait(b_full + 8 * stage, phase, abort_flag)) {
                             fail(5);
                             ok = false;
                             break;
                         }
                         fence_after();
-                        // All four k-steps of every k-block, the zero columns past
-                        // 3d + 7 included (they add exact zeros): a loop of constant
-                        // trip count keeps the tensor pipe fed, skipping them does not.
-                        const uint64_t db0 = dB0 + static_cast<uint64_t>(stage) * kTileDesc;
+                        const int steps = kb + 1 < KB ? BK / UK : TAIL;
+                        const uint64_t db0 = dB0 + static_cast<uint64_t>(stage) * kBDesc;
 #pragma unroll
                         for (int ks = 0; ks < BK / UK; ++ks) {
+                            if (ks < steps) {
 #pragma unroll
-                            for (int mt = 0; mt < MT; ++mt) {
-                                const uint64_t da =
-                                    desc_sw128(sA + (mt * KB + kb) * kTileBytes) + 2 * ks;
-                                umma_bf16(dcol + mt * BN, da, db0 + 2 * ks, kIdesc,
-                                          (kb | ks) != 0 ? 1u : 0u);
+                                for (int mt = 0; mt < MT; ++mt) {
+                                    const uint64_t da =
+                                        desc_sw128(sA + (mt * KB + kb) * kATileBytes) + 2 * ks;
+                                    umma_bf16(dcol + mt * BN, da, db0 + 2 * ks, kIdesc,
+                                              (kb | ks) != 0 ? 1u : 0u);
+                                }
                             }
                         }
                         umma_commit(b_empty + 8 * stage);
+                        if (++stage == ST) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
                     }
                     if (ok) umma_commit(b_tfull + 8 * buf);
                 }
@@ -336,12 +410,12 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
         }
     } else {
         // --------------------------------------------------- epilogue
-        // Warp w reads TMEM lanes 32 * (w % 4) (hardware rule); the four warps
-        // of each quarter split (query tile, column half).
+        // Warp w reads TMEM lanes 32 * (w % 4) (hardware rule); the warps of
+        // each quarter split (query tile, 64-column group).
         const int quarter = warp & 3;
         const int slot = (warp - 2) >> 2;
-        const int mt = slot >> 1;
-        const int half = slot & 1;
+        const int mt = slot / GPT;
+        const int cq = slot % GPT;
         const uint32_t scratch = b_full + kBarBytes + (warp - 2) * kScratchBytes;
         uint64_t cg = 0;
         bool ok = true;
@@ -349,9 +423,9 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
             const Unit w = unit_of(p, unit);
             const int32_t row = (w.group * MT + mt) * BM + quarter * 32 + lane;
             const bool row_ok = row < p.n_q;
-            const int32_t list_base = w.split * 2 + half;  // list of (row, split, half)
+            const int32_t list_base = w.split * GPT + cq;  // list of (row, split, group)
             auto list_of = [&](int32_t srow) {
-                return p.lists + (static_cast<int64_t>(srow) * 2 * p.n_split + list_base) * S;
+                return p.lists + (static_cast<int64_t>(srow) * GPT * p.n_split + list_base) * S;
             };
             float tau = INFINITY;  // this list's current S-th smallest bound
             for (int32_t c = 0; c < w.len; ++c, ++cg) {
@@ -363,7 +437,7 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
                 }
                 fence_after();
                 const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
-                                       buf * (MT * BN) + mt * BN + half * (BN / 2);
+                                       buf * (MT * BN) + mt * BN + cq * 64;
                 uint32_t r[2][32];
                 tmem_ld32(taddr, r[0]);
                 tmem_ld32(taddr + 32, r[1]);
@@ -375,7 +449,7 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
                 const float m0 = min32(r[0]), m1 = min32(r[1]);
                 unsigned pend = __ballot_sync(0xffffffffu, row_ok && fminf(m0, m1) < tau);
                 if (pend == 0) continue;
-                const int32_t colh = tile_at(c, w) * BN + half * (BN / 2);
+                const int32_t colh = tile_at(c, w) * BN + cq * 64;
                 const int32_t valid_cols = static_cast<int32_t>(p.n_r - colh);
                 // Rows are served one at a time; the next pending row's list is
                 // loaded while the current one is merged, hiding its L2 latency.
@@ -461,53 +535,94 @@ __global__ void __launch_bounds__(tc_threads<MT>(), 1)
 }
 
 // ------------------------------------------------------------ operands --
+// Largest FP32 squared norm (non-negative floats order as unsigned ints).
+__global__ void max_sq_kernel(const float* __restrict__ sq, int64_t n, unsigned* __restrict__ out) {
+    float m = 0.0f;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        m = fmaxf(m, sq[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(out, __float_as_uint(m));
+}
+
+// s = 2^e with the largest e such that max_sq * s^2 <= 2^15: every scaled
+// squared norm, every |2 h| and every folded row term then fits FP16
+// (max 65504) with room to spare.
+__global__ void scale_kernel(const unsigned* __restrict__ max_bits, ScaleInfo* __restrict__ out) {
+    const float m = __uint_as_float(*max_bits);
+    int e = 0;
+    if (m > 0.0f && isfinite(m)) {
+        int ex = 0;
+        frexpf(m, &ex);  // m < 2^ex
+        const int t = 15 - ex;
+        e = t >= 0 ? t / 2 : -((-t + 1) / 2);
+        e = max(-60, min(60, e));
+    }
+    out->s = ldexpf(1.0f, e);
+    out->s2 = ldexpf(1.0f, 2 * e);
+}
+
+// Three FP16 parts whose sum is v within 2^-33 |v| (plus subnormal spacing).
+__device__ __forceinline__ void split3(float v, __half* o) {
+    const __half p1 = __float2half_rn(v);
+    const float r1 = v - __half2float(p1);
+    const __half p2 = __float2half_rn(r1);
+    const float r2 = r1 - __half2float(p2);
+    o[0] = p1;
+    o[1] = p2;
+    o[2] = __float2half_rn(r2);
+}
+
+// One warp per operand row: the FP16 row (scaled or unit-normalised), the
+// six folded columns, and zeros up to the stored width.  `sq` holds the
+// FP32 squared norms in the reference's order (row_norms).
 __global__ void prep_kernel(const float* __restrict__ X, const float* __restrict__ sq, int64_t n,
-                            int d, int kp, float c1, float c2, bool is_query,
-                            __nv_bfloat16* __restrict__ out) {
+                            int d, int kst, const ScaleInfo* __restrict__ sc, double c, double c0,
+                            bool cosine, bool is_query, __half* __restrict__ out) {
     const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
     const float* x = X + row * d;
-    __nv_bfloat16* o = out + row * kp;
-    for (int c = lane; c < d; c += 32) {
-        const float v = x[c];
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-        const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-        if (is_query) {
-            const __nv_bfloat16 h2 = __float2bfloat16_rn(-2.0f * __bfloat162float(h));
-            o[c] = h2;
-            o[d + c] = h2;
-            o[2 * d + c] = __float2bfloat16_rn(-2.0f * __bfloat162float(l));
-        } else {
-            o[c] = h;
-            o[d + c] = l;
-            o[2 * d + c] = h;
-        }
+    __half* o = out + row * kst;
+    const float n2 = sq[row];
+    float mul;
+    if (cosine) {
+        const float nrm = __fsqrt_rn(n2);
+        mul = nrm > 0.0f ? __frcp_rn(nrm) : 0.0f;
+    } else {
+        mul = sc->s;
     }
-    for (int c = 3 * d + 7 + lane; c < kp; c += 32) o[c] = __float2bfloat16_rn(0.0f);
+    for (int t = lane; t < d; t += 32) {
+        const __half h = __float2half_rn(x[t] * mul);
+        o[t] = !is_query ? h : (cosine ? __hneg(h) : __float2half_rn(-2.0f * __half2float(h)));
+    }
+    for (int t = d + kNormCols + lane; t < kst; t += 32) o[t] = __float2half_rn(0.0f);
     if (lane == 0) {
-        const float n2 = sq[row];
-        const float v = (1.0f - c2) * n2;
-        const __nv_bfloat16 s1 = __float2bfloat16_rn(v);
-        const float r1 = v - __bfloat162float(s1);
-        const __nv_bfloat16 s2 = __float2bfloat16_rn(r1);
-        const __nv_bfloat16 s3 = __float2bfloat16_rn(r1 - __bfloat162float(s2));
-        const __nv_bfloat16 one = __float2bfloat16_rn(1.0f);
-        const float rn = sqrtf(n2);
-        __nv_bfloat16* a = o + 3 * d;
+        float a;
+        if (cosine)
+            a = is_query ? static_cast<float>(1.0 - c0) : 0.0f;
+        else
+            a = static_cast<float>((1.0 - c) * static_cast<double>(n2) *
+                                       static_cast<double>(sc->s2) -
+                                   0.5 * c0);
+        const __half one = __float2half_rn(1.0f);
+        __half parts[3];
+        split3(a, parts);
         if (is_query) {
-            a[0] = s1; a[1] = s2; a[2] = s3;
-            a[3] = one; a[4] = one; a[5] = one;
-            a[6] = __float2bfloat16_rn(-c1 * rn);
+            o[d] = one; o[d + 1] = one; o[d + 2] = one;
+            o[d + 3] = parts[0]; o[d + 4] = parts[1]; o[d + 5] = parts[2];
         } else {
-            a[0] = one; a[1] = one; a[2] = one;
-            a[3] = s1; a[4] = s2; a[5] = s3;
-            a[6] = __float2bfloat16_rn(rn);
+            o[d] = parts[0]; o[d + 1] = parts[1]; o[d + 2] = parts[2];
+            o[d + 3] = one; o[d + 4] = one; o[d + 5] = one;
         }
     }
 }
 
 // ------------------------------------------------------------ re-rank ---
+// Squared euclidean distance with the reference's operations in its order
+// (squared_distance, rust_umap/src/lib.rs:2445-2492: for d >= 64, eight
+// strided lanes of acc + diff * diff summed in order, then the scalar tail).
 __device__ __forceinline__ float sqdist_ref(const float* __restrict__ x, const float* __restrict__ y,
                                             int d) {
     if (d >= 64) {
@@ -554,25 +669,70 @@ __device__ __forceinline__ float sqdist_ref(const float* __restrict__ x, const f
     return s;
 }
 
-__global__ void rerank_kernel(const float* __restrict__ Q, const float* __restrict__ R,
-                              const float* __restrict__ qsq, const float* __restrict__ rsq,
-                              const uint64_t* __restrict__ lists, int n_lists, int64_t n_q,
-                              int d, int k, double c1, double c2,
-                              const int32_t* __restrict__ perm, int32_t* __restrict__ out_idx,
-                              float* __restrict__ out_dist, int* __restrict__ fb_count,
-                              int32_t* __restrict__ fb_rows) {
+// Dot product in the reference's order (dot_product_avx2 / _scalar,
+// lib.rs:2653-2738: the same eight-lane layout as squared_distance for d >= 64).
+__device__ __forceinline__ float dot_ref(const float* __restrict__ x, const float* __restrict__ y,
+                                         int d) {
+    if (d >= 64) {
+        float lane[8];
+#pragma unroll
+        for (int l = 0; l < 8; ++l) lane[l] = 0.0f;
+        int i = 0;
+        for (; i + 8 <= d; i += 8)
+#pragma unroll
+            for (int l = 0; l < 8; ++l) lane[l] = __fadd_rn(lane[l], __fmul_rn(x[i + l], y[i + l]));
+        float s = lane[0];
+#pragma unroll
+        for (int l = 1; l < 8; ++l) s = __fadd_rn(s, lane[l]);
+        for (; i < d; ++i) s = __fadd_rn(s, __fmul_rn(x[i], y[i]));
+        return s;
+    }
+    float s = 0.0f;
+    for (int i = 0; i < d; ++i) s = __fadd_rn(s, __fmul_rn(x[i], y[i]));
+    return s;
+}
+
+// cosine_distance_with_norms (lib.rs:2740-2765) from the dot and L2 norms.
+__device__ __forceinline__ float cosine_ref(float dot, float xn, float yn) {
+    if (xn == 0.0f && yn == 0.0f) return 0.0f;
+    if (xn == 0.0f || yn == 0.0f) return 1.0f;
+    float c = __fdiv_rn(dot, __fmul_rn(xn, yn));
+    c = fminf(fmaxf(c, -1.0f), 1.0f);
+    return __fsub_rn(1.0f, c);
+}
+
+struct RerankArgs {
+    const float* Q;        // query rows in operand order
+    const float* R;        // candidate rows in operand order
+    const float* qsq;      // FP32 squared norms (reference order), operand order
+    const float* rsq;
+    const uint64_t* lists;
+    int n_lists;
+    int64_t n_q;
+    int d, k;
+    double c, c0;
+    bool cosine;
+    const ScaleInfo* sc;
+    const int32_t* omap;   // query position -> output row (null: identity)
+    const int32_t* rmap;   // candidate position -> original index (null: identity)
+    int32_t* out_idx;
+    float* out_dist;
+    int* fb_count;
+    int32_t* fb_rows;      // output rows that could not be certified
+};
+
+__global__ void rerank_kernel(RerankArgs a) {
     const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (row >= n_q) return;
-    // rows in cell order (perm non-null): position -> original row; keys, outputs
-    // and fallback rows use original indices, so ties break as in the reference
-    const int64_t orow = perm != nullptr ? perm[row] : row;
-    const uint64_t* rl = lists + row * n_lists * S;
+    if (row >= a.n_q) return;
+    const int k = a.k, d = a.d;
+    const int64_t orow = a.omap != nullptr ? a.omap[row] : row;
+    const uint64_t* rl = a.lists + row * a.n_lists * S;
     // The smallest bound a candidate missing from every list can have: a full
     // list left out only candidates with L >= its largest entry, a list that
     // is not full kept every candidate of its range.
     double bound = INFINITY;
-    for (int h = 0; h < n_lists; ++h) {
+    for (int h = 0; h < a.n_lists; ++h) {
         const uint64_t lk = rl[h * S + lane];
         const bool valid = lk != ~0ull;
         float lmax = valid ? o2f(static_cast<uint32_t>(lk >> 32)) : -INFINITY;
@@ -586,17 +746,19 @@ __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restri
     // smallest U.  A candidate with L > T has k others with d <= U <= T < L <= d
     // ahead of it, so only candidates with L <= T can rank in the top k: each
     // list (sorted by L) contributes a prefix, usually empty.
-    const double nq = qsq[row];
+    const double s2 = a.cosine ? 1.0 : static_cast<double>(a.sc->s2);
+    const double nq = static_cast<double>(a.qsq[row]) * s2;
     int below = 0;
     float topu = INFINITY;  // the 32 smallest U, sorted across the warp
-    for (int h = 0; h < n_lists; ++h) {
+    for (int h = 0; h < a.n_lists; ++h) {
         const uint64_t lk = rl[h * S + lane];
         const float l0 = o2f(static_cast<uint32_t>(__shfl_sync(0xffffffffu, lk, 0) >> 32));
         double U = INFINITY;
         if (lk != ~0ull) {
-            const double nc = rsq[static_cast<uint32_t>(lk)];
+            const double nc =
+                a.cosine ? 0.0 : static_cast<double>(a.rsq[static_cast<uint32_t>(lk)]) * s2;
             U = static_cast<double>(o2f(static_cast<uint32_t>(lk >> 32))) +
-                2.0 * (c1 * sqrt(nq * nc) + c2 * (nq + nc));
+                2.0 * (a.c * (nq + nc) + a.c0) * (1.0 + 1e-6);
         }
         below += __popc(__ballot_sync(0xffffffffu, U < bound));
         // a list whose smallest L already exceeds the k-th smallest U so far
@@ -616,62 +778,114 @@ __global__ void rerank_kernel(const float* __restrict__ Q, const float* __restri
     // Exact keys in the reference's order for the candidates with L <= T; the
     // 32 smallest are kept sorted across the warp (bitonic merge of each
     // list's keys into them).
+    const float* qrow = a.Q + row * d;
+    const float qn = a.cosine ? __fsqrt_rn(a.qsq[row]) : 0.0f;
     uint64_t top = ~0ull;
-    for (int h = 0; h < n_lists; ++h) {
+    for (int h = 0; h < a.n_lists; ++h) {
         const uint64_t lk = rl[h * S + lane];
         const bool take = lk != ~0ull && o2f(static_cast<uint32_t>(lk >> 32)) <= T;
         if (__ballot_sync(0xffffffffu, take) == 0) continue;
         uint64_t key = ~0ull;
         if (take) {
             const uint32_t j = static_cast<uint32_t>(lk);
-            key = knn_key(sqdist_ref(Q + row * d, R + static_cast<int64_t>(j) * d, d),
-                          perm != nullptr ? static_cast<uint32_t>(perm[j]) : j);
+            const float* crow = a.R + static_cast<int64_t>(j) * d;
+            const float dist = a.cosine
+                                   ? cosine_ref(dot_ref(qrow, crow, d), qn, __fsqrt_rn(a.rsq[j]))
+                                   : sqdist_ref(qrow, crow, d);
+            key = knn_key(dist, a.rmap != nullptr ? static_cast<uint32_t>(a.rmap[j]) : j);
         }
         top = warp_merge_keys(top, key);
     }
-    if (lane < k) {
-        out_idx[orow * k + lane] = static_cast<int32_t>(key_index(top));
-        out_dist[orow * k + lane] = __fsqrt_rn(key_dist(top));
+    // A zero cosine query has distance 0 to zero rows and 1 to the rest, which
+    // its bound (built for unit rows) does not cover: it goes to the plain path.
+    const bool failed = below < k || (a.cosine && a.qsq[row] == 0.0f);
+    if (!failed && lane < k) {
+        a.out_idx[orow * k + lane] = static_cast<int32_t>(key_index(top));
+        const float kd = key_dist(top);
+        a.out_dist[orow * k + lane] = a.cosine ? kd : __fsqrt_rn(kd);
     }
-    if (below < k && lane == 0) fb_rows[atomicAdd(fb_count, 1)] = static_cast<int32_t>(orow);
+    if (failed && lane == 0) a.fb_rows[atomicAdd(a.fb_count, 1)] = static_cast<int32_t>(orow);
+}
+
+__global__ void gather_rows_kernel(const float* __restrict__ X, const int32_t* __restrict__ perm,
+                                   int64_t n, int d, float* __restrict__ out) {
+    const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float* src = X + static_cast<int64_t>(perm[row]) * d;
+    float* dst = out + row * d;
+    for (int t = lane; t < d; t += 32) dst[t] = src[t];
 }
 
 // --------------------------------------------------------------- host ----
-CUtensorMap make_map(const void* base, int64_t rows, int kp) {
-    return make_bf16_map(base, rows, kp, BM);
+// Kernel shape: MT query tiles x BN candidate rows, ring stages.
+struct Shape {
+    int mt = 0, bn = 0, st = 0;
+    size_t smem = 0;
+    int lists() const { return bn / 64; }  // lists per row and candidate split
+};
+
+size_t smem_bytes(int mt, int bn, int kb, int st) {
+    // tiles + 1 KiB alignment slack + barriers/flags + epilogue scratch
+    return static_cast<size_t>(mt) * kb * kATileBytes + static_cast<size_t>(st) * bn * BK * 2 +
+           1024 + kBarBytes + static_cast<size_t>(4 * mt * (bn / 64)) * kScratchBytes;
 }
 
-int query_tiles_for(int kb) { return kb <= 4 ? 2 : (kb <= 10 ? 1 : 0); }
+// One query tile against 256-candidate tiles (four lists per row) while the
+// operands fit with at least three ring stages, else against 128-candidate
+// tiles (two lists per row, eight epilogue warps).
+Shape shape_for(int kb) {
+    const int cand[2][2] = {{1, 256}, {1, 128}};
+    for (const auto& c : cand) {
+        int st = kMaxStages;
+        while (st >= 2 && smem_bytes(c[0], c[1], kb, st) > kSmemLimit) --st;
+        if (st >= (c[1] == 256 ? 3 : 2))
+            return Shape{c[0], c[1], st, smem_bytes(c[0], c[1], kb, st)};
+    }
+    return Shape{};
+}
 
-template <int MT, int ST>
-void launch_tc(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, cudaStream_t s) {
-    // tiles + 1 KiB alignment slack + barriers/flags + epilogue scratch
-    const size_t smem = static_cast<size_t>(MT * a.kb + ST) * kTileBytes + 1024 + kBarBytes +
-                        static_cast<size_t>(8 * MT) * kScratchBytes;
-    auto kern = tc_knn_kernel<MT, ST>;
+template <int MT, int BN>
+void launch_tc_t(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, size_t smem,
+                 cudaStream_t s) {
+    auto kern = tc_knn_kernel<MT, BN>;
     UMAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
     int dev = 0, sms = 0;
     UMAPB_CUDA(cudaGetDevice(&dev));
     UMAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int64_t grid = std::min<int64_t>(a.n_units, sms);
-    kern<<<static_cast<unsigned>(grid), tc_threads<MT>(), smem, s>>>(ma, mb, a);
+    kern<<<static_cast<unsigned>(grid), tc_threads<MT, BN>(), smem, s>>>(ma, mb, a);
     UMAPB_LAUNCH_CHECK();
+}
+
+void launch_tc(const Shape& sh, const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a,
+               cudaStream_t s) {
+    if (sh.mt == 1 && sh.bn == 256)
+        launch_tc_t<1, 256>(ma, mb, a, sh.smem, s);
+    else if (sh.mt == 2 && sh.bn == 128)
+        launch_tc_t<2, 128>(ma, mb, a, sh.smem, s);
+    else if (sh.mt == 1 && sh.bn == 128)
+        launch_tc_t<1, 128>(ma, mb, a, sh.smem, s);
+    else
+        invalid("tensor-core kNN: no kernel shape for these operands");
 }
 
 // Work decomposition: groups of MT query tiles; when the groups are fewer
 // than the SMs the candidate tiles are split too (at least 8 per split, and
 // no more units than SMs, so every unit starts at once), so small query sets
-// still occupy the GPU.
-TcArgs plan(int64_t n_q, int64_t n_r, int d, bool allow_split) {
-    const int kp = padded_k(d);
+// still occupy the GPU.  `min_split` forces at least that many splits (more
+// lists per row) where the candidate tiles allow.
+TcArgs plan(int64_t n_q, int64_t n_r, const Geom& g, const Shape& sh, bool allow_split,
+            int min_split) {
     TcArgs a{};
     a.n_q = n_q;
     a.n_r = n_r;
-    a.kb = kp / BK;
-    a.n_ctiles = ceil_div(n_r, BN);
-    const int mt = query_tiles_for(a.kb);
-    const int64_t groups = ceil_div(n_q, static_cast<int64_t>(BM) * mt);
+    a.kb = g.kb;
+    a.tail = g.tail;
+    a.st = sh.st;
+    a.n_ctiles = ceil_div(n_r, sh.bn);
+    const int64_t groups = ceil_div(n_q, static_cast<int64_t>(BM) * sh.mt);
     int64_t split = 1;
     if (allow_split) {
         int dev = 0, sms = 0;
@@ -681,6 +895,7 @@ TcArgs plan(int64_t n_q, int64_t n_r, int d, bool allow_split) {
             split = std::min<int64_t>(std::max<int64_t>(sms / groups, 1),
                                       std::max<int64_t>(1, a.n_ctiles / 8));
     }
+    split = std::max<int64_t>(split, std::min<int64_t>(min_split, a.n_ctiles));
     a.split_tiles = ceil_div(a.n_ctiles, split);
     a.n_split = static_cast<int>(ceil_div(a.n_ctiles, a.split_tiles));
     a.n_units = groups * a.n_split;
@@ -782,7 +997,8 @@ __global__ void __launch_bounds__(256) cell_assign_kernel(const float* __restric
 // of the cell that the group's first row belongs to (binary search in the
 // sorted cell keys).
 __global__ void group_start_kernel(const uint8_t* __restrict__ skey, int64_t groups,
-                                   int rows_per_group, int32_t* __restrict__ start_tile) {
+                                   int rows_per_group, int tile_rows,
+                                   int32_t* __restrict__ start_tile) {
     const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= groups) return;
     const int64_t r0 = g * rows_per_group;
@@ -795,17 +1011,7 @@ __global__ void group_start_kernel(const uint8_t* __restrict__ skey, int64_t gro
         else
             hi = mid;
     }
-    start_tile[g] = static_cast<int32_t>(lo / BN);
-}
-
-__global__ void gather_rows_kernel(const float* __restrict__ X, const int32_t* __restrict__ perm,
-                                   int64_t n, int d, float* __restrict__ out) {
-    const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const float* src = X + static_cast<int64_t>(perm[row]) * d;
-    float* dst = out + row * d;
-    for (int t = lane; t < d; t += 32) dst[t] = src[t];
+    start_tile[g] = static_cast<int32_t>(lo / tile_rows);
 }
 
 struct CellOrder {
@@ -831,7 +1037,7 @@ void launch_assign(const float* X, int64_t n, int d, uint8_t* cell, int32_t* iot
 }
 
 void cell_order(const float* X, int64_t n, int d, int cells, int rows_per_group, int64_t groups,
-                CellOrder& co, cudaStream_t s) {
+                int tile_rows, CellOrder& co, cudaStream_t s) {
     DevBuf<uint8_t> key(n, s), skey(n, s);
     DevBuf<int32_t> iota(n, s);
     co.perm.alloc(n, s);
@@ -851,7 +1057,7 @@ void cell_order(const float* X, int64_t n, int d, int cells, int rows_per_group,
                                                8, s));
     co.start_tile.alloc(groups, s);
     group_start_kernel<<<static_cast<unsigned>(ceil_div(groups, 256)), 256, 0, s>>>(
-        skey.get(), groups, rows_per_group, co.start_tile.get());
+        skey.get(), groups, rows_per_group, tile_rows, co.start_tile.get());
     UMAPB_LAUNCH_CHECK();
     co.rows.alloc(static_cast<size_t>(n) * d, s);
     gather_rows_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
@@ -859,12 +1065,54 @@ void cell_order(const float* X, int64_t n, int d, int cells, int rows_per_group,
     UMAPB_LAUNCH_CHECK();
 }
 
+
+void launch_prep(const float* X, const float* sq, int64_t n, int d, const Geom& g,
+                 const ScaleInfo* sc, const Bound& b, bool cosine, bool query, __half* out,
+                 cudaStream_t s) {
+    if (n == 0) return;
+    prep_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
+        X, sq, n, d, g.kst, sc, b.c, b.c0, cosine, query, out);
+    UMAPB_LAUNCH_CHECK();
+}
+
+void launch_max_sq(const float* sq, int64_t n, unsigned* out, cudaStream_t s) {
+    if (n == 0) return;
+    const int blocks = static_cast<int>(std::min<int64_t>(ceil_div(n, 256), 148 * 4));
+    max_sq_kernel<<<blocks, 256, 0, s>>>(sq, n, out);
+    UMAPB_LAUNCH_CHECK();
+}
+
+void launch_rerank(const RerankArgs& ra, cudaStream_t s) {
+    rerank_kernel<<<static_cast<unsigned>(ceil_div(ra.n_q * 32, 256)), 256, 0, s>>>(ra);
+    UMAPB_LAUNCH_CHECK();
+}
+
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    UMAPB_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+}
+
+struct EventPair {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    EventPair() {
+        UMAPB_CUDA(cudaEventCreate(&e0));
+        UMAPB_CUDA(cudaEventCreate(&e1));
+    }
+    ~EventPair() {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    EventPair(const EventPair&) = delete;
+    EventPair& operator=(const EventPair&) = delete;
+};
+
 }  // namespace
 
 bool knn_tc_supported(int d, int k, int metric) {
-    if (metric != UMAPB_METRIC_EUCLIDEAN) return false;
+    if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE) return false;
     if (k < 1 || k > S - 2 || d < 1) return false;
-    if (query_tiles_for(padded_k(d) / BK) == 0) return false;
+    if (shape_for(geom(d).kb).st == 0) return false;
     return device_is_sm100();
 }
 
@@ -874,22 +1122,23 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
         invalid("the tensor-core kNN path does not support this metric/shape on this device");
     if (n_q == 0) return;
     if (k > n_r) invalid("kNN needs k <= number of reference rows");
+    const bool cosine = metric == UMAPB_METRIC_COSINE;
     const bool self = Q == R && n_q == n_r;
-    const float* const Q0 = Q;  // original rows: the fallback recomputes rows of these
+    const float* const Q0 = Q;  // original rows: later passes read rows of these
     const float* const R0 = R;
-    const int kp = padded_k(d);
-    const int kb = kp / BK;
-    const double c1 = kBoundC1;
-    const double c2 = bound_c2(d);
-    TcArgs a = plan(n_q, n_r, d, true);
-    const int mt = query_tiles_for(kb);
+    const Geom g = geom(d);
+    const Shape sh = shape_for(g.kb);
+    const Bound bd = bound_for(d, g.kmma, cosine);
+    TcArgs a = plan(n_q, n_r, g, sh, true, 1);
     CellOrder co;
     const int cells = self && a.n_split == 1 ? cell_count(n_q, d) : 0;
     if (cells > 0) {
-        cell_order(Q, n_q, d, cells, mt * BM, ceil_div(n_q, static_cast<int64_t>(BM) * mt), co, s);
+        cell_order(Q, n_q, d, cells, sh.mt * BM, ceil_div(n_q, static_cast<int64_t>(BM) * sh.mt),
+                   sh.bn, co, s);
         Q = R = co.rows.get();
         a.start_tile = co.start_tile.get();
     }
+    const int32_t* perm = cells > 0 ? co.perm.get() : nullptr;
     DevBuf<float> qsq(n_q, s), rsq;
     row_norms(Q, n_q, d, nullptr, qsq.get(), s);
     if (!self) {
@@ -897,55 +1146,124 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
         row_norms(R, n_r, d, nullptr, rsq.get(), s);
     }
     const float* rsq_p = self ? qsq.get() : rsq.get();
-    DevBuf<__nv_bfloat16> A(n_q * kp, s), B(n_r * kp, s);
-    prep_kernel<<<static_cast<unsigned>(ceil_div(n_q * 32, 256)), 256, 0, s>>>(
-        Q, qsq.get(), n_q, d, kp, static_cast<float>(c1), static_cast<float>(c2), true, A.get());
+    // flags: [0] pass-1 kernel error, [1] pass-1 failed rows, [2] pass-2 kernel
+    // error, [3] pass-2 failed rows, [4] largest squared norm (bits)
+    DevBuf<int> flags(8, s);
+    UMAPB_CUDA(cudaMemsetAsync(flags.get(), 0, 8 * sizeof(int), s));
+    unsigned* max_bits = reinterpret_cast<unsigned*>(flags.get() + 4);
+    DevBuf<ScaleInfo> sc(1, s);
+    if (!cosine) {
+        launch_max_sq(qsq.get(), n_q, max_bits, s);
+        if (!self) launch_max_sq(rsq.get(), n_r, max_bits, s);
+    }
+    scale_kernel<<<1, 1, 0, s>>>(max_bits, sc.get());
     UMAPB_LAUNCH_CHECK();
-    prep_kernel<<<static_cast<unsigned>(ceil_div(n_r * 32, 256)), 256, 0, s>>>(
-        R, rsq_p, n_r, d, kp, static_cast<float>(c1), static_cast<float>(c2), false, B.get());
-    UMAPB_LAUNCH_CHECK();
-    const int n_lists = 2 * a.n_split;
-    DevBuf<uint64_t> lists(n_q * n_lists * S, s);
-    UMAPB_CUDA(cudaMemsetAsync(lists.get(), 0xFF, n_q * n_lists * S * 8, s));
-    DevBuf<int> err(1, s), fb_count(1, s);
-    UMAPB_CUDA(cudaMemsetAsync(err.get(), 0, 4, s));
-    UMAPB_CUDA(cudaMemsetAsync(fb_count.get(), 0, 4, s));
-    const CUtensorMap ma = make_map(A.get(), n_q, kp);
-    const CUtensorMap mb = make_map(B.get(), n_r, kp);
+    DevBuf<__half> A(static_cast<size_t>(n_q) * g.kst, s), B(static_cast<size_t>(n_r) * g.kst, s);
+    launch_prep(Q, qsq.get(), n_q, d, g, sc.get(), bd, cosine, true, A.get(), s);
+    launch_prep(R, rsq_p, n_r, d, g, sc.get(), bd, cosine, false, B.get(), s);
+    const int n_lists = sh.lists() * a.n_split;
+    DevBuf<uint64_t> lists(static_cast<size_t>(n_q) * n_lists * S, s);
+    UMAPB_CUDA(cudaMemsetAsync(lists.get(), 0xFF, lists.bytes(), s));
+    const CUtensorMap ma = make_f16_map(A.get(), n_q, g.kst, BM);
+    const CUtensorMap mb = make_f16_map(B.get(), n_r, g.kst, sh.bn);
     a.lists = lists.get();
-    a.err = err.get();
-    cudaEvent_t e0, e1;
-    UMAPB_CUDA(cudaEventCreate(&e0));
-    UMAPB_CUDA(cudaEventCreate(&e1));
-    UMAPB_CUDA(cudaEventRecord(e0, s));
-    if (mt == 2)
-        launch_tc<2, 4>(ma, mb, a, s);
-    else
-        launch_tc<1, 3>(ma, mb, a, s);
-    UMAPB_CUDA(cudaEventRecord(e1, s));
-    int err_h = 0;
-    UMAPB_CUDA(cudaMemcpyAsync(&err_h, err.get(), 4, cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
-    float ms = 0.0f;
-    UMAPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (err_h != 0)
-        throw Error(UMAPB_ERR_CUDA,
-                    "tensor-core kNN kernel stopped on a wait timeout (code " +
-                        std::to_string(err_h) + ")");
+    a.err = flags.get();
+    EventPair ev;
+    UMAPB_CUDA(cudaEventRecord(ev.e0, s));
+    launch_tc(sh, ma, mb, a, s);
+    UMAPB_CUDA(cudaEventRecord(ev.e1, s));
     DevBuf<int32_t> fb_rows(n_q, s);
-    rerank_kernel<<<static_cast<unsigned>(ceil_div(n_q * 32, 256)), 256, 0, s>>>(
-        Q, R, qsq.get(), rsq_p, lists.get(), n_lists, n_q, d, k, c1, c2,
-        cells > 0 ? co.perm.get() : nullptr, out_idx, out_dist, fb_count.get(), fb_rows.get());
-    UMAPB_LAUNCH_CHECK();
-    int fb = 0;
-    UMAPB_CUDA(cudaMemcpyAsync(&fb, fb_count.get(), 4, cudaMemcpyDeviceToHost, s));
+    RerankArgs ra{};
+    ra.Q = Q;
+    ra.R = R;
+    ra.qsq = qsq.get();
+    ra.rsq = rsq_p;
+    ra.lists = lists.get();
+    ra.n_lists = n_lists;
+    ra.n_q = n_q;
+    ra.d = d;
+    ra.k = k;
+    ra.c = bd.c;
+    ra.c0 = bd.c0;
+    ra.cosine = cosine;
+    ra.sc = sc.get();
+    ra.omap = perm;
+    ra.rmap = perm;
+    ra.out_idx = out_idx;
+    ra.out_dist = out_dist;
+    ra.fb_count = flags.get() + 1;
+    ra.fb_rows = fb_rows.get();
+    launch_rerank(ra, s);
+    int h[2] = {0, 0};
+    UMAPB_CUDA(cudaMemcpyAsync(h, flags.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
-    if (fb > 0) knn_plain(Q0, fb_rows.get(), fb, R0, n_r, d, k, metric, nullptr, nullptr, out_idx,
-                          out_dist, s);
+    if (h[0] != 0)
+        throw Error(UMAPB_ERR_CUDA, "tensor-core kNN kernel stopped on a wait timeout (code " +
+                                        std::to_string(h[0]) + ")");
+    float ms = elapsed_ms(ev.e0, ev.e1);
+    const int64_t fb = h[1];
+    int64_t fb_final = 0;
+    if (fb > 0) {
+        // Second pass: the failed rows as a query set against the same
+        // candidate operand, with at least two candidate splits (twice as many
+        // lists per row, so B rises further above the k-th neighbour).
+        lists.release();
+        A.release();
+        DevBuf<float> Q2(static_cast<size_t>(fb) * d, s), q2sq(fb, s);
+        gather_rows_kernel<<<static_cast<unsigned>(ceil_div(fb * 32, 256)), 256, 0, s>>>(
+            Q0, fb_rows.get(), fb, d, Q2.get());
+        UMAPB_LAUNCH_CHECK();
+        row_norms(Q2.get(), fb, d, nullptr, q2sq.get(), s);
+        DevBuf<__half> A2(static_cast<size_t>(fb) * g.kst, s);
+        launch_prep(Q2.get(), q2sq.get(), fb, d, g, sc.get(), bd, cosine, true, A2.get(), s);
+        TcArgs a2 = plan(fb, n_r, g, sh, true, 2);
+        const int n_lists2 = sh.lists() * a2.n_split;
+        DevBuf<uint64_t> lists2(static_cast<size_t>(fb) * n_lists2 * S, s);
+        UMAPB_CUDA(cudaMemsetAsync(lists2.get(), 0xFF, lists2.bytes(), s));
+        const CUtensorMap ma2 = make_f16_map(A2.get(), fb, g.kst, BM);
+        a2.lists = lists2.get();
+        a2.err = flags.get() + 2;
+        EventPair ev2;
+        UMAPB_CUDA(cudaEventRecord(ev2.e0, s));
+        launch_tc(sh, ma2, mb, a2, s);
+        UMAPB_CUDA(cudaEventRecord(ev2.e1, s));
+        DevBuf<int32_t> fb2_rows(fb, s);
+        RerankArgs rb = ra;
+        rb.Q = Q2.get();
+        rb.qsq = q2sq.get();
+        rb.lists = lists2.get();
+        rb.n_lists = n_lists2;
+        rb.n_q = fb;
+        rb.omap = fb_rows.get();
+        rb.rmap = perm;
+        rb.fb_count = flags.get() + 3;
+        rb.fb_rows = fb2_rows.get();
+        launch_rerank(rb, s);
+        int h2[2] = {0, 0};
+        UMAPB_CUDA(cudaMemcpyAsync(h2, flags.get() + 2, sizeof(h2), cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        if (h2[0] != 0)
+            throw Error(UMAPB_ERR_CUDA, "tensor-core kNN kernel stopped on a wait timeout (code " +
+                                            std::to_string(h2[0]) + ")");
+        ms += elapsed_ms(ev2.e0, ev2.e1);
+        fb_final = h2[1];
+        if (fb_final > 0) {
+            DevBuf<float> qn, rn;
+            if (cosine) {
+                qn.alloc(n_q, s);
+                row_norms(Q0, n_q, d, qn.get(), nullptr, s);
+                if (!self) {
+                    rn.alloc(n_r, s);
+                    row_norms(R0, n_r, d, rn.get(), nullptr, s);
+                }
+            }
+            knn_plain(Q0, fb2_rows.get(), fb_final, R0, n_r, d, k, metric, qn.get(),
+                      self ? qn.get() : rn.get(), out_idx, out_dist, s);
+        }
+    }
     if (stats) {
-        stats->fallback_rows = fb;
+        stats->fallback_rows = fb_final;
+        stats->second_pass_rows = fb;
         stats->kernel_ms = ms;
         stats->shortlist = S;
     }
@@ -960,7 +1278,9 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
 // this library holds until the process exits.  In host code the array's name
 // is only a host-side stand-in, so the device address is fetched once per
 // device with cudaGetSymbolAddress (on the first call made with that device
-// current) and reused afterwards.
+// current) and reused afterwards.  It runs one tensor-core pass; rows that
+// pass cannot certify are recomputed on the plain path over the caller's
+// rows, which needs no scratch.
 namespace umapb {
 namespace {
 constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(64) << 20;
@@ -994,9 +1314,11 @@ inline size_t round256(size_t b) { return (b + 255) & ~static_cast<size_t>(255);
 // bytes of scratch one call needs for n rows of d features
 size_t noalloc_need(int64_t n, int d) {
     const size_t rows = static_cast<size_t>(n);
-    const size_t kp = static_cast<size_t>(padded_k(d));
-    return round256(rows * 4) + 2 * round256(rows * kp * 2) + round256(rows * 2 * S * 8) +
-           round256(8) + round256(rows * 4);
+    const Geom g = geom(d);
+    const Shape sh = shape_for(g.kb);
+    return round256(rows * 4) + 2 * round256(rows * g.kst * 2) +
+           round256(rows * sh.lists() * S * 8) + round256(8 * sizeof(int)) +
+           round256(sizeof(ScaleInfo)) + round256(rows * 4);
 }
 
 void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, float* out_dist,
@@ -1005,7 +1327,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     if (k < 1 || k > n) invalid("k must be in [1, n_rows]");
     if (!knn_tc_supported(d, k, UMAPB_METRIC_EUCLIDEAN))
         invalid("the allocation-free kNN runs the tensor-core path only (sm_100, euclidean, "
-                "k <= 30, n_cols <= 210)");
+                "k <= 30, n_cols within the tensor-core operand limit)");
     const size_t need = noalloc_need(n, d);
     if (need > kNoAllocScratchBytes) {
         int64_t max_rows = 0;
@@ -1015,10 +1337,9 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
                 std::to_string(kNoAllocScratchBytes) + " bytes (about " +
                 std::to_string(max_rows) + " rows at " + std::to_string(d) + " columns)");
     }
-    const int kp = padded_k(d);
-    const int kb = kp / BK;
-    const double c1 = kBoundC1;
-    const double c2 = bound_c2(d);
+    const Geom g = geom(d);
+    const Shape sh = shape_for(g.kb);
+    const Bound bd = bound_for(d, g.kmma, false);
     unsigned char* base = noalloc_scratch();
     size_t off = 0;
     auto carve = [&](size_t bytes) {
@@ -1027,44 +1348,57 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
         return p;
     };
     float* sq = reinterpret_cast<float*>(carve(static_cast<size_t>(n) * 4));
-    __nv_bfloat16* A = reinterpret_cast<__nv_bfloat16*>(carve(static_cast<size_t>(n) * kp * 2));
-    __nv_bfloat16* B = reinterpret_cast<__nv_bfloat16*>(carve(static_cast<size_t>(n) * kp * 2));
-    uint64_t* lists = reinterpret_cast<uint64_t*>(carve(static_cast<size_t>(n) * 2 * S * 8));
-    int* flags = reinterpret_cast<int*>(carve(8));  // [0] = kernel error, [1] = fallback count
+    __half* A = reinterpret_cast<__half*>(carve(static_cast<size_t>(n) * g.kst * 2));
+    __half* B = reinterpret_cast<__half*>(carve(static_cast<size_t>(n) * g.kst * 2));
+    uint64_t* lists =
+        reinterpret_cast<uint64_t*>(carve(static_cast<size_t>(n) * sh.lists() * S * 8));
+    // [0] kernel error, [1] rows to recompute, [4] largest squared norm (bits)
+    int* flags = reinterpret_cast<int*>(carve(8 * sizeof(int)));
+    ScaleInfo* sc = reinterpret_cast<ScaleInfo*>(carve(sizeof(ScaleInfo)));
     int32_t* fb_rows = reinterpret_cast<int32_t*>(carve(static_cast<size_t>(n) * 4));
 
     // every call starts from cleared shortlists and flags (the array keeps
     // the previous call's contents)
-    UMAPB_CUDA(cudaMemsetAsync(lists, 0xFF, static_cast<size_t>(n) * 2 * S * 8, s));
-    UMAPB_CUDA(cudaMemsetAsync(flags, 0, 8, s));
+    UMAPB_CUDA(cudaMemsetAsync(lists, 0xFF, static_cast<size_t>(n) * sh.lists() * S * 8, s));
+    UMAPB_CUDA(cudaMemsetAsync(flags, 0, 8 * sizeof(int), s));
     row_norms(X, n, d, nullptr, sq, s);
-    prep_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
-        X, sq, n, d, kp, static_cast<float>(c1), static_cast<float>(c2), true, A);
+    unsigned* max_bits = reinterpret_cast<unsigned*>(flags + 4);
+    launch_max_sq(sq, n, max_bits, s);
+    scale_kernel<<<1, 1, 0, s>>>(max_bits, sc);
     UMAPB_LAUNCH_CHECK();
-    prep_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
-        X, sq, n, d, kp, static_cast<float>(c1), static_cast<float>(c2), false, B);
-    UMAPB_LAUNCH_CHECK();
-    const CUtensorMap ma = make_map(A, n, kp);
-    const CUtensorMap mb = make_map(B, n, kp);
-    const int mt = query_tiles_for(kb);
-    TcArgs a = plan(n, n, d, false);  // one split: the scratch holds 2 lists per row
+    launch_prep(X, sq, n, d, g, sc, bd, false, true, A, s);
+    launch_prep(X, sq, n, d, g, sc, bd, false, false, B, s);
+    const CUtensorMap ma = make_f16_map(A, n, g.kst, BM);
+    const CUtensorMap mb = make_f16_map(B, n, g.kst, sh.bn);
+    TcArgs a = plan(n, n, g, sh, false, 1);  // one split: the scratch holds one set of lists
     a.lists = lists;
     a.err = flags;
-    if (mt == 2)
-        launch_tc<2, 4>(ma, mb, a, s);
-    else
-        launch_tc<1, 3>(ma, mb, a, s);
+    launch_tc(sh, ma, mb, a, s);
+    RerankArgs ra{};
+    ra.Q = X;
+    ra.R = X;
+    ra.qsq = sq;
+    ra.rsq = sq;
+    ra.lists = lists;
+    ra.n_lists = sh.lists();
+    ra.n_q = n;
+    ra.d = d;
+    ra.k = k;
+    ra.c = bd.c;
+    ra.c0 = bd.c0;
+    ra.cosine = false;
+    ra.sc = sc;
+    ra.out_idx = out_idx;
+    ra.out_dist = out_dist;
+    ra.fb_count = flags + 1;
+    ra.fb_rows = fb_rows;
+    launch_rerank(ra, s);
     int flags_h[2] = {0, 0};
-    UMAPB_CUDA(cudaMemcpyAsync(flags_h, flags, 8, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(flags_h, flags, sizeof(flags_h), cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
     if (flags_h[0] != 0)
         throw Error(UMAPB_ERR_CUDA, "tensor-core kNN kernel stopped on a wait timeout (code " +
                                         std::to_string(flags_h[0]) + ")");
-    rerank_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
-        X, X, sq, sq, lists, 2, n, d, k, c1, c2, nullptr, out_idx, out_dist, flags + 1, fb_rows);
-    UMAPB_LAUNCH_CHECK();
-    UMAPB_CUDA(cudaMemcpyAsync(flags_h, flags, 8, cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
     if (flags_h[1] > 0)
         knn_plain(X, fb_rows, flags_h[1], X, n, d, k, UMAPB_METRIC_EUCLIDEAN, nullptr, nullptr,
                   out_idx, out_dist, s);

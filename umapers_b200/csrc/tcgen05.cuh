@@ -121,6 +121,13 @@ constexpr uint32_t idesc_bf16(int m, int n) {
            (static_cast<uint32_t>(m >> 4) << 24);
 }
 
+// kind::f16 instruction descriptor: F32 accumulate, FP16 A and B (format
+// code 0 in both operand fields), both K-major, shape M x N.
+constexpr uint32_t idesc_f16(int m, int n) {
+    return (1u << 4) | (static_cast<uint32_t>(n >> 3) << 17) |
+           (static_cast<uint32_t>(m >> 4) << 24);
+}
+
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
                                           uint32_t idesc, uint32_t acc) {
     asm volatile(
@@ -210,6 +217,27 @@ inline CUtensorMap make_bf16_map(const void* base, int64_t rows, int64_t cols, i
     const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), static_cast<cuuint32_t>(box_rows)};
     const cuuint32_t estr[2] = {1, 1};
     const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base),
+                                 dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                 CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(UMAPB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+// Tensor map over a row-major FP16 matrix of `rows` x `cols` (cols a
+// multiple of 16 and at least 64, base 16-byte aligned) with box {64 columns,
+// box_rows rows} and the 128-byte swizzle.  Columns and rows past the end
+// read as zero, so the last 64-column block of a row may be partial.
+inline CUtensorMap make_f16_map(const void* base, int64_t rows, int64_t cols, int box_rows) {
+    if (cols % 16 != 0 || cols < kBK || (reinterpret_cast<uintptr_t>(base) & 15) != 0 ||
+        box_rows < 1 || box_rows > 256)
+        throw Error(UMAPB_ERR_CUDA, "tensor map operand is not 16-column / 16-byte aligned");
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols) * 2};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(kBK), static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base),
                                  dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
