@@ -155,6 +155,11 @@ uint64_t umapb_kernel_launches(void);
 int32_t umapb_pool_bytes(int64_t* reserved, int64_t* used);
 /* Defaults of UmapParams::default (rust_umap/src/lib.rs:170-195). */
 void umapb_params_default(umapb_params* params);
+/* should_use_approximate_knn (rust_umap/src/lib.rs:2285-2311): 1 when a fit
+ * of n_rows x n_cols with these parameters takes the NN-descent path.  Host
+ * only; needs no device. */
+int32_t umapb_should_use_approximate_knn(const umapb_params* params, int64_t n_rows,
+                                         int64_t n_cols);
 
 /* ---- model lifecycle: UmapCore.__new__ (umap_rs/src/lib.rs:549-630) ---- */
 
@@ -256,6 +261,20 @@ int32_t umapb_transform(umapb_model* model, const float* query, int64_t n_rows,
 int32_t umapb_profile_fit_transform(umapb_model* model, const float* data, int64_t n_rows,
                                     int64_t n_cols, float* out, umapb_timings* timings,
                                     umapb_fit_info* info);
+
+/* The deterministic stages of transform_from_knn (rust_umap/src/lib.rs:
+ * 1738-1763) for query rows of a fitted model: the exact query kNN to the
+ * fitted rows, smooth_knn_dist with local_connectivity - 1 (lib.rs:3424-3523),
+ * compute_membership_strengths_bipartite (lib.rs:3562-3595) after prune_edges
+ * with the transform's epoch count (lib.rs:3804-3822), and
+ * init_graph_transform (lib.rs:4793-4836), i.e. transform's output before
+ * optimize_layout_transform.  sigmas/rhos: n_rows floats; heads/tails/
+ * weights: edges grouped by query in kNN order (at most edge_capacity);
+ * init: n_rows x n_components. */
+int32_t umapb_transform_graph(umapb_model* model, const float* query, int64_t n_rows,
+                              int64_t n_cols, float* sigmas, float* rhos, int32_t* heads,
+                              int32_t* tails, float* weights, int64_t edge_capacity,
+                              int64_t* n_edges, float* init);
 
 /* Device-resident variants of fit_transform / transform: `data`, `query` and
  * `out` are device pointers (no host copies inside).  They have no reference

@@ -58,6 +58,8 @@ _SIGS = {
     "orc_fit_transform_dens": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
     "orc_local_radii": (None, [_vp, _vp, _i64, _i64, _f32, _vp]),
     "orc_transform": (_i32, [_vp, _i64, _vp, _vp, _i64, _i64, _vp, _f32, _f32, _vp]),
+    "orc_transform_graph": (_i64, [_vp, _i64, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp,
+                                   _vp, _i64, _vp]),
     "orc_optimize_layout_transform": (
         None,
         [_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _i64, _f32, _f32, _f32, _i64, _f32,
@@ -382,6 +384,28 @@ def transform(train, train_emb, q, a: float, b: float, **kw):
     load().orc_transform(_p(train), train.shape[0], _p(train_emb), _p(q), q.shape[0],
                          q.shape[1], ctypes.byref(p), a, b, _p(out))
     return out
+
+
+def transform_graph(train, train_emb, q, **kw):
+    """sigma, rho, pruned bipartite edges (head, tail, weight) and the
+    initial positions of transform_from_knn before its SGD."""
+    train, q = _f32m(train), _f32m(q)
+    train_emb = _f32m(train_emb)
+    p = _params(**kw)
+    nq = q.shape[0]
+    cap = nq * max(1, p.n_neighbors)
+    sig = np.empty(nq, np.float32)
+    rho = np.empty(nq, np.float32)
+    h = np.empty(cap, np.int32)
+    t = np.empty(cap, np.int32)
+    w = np.empty(cap, np.float32)
+    init = np.empty((nq, p.n_components), np.float32)
+    m = load().orc_transform_graph(_p(train), train.shape[0], _p(train_emb), _p(q), nq,
+                                   q.shape[1], ctypes.byref(p), _p(sig), _p(rho), _p(h), _p(t),
+                                   _p(w), cap, _p(init))
+    if m < 0:
+        raise ValueError("edge capacity too small")
+    return sig, rho, h[:m].copy(), t[:m].copy(), w[:m].copy(), init
 
 
 def optimize_layout_transform(emb, base, heads, tails, weights, n_epochs, a, b, alpha, neg_rate,

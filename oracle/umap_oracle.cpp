@@ -2298,6 +2298,42 @@ int32_t orc_transform(const float* train, int64_t n_train, const float* train_em
     return 0;
 }
 
+// The deterministic stages of transform_from_knn (lib.rs:1738-1763): query
+// kNN, smooth_knn_dist with local_connectivity - 1, bipartite membership,
+// prune_edges with the transform's epoch count and init_graph_transform.
+// Returns the edge count, or -1 when `cap` is too small.
+int64_t orc_transform_graph(const float* train, int64_t n_train, const float* train_emb,
+                            const float* q, int64_t nq, int64_t d, const umapb_params* p,
+                            float* sigmas, float* rhos, int32_t* heads, int32_t* tails,
+                            float* weights, int64_t cap, float* init) {
+    if (nq == 0) return 0;
+    const size_t k = std::min<size_t>(p->n_neighbors, n_train);
+    const size_t n_epochs =
+        p->n_epochs >= 0 ? std::max<size_t>(p->n_epochs, 1) : (nq <= 10000 ? 100 : 30);
+    const Knn knn = exact_knn_query(q, nq, train, n_train, d, k, p->metric);
+    const float lc = std::max(p->local_connectivity - 1.0f, 0.0f);
+    std::vector<float> sig, rho;
+    smooth_knn_dist_t<float>(knn.dist, static_cast<float>(k), lc, DEFAULT_BANDWIDTH, false, sig,
+                             rho);
+    auto edges = membership_bipartite(knn, sig, rho);
+    prune_edges(edges, n_epochs);
+    if (static_cast<int64_t>(edges.size()) > cap) return -1;
+    const size_t dim = static_cast<size_t>(p->n_components);
+    std::vector<float> base(train_emb, train_emb + n_train * dim);
+    Coords emb = init_graph_transform(nq, dim, edges, base);
+    for (int64_t i = 0; i < nq; ++i) {
+        sigmas[i] = sig[i];
+        rhos[i] = rho[i];
+        for (size_t j = 0; j < dim; ++j) init[i * dim + j] = emb[i][j];
+    }
+    for (size_t e = 0; e < edges.size(); ++e) {
+        heads[e] = static_cast<int32_t>(edges[e].head);
+        tails[e] = static_cast<int32_t>(edges[e].tail);
+        weights[e] = edges[e].weight;
+    }
+    return static_cast<int64_t>(edges.size());
+}
+
 // optimize_layout_transform on explicit inputs (the thread-count determinism
 // test of the reference, lib.rs:6193-6236, drives this function directly).
 void orc_optimize_layout_transform(float* emb, int64_t nq, int64_t dim, const float* base,

@@ -60,3 +60,22 @@ def test_create_destroy_needs_no_device():
     assert lib.umapb_create(ctypes.byref(p), ctypes.byref(h)) == 0
     assert lib.umapb_n_features(h) == -1 and lib.umapb_n_components(h) == 2
     lib.umapb_destroy(h)
+
+
+def test_ann_switch_matches_reference_pins(pins):
+    # auto_approximate_knn_delays_crossover_beyond_public_threshold
+    # (rust_umap/src/lib.rs:5814-5840): default parameters, threshold 4096
+    lib = _lib.load()
+    p = _lib.Params()
+    lib.umapb_params_default(ctypes.byref(p))
+    assert len(pins["ann_switch"]) == 5
+    for case in pins["ann_switch"]:
+        got = lib.umapb_should_use_approximate_knn(ctypes.byref(p), case["n"], case["d"])
+        assert bool(got) == case["expect"], case
+    # the switch is off entirely without use_approximate_knn, and any size
+    # above a zero threshold takes the approximate path
+    p.use_approximate_knn = 0
+    assert lib.umapb_should_use_approximate_knn(ctypes.byref(p), 10 ** 6, 64) == 0
+    p.use_approximate_knn = 1
+    p.approx_knn_threshold = 0
+    assert lib.umapb_should_use_approximate_knn(ctypes.byref(p), 2, 64) == 1

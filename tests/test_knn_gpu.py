@@ -135,3 +135,73 @@ def test_tensor_knn_1m_x_64_sampled_rows(orc):
     assert np.all(np.diff(td, axis=1) >= 0)
     print("fallback rows", fb)
     assert fb <= 10_000
+
+
+@pytest.mark.parametrize("n,d,k", [(2000, 64, 15), (1500, 40, 10), (2500, 130, 30)])
+def test_tensor_knn_cosine_bit_exact(orc, n, d, k):
+    # unit-normalised FP16 tiles, bound on 1 - cos, re-rank with the
+    # reference's cosine_distance_with_norms (clamp, zero-norm rules)
+    x = workloads.isotropic_mixture(n, d, 6, 3.0, seed=n + 5 * d)
+    x[7] = 0.0  # zero query row: recomputed on the plain path
+    x[11] = -x[12]  # opposite rows: cosine distance 2
+    ti, td, fb = gu.knn_exact(x, k, metric="cosine", backend="tensor")
+    oi, od = orc.exact_knn(x, k, metric="cosine")
+    np.testing.assert_array_equal(ti, oi)
+    np.testing.assert_array_equal(td, od)
+    assert 1 <= fb <= n // 20
+
+
+def test_tensor_knn_cosine_20000x192(orc):
+    x = workloads.isotropic_mixture(20_000, 192, 10, 4.0, seed=7)
+    ti, td, _ = gu.knn_exact(x, 15, metric="cosine", backend="tensor")
+    pi, pd, _ = gu.knn_exact(x, 15, metric="cosine", backend="plain")
+    np.testing.assert_array_equal(ti, pi)
+    np.testing.assert_array_equal(td, pd)
+    rows = np.random.default_rng(3).choice(20_000, 100, replace=False)
+    oi, od = orc.exact_knn_rows(x, rows, 15, metric="cosine")
+    np.testing.assert_array_equal(ti[rows], oi)
+    np.testing.assert_array_equal(td[rows], od)
+
+
+def test_tensor_knn_cosine_query_to_reference(orc):
+    fit, q = workloads.transform_mixture(n_fit=4000, n_query=600, d=96, n_comp=10)
+    ti, td = gu.knn_query(q, fit, 15, metric="cosine", backend="tensor")
+    oi, od = orc.knn_query(q, fit, 15, metric="cosine")
+    np.testing.assert_array_equal(ti, oi)
+    np.testing.assert_array_equal(td, od)
+
+
+def test_tensor_knn_second_pass_rows_stay_exact():
+    # Well-separated clusters far from the origin: |x|^2 is about 16 d while
+    # neighbour distances are about 2 d, so the one-term FP16 bound leaves
+    # some rows uncertified after the first pass (four lists per row).  They
+    # are re-run with twice the lists; the result equals the plain FP32 path
+    # on every row.
+    from umapers import Umap
+
+    x = workloads.isotropic_mixture(30_000, 128, 20, 4.0, seed=5)
+    prof = Umap(n_neighbors=15, n_epochs=20, ann_mode="exact", knn_backend="tensor",
+                init="random").profile_fit_transform(x)
+    assert prof["knn_backend"] == "tensor"
+    print("second pass rows", prof["knn_second_pass_rows"], "plain rows", prof["knn_fallback_rows"])
+    assert prof["knn_second_pass_rows"] > 0
+    assert prof["knn_fallback_rows"] <= prof["knn_second_pass_rows"] // 10
+    ti, td, _ = gu.knn_exact(x, 15, backend="tensor")
+    pi, pd, _ = gu.knn_exact(x, 15, backend="plain")
+    np.testing.assert_array_equal(ti, pi)
+    np.testing.assert_array_equal(td, pd)
+
+
+@pytest.mark.parametrize("d", [500, 640])
+def test_tensor_knn_wide_rows(orc, d):
+    # 128-candidate tiles (two lists per row) once 256-candidate tiles no
+    # longer fit shared memory beside the resident query tile
+    x = workloads.isotropic_mixture(3000, d, 8, 1.0, seed=d)
+    ti, td, fb = gu.knn_exact(x, 12, backend="tensor")
+    rows = np.random.default_rng(d).choice(3000, 80, replace=False)
+    oi, od = orc.exact_knn_rows(x, rows, 12)
+    np.testing.assert_array_equal(ti[rows], oi)
+    np.testing.assert_array_equal(td[rows], od)
+    pi, pd, _ = gu.knn_exact(x, 12, backend="plain")
+    np.testing.assert_array_equal(ti, pi)
+    np.testing.assert_array_equal(td, pd)

@@ -1,0 +1,125 @@
+"""Parity of whole fits and transforms with the oracle on the benchmark
+configurations' own inputs (seeded synthetic stand-ins of their shapes and
+distributions), and exact parity of the deterministic transform stages.
+
+The SGD layouts race Hogwild-style on the GPU and run sequentially in the
+oracle (the reference's order), so layouts are compared by quality:
+trustworthiness@15 and 15-NN preservation within 0.005 of the oracle's
+(configurations 1 and 2), trustworthiness@15 within 0.01 for the transforms
+(configuration 5).  Where a single fit's Hogwild variance is comparable to
+the tolerance (1 000 rows), the median over three seeds is compared on both
+sides.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from umapers import Umap
+from umapers_b200 import _lib, diagnostics, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _median_quality(x, embs):
+    qs = [diagnostics.quality(x, e) for e in embs]
+    return {key: float(np.median([q[key] for q in qs])) for key in qs[0]}
+
+
+def test_config1_gaussian_1000x32_matches_oracle(orc):
+    # 1000 x 32 N(0, 1), seed 42; k = 15, 200 epochs, exact kNN, spectral init
+    x = workloads.gaussian(1000, 32, seed=42)
+    seeds = (42, 43, 44)
+    g = [Umap(n_neighbors=15, n_epochs=200, ann_mode="exact", random_seed=s).fit_transform(x)
+         for s in seeds]
+    o = [orc.fit_transform(x, n_neighbors=15, n_epochs=200, use_approximate_knn=0, random_seed=s)
+         for s in seeds]
+    qg, qo = _median_quality(x, g), _median_quality(x, o)
+    print("gpu", qg, "oracle", qo)
+    assert abs(qg["trustworthiness"] - qo["trustworthiness"]) <= 0.005
+    assert abs(qg["knn_preservation"] - qo["knn_preservation"]) <= 0.005
+
+
+def test_config2_mixture_20000x192_full_fit_matches_oracle(orc):
+    # 20 000 x 192, 10-component mixture (means ~ N(0, 4^2)), seed 7; the
+    # tensor-core kNN, 200 epochs, 2-D; the oracle fits the same rows
+    x = workloads.isotropic_mixture(20_000, 192, 10, 4.0, seed=7)
+    m = Umap(n_neighbors=15, n_epochs=200, ann_mode="exact", knn_backend="tensor")
+    prof = m.profile_fit_transform(x)
+    assert prof["knn_backend"] == "tensor"
+    g = prof["embedding"]
+    o = orc.fit_transform(x, n_neighbors=15, n_epochs=200, use_approximate_knn=0)
+    qg, qo = diagnostics.quality(x, g), diagnostics.quality(x, o)
+    print("gpu", qg, "oracle", qo, "second pass", prof["knn_second_pass_rows"],
+          "plain rows", prof["knn_fallback_rows"])
+    assert abs(qg["trustworthiness"] - qo["trustworthiness"]) <= 0.005
+    assert abs(qg["knn_preservation"] - qo["knn_preservation"]) <= 0.005
+
+
+def test_config5_transforms_of_a_query_sample_match_oracle(orc):
+    # fit 200 000 x 128 (20-component mixture, seed 5) with the surrogate
+    # trained as configured (128-512-512-2, Adam 1e-3, batch 4096, 20 epochs);
+    # 2 000 queries of the same mixture (seed 6) through the plain transform,
+    # the surrogate with its gate, and the oracle's transform from the same
+    # fitted rows and embedding
+    fit, query = workloads.transform_mixture(200_000, 2_000, 128, 20, seed=5, query_seed=6)
+    m = Umap(n_neighbors=15, ann_mode="exact", transform_mode="surrogate",
+             surrogate_kwds={"hidden": 512, "epochs": 20, "batch_size": 4096,
+                             "learning_rate": 1e-3})
+    m.fit(fit)
+    a, b = m._core.ab_params
+    plain = m.transform(query, method="plain")
+    sur = m.transform(query, method="surrogate")
+    ref = orc.transform(fit, m.embedding_, query, a, b, n_neighbors=15)
+    tp, ts, to = (diagnostics.quality(query, e)["trustworthiness"] for e in (plain, sur, ref))
+    print(f"trust plain {tp:.4f} surrogate {ts:.4f} oracle {to:.4f}; "
+          f"gated {m.transform_fallback_.mean():.4f}")
+    assert abs(tp - to) <= 0.01
+    assert abs(ts - to) <= 0.01
+
+
+def _gpu_transform_graph(m, query):
+    lib = _lib.load()
+    q = np.ascontiguousarray(query, np.float32)
+    nq, d = q.shape
+    k = m.n_neighbors
+    cap = nq * k
+    sig = np.empty(nq, np.float32)
+    rho = np.empty(nq, np.float32)
+    h = np.empty(cap, np.int32)
+    t = np.empty(cap, np.int32)
+    w = np.empty(cap, np.float32)
+    ne = ctypes.c_int64(0)
+    init = np.empty((nq, m.n_components), np.float32)
+    _lib.check(lib.umapb_transform_graph(m._core._handle, q.ctypes.data, nq, d, sig.ctypes.data,
+                                         rho.ctypes.data, h.ctypes.data, t.ctypes.data,
+                                         w.ctypes.data, cap, ctypes.byref(ne), init.ctypes.data))
+    e = ne.value
+    return sig, rho, h[:e], t[:e], w[:e], init
+
+
+@pytest.mark.parametrize("n_components", [2, 3])
+def test_transform_graph_and_init_match_oracle(orc, n_components):
+    """transform_from_knn's deterministic stages (lib.rs:1738-1763): sigma and
+    rho with local_connectivity - 1, the bipartite membership weights
+    (lib.rs:3562-3595) after prune, and init_graph_transform
+    (lib.rs:4793-4836), against the oracle's restatement from the same fitted
+    rows and embedding.  rho and the edge lists are exact; sigma and the
+    weights within 1e-5 relative; the initial positions within 1e-5 of the
+    embedding's spread (they are weighted means of fitted positions)."""
+    fit, query = workloads.transform_mixture(4000, 600, 32, 8, seed=3, query_seed=4)
+    query[:50] = fit[100:150]  # queries at fitted points: weight-1 neighbours copy a position
+    m = Umap(n_neighbors=15, n_components=n_components, ann_mode="exact", n_epochs=50)
+    m.fit(fit)
+    sig, rho, h, t, w, init = _gpu_transform_graph(m, query)
+    osig, orho, oh, ot, ow, oinit = orc.transform_graph(fit, m.embedding_, query, n_neighbors=15,
+                                                        n_components=n_components, n_epochs=50)
+    np.testing.assert_array_equal(rho, orho)
+    np.testing.assert_allclose(sig, osig, rtol=1e-5)
+    np.testing.assert_array_equal(h, oh)
+    np.testing.assert_array_equal(t, ot)
+    np.testing.assert_allclose(w, ow, rtol=1e-5, atol=0)
+    spread = float(np.ptp(m.embedding_, axis=0).max())
+    np.testing.assert_allclose(init, oinit, rtol=0, atol=1e-5 * spread)
+    # the fitted points themselves: a weight-1 neighbour copies its position exactly
+    np.testing.assert_array_equal(init[:50], oinit[:50])

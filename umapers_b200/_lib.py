@@ -197,6 +197,7 @@ _u64 = ctypes.c_uint64
 SIGNATURES = {
     "umapb_version": (ctypes.c_char_p, []),
     "umapb_abi_version": (_i32, []),
+    "umapb_should_use_approximate_knn": (_i32, [_vp, _i64, _i64]),
     "umapb_last_error": (ctypes.c_char_p, []),
     "umapb_kernel_launches": (_u64, []),
     "umapb_pool_bytes": (_i32, [_vp, _vp]),
@@ -214,6 +215,8 @@ SIGNATURES = {
         [_vp, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _i32, _i32, _vp],
     ),
     "umapb_transform": (_i32, [_vp, _vp, _i64, _i64, _vp]),
+    "umapb_transform_graph": (_i32, [_vp, _vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _vp,
+                                     _vp]),
     "umapb_fit_csr": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64]),
     "umapb_fit_transform_csr": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _vp]),
     "umapb_fit_transform_csr_stateless": (_i32, [_vp, _vp, _vp, _vp, _i64, _i64, _vp]),

@@ -676,11 +676,26 @@ void trim_precomputed(const int64_t* idx, const float* dist, int64_t n, int64_t 
     }
 }
 
+// Host buffers for the deterministic transform stages (umapb_transform_graph).
+struct TransformStages {
+    float* sigmas = nullptr;
+    float* rhos = nullptr;
+    int32_t* heads = nullptr;
+    int32_t* tails = nullptr;
+    float* weights = nullptr;
+    int64_t capacity = 0;
+    int64_t* n_edges = nullptr;
+};
+
 // transform_from_knn (lib.rs:1738-1780) on a device kNN table: bipartite
 // membership, weighted init and the per-query SGD.  The default epoch count
 // follows the size of the whole request, `epoch_rows` (lib.rs:1650-1657).
+// With `stages`, sigma, rho and the pruned edges are copied out and out_dev
+// receives init_graph_transform's positions: the same transform kernel runs
+// with no SGD epoch.
 void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* dist, int64_t nq,
-                               int k, int64_t epoch_rows, float* out_dev) {
+                               int k, int64_t epoch_rows, float* out_dev,
+                               const TransformStages* stages = nullptr) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int dim = static_cast<int>(p.n_components);
@@ -691,6 +706,26 @@ void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* 
     smooth_knn(dist, nq, k, static_cast<float>(k), lc, 1.0f, false, sig.get(), rho.get(), s);
     Graph g;
     bipartite_graph(idx, dist, sig.get(), rho.get(), nq, k, n_epochs, g, s);
+    if (stages) {
+        if (g.n_edges > stages->capacity)
+            invalid("edge capacity " + std::to_string(stages->capacity) + " below the " +
+                    std::to_string(g.n_edges) + " transform edges");
+        UMAPB_CUDA(cudaMemcpyAsync(stages->sigmas, sig.get(), nq * 4, cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaMemcpyAsync(stages->rhos, rho.get(), nq * 4, cudaMemcpyDeviceToHost, s));
+        if (g.n_edges > 0) {
+            UMAPB_CUDA(cudaMemcpyAsync(stages->heads, g.heads.get(), g.n_edges * 4,
+                                       cudaMemcpyDeviceToHost, s));
+            UMAPB_CUDA(cudaMemcpyAsync(stages->tails, g.tails.get(), g.n_edges * 4,
+                                       cudaMemcpyDeviceToHost, s));
+            UMAPB_CUDA(cudaMemcpyAsync(stages->weights, g.weights.get(), g.n_edges * 4,
+                                       cudaMemcpyDeviceToHost, s));
+        }
+        *stages->n_edges = g.n_edges;
+        transform_layout(out_dev, nq, dim, m->emb.get(), m->n_fit, g, 0, m->a, m->b,
+                         p.learning_rate / 4.0f, p.negative_sample_rate, p.repulsion_strength,
+                         p.random_seed ^ 0xA24BAED40B53C117ULL, s);
+        return;
+    }
     transform_layout(out_dev, nq, dim, m->emb.get(), m->n_fit, g, n_epochs, m->a, m->b,
                      p.learning_rate / 4.0f, p.negative_sample_rate, p.repulsion_strength,
                      p.random_seed ^ 0xA24BAED40B53C117ULL, s);
@@ -701,7 +736,7 @@ void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* 
 // (exact_nearest_neighbors_dense_query, sparse.rs:753-910, gives the same
 // distances).
 void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out_dev,
-                      int64_t epoch_rows = -1) {
+                      int64_t epoch_rows = -1, const TransformStages* stages = nullptr) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int k = static_cast<int>(std::min<int64_t>(p.n_neighbors, m->n_fit));
@@ -716,7 +751,7 @@ void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, fl
         knn_exact_device(Qd, nq, m->X.get(), m->n_fit, static_cast<int>(d), k, p.metric,
                          p.knn_backend, idx.get(), dist.get(), nullptr, nullptr, nullptr, s);
     }
-    transform_from_knn_device(m, idx.get(), dist.get(), nq, k, epoch_rows, out_dev);
+    transform_from_knn_device(m, idx.get(), dist.get(), nq, k, epoch_rows, out_dev, stages);
 }
 
 void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
@@ -800,6 +835,12 @@ extern "C" {
 
 const char* umapb_version(void) { return kVersion; }
 int32_t umapb_abi_version(void) { return UMAPB_ABI_VERSION; }
+
+int32_t umapb_should_use_approximate_knn(const umapb_params* params, int64_t n_rows,
+                                         int64_t n_cols) {
+    if (!params) return 0;
+    return should_use_approximate_knn(*params, n_rows, n_cols) ? 1 : 0;
+}
 const char* umapb_last_error(void) { return g_last_error.c_str(); }
 uint64_t umapb_kernel_launches(void) { return g_kernel_launches.load(); }
 
@@ -1106,6 +1147,41 @@ int32_t umapb_transform(umapb_model* m, const float* query, int64_t n_rows, int6
         if (bad != INT64_MAX) invalid("input contains non-finite value at row " + std::to_string(bad));
         transform_device(m, Q.get(), n_rows, n_cols, outd.get());
         UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * m->p.n_components * 4,
+                                   cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int32_t umapb_transform_graph(umapb_model* m, const float* query, int64_t n_rows, int64_t n_cols,
+                              float* sigmas, float* rhos, int32_t* heads, int32_t* tails,
+                              float* weights, int64_t edge_capacity, int64_t* n_edges,
+                              float* init) {
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(m->mu);
+        if (!m->fitted) throw Error(UMAPB_ERR_NOT_FITTED, "model is not fitted yet");
+        if (!n_edges) invalid("n_edges must not be null");
+        *n_edges = 0;
+        if (n_rows == 0) return;
+        if (n_cols != m->d_fit)
+            throw Error(UMAPB_ERR_FEATURE_MISMATCH,
+                        "feature mismatch: expected " + std::to_string(m->d_fit) + ", got " +
+                            std::to_string(n_cols));
+        m->ensure_device();
+        cudaStream_t s = m->stream;
+        DevBuf<float> Q, outd(n_rows * m->p.n_components, s);
+        upload(Q, query, n_rows * n_cols, s);
+        const int64_t bad = first_nonfinite_row(Q.get(), n_rows, static_cast<int>(n_cols), s);
+        if (bad != INT64_MAX) invalid("input contains non-finite value at row " + std::to_string(bad));
+        TransformStages st;
+        st.sigmas = sigmas;
+        st.rhos = rhos;
+        st.heads = heads;
+        st.tails = tails;
+        st.weights = weights;
+        st.capacity = edge_capacity;
+        st.n_edges = n_edges;
+        transform_device(m, Q.get(), n_rows, n_cols, outd.get(), -1, &st);
+        UMAPB_CUDA(cudaMemcpyAsync(init, outd.get(), n_rows * m->p.n_components * 4,
                                    cudaMemcpyDeviceToHost, s));
         UMAPB_CUDA(cudaStreamSynchronize(s));
     });
