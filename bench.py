@@ -20,10 +20,15 @@ surrogate with its gate and plain fallback, and through the plain transform
 end from pinned host memory, trustworthiness@15 of both on 10,000 queries.
 
 --impl reference times the CPU restatement of the reference's path (the
-oracle) on the host cores: each step fits a 20,000-row sample of the same
-mixture and extrapolates per stage to 1,000,000 rows (kNN ~ n^2, the other
-stages ~ n).  Multi-GPU runs are replicas: every rank fits its own copy and
-the step time is the maximum over ranks.
+oracle) on all host cores.  Its exact kNN is timed directly on the full
+matrix: each step searches a fixed block of 2,000 query rows against all
+1,000,000 rows and scales by the query count only (the rows searched and their
+memory traffic are those of the real fit).  The other stages (graph, spectral
+init, SGD) are timed once per run by oracle fits of the first 25,000 and
+50,000 rows; each stage is extrapolated to 1,000,000 rows along the power law
+through its two times (the fitted exponent is reported).  Multi-GPU runs are
+replicas: every rank fits its own copy and the step time is the maximum over
+ranks.
 """
 from __future__ import annotations
 
@@ -45,7 +50,8 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "fit s @1M×64 TC vs FP32 kNN; transform rows/s MLP vs plain at equal trust@15"
 N_ROWS, N_DIM, K, EPOCHS = 1_000_000, 64, 15, 200
-SAMPLE_ROWS = 20_000
+KNN_BLOCK = 2_000               # query rows of the CPU kNN block (against all N_ROWS)
+CAL_SIZES = (25_000, 50_000)   # rows of the two CPU fits that time the other stages
 T_FIT, T_QUERY, T_DIM = 200_000, 1_000_000, 128
 T_SAMPLE = 2_000  # queries of the CPU transform baseline
 
@@ -155,16 +161,47 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_reference_step(x_sample: np.ndarray, threads: int) -> tuple[float, dict]:
-    """One oracle fit of the sample, extrapolated per stage to N_ROWS."""
+def cpu_calibrate(x: np.ndarray, threads: int) -> dict:
+    """Oracle fits of the first 25,000 and 50,000 rows: per stage other than
+    the kNN (graph, spectral init, SGD) the two times, the exponent of the
+    power law through them and its value at N_ROWS."""
+    import math
+
     from oracle import oracle
 
     oracle.set_threads(threads)
-    _, st = oracle.fit_transform(x_sample, return_stats=True, n_neighbors=K, n_epochs=EPOCHS,
-                                 use_approximate_knn=0)
-    scale = N_ROWS / x_sample.shape[0]
-    extrap = st["knn_sec"] * scale * scale + (st["graph_sec"] + st["init_sec"] + st["sgd_sec"]) * scale
-    return extrap, st
+    runs = {}
+    for n in CAL_SIZES:
+        _, runs[n] = oracle.fit_transform(x[:n].copy(), return_stats=True, n_neighbors=K,
+                                          n_epochs=EPOCHS, use_approximate_knn=0)
+    n1, n2 = CAL_SIZES
+    out = {}
+    for stage in ("graph_sec", "init_sec", "sgd_sec"):
+        t1, t2 = float(runs[n1][stage]), float(runs[n2][stage])
+        alpha = math.log(max(t2, 1e-9) / max(t1, 1e-9)) / math.log(n2 / n1)
+        out[stage] = {"sec": [round(t1, 3), round(t2, 3)], "exponent": round(alpha, 3),
+                      "at_n": round(t2 * (N_ROWS / n2) ** alpha, 2)}
+    return out
+
+
+def cpu_knn_block(x: np.ndarray, threads: int) -> float:
+    """The oracle's exact kNN of the first KNN_BLOCK rows against all rows of
+    x, scaled by the query count to all N_ROWS queries."""
+    from oracle import oracle
+
+    oracle.set_threads(threads)
+    rows = np.arange(KNN_BLOCK, dtype=np.int64)
+    t0 = time.perf_counter()
+    oracle.exact_knn_rows(x, rows, K)
+    return (time.perf_counter() - t0) * x.shape[0] / KNN_BLOCK
+
+
+def cpu_sample_note(cal: dict) -> str:
+    return (f"exact kNN: oracle search of {KNN_BLOCK} query rows against all {N_ROWS} rows "
+            f"(the full 256 MB matrix), scaled by the query count; graph / spectral init / SGD: "
+            f"oracle fits of {CAL_SIZES[0]} and {CAL_SIZES[1]} rows, each stage extrapolated "
+            f"to {N_ROWS} rows along the power law through its two times "
+            + json.dumps(cal))
 
 
 def run_reference(args) -> None:
@@ -174,14 +211,13 @@ def run_reference(args) -> None:
     from umapers_b200 import workloads
 
     threads = os.cpu_count() or 1
-    x = workloads.anisotropic_mixture(N_ROWS, N_DIM, 50, seed=11)[:SAMPLE_ROWS].copy()
+    x = workloads.anisotropic_mixture(N_ROWS, N_DIM, 50, seed=11)
+    cal = cpu_calibrate(x, threads)
+    rest = sum(v["at_n"] for v in cal.values())
     for _ in range(args.warmup):
-        cpu_reference_step(x, threads)
-    vals, last = [], {}
-    for _ in range(args.steps):
-        v, last = cpu_reference_step(x, threads)
-        vals.append(v)
-    value = float(np.mean(vals))
+        cpu_knn_block(x, threads)
+    knn = [cpu_knn_block(x, threads) for _ in range(args.steps)]
+    value = float(np.mean(knn)) + rest
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -197,12 +233,14 @@ def run_reference(args) -> None:
         "dtype": "f32",
         "data": "synthetic: 50-component anisotropic Gaussian mixture, seed 11",
         "config": {"workload": f"fit {N_ROWS} x {N_DIM}, k={K}, exact kNN, spectral init, "
-                               f"{EPOCHS} epochs, 2-D", "parallelism": "host cores"},
+                               f"{EPOCHS} epochs, 2-D; each step: the exact kNN of a "
+                               f"{KNN_BLOCK}-row query block against all {N_ROWS} rows",
+                   "parallelism": "host cores",
+                   "knn_sec_at_n": round(float(np.mean(knn)), 2),
+                   "other_stages_sec_at_n": round(rest, 2)},
         "cpu_baseline": {
             "value": round(value, 3), "unit": "s", "cores": threads, "kind": "port",
-            "sample": f"oracle fit of the first {SAMPLE_ROWS} rows per step; kNN time scaled by "
-                      f"(N/n)^2, graph/init/SGD by N/n; last sample stages "
-                      + json.dumps({k: round(float(v), 3) for k, v in last.items()}),
+            "sample": cpu_sample_note(cal),
         },
         "e2e": {"value": round(value, 3), "unit": "s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -332,6 +370,23 @@ def run_gpu(args) -> None:
             "note": "algorithmic bytes of the sampled edges; peak = measured HBM copy ("
                     + pk["source"] + ")",
         }
+        # spectral init: 256 products of the normalised adjacency with an
+        # N x 20 FP32 block (row_ptr/tails/weights read, 80 B gathered per
+        # edge, the block read and written) and a CholQR2 (4 passes over the
+        # block) after every 4th product
+        init_t = float(np.mean([st["init_sec"] for st in stage]))
+        spec_bytes = 256 * (info.n_edges * (4 + 4 + 80) + N_ROWS * 80 * 2) + 64 * N_ROWS * 80 * 4
+        roof_spec = {
+            "kernel": "spmm_kernel + CholQR2 (spectral init stage)",
+            "bound": "hbm",
+            "achieved": round(spec_bytes / init_t / 1e9, 1),
+            "peak": pk["hbm_gbs"],
+            "unit": "GB/s",
+            "frac": round(spec_bytes / init_t / 1e9 / pk["hbm_gbs"], 4),
+            "traffic": None,
+            "note": "algorithmic bytes of 256 block products and 64 CholQR2 over the whole "
+                    "init stage time; peak = measured HBM copy (" + pk["source"] + ")",
+        }
         dominant = roof_knn if knn_t >= sgd_t else roof_sgd
         q = diagnostics.quality(x, emb, sample=10_000, seed=11)
         line = {
@@ -345,7 +400,7 @@ def run_gpu(args) -> None:
             "higher_is_better": False,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "bf16x3->f32 (kNN tiles), f32" if backend == "tensor" else "f32",
+            "dtype": "fp16->f32 (kNN tiles), f32" if backend == "tensor" else "f32",
             "data": "synthetic: 50-component anisotropic Gaussian mixture, seed 11",
             "config": {
                 "workload": f"fit {N_ROWS} x {N_DIM}, k={K}, exact kNN ({backend}), spectral "
@@ -360,7 +415,7 @@ def run_gpu(args) -> None:
                     "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": int(emb.nbytes)},
             "gpu_launches": int(launches),
             "roofline": dominant,
-            "rooflines": {"knn": roof_knn, "sgd": roof_sgd},
+            "rooflines": {"knn": roof_knn, "sgd": roof_sgd, "spectral": roof_spec},
             "stages_sec": {k: round(float(np.mean([s[k] for s in stage])), 4)
                            for k in ("knn_sec", "smooth_knn_sec", "membership_sec", "symmetrize_sec",
                                      "prune_sec", "init_sec",
@@ -386,11 +441,11 @@ def run_gpu(args) -> None:
             line["knn_configs"] = extra
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            v, st = cpu_reference_step(x[:SAMPLE_ROWS].copy(), threads)
+            cal = cpu_calibrate(x, threads)
+            v = cpu_knn_block(x, threads) + sum(c["at_n"] for c in cal.values())
             line["cpu_baseline"] = {
                 "value": round(v, 2), "unit": "s", "cores": threads, "kind": "port",
-                "sample": f"oracle fit of {SAMPLE_ROWS} rows of the same mixture, extrapolated "
-                          f"per stage to {N_ROWS} rows (kNN x (N/n)^2, rest x N/n)",
+                "sample": cpu_sample_note(cal),
             }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -483,13 +538,20 @@ def knn_legs(args, lib, x: np.ndarray) -> dict:
     ni = np.empty((n, K), np.int64)
     nd = np.empty((n, K), np.float32)
     ran = ctypes.c_int64(0)
+    n_eval = ctypes.c_int64(0)
+    nd_ksec = ctypes.c_double(0.0)
     seed = 42 ^ 0xC0FEFEED1234ABCD
-    t_nd = float("inf")
+    t_nd, k_nd = float("inf"), float("inf")
     for _ in range(2):
         t0 = time.perf_counter()
         _lib.check(lib.umapb_nndescent(x.ctypes.data, n, x.shape[1], K, 0, 30, 10, seed,
-                                       ni.ctypes.data, nd.ctypes.data, ctypes.byref(ran)))
+                                       ni.ctypes.data, nd.ctypes.data, ctypes.byref(ran),
+                                       ctypes.byref(n_eval), ctypes.byref(nd_ksec)))
         t_nd = min(t_nd, time.perf_counter() - t0)
+        k_nd = min(k_nd, nd_ksec.value)
+    # gathered candidate rows (D x 4 B each) plus, per list pass, the k-entry
+    # lists read and written (index + distance, 8 B each)
+    nd_bytes = n_eval.value * x.shape[1] * 4 + (ran.value + 1) * n * K * 8 * 2
     ei = np.empty((n, K), np.int64)
     ed = np.empty((n, K), np.float32)
     _lib.check(lib.umapb_knn_exact(x.ctypes.data, n, x.shape[1], K, 0, 1, ei.ctypes.data,
@@ -517,8 +579,16 @@ def knn_legs(args, lib, x: np.ndarray) -> dict:
         "note": "host API from a host array (the 256 MB upload inside), one fit; compare with "
                 "the headline's e2e and quality"}
     out["sparse_cosine_200000x2000"] = sparse_leg(args, lib)
+    pk = peaks()
     out["nndescent_1m_x64"] = {
-        "knn_s": round(t_nd, 4), "iters": int(ran.value), "recall_at_15": round(recall, 4),
+        "knn_s": round(t_nd, 4), "kernel_s": round(k_nd, 4), "iters": int(ran.value),
+        "recall_at_15": round(recall, 4), "candidates_evaluated": int(n_eval.value),
+        "roofline": {"kernel": "nd_init_kernel + nd_iter_kernel", "bound": "hbm",
+                     "achieved": round(nd_bytes / k_nd / 1e9, 1), "peak": pk["hbm_gbs"],
+                     "unit": "GB/s", "frac": round(nd_bytes / k_nd / 1e9 / pk["hbm_gbs"], 4),
+                     "traffic": None,
+                     "note": "algorithmic bytes: evaluated candidates x D x 4 B + k-lists read "
+                             "and written per pass, over the kernels' CUDA-event time"},
         "note": "host API (includes the 256 MB upload), max_candidates=30, n_iters=10; recall "
                 "against the exact neighbours on 2,000 rows"}
     return out

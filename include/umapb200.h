@@ -367,10 +367,14 @@ int32_t umapb_knn_csr_query(const int64_t* q_indptr, const int64_t* q_indices,
 
 /* NN-descent variant (approximate_nearest_neighbors_with_distance,
  * rust_umap/src/lib.rs:3086-3151) on the GPU; `seed` plays the role of
- * random_seed ^ 0xC0FE_FEED_1234_ABCD (lib.rs:2327). */
+ * random_seed ^ 0xC0FE_FEED_1234_ABCD (lib.rs:2327).  `candidates_evaluated`
+ * and `kernel_sec` (each may be NULL) receive the number of candidate
+ * distances computed (initial lists included) and the CUDA-event time of the
+ * NN-descent kernels. */
 int32_t umapb_nndescent(const float* data, int64_t n_rows, int64_t n_cols, int64_t k,
                         int32_t metric, int64_t candidate_pool, int64_t n_iters,
-                        uint64_t seed, int64_t* indices, float* dists, int64_t* iters_run);
+                        uint64_t seed, int64_t* indices, float* dists, int64_t* iters_run,
+                        int64_t* candidates_evaluated, double* kernel_sec);
 
 /* smooth_knn_dist (rust_umap/src/lib.rs:3424-3523): dists is n_rows x n_cols. */
 int32_t umapb_smooth_knn_dist(const float* dists, int64_t n_rows, int64_t n_cols, float k,

@@ -34,15 +34,21 @@ def knn_query(q, r, k, metric="euclidean", backend="plain"):
     return idx, dist
 
 
-def nndescent(x, k, candidates, iters, seed, metric="euclidean"):
+def nndescent(x, k, candidates, iters, seed, metric="euclidean", stats=None):
     x = np.ascontiguousarray(x, np.float32)
     n, d = x.shape
     idx = np.empty((n, k), np.int64)
     dist = np.empty((n, k), np.float32)
     ran = ctypes.c_int64(0)
+    evaluated = ctypes.c_int64(0)
+    ksec = ctypes.c_double(0.0)
     _lib.check(_lib.load().umapb_nndescent(_p(x), n, d, k, METRIC[metric], candidates, iters,
                                            seed & 0xFFFFFFFFFFFFFFFF, _p(idx), _p(dist),
-                                           ctypes.byref(ran)))
+                                           ctypes.byref(ran), ctypes.byref(evaluated),
+                                           ctypes.byref(ksec)))
+    if stats is not None:
+        stats["candidates"] = evaluated.value
+        stats["kernel_sec"] = ksec.value
     return idx, dist, ran.value
 
 

@@ -514,7 +514,7 @@ class UmapCore:
         ap_d = np.empty((n, k), np.float32)
         _lib.check(self._lib.umapb_nndescent(_lib.ptr(arr), n, d, k, p.metric,
                                              p.approx_knn_candidates, p.approx_knn_iters, seed,
-                                             _lib.ptr(ap_i), _lib.ptr(ap_d), None))
+                                             _lib.ptr(ap_i), _lib.ptr(ap_d), None, None, None))
         per_row = np.empty(n, np.float32)
         rows = np.arange(n)
         for r in range(n):

@@ -1378,7 +1378,8 @@ int32_t umapb_knn_csr_query(const int64_t* q_indptr, const int64_t* q_indices,
 
 int32_t umapb_nndescent(const float* data, int64_t n, int64_t d, int64_t k, int32_t metric,
                         int64_t candidate_pool, int64_t n_iters, uint64_t seed, int64_t* indices,
-                        float* dists, int64_t* iters_run) {
+                        float* dists, int64_t* iters_run, int64_t* candidates_evaluated,
+                        double* kernel_sec) {
     return guarded([&] {
         if (n <= 1 || d <= 0) invalid("need at least two rows");
         if (k < 1 || k >= n) invalid("k must be in [1, n_rows)");
@@ -1387,9 +1388,12 @@ int32_t umapb_nndescent(const float* data, int64_t n, int64_t d, int64_t k, int3
         upload(X, data, n * d, ss.s);
         DevBuf<int32_t> idx(n * k, ss.s);
         DevBuf<float> dist(n * k, ss.s);
+        NdStats st;
         const int64_t ran = umapb::nndescent(X.get(), n, static_cast<int>(d), static_cast<int>(k),
                                              metric, candidate_pool, n_iters, seed, idx.get(),
-                                             dist.get(), ss.s);
+                                             dist.get(), ss.s, &st);
+        if (candidates_evaluated) *candidates_evaluated = st.candidates;
+        if (kernel_sec) *kernel_sec = st.kernel_sec;
         std::vector<int32_t> ih(n * k);
         UMAPB_CUDA(cudaMemcpyAsync(ih.data(), idx.get(), n * k * 4, cudaMemcpyDeviceToHost, ss.s));
         UMAPB_CUDA(cudaMemcpyAsync(dists, dist.get(), n * k * 4, cudaMemcpyDeviceToHost, ss.s));

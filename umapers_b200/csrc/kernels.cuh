@@ -126,9 +126,13 @@ void gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int64_t M, int
 int gemm_take_error(cudaStream_t s);
 
 // ---------------------------------------------------------- nndescent.cu
+struct NdStats {
+    int64_t candidates = 0;   // candidate distances evaluated, initial lists included
+    double kernel_sec = 0.0;  // CUDA-event time of the initial and iteration kernels
+};
 int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t candidate_pool,
                   int64_t n_iters, uint64_t seed, int32_t* out_idx, float* out_dist,
-                  cudaStream_t s);
+                  cudaStream_t s, NdStats* stats = nullptr);
 
 // -------------------------------------------------------------- graph.cu
 struct Graph {

@@ -13,6 +13,14 @@
 // memory and are ordered with warp bitonic sorts.  Distances use the
 // reference's summation order (euclidean = sqrt of the squared distance,
 // lib.rs:3167).  Random streams are counter-based per (row, iteration).
+//
+// Candidate evaluation is a gather of whole rows.  For d >= 64 the warp
+// splits into four groups of eight lanes; a group evaluates one candidate,
+// lane r of the group accumulating the reference's AVX2 lane r (dims r,
+// r + 8, ...) from the row's consecutive 32-byte sectors, so each step of a
+// group reads one sector and a warp four candidates at once.  The group's
+// eight partial sums are added in lane order, then the scalar tail, exactly
+// as the reference does.  The query row sits in shared memory.
 #include <climits>
 
 #include "kernels.cuh"
@@ -21,69 +29,6 @@ namespace umapb {
 namespace {
 
 constexpr int kWarps = 4;
-
-__device__ inline float sqdist_ref(const float* __restrict__ x, const float* __restrict__ y, int d) {
-    if (d >= 64) {
-        float lane[8];
-#pragma unroll
-        for (int l = 0; l < 8; ++l) lane[l] = 0.0f;
-        int i = 0;
-        for (; i + 8 <= d; i += 8)
-#pragma unroll
-            for (int l = 0; l < 8; ++l) {
-                const float df = __fsub_rn(x[i + l], y[i + l]);
-                lane[l] = __fadd_rn(lane[l], __fmul_rn(df, df));
-            }
-        float s = lane[0];
-#pragma unroll
-        for (int l = 1; l < 8; ++l) s = __fadd_rn(s, lane[l]);
-        for (; i < d; ++i) {
-            const float df = __fsub_rn(x[i], y[i]);
-            s = __fadd_rn(s, __fmul_rn(df, df));
-        }
-        return s;
-    }
-    float s = 0.0f;
-    for (int i = 0; i < d; ++i) {
-        const float df = __fsub_rn(x[i], y[i]);
-        s = __fadd_rn(s, __fmul_rn(df, df));
-    }
-    return s;
-}
-
-__device__ inline float dot_ref(const float* __restrict__ x, const float* __restrict__ y, int d) {
-    if (d >= 64) {
-        float lane[8];
-#pragma unroll
-        for (int l = 0; l < 8; ++l) lane[l] = 0.0f;
-        int i = 0;
-        for (; i + 8 <= d; i += 8)
-#pragma unroll
-            for (int l = 0; l < 8; ++l) lane[l] = __fadd_rn(lane[l], __fmul_rn(x[i + l], y[i + l]));
-        float s = lane[0];
-#pragma unroll
-        for (int l = 1; l < 8; ++l) s = __fadd_rn(s, lane[l]);
-        for (; i < d; ++i) s = __fadd_rn(s, __fmul_rn(x[i], y[i]));
-        return s;
-    }
-    float s = 0.0f;
-    for (int i = 0; i < d; ++i) s = __fadd_rn(s, __fmul_rn(x[i], y[i]));
-    return s;
-}
-
-__device__ inline float pair_distance(const float* X, const float* norms, int64_t i, int64_t j,
-                                      int d, bool cosine) {
-    const float* x = X + i * d;
-    const float* y = X + j * d;
-    if (!cosine) return __fsqrt_rn(sqdist_ref(x, y, d));
-    const float xn = norms[i], yn = norms[j];
-    const float dot = dot_ref(x, y, d);
-    if (xn == 0.0f && yn == 0.0f) return 0.0f;
-    if (xn == 0.0f || yn == 0.0f) return 1.0f;
-    float c = __fdiv_rn(dot, __fmul_rn(xn, yn));
-    c = fminf(fmaxf(c, -1.0f), 1.0f);
-    return __fsub_rn(1.0f, c);
-}
 
 // Bitonic sort of `cnt` (<= cap, cap a power of two) 64-bit keys in shared
 // memory by one warp; slots past `cnt` must hold ~0.
@@ -106,6 +51,95 @@ __device__ inline void warp_sort_u64(uint64_t* a, int cap) {
     }
 }
 
+// Distance of query row i (in shared memory `qs`) to the candidates in
+// keys[0, m) (row indices), written back in place as (distance, index) keys.
+// Every lane of the warp calls it with the same m.
+__device__ inline void eval_candidates(const float* __restrict__ X, const float* __restrict__ norms,
+                                       int64_t i, int d, bool cosine, const float* qs,
+                                       uint64_t* keys, int m) {
+    const int lane = threadIdx.x & 31;
+    if (d < 64) {
+        // the reference's scalar loop: one lane per candidate
+        for (int c = lane; c < m; c += 32) {
+            const int64_t j = static_cast<int64_t>(keys[c]);
+            const float* y = X + j * d;
+            float sum = 0.0f;
+            for (int t = 0; t < d; ++t) {
+                if (cosine) {
+                    sum = __fadd_rn(sum, __fmul_rn(qs[t], y[t]));
+                } else {
+                    const float df = __fsub_rn(qs[t], y[t]);
+                    sum = __fadd_rn(sum, __fmul_rn(df, df));
+                }
+            }
+            float dist;
+            if (!cosine) {
+                dist = __fsqrt_rn(sum);
+            } else {
+                const float xn = norms[i], yn = norms[j];
+                if (xn == 0.0f && yn == 0.0f) {
+                    dist = 0.0f;
+                } else if (xn == 0.0f || yn == 0.0f) {
+                    dist = 1.0f;
+                } else {
+                    float cs = __fdiv_rn(sum, __fmul_rn(xn, yn));
+                    cs = fminf(fmaxf(cs, -1.0f), 1.0f);
+                    dist = __fsub_rn(1.0f, cs);
+                }
+            }
+            keys[c] = knn_key(dist, static_cast<uint32_t>(j));
+        }
+        return;
+    }
+    const int g = lane >> 3, r = lane & 7, leader = lane & ~7;
+    const int body = (d / 8) * 8;
+    for (int base = 0; base < m; base += 4) {
+        const int c = base + g;
+        const bool act = c < m;
+        const int64_t j = act ? static_cast<int64_t>(keys[c]) : i;
+        const float* y = X + j * d;
+        float acc = 0.0f;
+        if (cosine) {
+            for (int t = r; t < body; t += 8) acc = __fadd_rn(acc, __fmul_rn(qs[t], __ldg(y + t)));
+        } else {
+            for (int t = r; t < body; t += 8) {
+                const float df = __fsub_rn(qs[t], __ldg(y + t));
+                acc = __fadd_rn(acc, __fmul_rn(df, df));
+            }
+        }
+        // lanes summed in order, then the tail (lib.rs:2468-2492, 2717-2738)
+        float sum = __shfl_sync(0xffffffffu, acc, leader);
+#pragma unroll
+        for (int l = 1; l < 8; ++l) sum = __fadd_rn(sum, __shfl_sync(0xffffffffu, acc, leader + l));
+        if (r == 0 && act) {
+            for (int t = body; t < d; ++t) {
+                if (cosine) {
+                    sum = __fadd_rn(sum, __fmul_rn(qs[t], y[t]));
+                } else {
+                    const float df = __fsub_rn(qs[t], y[t]);
+                    sum = __fadd_rn(sum, __fmul_rn(df, df));
+                }
+            }
+            float dist;
+            if (!cosine) {
+                dist = __fsqrt_rn(sum);
+            } else {
+                const float xn = norms[i], yn = norms[j];
+                if (xn == 0.0f && yn == 0.0f) {
+                    dist = 0.0f;
+                } else if (xn == 0.0f || yn == 0.0f) {
+                    dist = 1.0f;
+                } else {
+                    float cs = __fdiv_rn(sum, __fmul_rn(xn, yn));
+                    cs = fminf(fmaxf(cs, -1.0f), 1.0f);
+                    dist = __fsub_rn(1.0f, cs);
+                }
+            }
+            keys[c] = knn_key(dist, static_cast<uint32_t>(j));
+        }
+    }
+}
+
 struct NdArgs {
     const float* X;
     const float* norms;
@@ -123,17 +157,27 @@ struct NdArgs {
     int32_t* new_idx;
     float* new_dist;
     int* changed;
+    unsigned long long* evaluated;  // kEvalSlots counters of candidates evaluated
 };
+
+constexpr int kEvalSlots = 64;  // spread the per-warp counts over 64 addresses
+
+// Shared memory of one warp: cap keys, cap candidate indices, the query row.
+__host__ __device__ inline size_t nd_warp_smem(int cap, int d) {
+    return static_cast<size_t>(cap) * 12 + static_cast<size_t>((d + 3) / 4) * 16;
+}
 
 // initial lists: self + `pool` unique random rows, best k kept (lib.rs:3100-3115)
 __global__ void __launch_bounds__(kWarps * 32) nd_init_kernel(NdArgs p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint64_t* keys = reinterpret_cast<uint64_t*>(smem) + warp * p.cap;
-    int32_t* cand = reinterpret_cast<int32_t*>(reinterpret_cast<uint64_t*>(smem) + kWarps * p.cap) +
-                    warp * p.cap;
+    unsigned char* ws = smem + warp * nd_warp_smem(p.cap, p.d);
+    uint64_t* keys = reinterpret_cast<uint64_t*>(ws);
+    int32_t* cand = reinterpret_cast<int32_t*>(keys + p.cap);
+    float* qs = reinterpret_cast<float*>(cand + p.cap);
     const int64_t i = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
     if (i >= p.n) return;
+    for (int t = lane; t < p.d; t += 32) qs[t] = p.X[i * p.d + t];
     int cnt = 0;
     if (lane == 0) {
         cand[cnt++] = static_cast<int32_t>(i);
@@ -148,15 +192,13 @@ __global__ void __launch_bounds__(kWarps * 32) nd_init_kernel(NdArgs p) {
     }
     cnt = __shfl_sync(0xffffffffu, cnt, 0);
     __syncwarp();
-    for (int c = lane; c < p.cap; c += 32) {
-        uint64_t key = ~0ULL;
-        if (c < cnt) {
-            const int32_t j = cand[c];
-            key = knn_key(pair_distance(p.X, p.norms, i, j, p.d, p.cosine), static_cast<uint32_t>(j));
-        }
-        keys[c] = key;
-    }
+    for (int c = lane; c < p.cap; c += 32)
+        keys[c] = c < cnt ? static_cast<uint64_t>(cand[c]) : ~0ULL;
     __syncwarp();
+    eval_candidates(p.X, p.norms, i, p.d, p.cosine, qs, keys, cnt);
+    __syncwarp();
+    if (lane == 0)
+        atomicAdd(p.evaluated + blockIdx.x % kEvalSlots, static_cast<unsigned long long>(cnt));
     warp_sort_u64(keys, p.cap);
     for (int c = lane; c < p.k; c += 32) {
         p.new_idx[i * p.k + c] = static_cast<int32_t>(key_index(keys[c]));
@@ -167,9 +209,12 @@ __global__ void __launch_bounds__(kWarps * 32) nd_init_kernel(NdArgs p) {
 __global__ void __launch_bounds__(kWarps * 32) nd_iter_kernel(NdArgs p, uint64_t iteration) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint64_t* keys = reinterpret_cast<uint64_t*>(smem) + warp * p.cap;
+    unsigned char* ws = smem + warp * nd_warp_smem(p.cap, p.d);
+    uint64_t* keys = reinterpret_cast<uint64_t*>(ws);
+    float* qs = reinterpret_cast<float*>(reinterpret_cast<int32_t*>(keys + p.cap) + p.cap);
     const int64_t i = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
     if (i >= p.n) return;
+    for (int t = lane; t < p.d; t += 32) qs[t] = p.X[i * p.d + t];
     const int k = p.k;
     // neighbours and neighbours of neighbours, as index keys (duplicates removed after sorting)
     int cnt = 0;
@@ -217,16 +262,12 @@ __global__ void __launch_bounds__(kWarps * 32) nd_iter_kernel(NdArgs p, uint64_t
     __syncwarp();
     const int m = min(uniq, p.maxc);
     // evaluate every candidate
-    for (int c = lane; c < p.cap; c += 32) {
-        uint64_t key = ~0ULL;
-        if (c < m) {
-            const int64_t j = static_cast<int64_t>(keys[c]);
-            key = knn_key(pair_distance(p.X, p.norms, i, j, p.d, p.cosine), static_cast<uint32_t>(j));
-        }
-        __syncwarp();
-        keys[c] = key;
-    }
+    for (int c = m + lane; c < p.cap; c += 32) keys[c] = ~0ULL;
     __syncwarp();
+    eval_candidates(p.X, p.norms, i, p.d, p.cosine, qs, keys, m);
+    __syncwarp();
+    if (lane == 0)
+        atomicAdd(p.evaluated + blockIdx.x % kEvalSlots, static_cast<unsigned long long>(m));
     warp_sort_u64(keys, p.cap);
     bool diff = false;
     for (int c = lane; c < k; c += 32) {
@@ -243,7 +284,7 @@ __global__ void __launch_bounds__(kWarps * 32) nd_iter_kernel(NdArgs p, uint64_t
 
 int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t candidate_pool,
                   int64_t n_iters, uint64_t seed, int32_t* out_idx, float* out_dist,
-                  cudaStream_t s) {
+                  cudaStream_t s, NdStats* stats) {
     if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE)
         invalid("the B200 NN-descent kernel supports metric euclidean and cosine");
     if (n < 2 || k < 1 || k >= n) invalid("NN-descent needs 1 <= k < n_rows");
@@ -254,8 +295,9 @@ int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t c
     int cap = 32;
     const int need = std::max(k + k * k + 1 + expl, pool + 1);
     while (cap < need) cap <<= 1;
-    const size_t smem = static_cast<size_t>(kWarps) * cap * 12;
-    if (smem > 200 * 1024) invalid("n_neighbors too large for the NN-descent kernel");
+    const size_t smem = static_cast<size_t>(kWarps) * nd_warp_smem(cap, d);
+    if (smem > 200 * 1024)
+        invalid("n_neighbors / n_features too large for the NN-descent kernel");
     DevBuf<float> norms;
     if (metric == UMAPB_METRIC_COSINE) {
         norms.alloc(n, s);
@@ -264,7 +306,10 @@ int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t c
     DevBuf<int32_t> idx_b(n * k, s);
     DevBuf<float> dist_b(n * k, s);
     DevBuf<int> changed(1, s);
+    DevBuf<unsigned long long> evaluated(kEvalSlots, s);
+    UMAPB_CUDA(cudaMemsetAsync(evaluated.get(), 0, kEvalSlots * 8, s));
     NdArgs p{};
+    p.evaluated = evaluated.get();
     p.X = X;
     p.norms = norms.get();
     p.n = n;
@@ -289,8 +334,20 @@ int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t c
     float* nxt_d = dist_b.get();
     p.new_idx = cur_i;
     p.new_dist = cur_d;
+    cudaEvent_t e0, e1;
+    UMAPB_CUDA(cudaEventCreate(&e0));
+    UMAPB_CUDA(cudaEventCreate(&e1));
+    float kernel_ms = 0.0f;
+    UMAPB_CUDA(cudaEventRecord(e0, s));
     nd_init_kernel<<<grid, kWarps * 32, smem, s>>>(p);
     UMAPB_LAUNCH_CHECK();
+    UMAPB_CUDA(cudaEventRecord(e1, s));
+    UMAPB_CUDA(cudaEventSynchronize(e1));
+    {
+        float ms = 0.0f;
+        UMAPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        kernel_ms += ms;
+    }
     int64_t ran = 0;
     for (int64_t it = 0; it < n_iters; ++it) {
         UMAPB_CUDA(cudaMemsetAsync(changed.get(), 0, 4, s));
@@ -298,15 +355,31 @@ int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t c
         p.old_dist = cur_d;
         p.new_idx = nxt_i;
         p.new_dist = nxt_d;
+        UMAPB_CUDA(cudaEventRecord(e0, s));
         nd_iter_kernel<<<grid, kWarps * 32, smem, s>>>(p, static_cast<uint64_t>(it + 1));
         UMAPB_LAUNCH_CHECK();
+        UMAPB_CUDA(cudaEventRecord(e1, s));
         std::swap(cur_i, nxt_i);
         std::swap(cur_d, nxt_d);
         ran = it + 1;
         int h = 0;
         UMAPB_CUDA(cudaMemcpyAsync(&h, changed.get(), 4, cudaMemcpyDeviceToHost, s));
         UMAPB_CUDA(cudaStreamSynchronize(s));
+        float ms = 0.0f;
+        UMAPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        kernel_ms += ms;
         if (!h) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+        unsigned long long ev[kEvalSlots] = {};
+        UMAPB_CUDA(cudaMemcpyAsync(ev, evaluated.get(), sizeof(ev), cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        int64_t total = 0;
+        for (int e = 0; e < kEvalSlots; ++e) total += static_cast<int64_t>(ev[e]);
+        stats->candidates = total;
+        stats->kernel_sec = kernel_ms * 1e-3;
     }
     if (cur_i != out_idx) {
         UMAPB_CUDA(cudaMemcpyAsync(out_idx, cur_i, n * k * 4, cudaMemcpyDeviceToDevice, s));
