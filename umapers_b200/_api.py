@@ -523,13 +523,13 @@ class Umap:
         y:
             Ignored unless ``target_metric="categorical"``.
         out:
-            Optional writable ``float32`` buffer of shape
-            ``(n_samples, n_components)``; filled in place and returned.
+            Optional writable, C-contiguous buffer of dtype ``float32`` and
+            shape ``(n_samples, n_components)``; filled in place and returned.
 
         Returns
         -------
         numpy.ndarray
-            The embedding, shape ``(n_samples, n_components)``.
+            The embedding, dtype ``float32``, shape ``(n_samples, n_components)``.
         """
         csr = _maybe_as_csr_parts(data, "data")
         if csr is not None:
@@ -598,6 +598,10 @@ class Umap:
         out: np.ndarray | None = None,
     ) -> np.ndarray:
         """Fit from a precomputed kNN graph and return the embedding.
+
+        An advanced entry point for callers that already hold neighbour lists
+        (from another index, or a cached run): the kNN stage is skipped and
+        the given lists feed the fuzzy graph directly.
 
         Parameters
         ----------
