@@ -46,7 +46,9 @@
 //    are recomputed.
 // 4. Rows that fail (near-ties wider than the bound, or too few listed
 //    candidates below B) run a second pass as a query set with at least two
-//    candidate splits, i.e. twice as many lists per row; rows that still fail
+//    candidate splits, i.e. twice as many lists per row, on operands in the
+//    three-term FP16 split h.h' + h.l' + l.h' (l = fp16(x - h), K' =
+//    3d + 6), whose bound is about 2^-21 of the norms; rows that still fail
 //    (duplicates beyond the lists, zero cosine rows) are recomputed by
 //    knn_plain.
 //
@@ -79,15 +81,17 @@ constexpr int kNormCols = 6;              // 3 + 3 FP16 columns of the folded ro
 constexpr int kMaxStages = 8;
 constexpr size_t kSmemLimit = 227 * 1024;
 
-// Operand geometry for d features: K' columns used by the MMA (kmma), the
-// stored row length (at least one 64-column block), k-blocks, and the k-steps
-// of 16 columns issued in the last k-block.
+// Operand geometry for d features in `terms` product terms (1: h.h'; 3: the
+// split h.h' + h.l' + l.h' with l = fp16(x - h)): K' columns used by the MMA
+// (kmma), the stored row length (at least one 64-column block), k-blocks,
+// and the k-steps of 16 columns issued in the last k-block.
 struct Geom {
-    int kmma, kst, kb, tail;
+    int terms, kmma, kst, kb, tail;
 };
-inline Geom geom(int d) {
+inline Geom geom(int d, int terms = 1) {
     Geom g;
-    g.kmma = ((d + kNormCols + UK - 1) / UK) * UK;
+    g.terms = terms;
+    g.kmma = ((terms * d + kNormCols + UK - 1) / UK) * UK;
     g.kst = std::max(g.kmma, BK);
     g.kb = (g.kmma + BK - 1) / BK;
     g.tail = (g.kmma - BK * (g.kb - 1)) / UK;
@@ -99,6 +103,8 @@ inline Geom geom(int d) {
 // scaled FP32 squared norms), e = c0 for cosine.  Terms (u = 2^-11 the FP16
 // unit roundoff, eta = 2^-25 half the FP16 subnormal spacing):
 //   2u + u^2            the one-term FP16 product, |x||y| <= (n_i + n_j) / 2
+//                       (3.1 * 2^-22 for the three-term split: |l| <= u|x|,
+//                       |x - h - l| <= u^2 |x|)
 //   2.01 K' 2^-23       FP32 accumulation of K' terms (truncating adders)
 //   d 2^-24             the FP32 norms
 //   2 (d + 16) 2^-24    the reference's FP32 sum and subtractions (d <= 2(n_i + n_j))
@@ -108,21 +114,23 @@ inline Geom geom(int d) {
 struct Bound {
     double c, c0;
 };
-inline Bound bound_for(int d, int kmma, bool cosine) {
+inline Bound bound_for(int d, const Geom& g, bool cosine) {
     const double u = std::ldexp(1.0, -11), eta = std::ldexp(1.0, -25);
     const double sd = std::sqrt(static_cast<double>(d));
+    const double prod = g.terms == 1 ? 2.0 * u + u * u : 3.1 * u * u;
+    const double t = g.terms;  // subnormal errors enter once per product term
     Bound b;
     if (!cosine) {
-        b.c = 1.25 * (2.0 * u + u * u + 2.01 * kmma * std::ldexp(1.0, -23) +
-                      d * std::ldexp(1.0, -24) + 2.0 * (d + 16) * std::ldexp(1.0, -24) +
-                      2.0 * eta * sd * 1.01 + std::ldexp(1.0, -23));
-        b.c0 = 2.0 * (4.1 * eta * sd + 6.0 * eta);
+        b.c = 1.25 * (prod + 2.01 * g.kmma * std::ldexp(1.0, -23) + d * std::ldexp(1.0, -24) +
+                      2.0 * (d + 16) * std::ldexp(1.0, -24) + 2.0 * t * eta * sd * 1.01 +
+                      std::ldexp(1.0, -23));
+        b.c0 = 2.0 * (4.1 * t * eta * sd + 6.0 * eta);
     } else {
-        // unit rows: |x^.y^ - cos| <= (2u + u^2)(1 + d 2^-23) + subnormals,
+        // unit rows: |x^.y^ - cos| <= prod (1 + d 2^-23) + subnormals,
         // |cos_ref - cos| <= (2d + 16) 2^-24 (dot, norms, product, division)
         b.c = 0.0;
-        b.c0 = 1.25 * (2.0 * u + u * u + 4.0 * eta * sd +
-                       (3.0 * d + 2.01 * kmma + 16.0) * std::ldexp(1.0, -23)) +
+        b.c0 = 1.25 * (prod + 4.0 * t * eta * sd +
+                       (3.0 * d + 2.01 * g.kmma + 16.0) * std::ldexp(1.0, -23)) +
                12.0 * eta;
     }
     return b;
@@ -574,12 +582,14 @@ __device__ __forceinline__ void split3(float v, __half* o) {
     o[2] = __float2half_rn(r2);
 }
 
-// One warp per operand row: the FP16 row (scaled or unit-normalised), the
-// six folded columns, and zeros up to the stored width.  `sq` holds the
-// FP32 squared norms in the reference's order (row_norms).
+// One warp per operand row: the FP16 row (scaled or unit-normalised) in one
+// term ([alpha h] against [h]) or three ([alpha h | alpha h | alpha l]
+// against [h | l | h]), the six folded columns, and zeros up to the stored
+// width.  `sq` holds the FP32 squared norms in the reference's order
+// (row_norms).
 __global__ void prep_kernel(const float* __restrict__ X, const float* __restrict__ sq, int64_t n,
-                            int d, int kst, const ScaleInfo* __restrict__ sc, double c, double c0,
-                            bool cosine, bool is_query, __half* __restrict__ out) {
+                            int d, int terms, int kst, const ScaleInfo* __restrict__ sc, double c,
+                            double c0, bool cosine, bool is_query, __half* __restrict__ out) {
     const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
@@ -593,11 +603,28 @@ __global__ void prep_kernel(const float* __restrict__ X, const float* __restrict
     } else {
         mul = sc->s;
     }
+    const float alpha = cosine ? -1.0f : -2.0f;  // exact scalings of FP16 values
     for (int t = lane; t < d; t += 32) {
-        const __half h = __float2half_rn(x[t] * mul);
-        o[t] = !is_query ? h : (cosine ? __hneg(h) : __float2half_rn(-2.0f * __half2float(h)));
+        const float v = x[t] * mul;
+        const __half h = __float2half_rn(v);
+        if (terms == 1) {
+            o[t] = is_query ? __float2half_rn(alpha * __half2float(h)) : h;
+        } else {
+            const __half l = __float2half_rn(v - __half2float(h));
+            if (is_query) {
+                const __half ah = __float2half_rn(alpha * __half2float(h));
+                o[t] = ah;
+                o[d + t] = ah;
+                o[2 * d + t] = __float2half_rn(alpha * __half2float(l));
+            } else {
+                o[t] = h;
+                o[d + t] = l;
+                o[2 * d + t] = h;
+            }
+        }
     }
-    for (int t = d + kNormCols + lane; t < kst; t += 32) o[t] = __float2half_rn(0.0f);
+    const int nc = terms * d;  // first folded column
+    for (int t = nc + kNormCols + lane; t < kst; t += 32) o[t] = __float2half_rn(0.0f);
     if (lane == 0) {
         float a;
         if (cosine)
@@ -610,11 +637,11 @@ __global__ void prep_kernel(const float* __restrict__ X, const float* __restrict
         __half parts[3];
         split3(a, parts);
         if (is_query) {
-            o[d] = one; o[d + 1] = one; o[d + 2] = one;
-            o[d + 3] = parts[0]; o[d + 4] = parts[1]; o[d + 5] = parts[2];
+            o[nc] = one; o[nc + 1] = one; o[nc + 2] = one;
+            o[nc + 3] = parts[0]; o[nc + 4] = parts[1]; o[nc + 5] = parts[2];
         } else {
-            o[d] = parts[0]; o[d + 1] = parts[1]; o[d + 2] = parts[2];
-            o[d + 3] = one; o[d + 4] = one; o[d + 5] = one;
+            o[nc] = parts[0]; o[nc + 1] = parts[1]; o[nc + 2] = parts[2];
+            o[nc + 3] = one; o[nc + 4] = one; o[nc + 5] = one;
         }
     }
 }
@@ -1071,7 +1098,7 @@ void launch_prep(const float* X, const float* sq, int64_t n, int d, const Geom& 
                  cudaStream_t s) {
     if (n == 0) return;
     prep_kernel<<<static_cast<unsigned>(ceil_div(n * 32, 256)), 256, 0, s>>>(
-        X, sq, n, d, g.kst, sc, b.c, b.c0, cosine, query, out);
+        X, sq, n, d, g.terms, g.kst, sc, b.c, b.c0, cosine, query, out);
     UMAPB_LAUNCH_CHECK();
 }
 
@@ -1128,7 +1155,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     const float* const R0 = R;
     const Geom g = geom(d);
     const Shape sh = shape_for(g.kb);
-    const Bound bd = bound_for(d, g.kmma, cosine);
+    const Bound bd = bound_for(d, g, cosine);
     TcArgs a = plan(n_q, n_r, g, sh, true, 1);
     CellOrder co;
     const int cells = self && a.n_split == 1 ? cell_count(n_q, d) : 0;
@@ -1204,31 +1231,49 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     const int64_t fb = h[1];
     int64_t fb_final = 0;
     if (fb > 0) {
-        // Second pass: the failed rows as a query set against the same
-        // candidate operand, with at least two candidate splits (twice as many
-        // lists per row, so B rises further above the k-th neighbour).
+        // Second pass: the failed rows as a query set, with at least two
+        // candidate splits (twice as many lists per row) and, where the
+        // operands fit shared memory, the three-term FP16 split, whose bound
+        // is about 2^-21 of the norms instead of 2^-10.
         lists.release();
         A.release();
+        Geom g2 = geom(d, 3);
+        Shape sh2 = shape_for(g2.kb);
+        if (sh2.st == 0) {
+            g2 = g;
+            sh2 = sh;
+        }
+        const Bound bd2 = bound_for(d, g2, cosine);
+        DevBuf<__half> B2;
+        CUtensorMap mb2 = mb;
+        if (g2.terms != g.terms) {
+            B.release();
+            B2.alloc(static_cast<size_t>(n_r) * g2.kst, s);
+            launch_prep(R, rsq_p, n_r, d, g2, sc.get(), bd2, cosine, false, B2.get(), s);
+            mb2 = make_f16_map(B2.get(), n_r, g2.kst, sh2.bn);
+        }
         DevBuf<float> Q2(static_cast<size_t>(fb) * d, s), q2sq(fb, s);
         gather_rows_kernel<<<static_cast<unsigned>(ceil_div(fb * 32, 256)), 256, 0, s>>>(
             Q0, fb_rows.get(), fb, d, Q2.get());
         UMAPB_LAUNCH_CHECK();
         row_norms(Q2.get(), fb, d, nullptr, q2sq.get(), s);
-        DevBuf<__half> A2(static_cast<size_t>(fb) * g.kst, s);
-        launch_prep(Q2.get(), q2sq.get(), fb, d, g, sc.get(), bd, cosine, true, A2.get(), s);
-        TcArgs a2 = plan(fb, n_r, g, sh, true, 2);
-        const int n_lists2 = sh.lists() * a2.n_split;
+        DevBuf<__half> A2(static_cast<size_t>(fb) * g2.kst, s);
+        launch_prep(Q2.get(), q2sq.get(), fb, d, g2, sc.get(), bd2, cosine, true, A2.get(), s);
+        TcArgs a2 = plan(fb, n_r, g2, sh2, true, 2);
+        const int n_lists2 = sh2.lists() * a2.n_split;
         DevBuf<uint64_t> lists2(static_cast<size_t>(fb) * n_lists2 * S, s);
         UMAPB_CUDA(cudaMemsetAsync(lists2.get(), 0xFF, lists2.bytes(), s));
-        const CUtensorMap ma2 = make_f16_map(A2.get(), fb, g.kst, BM);
+        const CUtensorMap ma2 = make_f16_map(A2.get(), fb, g2.kst, BM);
         a2.lists = lists2.get();
         a2.err = flags.get() + 2;
         EventPair ev2;
         UMAPB_CUDA(cudaEventRecord(ev2.e0, s));
-        launch_tc(sh, ma2, mb, a2, s);
+        launch_tc(sh2, ma2, mb2, a2, s);
         UMAPB_CUDA(cudaEventRecord(ev2.e1, s));
         DevBuf<int32_t> fb2_rows(fb, s);
         RerankArgs rb = ra;
+        rb.c = bd2.c;
+        rb.c0 = bd2.c0;
         rb.Q = Q2.get();
         rb.qsq = q2sq.get();
         rb.lists = lists2.get();
@@ -1339,7 +1384,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     }
     const Geom g = geom(d);
     const Shape sh = shape_for(g.kb);
-    const Bound bd = bound_for(d, g.kmma, false);
+    const Bound bd = bound_for(d, g, false);
     unsigned char* base = noalloc_scratch();
     size_t off = 0;
     auto carve = [&](size_t bytes) {

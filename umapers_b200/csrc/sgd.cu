@@ -11,6 +11,14 @@
 // sample) instead of the reference's shared SmallRng, so results do not depend
 // on scheduling.  The embedding (n x dim FP32, 8 MB at 1M x 2) stays in L2.
 //
+// Small graphs (n_vertices x dim within kSmallLayoutFloats) run instead in
+// one CTA that holds the embedding in shared memory for all epochs: the
+// edges are coloured greedily in graph order so that no two edges of a colour
+// share a vertex, and each epoch walks the colours in order, a colour's
+// edges in parallel (Gauss-Seidel by colour).  Heads and tails are then
+// updated without atomics, negatives read the epoch's starting positions,
+// and the result is the same on every run.
+//
 // transform_layout: init_graph_transform (lib.rs:4793-4836) followed by
 // optimize_layout_transform (lib.rs:5444-5544).  Queries never interact, so
 // one thread runs one query's whole schedule sequentially, as the reference's
@@ -413,6 +421,244 @@ __global__ void __launch_bounds__(256) sgd_epoch_nd(SgdArgs p) {
         }
     }
     if (p.block_samples) count_block_samples(p.block_samples, sampled);
+}
+
+// ------------------------------------------------------ small graphs ----
+// Graphs with n_vertices * dim up to this many floats take the one-CTA
+// coloured layout (two copies in shared memory: 128 KiB).
+constexpr int64_t kSmallLayoutFloats = 16384;
+constexpr int kSmallThreads = 1024;
+
+struct SmallArgs {
+    float* emb;               // n x dim, global (read at start, written at end)
+    const int32_t* heads;     // edges ordered by (colour, graph order)
+    const int32_t* tails;
+    const float* eps;
+    float* next;
+    float* next_neg;
+    const int32_t* color_ptr; // n_colors + 1 offsets
+    int n_colors;
+    uint32_t n_vertices;
+    int dim;
+    int64_t n_epochs;
+    float lr, a, b, att_factor, rep_factor, neg_rate_f;
+    const int64_t* edge_id;   // graph-order id of each edge (keys its negative stream)
+    uint64_t seed;
+    unsigned long long* samples;  // attractive samples over all epochs
+};
+
+// The reference's per-edge arithmetic (lib.rs:5172-5318) on shared-memory
+// positions: `cur` is the live embedding, `snap` its state at the start of
+// the epoch (read by the negative samples).
+__global__ void __launch_bounds__(kSmallThreads, 1) sgd_small_kernel(SmallArgs p) {
+    extern __shared__ float sm[];
+    const int dim = p.dim;
+    const int64_t nf = static_cast<int64_t>(p.n_vertices) * dim;
+    float* cur = sm;
+    float* snap = sm + nf;
+    for (int64_t i = threadIdx.x; i < nf; i += blockDim.x) cur[i] = p.emb[i];
+    unsigned long long sampled = 0;
+    const float nef = static_cast<float>(p.n_epochs);
+    for (int64_t epoch = 0; epoch < p.n_epochs; ++epoch) {
+        __syncthreads();
+        for (int64_t i = threadIdx.x; i < nf; i += blockDim.x) snap[i] = cur[i];
+        __syncthreads();
+        const float alpha = p.lr * (1.0f - static_cast<float>(epoch) / nef);
+        const float ef = static_cast<float>(epoch);
+        for (int c = 0; c < p.n_colors; ++c) {
+            for (int32_t e = p.color_ptr[c] + threadIdx.x; e < p.color_ptr[c + 1];
+                 e += blockDim.x) {
+                const float nxt = p.next[e];
+                if (nxt > ef) continue;
+                ++sampled;
+                const int32_t head = p.heads[e], tail = p.tails[e];
+                float h[kMaxDim];
+                for (int d = 0; d < dim; ++d) h[d] = cur[head * dim + d];
+                if (head != tail) {
+                    float d2 = 0.0f;
+                    for (int d = 0; d < dim; ++d) {
+                        const float df = __fsub_rn(h[d], cur[tail * dim + d]);
+                        d2 = __fadd_rn(d2, __fmul_rn(df, df));
+                    }
+                    if (d2 > 0.0f) {
+                        const float pb = pow_pos(d2, p.b);
+                        const float gc = __fdiv_rn(__fmul_rn(p.att_factor, __fdiv_rn(pb, d2)),
+                                                   __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
+                        for (int d = 0; d < dim; ++d) {
+                            const float g = clip4(__fmul_rn(gc, __fsub_rn(h[d], cur[tail * dim + d])));
+                            const float mv = __fmul_rn(g, alpha);
+                            h[d] = __fadd_rn(h[d], mv);
+                            cur[tail * dim + d] = __fsub_rn(cur[tail * dim + d], mv);
+                        }
+                    }
+                }
+                const float eps = p.eps[e];
+                p.next[e] = __fadd_rn(nxt, eps);
+                const float en = __fdiv_rn(eps, p.neg_rate_f);
+                if (isfinite(en) && en > 0.0f) {
+                    const float nn = p.next_neg[e];
+                    const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(ef, nn), en));
+                    const uint64_t eid = static_cast<uint64_t>(p.edge_id[e]);
+                    for (uint32_t sn = 0; sn < n_neg; ++sn) {
+                        const uint64_t word =
+                            rng_word(p.seed, eid, (static_cast<uint64_t>(epoch) << 32) | sn);
+                        const uint32_t neg = rng_below(word, p.n_vertices);
+                        if (neg == static_cast<uint32_t>(head)) continue;
+                        const float* o = snap + static_cast<int64_t>(neg) * dim;
+                        float d2 = 0.0f;
+                        for (int d = 0; d < dim; ++d) {
+                            const float df = __fsub_rn(h[d], o[d]);
+                            d2 = __fadd_rn(d2, __fmul_rn(df, df));
+                        }
+                        if (d2 > 0.0f) {
+                            const float pb = pow_pos(d2, p.b);
+                            const float gc = __fdiv_rn(
+                                p.rep_factor,
+                                __fmul_rn(__fadd_rn(0.001f, d2), __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
+                            if (gc > 0.0f)
+                                for (int d = 0; d < dim; ++d)
+                                    h[d] = __fadd_rn(
+                                        h[d], __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(h[d], o[d]))),
+                                                        alpha));
+                        }
+                    }
+                    p.next_neg[e] = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), en));
+                }
+                for (int d = 0; d < dim; ++d) cur[head * dim + d] = h[d];
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < nf; i += blockDim.x) p.emb[i] = cur[i];
+    if (p.samples && sampled) atomicAdd(p.samples, sampled);
+}
+
+// Greedy edge colouring in graph order: each edge takes the smallest colour
+// not yet used at its head or its tail.  Returns the colour of every edge.
+std::vector<int32_t> color_edges(const std::vector<int32_t>& heads,
+                                 const std::vector<int32_t>& tails, int64_t n, int* n_colors) {
+    const int64_t m = static_cast<int64_t>(heads.size());
+    std::vector<std::vector<uint64_t>> used(n);
+    std::vector<int32_t> color(m);
+    int top = 0;
+    auto is_used = [&](int64_t v, int c) {
+        const auto& u = used[v];
+        const size_t w = static_cast<size_t>(c) >> 6;
+        return w < u.size() && ((u[w] >> (c & 63)) & 1u);
+    };
+    auto mark = [&](int64_t v, int c) {
+        auto& u = used[v];
+        const size_t w = static_cast<size_t>(c) >> 6;
+        if (u.size() <= w) u.resize(w + 1, 0);
+        u[w] |= uint64_t{1} << (c & 63);
+    };
+    for (int64_t e = 0; e < m; ++e) {
+        const int64_t h = heads[e], t = tails[e];
+        int c = 0;
+        while (is_used(h, c) || is_used(t, c)) ++c;
+        color[e] = c;
+        mark(h, c);
+        mark(t, c);
+        top = std::max(top, c + 1);
+    }
+    *n_colors = top;
+    return color;
+}
+
+// The one-CTA coloured layout of a small graph; returns the sample count.
+double optimize_layout_small(float* emb, int64_t n_vertices, int dim, const Graph& g,
+                             int64_t n_epochs, float a, float b, float lr, int64_t neg_rate,
+                             float repulsion, uint64_t seed, float* kernel_ms, cudaStream_t s) {
+    const int64_t m = g.n_edges;
+    std::vector<int32_t> hh(m), th(m);
+    UMAPB_CUDA(cudaMemcpyAsync(hh.data(), g.heads.get(), m * 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(th.data(), g.tails.get(), m * 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    int n_colors = 0;
+    const std::vector<int32_t> color = color_edges(hh, th, n_vertices, &n_colors);
+    std::vector<int32_t> ptr(n_colors + 1, 0);
+    for (int32_t c : color) ++ptr[c + 1];
+    for (int c = 0; c < n_colors; ++c) ptr[c + 1] += ptr[c];
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1), oh(m), ot(m);
+    std::vector<int64_t> oid(m);
+    for (int64_t e = 0; e < m; ++e) {
+        const int32_t at = fill[color[e]]++;
+        oh[at] = hh[e];
+        ot[at] = th[e];
+        oid[at] = e;
+    }
+    const float mx = std::max(max_weight(g.weights.get(), m, s), 1e-12f);
+    const float nef = static_cast<float>(n_epochs);
+    const float nrf = static_cast<float>(neg_rate);
+    // edge periods in graph order (make_epochs_per_sample, lib.rs:4937-4960),
+    // then permuted into colour order on the host
+    DevBuf<float> eps_raw(m, s);
+    epochs_per_sample_kernel<<<static_cast<unsigned>(ceil_div(m, 256)), 256, 0, s>>>(
+        g.weights.get(), m, mx, nef, nrf, eps_raw.get(), nullptr, nullptr);
+    UMAPB_LAUNCH_CHECK();
+    std::vector<float> er(m), eo(m), no(m);
+    UMAPB_CUDA(cudaMemcpyAsync(er.data(), eps_raw.get(), m * 4, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    for (int64_t e = 0; e < m; ++e) {
+        eo[e] = er[oid[e]];
+        no[e] = eo[e] / nrf;  // the same FP32 division as gather_edges_kernel
+    }
+    DevBuf<int32_t> dh(m, s), dt(m, s), dptr(n_colors + 1, s);
+    DevBuf<int64_t> did(m, s);
+    DevBuf<float> deps(m, s), dnext(m, s), dneg(m, s);
+    DevBuf<unsigned long long> samples(1, s);
+    UMAPB_CUDA(cudaMemcpyAsync(dh.get(), oh.data(), m * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(dt.get(), ot.data(), m * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(did.get(), oid.data(), m * 8, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(dptr.get(), ptr.data(), (n_colors + 1) * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(deps.get(), eo.data(), m * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(dnext.get(), eo.data(), m * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(dneg.get(), no.data(), m * 4, cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemsetAsync(samples.get(), 0, 8, s));
+    SmallArgs p{};
+    p.emb = emb;
+    p.heads = dh.get();
+    p.tails = dt.get();
+    p.eps = deps.get();
+    p.next = dnext.get();
+    p.next_neg = dneg.get();
+    p.color_ptr = dptr.get();
+    p.n_colors = n_colors;
+    p.n_vertices = static_cast<uint32_t>(n_vertices);
+    p.dim = dim;
+    p.n_epochs = n_epochs;
+    p.lr = lr;
+    p.a = a;
+    p.b = b;
+    p.att_factor = -2.0f * a * b;
+    p.rep_factor = 2.0f * repulsion * b;
+    p.neg_rate_f = nrf;
+    p.edge_id = did.get();
+    p.seed = seed;
+    p.samples = samples.get();
+    const size_t smem = static_cast<size_t>(2 * n_vertices * dim) * sizeof(float);
+    UMAPB_CUDA(cudaFuncSetAttribute(sgd_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (kernel_ms) {
+        UMAPB_CUDA(cudaEventCreate(&e0));
+        UMAPB_CUDA(cudaEventCreate(&e1));
+        UMAPB_CUDA(cudaEventRecord(e0, s));
+    }
+    sgd_small_kernel<<<1, kSmallThreads, smem, s>>>(p);
+    UMAPB_LAUNCH_CHECK();
+    if (kernel_ms) {
+        UMAPB_CUDA(cudaEventRecord(e1, s));
+        UMAPB_CUDA(cudaEventSynchronize(e1));
+        UMAPB_CUDA(cudaEventElapsedTime(kernel_ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    unsigned long long h = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&h, samples.get(), 8, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    return static_cast<double>(h);
 }
 
 // ------------------------------------------------------------ transform --
@@ -1092,6 +1338,9 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
     const int64_t m = g.n_edges;
     if (m == 0 || n_vertices == 0 || n_epochs == 0) return 0.0;
     if (dim > kMaxDim) invalid("n_components above 16 is not supported by the GPU layout kernel");
+    if (!dens && n_vertices * dim <= kSmallLayoutFloats && m <= 0x7FFFFFFFll)
+        return optimize_layout_small(emb, n_vertices, dim, g, n_epochs, a, b, lr, neg_rate,
+                                     repulsion, seed, kernel_ms, s);
     const float mx = std::max(max_weight(g.weights.get(), m, s), 1e-12f);
     DevBuf<int32_t> sorted_heads, sorted_tails;
     if (m > 0x7FFFFFFFll) invalid("optimize_layout: too many edges");
