@@ -334,13 +334,15 @@ int32_t umapb_knn_exact(const float* data, int64_t n_rows, int64_t n_cols, int64
  * `dists` (n_rows x k f32) are device pointers; `stream` is a cudaStream_t
  * (NULL = legacy default stream).  Results equal umapb_knn_exact's.
  * Scratch comes from one static device array of 64 MiB that every GPU loading
- * the library holds until exit: about 43,000 rows at 64 columns; larger
+ * the library holds until exit: about 49,000 rows at 64 columns; larger
  * inputs are rejected with UMAPB_ERR_INVALID_PARAMETER naming the limit.  No
  * cudaMalloc/cudaFree or allocating library routine is called.  The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress),
- * so make that first call before any stream capture.  Every call reuses the
- * same array: calls that overlap on the GPU (other streams, other threads)
- * race and must be serialised by the caller. */
+ * so make that first call before any stream capture.  The call reads the
+ * kernel's status and the count of rows it recomputes on the plain path back
+ * to the host, so it waits for `stream` before it returns.  Every call reuses
+ * the same array: calls that overlap on the GPU (other streams, other
+ * threads) race and must be serialised by the caller. */
 int32_t umapb_knn_exact_noalloc(const float* data, int64_t n_rows, int64_t n_cols, int64_t k,
                                 int32_t* indices, float* dists, void* stream);
 
