@@ -25,10 +25,11 @@ int64_t first_nonfinite_row(const float* X, int64_t n, int d, cudaStream_t s);
 // Exact kNN on FP32 CUDA cores in the reference's summation order.
 // Query row r is Q[q_rows ? q_rows[r] : r] and its result goes to output row
 // q_rows ? q_rows[r] : r.  Distances: euclidean = sqrt of the FP32 squared
-// distance; cosine = 1 - clamp(dot / (|q||r|)).
+// distance; cosine = 1 - clamp(dot / (|q||r|)).  Few query rows are spread
+// over the candidates with partial lists in scratch, unless !allow_scratch.
 void knn_plain(const float* Q, const int32_t* q_rows, int64_t n_q, const float* R, int64_t n_r,
                int d, int k, int metric, const float* qnorm, const float* rnorm,
-               int32_t* out_idx, float* out_dist, cudaStream_t s);
+               int32_t* out_idx, float* out_dist, cudaStream_t s, bool allow_scratch = true);
 
 // ------------------------------------------------------------- knn_tc.cu
 struct TcKnnStats {

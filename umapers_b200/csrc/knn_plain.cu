@@ -44,12 +44,17 @@ __device__ inline int lane_pos(int dim, const LaneLayout& L) {
     return (dim % L.nl) * L.ll + dim / L.nl;
 }
 
+// Candidate rows [blockIdx.y * span, min(n_r, (blockIdx.y + 1) * span)) are
+// scanned by this CTA.  With `part` non-null the CTA writes its k smallest
+// keys to part[(blockIdx.y * n_q + row) * k ...] for knn_merge_kernel instead
+// of the final outputs.
 template <int QT, int CT, bool COSINE>
 __global__ void __launch_bounds__(kThreads)
     knn_plain_kernel(const float* __restrict__ Q, const int32_t* __restrict__ q_rows, int64_t n_q,
                      const float* __restrict__ R, int64_t n_r, int d, int k,
                      const float* __restrict__ qnorm, const float* __restrict__ rnorm,
-                     int32_t* __restrict__ out_idx, float* __restrict__ out_dist) {
+                     int32_t* __restrict__ out_idx, float* __restrict__ out_dist, int64_t span,
+                     uint64_t* __restrict__ part) {
     constexpr int TQ = QT / 16;
     constexpr int TC = CT / 16;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -83,12 +88,14 @@ __global__ void __launch_bounds__(kThreads)
     }
     for (int e = tid; e < QT * k; e += kThreads) lists[e] = ~0ULL;
 
-    for (int64_t c0 = 0; c0 < n_r; c0 += CT) {
+    const int64_t c_begin = static_cast<int64_t>(blockIdx.y) * span;
+    const int64_t c_end = min(n_r, c_begin + span);
+    for (int64_t c0 = c_begin; c0 < c_end; c0 += CT) {
         __syncthreads();  // previous tile's list updates are done
         for (int e = tid; e < CT * d; e += kThreads) {
             const int r = e / d, dim = e % d;
             const int64_t cc = c0 + r;
-            Cs[lane_pos(dim, L) * CT + r] = cc < n_r ? R[cc * d + dim] : 0.0f;
+            Cs[lane_pos(dim, L) * CT + r] = cc < c_end ? R[cc * d + dim] : 0.0f;
         }
         __syncthreads();
 
@@ -154,7 +161,7 @@ __global__ void __launch_bounds__(kThreads)
                     // cosine_distance_with_norms (rust_umap/src/lib.rs:2740-2765)
                     const int64_t cc = c0 + tx * TC + j;
                     const float xn = qn_s[ty * TQ + i];
-                    const float yn = cc < n_r ? rnorm[cc] : 0.0f;
+                    const float yn = cc < c_end ? rnorm[cc] : 0.0f;
                     if (xn == 0.0f && yn == 0.0f) {
                         v = 0.0f;
                     } else if (xn == 0.0f || yn == 0.0f) {
@@ -172,7 +179,7 @@ __global__ void __launch_bounds__(kThreads)
         if (tid < QT && r0 + tid < n_q) {
             uint64_t* list = lists + tid * k;
             uint64_t thr = list[k - 1];
-            const int64_t rem = n_r - c0;
+            const int64_t rem = c_end - c0;
             const int cmax = rem < CT ? static_cast<int>(rem) : CT;
             for (int c = 0; c < cmax; ++c) {
                 const uint64_t key = knn_key(dt[tid * (CT + 1) + c], static_cast<uint32_t>(c0 + c));
@@ -189,6 +196,13 @@ __global__ void __launch_bounds__(kThreads)
         }
     }
     __syncthreads();
+    if (part != nullptr) {
+        if (tid < QT && r0 + tid < n_q) {
+            uint64_t* o = part + (static_cast<int64_t>(blockIdx.y) * n_q + r0 + tid) * k;
+            for (int c = 0; c < k; ++c) o[c] = lists[tid * k + c];
+        }
+        return;
+    }
     if (tid < QT && r0 + tid < n_q) {
         const int64_t rr = r0 + tid;
         const int64_t dst = q_rows ? q_rows[rr] : rr;
@@ -203,23 +217,86 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+// One warp per query row: the k smallest of its `splits` sorted partial
+// lists (repeated warp minimum over the list heads), written as the final
+// outputs (sqrt of the squared distance for euclidean).
+__global__ void knn_merge_kernel(const uint64_t* __restrict__ part, int splits, int64_t n_q,
+                                 int k, const int32_t* __restrict__ q_rows, bool cosine,
+                                 int32_t* __restrict__ out_idx, float* __restrict__ out_dist) {
+    const int64_t row = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n_q) return;
+    const int64_t dst = q_rows ? q_rows[row] : row;
+    // lane l follows the heads of lists l, l + 32, ... (at most 8 per lane)
+    int pos[8];
+    for (int j = 0; j < 8; ++j) pos[j] = 0;
+    for (int c = 0; c < k; ++c) {
+        uint64_t best = ~0ull;
+        int bj = -1;
+        for (int j = 0; j < 8; ++j) {
+            const int sp = lane + 32 * j;
+            if (sp >= splits || pos[j] >= k) continue;
+            const uint64_t v = part[(static_cast<int64_t>(sp) * n_q + row) * k + pos[j]];
+            if (v < best) {
+                best = v;
+                bj = j;
+            }
+        }
+        uint64_t m = best;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const uint64_t t = __shfl_xor_sync(0xffffffffu, m, o);
+            m = t < m ? t : m;
+        }
+        // keys are unique (indices differ), so exactly one lane holds the minimum
+        if (best == m && bj >= 0 && m != ~0ull) ++pos[bj];
+        if (lane == 0) {
+            out_idx[dst * k + c] = static_cast<int32_t>(key_index(m));
+            const float dd = key_dist(m);
+            out_dist[dst * k + c] = cosine ? dd : __fsqrt_rn(dd);
+        }
+    }
+}
+
 template <int QT, int CT>
 size_t plain_smem(int d, int k) {
     return static_cast<size_t>(d) * (QT + CT) * 4 + static_cast<size_t>(QT) * (CT + 1) * 4 +
            static_cast<size_t>(QT) * k * 8 + 16;
 }
 
+// When the query tiles fill fewer than two waves and scratch may be
+// allocated, the candidate rows are split across CTAs (at least 64 tiles of
+// candidates each) and the partial lists merged per row.
 template <int QT, int CT, bool COS>
 void launch_plain(const float* Q, const int32_t* q_rows, int64_t n_q, const float* R, int64_t n_r,
                   int d, int k, const float* qn, const float* rn, int32_t* oi, float* od,
-                  cudaStream_t s) {
+                  cudaStream_t s, bool allow_scratch) {
     const size_t smem = plain_smem<QT, CT>(d, k);
     auto kern = knn_plain_kernel<QT, CT, COS>;
     UMAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
     const int64_t blocks = ceil_div(n_q, QT);
-    kern<<<static_cast<unsigned>(blocks), kThreads, smem, s>>>(Q, q_rows, n_q, R, n_r, d, k, qn,
-                                                              rn, oi, od);
+    int dev = 0, sms = 0;
+    UMAPB_CUDA(cudaGetDevice(&dev));
+    UMAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int64_t splits = 1;
+    if (allow_scratch && blocks < 2 * sms)
+        splits = std::min<int64_t>(std::min<int64_t>(ceil_div(2 * sms, blocks), 256),
+                                   std::max<int64_t>(1, n_r / (64 * CT)));
+    if (splits <= 1) {
+        kern<<<static_cast<unsigned>(blocks), kThreads, smem, s>>>(Q, q_rows, n_q, R, n_r, d, k,
+                                                                  qn, rn, oi, od, n_r, nullptr);
+        UMAPB_LAUNCH_CHECK();
+        return;
+    }
+    const int64_t span = ceil_div(ceil_div(n_r, splits), CT) * CT;
+    splits = ceil_div(n_r, span);
+    DevBuf<uint64_t> part(static_cast<size_t>(splits) * n_q * k, s);
+    kern<<<dim3(static_cast<unsigned>(blocks), static_cast<unsigned>(splits)), kThreads, smem, s>>>(
+        Q, q_rows, n_q, R, n_r, d, k, qn, rn, oi, od, span, part.get());
+    UMAPB_LAUNCH_CHECK();
+    knn_merge_kernel<<<static_cast<unsigned>(ceil_div(n_q * 32, 256)), 256, 0, s>>>(
+        part.get(), static_cast<int>(splits), n_q, k, q_rows, COS, oi, od);
     UMAPB_LAUNCH_CHECK();
 }
 
@@ -317,7 +394,7 @@ int64_t first_nonfinite_row(const float* X, int64_t n, int d, cudaStream_t s) {
 
 void knn_plain(const float* Q, const int32_t* q_rows, int64_t n_q, const float* R, int64_t n_r,
                int d, int k, int metric, const float* qnorm, const float* rnorm,
-               int32_t* out_idx, float* out_dist, cudaStream_t s) {
+               int32_t* out_idx, float* out_dist, cudaStream_t s, bool allow_scratch) {
     if (n_q == 0) return;
     if (k < 1 || k > n_r) invalid("kNN needs 1 <= k <= number of reference rows");
     const bool cos = metric == UMAPB_METRIC_COSINE;
@@ -327,17 +404,17 @@ void knn_plain(const float* Q, const int32_t* q_rows, int64_t n_q, const float* 
     if (plain_smem<64, 64>(d, k) <= limit) {
         if (cos)
             launch_plain<64, 64, true>(Q, q_rows, n_q, R, n_r, d, k, qnorm, rnorm, out_idx,
-                                       out_dist, s);
+                                       out_dist, s, allow_scratch);
         else
             launch_plain<64, 64, false>(Q, q_rows, n_q, R, n_r, d, k, qnorm, rnorm, out_idx,
-                                        out_dist, s);
+                                        out_dist, s, allow_scratch);
     } else if (plain_smem<32, 32>(d, k) <= limit) {
         if (cos)
             launch_plain<32, 32, true>(Q, q_rows, n_q, R, n_r, d, k, qnorm, rnorm, out_idx,
-                                       out_dist, s);
+                                       out_dist, s, allow_scratch);
         else
             launch_plain<32, 32, false>(Q, q_rows, n_q, R, n_r, d, k, qnorm, rnorm, out_idx,
-                                        out_dist, s);
+                                        out_dist, s, allow_scratch);
     } else {
         invalid("n_features/n_neighbors too large for the exact kNN tile (need d*256 + k*256 < 200 KiB)");
     }

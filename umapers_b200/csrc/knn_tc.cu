@@ -1446,7 +1446,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
                                         std::to_string(flags_h[0]) + ")");
     if (flags_h[1] > 0)
         knn_plain(X, fb_rows, flags_h[1], X, n, d, k, UMAPB_METRIC_EUCLIDEAN, nullptr, nullptr,
-                  out_idx, out_dist, s);
+                  out_idx, out_dist, s, false);
     UMAPB_CUDA(cudaStreamSynchronize(s));
 }
 
