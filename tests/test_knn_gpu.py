@@ -205,3 +205,25 @@ def test_tensor_knn_wide_rows(orc, d):
     pi, pd, _ = gu.knn_exact(x, 12, backend="plain")
     np.testing.assert_array_equal(ti, pi)
     np.testing.assert_array_equal(td, pd)
+
+
+@pytest.mark.parametrize("metric", ["euclidean", "cosine"])
+def test_tensor_knn_k50_bit_exact(orc, metric):
+    # 64-entry re-rank lists: k up to 62 stays on the tensor path
+    x = workloads.isotropic_mixture(2000, 64, 6, 3.0, seed=50)
+    ti, td, fb = gu.knn_exact(x, 50, metric=metric, backend="tensor")
+    oi, od = orc.exact_knn(x, 50, metric=metric)
+    np.testing.assert_array_equal(ti, oi)
+    np.testing.assert_array_equal(td, od)
+    assert fb <= 100
+
+
+def test_tensor_knn_k50_mixture_20000x192(orc):
+    x = workloads.isotropic_mixture(20_000, 192, 10, 4.0, seed=7)
+    ti, td, _ = gu.knn_exact(x, 50, backend="tensor")
+    pi, pd, _ = gu.knn_exact(x, 50, backend="plain")
+    np.testing.assert_array_equal(ti, pi)
+    np.testing.assert_array_equal(td, pd)
+    rows = np.random.default_rng(50).choice(20_000, 60, replace=False)
+    oi, od = orc.exact_knn_rows(x, rows, 50)
+    np.testing.assert_array_equal(ti[rows], oi)

@@ -74,6 +74,7 @@ constexpr int BM = 128;     // query rows per tile (UMMA M)
 constexpr int BK = kBK;     // FP16 columns per k-block (one 128-byte swizzle row)
 constexpr int UK = kUK;     // K of one tcgen05.mma kind::f16
 constexpr int S = 32;       // shortlist length per list
+constexpr int kMaxK = 62;   // neighbours per row on the tensor path (64-entry re-rank lists)
 constexpr int kATileBytes = BM * BK * 2;  // 16 KiB: one query tile's k-block
 constexpr int kBarBytes = 256;            // mbarriers, TMEM address, abort flag
 constexpr int kScratchBytes = 256;        // per epilogue warp: one row's 64 values
@@ -196,6 +197,44 @@ __device__ __forceinline__ uint64_t warp_merge_keys(uint64_t list, uint64_t keys
         m = (lane & st) ? (m > o ? m : o) : (m < o ? m : o);
     }
     return m;
+}
+
+// Sorts a bitonic sequence held one value per lane (five compare-exchange
+// stages), ascending with the lane index.
+template <typename T>
+__device__ __forceinline__ T warp_bitonic_sort(T m) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1) {
+        const T o = __shfl_xor_sync(0xffffffffu, m, st);
+        m = (lane & st) ? (m > o ? m : o) : (m < o ? m : o);
+    }
+    return m;
+}
+
+// A sorted list of the 64 smallest values seen, two per lane: `lo` holds
+// ranks 0-31 and `hi` ranks 32-63, each ascending across the lanes.
+// Merging 32 new values (any order): the 32 smallest of lo and the chunk
+// become lo; the 32 largest of those, merged with hi, give hi.
+template <typename T>
+__device__ __forceinline__ void warp_merge64(T& lo, T& hi, T chunk) {
+    const int lane = threadIdx.x & 31;
+    const T srt = warp_sort_asc<T>(chunk);
+    const T rev = __shfl_sync(0xffffffffu, srt, 31 - lane);
+    const T a = lo < rev ? lo : rev;
+    const T b = lo < rev ? rev : lo;
+    lo = warp_bitonic_sort<T>(a);
+    const T rest = warp_bitonic_sort<T>(b);
+    const T rrev = __shfl_sync(0xffffffffu, rest, 31 - lane);
+    hi = warp_bitonic_sort<T>(hi < rrev ? hi : rrev);
+}
+
+// The value of rank r (< 64) of a lo/hi pair.
+template <typename T>
+__device__ __forceinline__ T rank_of(T lo, T hi, int r) {
+    const T a = __shfl_sync(0xffffffffu, lo, r & 31);
+    const T b = __shfl_sync(0xffffffffu, hi, r & 31);
+    return r < 32 ? a : b;
 }
 
 // A chunk with at least this many qualifying keys is merged in one bitonic
@@ -776,7 +815,9 @@ __global__ void rerank_kernel(RerankArgs a) {
     const double s2 = a.cosine ? 1.0 : static_cast<double>(a.sc->s2);
     const double nq = static_cast<double>(a.qsq[row]) * s2;
     int below = 0;
-    float topu = INFINITY;  // the 32 smallest U, sorted across the warp
+    // the 64 smallest U, sorted across the warp (hi stays +inf for k <= 32)
+    float topu = INFINITY, topu_hi = INFINITY;
+    const bool wide = k > 32;
     for (int h = 0; h < a.n_lists; ++h) {
         const uint64_t lk = rl[h * S + lane];
         const float l0 = o2f(static_cast<uint32_t>(__shfl_sync(0xffffffffu, lk, 0) >> 32));
@@ -790,24 +831,23 @@ __global__ void rerank_kernel(RerankArgs a) {
         below += __popc(__ballot_sync(0xffffffffu, U < bound));
         // a list whose smallest L already exceeds the k-th smallest U so far
         // cannot lower it
-        if (!(l0 <= __shfl_sync(0xffffffffu, topu, k - 1))) continue;
-        const float u = warp_sort_asc<float>(__double2float_ru(U));
-        const float ur = __shfl_sync(0xffffffffu, u, 31 - lane);
-        float m = fminf(topu, ur);
-#pragma unroll
-        for (int st = 16; st > 0; st >>= 1) {
-            const float o = __shfl_xor_sync(0xffffffffu, m, st);
-            m = (lane & st) ? fmaxf(m, o) : fminf(m, o);
+        if (!(l0 <= rank_of<float>(topu, topu_hi, k - 1))) continue;
+        const float uc = __double2float_ru(U);
+        if (wide) {
+            warp_merge64<float>(topu, topu_hi, uc);
+        } else {
+            const float u = warp_sort_asc<float>(uc);
+            const float ur = __shfl_sync(0xffffffffu, u, 31 - lane);
+            topu = warp_bitonic_sort<float>(fminf(topu, ur));
         }
-        topu = m;
     }
-    const float T = __shfl_sync(0xffffffffu, topu, k - 1);
+    const float T = rank_of<float>(topu, topu_hi, k - 1);
     // Exact keys in the reference's order for the candidates with L <= T; the
-    // 32 smallest are kept sorted across the warp (bitonic merge of each
-    // list's keys into them).
+    // 32 (k <= 32) or 64 smallest are kept sorted across the warp (bitonic
+    // merge of each list's keys into them).
     const float* qrow = a.Q + row * d;
     const float qn = a.cosine ? __fsqrt_rn(a.qsq[row]) : 0.0f;
-    uint64_t top = ~0ull;
+    uint64_t top = ~0ull, top_hi = ~0ull;
     for (int h = 0; h < a.n_lists; ++h) {
         const uint64_t lk = rl[h * S + lane];
         const bool take = lk != ~0ull && o2f(static_cast<uint32_t>(lk >> 32)) <= T;
@@ -821,15 +861,23 @@ __global__ void rerank_kernel(RerankArgs a) {
                                    : sqdist_ref(qrow, crow, d);
             key = knn_key(dist, a.rmap != nullptr ? static_cast<uint32_t>(a.rmap[j]) : j);
         }
-        top = warp_merge_keys(top, key);
+        if (wide)
+            warp_merge64<uint64_t>(top, top_hi, key);
+        else
+            top = warp_merge_keys(top, key);
     }
     // A zero cosine query has distance 0 to zero rows and 1 to the rest, which
     // its bound (built for unit rows) does not cover: it goes to the plain path.
     const bool failed = below < k || (a.cosine && a.qsq[row] == 0.0f);
-    if (!failed && lane < k) {
-        a.out_idx[orow * k + lane] = static_cast<int32_t>(key_index(top));
-        const float kd = key_dist(top);
-        a.out_dist[orow * k + lane] = a.cosine ? kd : __fsqrt_rn(kd);
+    if (!failed) {
+        for (int half = 0; half < 2; ++half) {
+            const int r = half * 32 + lane;
+            if (r >= k) break;
+            const uint64_t key = half == 0 ? top : top_hi;
+            a.out_idx[orow * k + r] = static_cast<int32_t>(key_index(key));
+            const float kd = key_dist(key);
+            a.out_dist[orow * k + r] = a.cosine ? kd : __fsqrt_rn(kd);
+        }
     }
     if (failed && lane == 0) a.fb_rows[atomicAdd(a.fb_count, 1)] = static_cast<int32_t>(orow);
 }
@@ -1138,7 +1186,7 @@ struct EventPair {
 
 bool knn_tc_supported(int d, int k, int metric) {
     if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE) return false;
-    if (k < 1 || k > S - 2 || d < 1) return false;
+    if (k < 1 || k > kMaxK || d < 1) return false;
     if (shape_for(geom(d).kb).st == 0) return false;
     return device_is_sm100();
 }
@@ -1372,7 +1420,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     if (k < 1 || k > n) invalid("k must be in [1, n_rows]");
     if (!knn_tc_supported(d, k, UMAPB_METRIC_EUCLIDEAN))
         invalid("the allocation-free kNN runs the tensor-core path only (sm_100, euclidean, "
-                "k <= 30, n_cols within the tensor-core operand limit)");
+                "k <= 62, n_cols within the tensor-core operand limit)");
     const size_t need = noalloc_need(n, d);
     if (need > kNoAllocScratchBytes) {
         int64_t max_rows = 0;
