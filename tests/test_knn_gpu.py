@@ -192,10 +192,11 @@ def test_tensor_knn_second_pass_rows_stay_exact():
     np.testing.assert_array_equal(td, pd)
 
 
-@pytest.mark.parametrize("d", [500, 640])
+@pytest.mark.parametrize("d", [500, 640, 784, 1100])
 def test_tensor_knn_wide_rows(orc, d):
     # 128-candidate tiles (two lists per row) once 256-candidate tiles no
-    # longer fit shared memory beside the resident query tile
+    # longer fit shared memory beside the resident query tile; past that the
+    # query tile streams through the ring with the candidate tiles
     x = workloads.isotropic_mixture(3000, d, 8, 1.0, seed=d)
     ti, td, fb = gu.knn_exact(x, 12, backend="tensor")
     rows = np.random.default_rng(d).choice(3000, 80, replace=False)
@@ -226,4 +227,21 @@ def test_tensor_knn_k50_mixture_20000x192(orc):
     np.testing.assert_array_equal(td, pd)
     rows = np.random.default_rng(50).choice(20_000, 60, replace=False)
     oi, od = orc.exact_knn_rows(x, rows, 50)
+    np.testing.assert_array_equal(ti[rows], oi)
+
+
+def test_tensor_knn_pixel_like_rows_784(orc):
+    # non-negative rows far from the origin (pixel intensities 0..255, 784
+    # columns): the scaled one-term bound is wide against neighbour gaps, the
+    # second pass settles the rest; every row equals the plain path
+    rng = np.random.default_rng(784)
+    base = rng.uniform(0, 255, size=(10, 784))
+    lab = rng.integers(0, 10, size=6000)
+    x = np.clip(base[lab] + rng.normal(0, 40, size=(6000, 784)), 0, 255).astype(np.float32)
+    ti, td, _ = gu.knn_exact(x, 15, backend="tensor")
+    pi, pd, _ = gu.knn_exact(x, 15, backend="plain")
+    np.testing.assert_array_equal(ti, pi)
+    np.testing.assert_array_equal(td, pd)
+    rows = rng.choice(6000, 40, replace=False)
+    oi, od = orc.exact_knn_rows(x, rows, 15)
     np.testing.assert_array_equal(ti[rows], oi)

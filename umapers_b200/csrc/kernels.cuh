@@ -31,6 +31,9 @@ void knn_plain(const float* Q, const int32_t* q_rows, int64_t n_q, const float* 
                int d, int k, int metric, const float* qnorm, const float* rnorm,
                int32_t* out_idx, float* out_dist, cudaStream_t s, bool allow_scratch = true);
 
+// True when the plain kernel's tiles fit shared memory for this width and k.
+bool knn_plain_supported(int d, int k);
+
 // ------------------------------------------------------------- knn_tc.cu
 struct TcKnnStats {
     int64_t fallback_rows = 0;     // rows recomputed on the plain path

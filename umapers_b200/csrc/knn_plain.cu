@@ -392,6 +392,10 @@ int64_t first_nonfinite_row(const float* X, int64_t n, int d, cudaStream_t s) {
     return h == ~0ULL ? INT64_MAX : static_cast<int64_t>(h);
 }
 
+bool knn_plain_supported(int d, int k) {
+    return plain_smem<16, 16>(d, k) <= 200 * 1024;
+}
+
 void knn_plain(const float* Q, const int32_t* q_rows, int64_t n_q, const float* R, int64_t n_r,
                int d, int k, int metric, const float* qnorm, const float* rnorm,
                int32_t* out_idx, float* out_dist, cudaStream_t s, bool allow_scratch) {
@@ -415,8 +419,15 @@ void knn_plain(const float* Q, const int32_t* q_rows, int64_t n_q, const float* 
         else
             launch_plain<32, 32, false>(Q, q_rows, n_q, R, n_r, d, k, qnorm, rnorm, out_idx,
                                         out_dist, s, allow_scratch);
+    } else if (plain_smem<16, 16>(d, k) <= limit) {
+        if (cos)
+            launch_plain<16, 16, true>(Q, q_rows, n_q, R, n_r, d, k, qnorm, rnorm, out_idx,
+                                       out_dist, s, allow_scratch);
+        else
+            launch_plain<16, 16, false>(Q, q_rows, n_q, R, n_r, d, k, qnorm, rnorm, out_idx,
+                                        out_dist, s, allow_scratch);
     } else {
-        invalid("n_features/n_neighbors too large for the exact kNN tile (need d*256 + k*256 < 200 KiB)");
+        invalid("n_features/n_neighbors too large for the exact kNN tile (need d*128 + k*128 < 200 KiB)");
     }
 }
 

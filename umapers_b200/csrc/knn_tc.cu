@@ -290,29 +290,33 @@ __device__ __forceinline__ int32_t tile_at(int32_t t, const Unit& w) {
 // Kernel shapes: MT query tiles of 128 rows share each BN-row candidate tile;
 // 2 TMEM buffers of MT x BN columns; one epilogue warp per (TMEM lane quarter,
 // query tile, 64-column group).
+// With SA (streamed A) the query tile is not resident: every ring stage
+// carries the query tile's k-block beside the candidate tile's, so rows of
+// any width fit shared memory at 1.5x the L2 reads of the resident form.
 template <int MT, int BN>
 constexpr int epi_warps() { return 4 * MT * (BN / 64); }
 template <int MT, int BN>
 constexpr int tc_threads() { return 64 + 32 * epi_warps<MT, BN>(); }
 
-template <int MT, int BN>
+template <int MT, int BN, bool SA>
 __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
     tc_knn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                   TcArgs p) {
     static_assert(MT * BN <= 256 && (BN == 128 || BN == 256), "at most 512 TMEM columns");
     constexpr int kEpiWarps = epi_warps<MT, BN>();
     constexpr int kBTileBytes = BN * BK * 2;
+    constexpr int kStageBytes = SA ? MT * kATileBytes + kBTileBytes : kBTileBytes;
+    constexpr int kStageB = SA ? MT * kATileBytes : 0;  // candidate tile within a stage
     constexpr uint32_t kIdesc = idesc_f16(BM, BN);
-    constexpr uint32_t kBDesc = kBTileBytes >> 4;  // one ring stage in descriptor units
     constexpr int GPT = BN / 64;                   // lists per candidate tile
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
     const int KB = p.kb, TAIL = p.tail, ST = p.st;
+    const int a_bytes = SA ? 0 : MT * KB * kATileBytes;  // resident query tiles
     const uint32_t sA = smem_u32(smem);
-    const uint32_t sB = sA + MT * KB * kATileBytes;
-    uint64_t* bars =
-        reinterpret_cast<uint64_t*>(smem + MT * KB * kATileBytes + ST * kBTileBytes);
+    const uint32_t sB = sA + a_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + a_bytes + ST * kStageBytes);
     const uint32_t b_full = smem_u32(bars);
     const uint32_t b_empty = b_full + 8 * ST;
     const uint32_t b_tfull = b_empty + 8 * ST;
@@ -362,17 +366,19 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
             int64_t u_iter = 0;
             for (int64_t unit = blockIdx.x; unit < p.n_units && !*abort_flag;
                  unit += gridDim.x, ++u_iter) {
-                if (u_iter > 0 && !mbar_wait(b_aempty, static_cast<uint32_t>((u_iter - 1) & 1),
-                                             abort_flag)) {
-                    fail(1);
-                    break;
-                }
                 const Unit w = unit_of(p, unit);
-                mbar_expect_tx(b_afull, MT * KB * kATileBytes);
-                for (int mt = 0; mt < MT; ++mt)
-                    for (int kb = 0; kb < KB; ++kb)
-                        tma_load_2d(sA + (mt * KB + kb) * kATileBytes, &tmA, b_afull, kb * BK,
-                                    static_cast<int>((w.group * MT + mt) * BM));
+                if (!SA) {
+                    if (u_iter > 0 &&
+                        !mbar_wait(b_aempty, static_cast<uint32_t>((u_iter - 1) & 1), abort_flag)) {
+                        fail(1);
+                        break;
+                    }
+                    mbar_expect_tx(b_afull, MT * KB * kATileBytes);
+                    for (int mt = 0; mt < MT; ++mt)
+                        for (int kb = 0; kb < KB; ++kb)
+                            tma_load_2d(sA + (mt * KB + kb) * kATileBytes, &tmA, b_afull, kb * BK,
+                                        static_cast<int>((w.group * MT + mt) * BM));
+                }
                 bool ok = true;
                 for (int32_t c = 0; c < w.len && ok; ++c) {
                     const int ty = static_cast<int>(tile_at(c, w) * BN);
@@ -382,9 +388,13 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                             ok = false;
                             break;
                         }
-                        mbar_expect_tx(b_full + 8 * stage, kBTileBytes);
-                        tma_load_2d(sB + stage * kBTileBytes, &tmB, b_full + 8 * stage, kb * BK,
-                                    ty);
+                        const uint32_t sbase = sB + stage * kStageBytes;
+                        mbar_expect_tx(b_full + 8 * stage, kStageBytes);
+                        if (SA)
+                            for (int mt = 0; mt < MT; ++mt)
+                                tma_load_2d(sbase + mt * kATileBytes, &tmA, b_full + 8 * stage,
+                                            kb * BK, static_cast<int>((w.group * MT + mt) * BM));
+                        tma_load_2d(sbase + kStageB, &tmB, b_full + 8 * stage, kb * BK, ty);
                         if (++stage == ST) {
                             stage = 0;
                             phase ^= 1;
@@ -402,13 +412,14 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
             uint64_t cg = 0;
             int64_t u_iter = 0;
             bool ok = true;
-            const uint64_t dB0 = desc_sw128(sB);
             for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x, ++u_iter) {
-                if (!mbar_wait(b_afull, static_cast<uint32_t>(u_iter & 1), abort_flag)) {
-                    fail(3);
-                    break;
+                if (!SA) {
+                    if (!mbar_wait(b_afull, static_cast<uint32_t>(u_iter & 1), abort_flag)) {
+                        fail(3);
+                        break;
+                    }
+                    fence_after();
                 }
-                fence_after();
                 const int32_t len = unit_of(p, unit).len;
                 for (int32_t c = 0; c < len && ok; ++c, ++cg) {
                     const uint32_t buf = static_cast<uint32_t>(cg & 1);
@@ -428,14 +439,17 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                         }
                         fence_after();
                         const int steps = kb + 1 < KB ? BK / UK : TAIL;
-                        const uint64_t db0 = dB0 + static_cast<uint64_t>(stage) * kBDesc;
+                        const uint32_t sbase = sB + stage * kStageBytes;
+                        const uint64_t db0 = desc_sw128(sbase + kStageB);
 #pragma unroll
                         for (int ks = 0; ks < BK / UK; ++ks) {
                             if (ks < steps) {
 #pragma unroll
                                 for (int mt = 0; mt < MT; ++mt) {
                                     const uint64_t da =
-                                        desc_sw128(sA + (mt * KB + kb) * kATileBytes) + 2 * ks;
+                                        (SA ? desc_sw128(sbase + mt * kATileBytes)
+                                            : desc_sw128(sA + (mt * KB + kb) * kATileBytes)) +
+                                        2 * ks;
                                     umma_bf16(dcol + mt * BN, da, db0 + 2 * ks, kIdesc,
                                               (kb | ks) != 0 ? 1u : 0u);
                                 }
@@ -449,7 +463,7 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                     }
                     if (ok) umma_commit(b_tfull + 8 * buf);
                 }
-                if (ok) umma_commit(b_aempty);
+                if (ok && !SA) umma_commit(b_aempty);
             }
             // every MMA issued by this thread has completed before TMEM is freed
             umma_commit(b_final);
@@ -896,34 +910,40 @@ __global__ void gather_rows_kernel(const float* __restrict__ X, const int32_t* _
 // Kernel shape: MT query tiles x BN candidate rows, ring stages.
 struct Shape {
     int mt = 0, bn = 0, st = 0;
+    bool stream = false;  // query tile streamed through the ring with the candidates
     size_t smem = 0;
     int lists() const { return bn / 64; }  // lists per row and candidate split
 };
 
-size_t smem_bytes(int mt, int bn, int kb, int st) {
+size_t smem_bytes(int mt, int bn, int kb, int st, bool stream) {
     // tiles + 1 KiB alignment slack + barriers/flags + epilogue scratch
-    return static_cast<size_t>(mt) * kb * kATileBytes + static_cast<size_t>(st) * bn * BK * 2 +
-           1024 + kBarBytes + static_cast<size_t>(4 * mt * (bn / 64)) * kScratchBytes;
+    const size_t a = stream ? 0 : static_cast<size_t>(mt) * kb * kATileBytes;
+    const size_t stage = static_cast<size_t>(bn) * BK * 2 + (stream ? mt * kATileBytes : 0);
+    return a + st * stage + 1024 + kBarBytes +
+           static_cast<size_t>(4 * mt * (bn / 64)) * kScratchBytes;
 }
 
-// One query tile against 256-candidate tiles (four lists per row) while the
-// operands fit with at least three ring stages, else against 128-candidate
-// tiles (two lists per row, eight epilogue warps).
+// One resident query tile against 256-candidate tiles (four lists per row)
+// while the operands fit with at least three ring stages, else against
+// 128-candidate tiles (two lists per row, eight epilogue warps); rows too
+// wide for a resident tile stream it with 256-candidate tiles.
 Shape shape_for(int kb) {
     const int cand[2][2] = {{1, 256}, {1, 128}};
     for (const auto& c : cand) {
         int st = kMaxStages;
-        while (st >= 2 && smem_bytes(c[0], c[1], kb, st) > kSmemLimit) --st;
+        while (st >= 2 && smem_bytes(c[0], c[1], kb, st, false) > kSmemLimit) --st;
         if (st >= (c[1] == 256 ? 3 : 2))
-            return Shape{c[0], c[1], st, smem_bytes(c[0], c[1], kb, st)};
+            return Shape{c[0], c[1], st, false, smem_bytes(c[0], c[1], kb, st, false)};
     }
-    return Shape{};
+    int st = kMaxStages;
+    while (st >= 3 && smem_bytes(1, 256, kb, st, true) > kSmemLimit) --st;
+    return Shape{1, 256, st, true, smem_bytes(1, 256, kb, st, true)};
 }
 
-template <int MT, int BN>
+template <int MT, int BN, bool SA>
 void launch_tc_t(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, size_t smem,
                  cudaStream_t s) {
-    auto kern = tc_knn_kernel<MT, BN>;
+    auto kern = tc_knn_kernel<MT, BN, SA>;
     UMAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
     int dev = 0, sms = 0;
@@ -936,12 +956,12 @@ void launch_tc_t(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, 
 
 void launch_tc(const Shape& sh, const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a,
                cudaStream_t s) {
-    if (sh.mt == 1 && sh.bn == 256)
-        launch_tc_t<1, 256>(ma, mb, a, sh.smem, s);
-    else if (sh.mt == 2 && sh.bn == 128)
-        launch_tc_t<2, 128>(ma, mb, a, sh.smem, s);
-    else if (sh.mt == 1 && sh.bn == 128)
-        launch_tc_t<1, 128>(ma, mb, a, sh.smem, s);
+    if (sh.stream && sh.mt == 1 && sh.bn == 256)
+        launch_tc_t<1, 256, true>(ma, mb, a, sh.smem, s);
+    else if (!sh.stream && sh.mt == 1 && sh.bn == 256)
+        launch_tc_t<1, 256, false>(ma, mb, a, sh.smem, s);
+    else if (!sh.stream && sh.mt == 1 && sh.bn == 128)
+        launch_tc_t<1, 128, false>(ma, mb, a, sh.smem, s);
     else
         invalid("tensor-core kNN: no kernel shape for these operands");
 }
@@ -1188,6 +1208,9 @@ bool knn_tc_supported(int d, int k, int metric) {
     if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE) return false;
     if (k < 1 || k > kMaxK || d < 1) return false;
     if (shape_for(geom(d).kb).st == 0) return false;
+    // rows the certificate cannot settle go to the plain kernel, whose tiles
+    // bound the width
+    if (!knn_plain_supported(d, k)) return false;
     return device_is_sm100();
 }
 
@@ -1287,7 +1310,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
         A.release();
         Geom g2 = geom(d, 3);
         Shape sh2 = shape_for(g2.kb);
-        if (sh2.st == 0) {
+        if (sh2.st == 0 || sh2.stream) {
             g2 = g;
             sh2 = sh;
         }
