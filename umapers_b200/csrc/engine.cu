@@ -1633,18 +1633,26 @@ int32_t umapb_surrogate_transform(umapb_model* m, const float* query, int64_t n_
                                        rows * n_cols * 4, cudaMemcpyHostToDevice, cs.s));
             UMAPB_CUDA(cudaEventRecord(cs.done[c], cs.s));
         }
-        int64_t nf = 0;
+        // The checks and the network are queued chunk by chunk with no host
+        // wait; the first non-finite row, the GEMM status and the gate count
+        // are read back once, before the fallback and the outputs.  (Copies
+        // from pageable host memory are staged by the driver and keep the
+        // host busy until they land; pinned rows let the queueing run ahead.)
+        DevBuf<unsigned long long> bad_row(1, s);
+        UMAPB_CUDA(cudaMemsetAsync(bad_row.get(), 0xFF, 8, s));
         for (int64_t c = 0; c < n_chunks; ++c) {
             const int64_t r0 = c * chunk, rows = std::min(chunk, n_rows - r0);
             UMAPB_CUDA(cudaStreamWaitEvent(s, cs.done[c], 0));
-            const int64_t bad =
-                first_nonfinite_row(Q.get() + r0 * n_cols, rows, static_cast<int>(n_cols), s);
-            if (bad != INT64_MAX)
-                invalid("input contains non-finite value at row " + std::to_string(r0 + bad));
-            nf += surrogate_infer(*m->surrogate, Q.get() + r0 * n_cols, rows,
-                                  static_cast<int>(n_cols), outd.get() + r0 * dim,
-                                  fl.get() + r0, s);
+            nonfinite_rows_async(Q.get() + r0 * n_cols, rows, static_cast<int>(n_cols), r0,
+                                 bad_row.get(), s);
+            surrogate_infer_async(*m->surrogate, Q.get() + r0 * n_cols, rows,
+                                  static_cast<int>(n_cols), outd.get() + r0 * dim, fl.get() + r0,
+                                  s);
         }
+        unsigned long long bad = 0;
+        UMAPB_CUDA(cudaMemcpyAsync(&bad, bad_row.get(), 8, cudaMemcpyDeviceToHost, s));
+        const int64_t nf = surrogate_count_flags(fl.get(), n_rows, s);  // synchronises s
+        if (bad != ~0ull) invalid("input contains non-finite value at row " + std::to_string(bad));
         if (n_fallback) *n_fallback = nf;
         if (use_fallback != 0) surrogate_fallback(m, Q.get(), n_rows, n_cols, outd.get(), fl.get(), nf);
         UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * dim * 4, cudaMemcpyDeviceToHost, s));

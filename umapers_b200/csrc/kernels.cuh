@@ -21,6 +21,11 @@ void row_norms(const float* X, int64_t n, int d, float* norms, float* sq, cudaSt
 
 // Index of the first row holding a non-finite value, or INT64_MAX.
 int64_t first_nonfinite_row(const float* X, int64_t n, int d, cudaStream_t s);
+// The same scan without a host synchronisation: the first non-finite row
+// index plus `row_offset` is folded into *first_row (atomic minimum; start it
+// at all ones).
+void nonfinite_rows_async(const float* X, int64_t n, int d, int64_t row_offset,
+                          unsigned long long* first_row, cudaStream_t s);
 
 // Exact kNN on FP32 CUDA cores in the reference's summation order.
 // Query row r is Q[q_rows ? q_rows[r] : r] and its result goes to output row
@@ -261,6 +266,12 @@ SurrogatePtr surrogate_train(const float* X, int64_t n, int d, const float* emb,
 // rejected rows (0 when flags is null).
 int64_t surrogate_infer(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
                         uint8_t* flags, cudaStream_t s);
+// The same inference with no host synchronisation (no gate count, no GEMM
+// status read); surrogate_count_flags then reads the GEMM status and counts
+// the gated rows of a whole request once.
+void surrogate_infer_async(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
+                           uint8_t* flags, cudaStream_t s);
+int64_t surrogate_count_flags(const uint8_t* flags, int64_t nq, cudaStream_t s);
 
 // dst[r] = src[ids[r]] and dst[ids[r]] = src[r] for rows of d floats.
 void gather_rows(const float* src, const int32_t* ids, int64_t n, int d, float* dst,

@@ -327,17 +327,18 @@ __global__ void row_norms_kernel(const float* __restrict__ X, int64_t n, int d,
 }
 
 __global__ void nonfinite_kernel(const float* __restrict__ X, int64_t total, int d,
-                                 unsigned long long* first_row) {
+                                 int64_t row_offset, unsigned long long* first_row) {
     for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
          e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        if (!isfinite(X[e])) atomicMin(first_row, static_cast<unsigned long long>(e / d));
+        if (!isfinite(X[e]))
+            atomicMin(first_row, static_cast<unsigned long long>(e / d + row_offset));
     }
 }
 
 // The same scan over a 16-byte aligned array: four 16-byte loads in flight
 // per thread; elements past the last whole float4 are checked one by one.
 __global__ void nonfinite_v4_kernel(const float* __restrict__ X, int64_t total, int d,
-                                    unsigned long long* first_row) {
+                                    int64_t row_offset, unsigned long long* first_row) {
     const float4* X4 = reinterpret_cast<const float4*>(X);
     const int64_t total4 = total >> 2;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -355,15 +356,15 @@ __global__ void nonfinite_v4_kernel(const float* __restrict__ X, int64_t total, 
 #pragma unroll
             for (int i = 0; i < 4; ++i)
                 if (!isfinite(c[i])) {
-                    atomicMin(first_row,
-                              static_cast<unsigned long long>((4 * (e + u * stride) + i) / d));
+                    atomicMin(first_row, static_cast<unsigned long long>(
+                                             (4 * (e + u * stride) + i) / d + row_offset));
                     break;
                 }
         }
     }
     const int64_t tail = (total4 << 2) + t;
     if (tail < total && !isfinite(X[tail]))
-        atomicMin(first_row, static_cast<unsigned long long>(tail / d));
+        atomicMin(first_row, static_cast<unsigned long long>(tail / d + row_offset));
 }
 
 }  // namespace
@@ -374,18 +375,22 @@ void row_norms(const float* X, int64_t n, int d, float* norms, float* sq, cudaSt
     UMAPB_LAUNCH_CHECK();
 }
 
+void nonfinite_rows_async(const float* X, int64_t n, int d, int64_t row_offset,
+                          unsigned long long* first_row, cudaStream_t s) {
+    const int64_t total = n * d;
+    if (total <= 0) return;
+    const int blocks = static_cast<int>(std::min<int64_t>(ceil_div(total, 256), 148 * 16));
+    if ((reinterpret_cast<uintptr_t>(X) & 15) == 0)
+        nonfinite_v4_kernel<<<blocks, 256, 0, s>>>(X, total, d, row_offset, first_row);
+    else
+        nonfinite_kernel<<<blocks, 256, 0, s>>>(X, total, d, row_offset, first_row);
+    UMAPB_LAUNCH_CHECK();
+}
+
 int64_t first_nonfinite_row(const float* X, int64_t n, int d, cudaStream_t s) {
     DevBuf<unsigned long long> flag(1, s);
     UMAPB_CUDA(cudaMemsetAsync(flag.get(), 0xFF, 8, s));
-    const int64_t total = n * d;
-    if (total > 0) {
-        const int blocks = static_cast<int>(std::min<int64_t>(ceil_div(total, 256), 148 * 16));
-        if ((reinterpret_cast<uintptr_t>(X) & 15) == 0)
-            nonfinite_v4_kernel<<<blocks, 256, 0, s>>>(X, total, d, flag.get());
-        else
-            nonfinite_kernel<<<blocks, 256, 0, s>>>(X, total, d, flag.get());
-        UMAPB_LAUNCH_CHECK();
-    }
+    nonfinite_rows_async(X, n, d, 0, flag.get(), s);
     unsigned long long h = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&h, flag.get(), 8, cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));

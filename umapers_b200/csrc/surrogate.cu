@@ -1012,6 +1012,26 @@ SurrogatePtr surrogate_train(const float* X, int64_t n, int d, const float* emb,
     return sg;
 }
 
+void surrogate_infer_async(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
+                           uint8_t* flags, cudaStream_t s) {
+    if (d != sg.L.din) invalid("surrogate input width differs from the fitted rows");
+    if (nq == 0) return;
+    infer_rows(sg, Q, nullptr, nq, out, flags, nullptr, nullptr, s);
+}
+
+int64_t surrogate_count_flags(const uint8_t* flags, int64_t nq, cudaStream_t s) {
+    check_gemm(s);
+    if (!flags || nq == 0) return 0;
+    DevBuf<unsigned long long> cnt(1, s);
+    UMAPB_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, s));
+    count_flags_kernel<<<std::min<int64_t>(grid_for(nq), 4096), 256, 0, s>>>(flags, nq, cnt.get());
+    UMAPB_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&h, cnt.get(), 8, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    return static_cast<int64_t>(h);
+}
+
 int64_t surrogate_infer(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
                         uint8_t* flags, cudaStream_t s) {
     if (d != sg.L.din) invalid("surrogate input width differs from the fitted rows");
