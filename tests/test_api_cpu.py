@@ -99,7 +99,9 @@ def test_empty_and_single_sample_inputs():
         Umap().fit(np.zeros((0, 3), np.float32))
     with pytest.raises(ValueError, match="need at least two samples"):
         Umap().fit(np.zeros((1, 3), np.float32))
-    with pytest.raises(ValueError, match="at least one feature"):
+    # the binding rejects zero columns before the core sees the rows
+    # (ensure_nonzero_columns, umap_rs/src/lib.rs:166-178)
+    with pytest.raises(ValueError, match="data must have at least one column"):
         Umap().fit(np.zeros((40, 0), np.float32))
 
 

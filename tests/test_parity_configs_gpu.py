@@ -6,8 +6,8 @@ The SGD layouts race Hogwild-style on the GPU and run sequentially in the
 oracle (the reference's order), so layouts are compared by quality:
 trustworthiness@15 and 15-NN preservation within 0.005 of the oracle's
 (configurations 1 and 2), trustworthiness@15 within 0.01 for the transforms
-(configuration 5).  Where a single fit's Hogwild variance is comparable to
-the tolerance (1 000 rows), the median over three seeds is compared on both
+(configuration 5).  Where a single fit's seed-to-seed spread is comparable to
+the tolerance (1 000 rows), the median over eight seeds is compared on both
 sides.
 """
 import ctypes
@@ -29,7 +29,10 @@ def _median_quality(x, embs):
 def test_config1_gaussian_1000x32_matches_oracle(orc):
     # 1000 x 32 N(0, 1), seed 42; k = 15, 200 epochs, exact kNN, spectral init
     x = workloads.gaussian(1000, 32, seed=42)
-    seeds = (42, 43, 44)
+    # structureless N(0, 1) rows: one fit's trustworthiness moves by about
+    # 0.005 between seeds (0.640-0.657 over eight oracle seeds), so medians
+    # over eight seeds are compared
+    seeds = tuple(range(42, 50))
     g = [Umap(n_neighbors=15, n_epochs=200, ann_mode="exact", random_seed=s).fit_transform(x)
          for s in seeds]
     o = [orc.fit_transform(x, n_neighbors=15, n_epochs=200, use_approximate_knn=0, random_seed=s)

@@ -194,8 +194,12 @@ def _out_buffer(out: Any, shape: tuple[int, int]) -> np.ndarray:
 
 def _ann_mode(ann_mode: Any, use_approx: bool, threshold: int) -> tuple[str, bool, int]:
     """ann_mode shortcut (_api.py:209-224): exact forces the exact kNN,
-    approximate forces NN-descent for every input size."""
-    mode = str(ann_mode).lower()
+    approximate forces NN-descent for every input size.  A canonical value is
+    kept as the same object, so sklearn's clone sees the parameter unchanged."""
+    if isinstance(ann_mode, str) and ann_mode in ("auto", "exact", "approximate"):
+        mode = ann_mode
+    else:
+        mode = str(ann_mode).lower()
     if mode == "auto":
         return mode, use_approx, threshold
     if mode == "exact":
@@ -220,7 +224,7 @@ def _target_metric(target_metric: Any) -> str | None:
     if metric in {"none", ""}:
         return None
     if metric == "categorical":
-        return metric
+        return target_metric if target_metric == metric else metric
     raise ValueError(f"unsupported target_metric '{target_metric}', expected None|categorical")
 
 
@@ -230,6 +234,8 @@ def _metric_config(metric: Any, metric_kwds: Any) -> tuple[str, Any, float | Non
         expected = "|".join(sorted(set(_METRIC_ALIASES.values())))
         raise ValueError(f"unsupported metric '{metric}', expected {expected}")
     name = _METRIC_ALIASES[name]
+    if isinstance(metric, str) and metric == name:
+        name = metric  # keep the caller's object (sklearn's clone compares identity)
     kwds = {} if metric_kwds is None else metric_kwds
     if not hasattr(kwds, "keys"):
         raise TypeError("metric_kwds must be a mapping or None")
@@ -390,7 +396,7 @@ class Umap:
         if transform_mode not in _TRANSFORM_MODES:
             raise ValueError(f"transform_mode must be one of {_TRANSFORM_MODES}")
         self.transform_mode = str(transform_mode)
-        self.surrogate_kwds = None if surrogate_kwds is None else dict(surrogate_kwds)
+        self.surrogate_kwds = surrogate_kwds
         self._core = UmapCore(
             n_neighbors=self.n_neighbors,
             n_components=self.n_components,

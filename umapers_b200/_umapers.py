@@ -59,9 +59,13 @@ def _usize(value: Any, name: str) -> int:
 
 
 def _matrix(x: Any, name: str) -> np.ndarray:
+    """A C-contiguous float32 2-D view of x, rejecting zero columns as the
+    PyO3 binding does (ensure_nonzero_columns, umap_rs/src/lib.rs:166-178)."""
     arr = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
     if arr.ndim != 2:
         raise ValueError(f"{name} must be a 2D array, got ndim={arr.ndim}")
+    if arr.shape[1] == 0:
+        raise ValueError(f"{name} must have at least one column")
     return arr
 
 
