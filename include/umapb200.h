@@ -367,6 +367,20 @@ int32_t umapb_knn_csr_query(const int64_t* q_indptr, const int64_t* q_indices,
                             int64_t n_cols, int64_t k, int32_t metric, int64_t* out_indices,
                             float* out_dists);
 
+/* NN-descent on CSR rows: the candidate rule of
+ * approximate_nearest_neighbors_with_distance (rust_umap/src/lib.rs:3086-3151)
+ * with candidates scored by the exact sparse kNN's distances (sparse_dot in
+ * ascending column order and the row norms, rust_umap/src/sparse.rs:90-97,
+ * 220-239, 605-626), euclidean or cosine.  The reference has no approximate
+ * path for sparse rows; a fit takes this one on an explicit approximate
+ * request (use_approximate_knn with approx_knn_threshold 0).  Outputs as
+ * umapb_nndescent. */
+int32_t umapb_nndescent_csr(const int64_t* indptr, const int64_t* indices, const float* data,
+                            int64_t n_rows, int64_t n_cols, int64_t k, int32_t metric,
+                            int64_t candidate_pool, int64_t n_iters, uint64_t seed,
+                            int64_t* indices_out, float* dists, int64_t* iters_run,
+                            int64_t* candidates_evaluated, double* kernel_sec);
+
 /* NN-descent variant (approximate_nearest_neighbors_with_distance,
  * rust_umap/src/lib.rs:3086-3151) on the GPU; `seed` plays the role of
  * random_seed ^ 0xC0FE_FEED_1234_ABCD (lib.rs:2327).  `candidates_evaluated`

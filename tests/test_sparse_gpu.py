@@ -10,6 +10,8 @@ sparse kNN equals the dense kNN of the same matrix, sparse and dense queries
 of a sparse model transform alike, sparse queries need a sparse model, and a
 disconnected sparse graph still gets a spectral layout.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -195,3 +197,74 @@ def test_module_fit_transform_and_formats(clusters):
     assert max(trust) - min(trust) <= 0.02
     m = Umap(n_neighbors=10, n_epochs=50).fit(x)
     assert m.n_features_in_ == 200 and m.n_samples_fit_ == 3000
+
+
+def _gpu_nndescent_csr(m, k, metric, candidates, iters, seed=99):
+    ip, ix, dv = _parts(m)
+    n, d = m.shape
+    idx = np.empty((n, k), np.int64)
+    dist = np.empty((n, k), np.float32)
+    ran, ev = ctypes.c_int64(0), ctypes.c_int64(0)
+    ksec = ctypes.c_double(0.0)
+    _lib.check(_lib.load().umapb_nndescent_csr(
+        ip.ctypes.data, ix.ctypes.data, dv.ctypes.data, n, d, k, {"euclidean": 0, "cosine": 2}[metric],
+        candidates, iters, seed, idx.ctypes.data, dist.ctypes.data, ctypes.byref(ran),
+        ctypes.byref(ev), ctypes.byref(ksec)))
+    return idx, dist, ran.value, ev.value
+
+
+def _topics(n, d, n_topics, per_row, seed):
+    """Text-like CSR rows: each row draws most of its columns from its topic's
+    block of preferred columns, the rest anywhere; LogNormal(0, 1) values."""
+    rng = np.random.default_rng(seed)
+    pref = [rng.choice(d, 60, replace=False) for _ in range(n_topics)]
+    rows, cols = [], []
+    for r in range(n):
+        t = rng.integers(n_topics)
+        c = np.concatenate([rng.choice(pref[t], int(per_row * 0.8), replace=False),
+                            rng.integers(0, d, per_row - int(per_row * 0.8))])
+        c = np.unique(c)
+        rows.append(np.full(c.shape[0], r))
+        cols.append(c)
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    vals = rng.lognormal(0.0, 1.0, size=rows.shape[0]).astype(np.float32)
+    m = sp.csr_matrix((vals, (rows, cols)), shape=(n, d))
+    m.sort_indices()
+    return m
+
+
+@pytest.mark.parametrize("metric", ["cosine", "euclidean"])
+def test_sparse_nndescent_recall_against_exact(metric):
+    """NN-descent on CSR rows (the reference's candidate rule, the exact
+    sparse kNN's distances): every listed distance equals the exact sparse
+    distance of that pair, lists are sorted with self first, and recall@15
+    against the exact sparse kNN (itself bit-exact with the oracle) is high
+    at the reference's default 50 candidates and 14 iterations."""
+    m = _topics(6000, 2000, 20, 20, seed=21)
+    k = 15
+    ai, ad, ran, ev = _gpu_nndescent_csr(m, k, metric, 50, 14)
+    ei, ed = _gpu_knn(m, k, metric)
+    assert 1 <= ran <= 14 and ev > 6000 * 50
+    assert np.all(ai[:, 0] == np.arange(6000)) and np.all(ad[:, 0] == 0.0)
+    assert np.all(np.diff(ad, axis=1) >= 0)
+    recall = np.mean([len(set(ai[r]) & set(ei[r])) / k for r in range(6000)])
+    print(metric, "recall", recall, "iterations", ran)
+    assert recall >= 0.8
+    # a pair listed by both has the same FP32 distance
+    for r in range(0, 6000, 97):
+        common = set(ai[r]) & set(ei[r])
+        for j in common:
+            assert ad[r][list(ai[r]).index(j)] == ed[r][list(ei[r]).index(j)]
+
+
+def test_sparse_fit_takes_nndescent_on_explicit_approximate_request():
+    m = _topics(3000, 500, 10, 20, seed=4)
+    emb = Umap(n_neighbors=15, metric="cosine", n_epochs=50, ann_mode="approximate",
+               random_seed=3).fit_transform(m)
+    exact = Umap(n_neighbors=15, metric="cosine", n_epochs=50, ann_mode="exact",
+                 random_seed=3).fit_transform(m)
+    dense = m.toarray()
+    ta = diagnostics.quality(dense, emb, sample=None)["trustworthiness"]
+    te = diagnostics.quality(dense, exact, sample=None)["trustworthiness"]
+    print("trust approximate", ta, "exact", te)
+    assert np.all(np.isfinite(emb)) and abs(ta - te) <= 0.02

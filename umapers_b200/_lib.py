@@ -247,6 +247,8 @@ SIGNATURES = {
     "umapb_knn_query": (_i32, [_vp, _i64, _vp, _i64, _i64, _i64, _i32, _i32, _vp, _vp]),
     "umapb_nndescent": (_i32, [_vp, _i64, _i64, _i64, _i32, _i64, _i64, _u64, _vp, _vp, _i64p,
                                _i64p, ctypes.POINTER(ctypes.c_double)]),
+    "umapb_nndescent_csr": (_i32, [_vp, _vp, _vp, _i64, _i64, _i64, _i32, _i64, _i64, _u64, _vp,
+                                   _vp, _i64p, _i64p, ctypes.POINTER(ctypes.c_double)]),
     "umapb_smooth_knn_dist": (_i32, [_vp, _i64, _i64, _f32, _f32, _f32, _i32, _vp, _vp]),
     "umapb_fuzzy_graph": (
         _i32,

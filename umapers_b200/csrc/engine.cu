@@ -220,6 +220,11 @@ bool should_use_approximate_knn(const umapb_params& p, int64_t n, int64_t d) {
     return true;
 }
 
+// CSR fits take NN-descent only on an explicit approximate request.
+bool sparse_uses_nndescent(const umapb_params& p, int64_t n) {
+    return p.use_approximate_knn && p.approx_knn_threshold == 0 && n > p.n_neighbors + 1;
+}
+
 int64_t default_epochs(const umapb_params& p, int64_t n) {
     return p.n_epochs >= 0 ? p.n_epochs : (n <= 10000 ? 500 : 200);
 }
@@ -629,7 +634,15 @@ void fit_csr_host(umapb_model* m, const int64_t* indptr, const int64_t* indices,
     const int k = static_cast<int>(m->p.n_neighbors);
     DevBuf<int32_t> idx(n * k, s);
     DevBuf<float> dist(n * k, s);
-    knn_sparse(csr, csr, ci, true, k, m->p.metric, idx.get(), dist.get(), s);
+    // The reference always runs the exact kNN on CSR rows.  An explicit
+    // approximate request (ann_mode="approximate": use_approximate_knn with a
+    // zero threshold) runs NN-descent on them instead, with the reference's
+    // candidate rule and the exact kNN's sparse distances.
+    if (sparse_uses_nndescent(m->p, n))
+        nndescent_csr(csr, k, m->p.metric, m->p.approx_knn_candidates, m->p.approx_knn_iters,
+                      m->p.random_seed ^ 0xC0FEFEED1234ABCDULL, idx.get(), dist.get(), s);
+    else
+        knn_sparse(csr, csr, ci, true, k, m->p.metric, idx.get(), dist.get(), s);
     StageClock clk(s, false);
     fit_from_knn(m, nullptr, n, d, idx.get(), dist.get(), k, nullptr, clk, &csr);
     m->csr = std::move(csr);
@@ -1343,6 +1356,36 @@ int32_t umapb_knn_csr(const int64_t* indptr, const int64_t* indices, const float
                                    ss.s));
         UMAPB_CUDA(cudaStreamSynchronize(ss.s));
         to_i64(ih, out_idx);
+    });
+}
+
+int32_t umapb_nndescent_csr(const int64_t* indptr, const int64_t* indices, const float* data,
+                            int64_t n_rows, int64_t n_cols, int64_t k, int32_t metric,
+                            int64_t candidate_pool, int64_t n_iters, uint64_t seed,
+                            int64_t* out_idx, float* out_dist, int64_t* iters_run,
+                            int64_t* candidates_evaluated, double* kernel_sec) {
+    return guarded([&] {
+        validate_csr_host(indptr, indices, data, n_rows, n_cols);
+        if (n_rows <= 1) invalid("need at least two rows");
+        if (k < 1 || k >= n_rows) invalid("k must be in [1, n_rows)");
+        ScopedStream ss;
+        CsrDevice csr;
+        csr_upload(indptr, indices, data, n_rows, n_cols, csr, ss.s);
+        DevBuf<int32_t> idx(n_rows * k, ss.s);
+        DevBuf<float> dist(n_rows * k, ss.s);
+        NdStats st;
+        const int64_t ran = nndescent_csr(csr, static_cast<int>(k), metric, candidate_pool,
+                                          n_iters, seed, idx.get(), dist.get(), ss.s, &st);
+        std::vector<int32_t> ih(n_rows * k);
+        UMAPB_CUDA(cudaMemcpyAsync(ih.data(), idx.get(), n_rows * k * 4, cudaMemcpyDeviceToHost,
+                                   ss.s));
+        UMAPB_CUDA(cudaMemcpyAsync(out_dist, dist.get(), n_rows * k * 4, cudaMemcpyDeviceToHost,
+                                   ss.s));
+        UMAPB_CUDA(cudaStreamSynchronize(ss.s));
+        to_i64(ih, out_idx);
+        if (iters_run) *iters_run = ran;
+        if (candidates_evaluated) *candidates_evaluated = st.candidates;
+        if (kernel_sec) *kernel_sec = st.kernel_sec;
     });
 }
 

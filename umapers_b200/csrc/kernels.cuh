@@ -142,6 +142,12 @@ struct NdStats {
 int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t candidate_pool,
                   int64_t n_iters, uint64_t seed, int32_t* out_idx, float* out_dist,
                   cudaStream_t s, NdStats* stats = nullptr);
+struct CsrDevice;
+// The same NN-descent on CSR rows: candidates scored by sparse dot products
+// in the reference's column order (the exact sparse kNN's distances).
+int64_t nndescent_csr(const CsrDevice& x, int k, int metric, int64_t candidate_pool,
+                      int64_t n_iters, uint64_t seed, int32_t* out_idx, float* out_dist,
+                      cudaStream_t s, NdStats* stats = nullptr);
 
 // -------------------------------------------------------------- graph.cu
 struct Graph {

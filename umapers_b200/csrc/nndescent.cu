@@ -22,6 +22,7 @@
 // eight partial sums are added in lane order, then the scalar tail, exactly
 // as the reference does.  The query row sits in shared memory.
 #include <climits>
+#include <vector>
 
 #include "kernels.cuh"
 
@@ -140,6 +141,68 @@ __device__ inline void eval_candidates(const float* __restrict__ X, const float*
     }
 }
 
+// CSR rows for the sparse variant: the reference's SparseCsrMatrix fields
+// (sparse.rs:9-147) with its norms (sum of v * v in stored order, sqrt).
+struct NdCsr {
+    const int64_t* ptr;
+    const int32_t* idx;
+    const float* val;
+    const float* sq;
+    const float* l2;
+    int max_nnz;
+};
+
+// Distance of CSR row i (its columns and values in shared memory) to the
+// candidates in keys[0, m), one lane per candidate: the sparse dot is a
+// merge of the two sorted column lists, products of shared columns added in
+// ascending column order from +0.0 (sparse_dot, sparse.rs:220-239), and the
+// distance comes from it and the norms as in the exact sparse kNN
+// (sparse.rs:605-626); a row's distance to itself is 0 (sparse.rs:614-617).
+__device__ inline void eval_candidates_csr(const NdCsr& x, int64_t i, int metric, const int32_t* qc,
+                                           const float* qv, int qn, uint64_t* keys, int m) {
+    const int lane = threadIdx.x & 31;
+    const float q_sq = x.sq[i], q_l2 = x.l2[i];
+    for (int c = lane; c < m; c += 32) {
+        const int64_t j = static_cast<int64_t>(keys[c]);
+        float dist = 0.0f;
+        if (j != i) {
+            float dot = 0.0f;
+            int a = 0;
+            int64_t b = x.ptr[j];
+            const int64_t be = x.ptr[j + 1];
+            while (a < qn && b < be) {
+                const int32_t ca = qc[a], cb = x.idx[b];
+                if (ca == cb) {
+                    dot = __fadd_rn(dot, __fmul_rn(qv[a], x.val[b]));
+                    ++a;
+                    ++b;
+                } else if (ca < cb) {
+                    ++a;
+                } else {
+                    ++b;
+                }
+            }
+            if (metric == UMAPB_METRIC_COSINE) {
+                const float r_l2 = x.l2[j];
+                if (q_l2 == 0.0f && r_l2 == 0.0f) {
+                    dist = 0.0f;
+                } else if (q_l2 == 0.0f || r_l2 == 0.0f) {
+                    dist = 1.0f;
+                } else {
+                    float cs = __fdiv_rn(dot, __fmul_rn(q_l2, r_l2));
+                    cs = fminf(fmaxf(cs, -1.0f), 1.0f);
+                    dist = __fsub_rn(1.0f, cs);
+                }
+            } else {
+                float t = __fsub_rn(__fadd_rn(q_sq, x.sq[j]), __fmul_rn(2.0f, dot));
+                if (!(t > 0.0f)) t = 0.0f;
+                dist = __fsqrt_rn(t);
+            }
+        }
+        keys[c] = knn_key(dist, static_cast<uint32_t>(j));
+    }
+}
+
 struct NdArgs {
     const float* X;
     const float* norms;
@@ -158,26 +221,60 @@ struct NdArgs {
     float* new_dist;
     int* changed;
     unsigned long long* evaluated;  // kEvalSlots counters of candidates evaluated
+    NdCsr csr;                       // sparse rows (the SP kernels)
+    int metric;
 };
 
 constexpr int kEvalSlots = 64;  // spread the per-warp counts over 64 addresses
 
-// Shared memory of one warp: cap keys, cap candidate indices, the query row.
-__host__ __device__ inline size_t nd_warp_smem(int cap, int d) {
-    return static_cast<size_t>(cap) * 12 + static_cast<size_t>((d + 3) / 4) * 16;
+// Shared memory of one warp: cap keys, cap candidate indices, the query row
+// (d floats dense; columns and values of at most `d` stored entries sparse).
+__host__ __device__ inline size_t nd_warp_smem(int cap, int d, bool sparse = false) {
+    return static_cast<size_t>(cap) * 12 + static_cast<size_t>((d + 3) / 4) * 16 * (sparse ? 2 : 1);
+}
+
+// The query row into the warp's shared memory; returns its stored entries
+// (sparse) or d (dense).
+template <bool SP>
+__device__ inline int load_query(const NdArgs& p, int64_t i, float* qs) {
+    const int lane = threadIdx.x & 31;
+    if (!SP) {
+        for (int t = lane; t < p.d; t += 32) qs[t] = p.X[i * p.d + t];
+        return p.d;
+    }
+    const int64_t b = p.csr.ptr[i];
+    const int qn = static_cast<int>(p.csr.ptr[i + 1] - b);
+    int32_t* qc = reinterpret_cast<int32_t*>(qs);
+    float* qv = qs + p.csr.max_nnz;
+    for (int t = lane; t < qn; t += 32) {
+        qc[t] = p.csr.idx[b + t];
+        qv[t] = p.csr.val[b + t];
+    }
+    return qn;
+}
+
+template <bool SP>
+__device__ inline void eval_any(const NdArgs& p, int64_t i, const float* qs, int qn,
+                                uint64_t* keys, int m) {
+    if (SP)
+        eval_candidates_csr(p.csr, i, p.metric, reinterpret_cast<const int32_t*>(qs),
+                            qs + p.csr.max_nnz, qn, keys, m);
+    else
+        eval_any<SP>(p, i, qs, qn, keys, m);
 }
 
 // initial lists: self + `pool` unique random rows, best k kept (lib.rs:3100-3115)
+template <bool SP>
 __global__ void __launch_bounds__(kWarps * 32) nd_init_kernel(NdArgs p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* ws = smem + warp * nd_warp_smem(p.cap, p.d);
+    unsigned char* ws = smem + warp * nd_warp_smem(p.cap, SP ? p.csr.max_nnz : p.d, SP);
     uint64_t* keys = reinterpret_cast<uint64_t*>(ws);
     int32_t* cand = reinterpret_cast<int32_t*>(keys + p.cap);
     float* qs = reinterpret_cast<float*>(cand + p.cap);
     const int64_t i = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
     if (i >= p.n) return;
-    for (int t = lane; t < p.d; t += 32) qs[t] = p.X[i * p.d + t];
+    const int qn = load_query<SP>(p, i, qs);
     int cnt = 0;
     if (lane == 0) {
         cand[cnt++] = static_cast<int32_t>(i);
@@ -195,7 +292,7 @@ __global__ void __launch_bounds__(kWarps * 32) nd_init_kernel(NdArgs p) {
     for (int c = lane; c < p.cap; c += 32)
         keys[c] = c < cnt ? static_cast<uint64_t>(cand[c]) : ~0ULL;
     __syncwarp();
-    eval_candidates(p.X, p.norms, i, p.d, p.cosine, qs, keys, cnt);
+    eval_any<SP>(p, i, qs, qn, keys, cnt);
     __syncwarp();
     if (lane == 0)
         atomicAdd(p.evaluated + blockIdx.x % kEvalSlots, static_cast<unsigned long long>(cnt));
@@ -206,15 +303,16 @@ __global__ void __launch_bounds__(kWarps * 32) nd_init_kernel(NdArgs p) {
     }
 }
 
+template <bool SP>
 __global__ void __launch_bounds__(kWarps * 32) nd_iter_kernel(NdArgs p, uint64_t iteration) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* ws = smem + warp * nd_warp_smem(p.cap, p.d);
+    unsigned char* ws = smem + warp * nd_warp_smem(p.cap, SP ? p.csr.max_nnz : p.d, SP);
     uint64_t* keys = reinterpret_cast<uint64_t*>(ws);
     float* qs = reinterpret_cast<float*>(reinterpret_cast<int32_t*>(keys + p.cap) + p.cap);
     const int64_t i = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
     if (i >= p.n) return;
-    for (int t = lane; t < p.d; t += 32) qs[t] = p.X[i * p.d + t];
+    const int qn = load_query<SP>(p, i, qs);
     const int k = p.k;
     // neighbours and neighbours of neighbours, as index keys (duplicates removed after sorting)
     int cnt = 0;
@@ -282,52 +380,28 @@ __global__ void __launch_bounds__(kWarps * 32) nd_iter_kernel(NdArgs p, uint64_t
 
 }  // namespace
 
-int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t candidate_pool,
-                  int64_t n_iters, uint64_t seed, int32_t* out_idx, float* out_dist,
-                  cudaStream_t s, NdStats* stats) {
-    if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE)
-        invalid("the B200 NN-descent kernel supports metric euclidean and cosine");
-    if (n < 2 || k < 1 || k >= n) invalid("NN-descent needs 1 <= k < n_rows");
-    const int64_t ck = std::max<int64_t>(candidate_pool, k);
-    const int pool = static_cast<int>(std::min<int64_t>(ck, n - 1));
-    const int maxc = static_cast<int>(ck * 4 + 1);
-    const int expl = static_cast<int>(std::min<int64_t>(std::max<int64_t>(k / 2, 4), maxc));
-    int cap = 32;
-    const int need = std::max(k + k * k + 1 + expl, pool + 1);
-    while (cap < need) cap <<= 1;
-    const size_t smem = static_cast<size_t>(kWarps) * nd_warp_smem(cap, d);
-    if (smem > 200 * 1024)
-        invalid("n_neighbors / n_features too large for the NN-descent kernel");
-    DevBuf<float> norms;
-    if (metric == UMAPB_METRIC_COSINE) {
-        norms.alloc(n, s);
-        row_norms(X, n, d, norms.get(), nullptr, s);
-    }
+namespace {
+
+// The iteration loop shared by the dense and CSR rows: initial lists, then
+// iterations until no row changes (lists alternate between the output arrays
+// and a scratch pair).
+template <bool SP>
+int64_t nndescent_run(NdArgs p, int64_t n, int k, int64_t n_iters, size_t smem, int32_t* out_idx,
+                      float* out_dist, cudaStream_t s, NdStats* stats) {
     DevBuf<int32_t> idx_b(n * k, s);
     DevBuf<float> dist_b(n * k, s);
     DevBuf<int> changed(1, s);
     DevBuf<unsigned long long> evaluated(kEvalSlots, s);
     UMAPB_CUDA(cudaMemsetAsync(evaluated.get(), 0, kEvalSlots * 8, s));
-    NdArgs p{};
     p.evaluated = evaluated.get();
-    p.X = X;
-    p.norms = norms.get();
-    p.n = n;
-    p.d = d;
-    p.k = k;
-    p.pool = pool;
-    p.maxc = maxc;
-    p.expl = expl;
-    p.cap = cap;
-    p.cosine = metric == UMAPB_METRIC_COSINE;
-    p.seed = seed;
     p.changed = changed.get();
-    UMAPB_CUDA(cudaFuncSetAttribute(nd_init_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    UMAPB_CUDA(cudaFuncSetAttribute(nd_init_kernel<SP>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
-    UMAPB_CUDA(cudaFuncSetAttribute(nd_iter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    UMAPB_CUDA(cudaFuncSetAttribute(nd_iter_kernel<SP>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
     const unsigned grid = static_cast<unsigned>(ceil_div(n, kWarps));
-    // lists alternate between the output arrays and the scratch pair
     int32_t* cur_i = out_idx;
     float* cur_d = out_dist;
     int32_t* nxt_i = idx_b.get();
@@ -339,7 +413,7 @@ int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t c
     UMAPB_CUDA(cudaEventCreate(&e1));
     float kernel_ms = 0.0f;
     UMAPB_CUDA(cudaEventRecord(e0, s));
-    nd_init_kernel<<<grid, kWarps * 32, smem, s>>>(p);
+    nd_init_kernel<SP><<<grid, kWarps * 32, smem, s>>>(p);
     UMAPB_LAUNCH_CHECK();
     UMAPB_CUDA(cudaEventRecord(e1, s));
     UMAPB_CUDA(cudaEventSynchronize(e1));
@@ -356,7 +430,7 @@ int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t c
         p.new_idx = nxt_i;
         p.new_dist = nxt_d;
         UMAPB_CUDA(cudaEventRecord(e0, s));
-        nd_iter_kernel<<<grid, kWarps * 32, smem, s>>>(p, static_cast<uint64_t>(it + 1));
+        nd_iter_kernel<SP><<<grid, kWarps * 32, smem, s>>>(p, static_cast<uint64_t>(it + 1));
         UMAPB_LAUNCH_CHECK();
         UMAPB_CUDA(cudaEventRecord(e1, s));
         std::swap(cur_i, nxt_i);
@@ -386,6 +460,82 @@ int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t c
         UMAPB_CUDA(cudaMemcpyAsync(out_dist, cur_d, n * k * 4, cudaMemcpyDeviceToDevice, s));
     }
     return ran;
+}
+
+// Candidate-rule sizes of approximate_nearest_neighbors_with_distance
+// (lib.rs:3097-3098) and the shared-memory key capacity they need.
+void nd_sizes(NdArgs& p, int64_t n, int k, int64_t candidate_pool) {
+    const int64_t ck = std::max<int64_t>(candidate_pool, k);
+    p.pool = static_cast<int>(std::min<int64_t>(ck, n - 1));
+    p.maxc = static_cast<int>(ck * 4 + 1);
+    p.expl = static_cast<int>(std::min<int64_t>(std::max<int64_t>(k / 2, 4), p.maxc));
+    int cap = 32;
+    const int need = std::max(k + k * k + 1 + p.expl, p.pool + 1);
+    while (cap < need) cap <<= 1;
+    p.cap = cap;
+}
+
+}  // namespace
+
+int64_t nndescent(const float* X, int64_t n, int d, int k, int metric, int64_t candidate_pool,
+                  int64_t n_iters, uint64_t seed, int32_t* out_idx, float* out_dist,
+                  cudaStream_t s, NdStats* stats) {
+    if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE)
+        invalid("the B200 NN-descent kernel supports metric euclidean and cosine");
+    if (n < 2 || k < 1 || k >= n) invalid("NN-descent needs 1 <= k < n_rows");
+    NdArgs p{};
+    nd_sizes(p, n, k, candidate_pool);
+    const size_t smem = static_cast<size_t>(kWarps) * nd_warp_smem(p.cap, d);
+    if (smem > 200 * 1024)
+        invalid("n_neighbors / n_features too large for the NN-descent kernel");
+    DevBuf<float> norms;
+    if (metric == UMAPB_METRIC_COSINE) {
+        norms.alloc(n, s);
+        row_norms(X, n, d, norms.get(), nullptr, s);
+    }
+    p.X = X;
+    p.norms = norms.get();
+    p.n = n;
+    p.d = d;
+    p.k = k;
+    p.cosine = metric == UMAPB_METRIC_COSINE;
+    p.metric = metric;
+    p.seed = seed;
+    return nndescent_run<false>(p, n, k, n_iters, smem, out_idx, out_dist, s, stats);
+}
+
+int64_t nndescent_csr(const CsrDevice& x, int k, int metric, int64_t candidate_pool,
+                      int64_t n_iters, uint64_t seed, int32_t* out_idx, float* out_dist,
+                      cudaStream_t s, NdStats* stats) {
+    if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE)
+        invalid("the B200 sparse NN-descent supports metric euclidean and cosine");
+    const int64_t n = x.n_rows;
+    if (n < 2 || k < 1 || k >= n) invalid("NN-descent needs 1 <= k < n_rows");
+    // the widest row bounds the query row kept in shared memory
+    std::vector<int64_t> ptr(n + 1);
+    UMAPB_CUDA(cudaMemcpyAsync(ptr.data(), x.indptr.get(), (n + 1) * 8, cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    int64_t max_nnz = 1;
+    for (int64_t i = 0; i < n; ++i) max_nnz = std::max(max_nnz, ptr[i + 1] - ptr[i]);
+    NdArgs p{};
+    nd_sizes(p, n, k, candidate_pool);
+    const size_t smem =
+        static_cast<size_t>(kWarps) * nd_warp_smem(p.cap, static_cast<int>(max_nnz), true);
+    if (max_nnz > (1 << 20) || smem > 200 * 1024)
+        invalid("rows with this many stored values are too wide for the sparse NN-descent kernel");
+    p.csr.ptr = x.indptr.get();
+    p.csr.idx = x.indices.get();
+    p.csr.val = x.values.get();
+    p.csr.sq = x.sq.get();
+    p.csr.l2 = x.l2.get();
+    p.csr.max_nnz = static_cast<int>(max_nnz);
+    p.n = n;
+    p.d = static_cast<int>(std::min<int64_t>(x.n_cols, 1 << 30));
+    p.k = k;
+    p.cosine = metric == UMAPB_METRIC_COSINE;
+    p.metric = metric;
+    p.seed = seed;
+    return nndescent_run<true>(p, n, k, n_iters, smem, out_idx, out_dist, s, stats);
 }
 
 }  // namespace umapb
