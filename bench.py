@@ -317,11 +317,12 @@ def run_gpu(args) -> None:
     sampler = ClockSampler(local)
     with sampler:
         dev_times = []
-        knn_sec, sgd_sec, stage, pool = [], [], [], []
+        knn_sec, sgd_sec, stage, pool, waits = [], [], [], [], []
         for _ in range(args.steps):
             dev_times.append(device_step())
             pool.append(pool_reserved_gb(lib))
             knn_sec.append(info.knn_kernel_sec)
+            waits.append((info.stage_wait_sec, info.stage_host_sec))
             sgd_sec.append(timings.optimize_sec)
             stage.append({f: getattr(timings, f) for f in _lib.TIMING_FIELDS})
         barrier()
@@ -433,6 +434,10 @@ def run_gpu(args) -> None:
             # step whose kNN stage is long while this stays flat lost its time
             # outside the kernel
             "step_knn_kernel_sec": [round(t, 4) for t in knn_sec],
+            # per step: host time waiting for the device at the stage
+            # boundaries, and the rest (host work and launches); a slow step
+            # whose wait grew lost its time on the device
+            "step_wait_host_sec": [[round(a, 4), round(b, 4)] for a, b in waits],
             "pool_reserved_gb": [pool0] + pool,
         }
         if transform is not None:

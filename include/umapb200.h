@@ -135,6 +135,10 @@ typedef struct umapb_fit_info {
     double knn_kernel_sec;        /* dominant kNN kernel, CUDA events */
     double sgd_edge_samples;      /* attractive edge samples over all epochs */
     int64_t knn_second_pass_rows; /* rows the first tensor-core pass could not certify */
+    double stage_wait_sec;        /* with timings: host time spent waiting for the device
+                                     at the stage boundaries (device still busy) */
+    double stage_host_sec;        /* with timings: the rest of the staged time (host work,
+                                     launch overhead) */
 } umapb_fit_info;
 
 typedef struct umapb_model umapb_model;

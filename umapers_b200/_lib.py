@@ -110,6 +110,8 @@ class FitInfo(ctypes.Structure):
         ("knn_kernel_sec", ctypes.c_double),
         ("sgd_edge_samples", ctypes.c_double),
         ("knn_second_pass_rows", ctypes.c_int64),
+        ("stage_wait_sec", ctypes.c_double),
+        ("stage_host_sec", ctypes.c_double),
     ]
 
 

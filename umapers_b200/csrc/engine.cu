@@ -234,16 +234,25 @@ double now_sec() {
         .count();
 }
 
+// Stage timer: each lap synchronises the stream and returns the wall time
+// since the previous lap.  It also splits that time into the part the host
+// spent waiting inside the synchronisation (the device still busy) and the
+// rest (host-side work and launch overhead), summed over the laps.
 struct StageClock {
     cudaStream_t s;
     bool on;
     double t0;
+    double wait_sec = 0.0;  // inside cudaStreamSynchronize
+    double host_sec = 0.0;  // outside it
     StageClock(cudaStream_t st, bool enabled) : s(st), on(enabled), t0(now_sec()) {}
     double lap() {
         if (!on) return 0.0;
+        const double tb = now_sec();
         UMAPB_CUDA(cudaStreamSynchronize(s));
         const double t = now_sec();
         const double dt = t - t0;
+        wait_sec += t - tb;
+        host_sec += tb - t0;
         t0 = t;
         return dt;
     }
@@ -516,6 +525,8 @@ void fit_host(umapb_model* m, const float* data, int64_t n, int64_t d, FitOutput
         out->t.total_sec = now_sec() - t_start;
         out->info.n_samples = n;
         out->info.n_features = d;
+        out->info.stage_wait_sec = clk.wait_sec;
+        out->info.stage_host_sec = clk.host_sec;
     }
 }
 
@@ -1079,6 +1090,8 @@ int32_t umapb_fit_transform_device(umapb_model* m, const float* data, int64_t n_
         fo.t.total_sec = now_sec() - t_start;
         fo.info.n_samples = n_rows;
         fo.info.n_features = n_cols;
+        fo.info.stage_wait_sec = clk.wait_sec;
+        fo.info.stage_host_sec = clk.host_sec;
         if (timings) *timings = fo.t;
         if (info) *info = fo.info;
     });
