@@ -179,3 +179,31 @@ def test_umap_transform_mode_surrogate_trains_on_fit():
     assert m.transform_fallback_.shape == (300,)
     with pytest.raises(ValueError, match="feature mismatch"):
         m.transform(x[:5, :31])
+
+
+def test_chunked_host_transform_equals_device_path_and_plain_for_gated_rows(trained):
+    """The host surrogate transform uploads 131,072-row chunks and runs each
+    chunk's gated rows through the plain transform while later chunks still
+    upload.  A gated row's random stream is keyed by its row in the request,
+    so the result equals the device-resident path bit for bit, and every
+    gated row equals the plain transform of the whole request."""
+    import torch
+
+    m, fit, query, _, _ = trained
+    q = np.concatenate([query, query[:400_000] + 0.0])[:600_000].copy()
+    q[::97] += 25.0  # out-of-distribution rows in every chunk: gated
+    out_h, flags_h = m._core.transform_surrogate(q, use_fallback=True)
+    lib = _lib.load()
+    qd = torch.from_numpy(q).cuda()
+    out_d = torch.empty((q.shape[0], 2), dtype=torch.float32, device="cuda")
+    flags_d = torch.empty(q.shape[0], dtype=torch.uint8, device="cuda")
+    nf = ctypes.c_int64(0)
+    _lib.check(lib.umapb_surrogate_transform_device(m._core._handle, qd.data_ptr(), q.shape[0],
+                                                    q.shape[1], 1, out_d.data_ptr(),
+                                                    flags_d.data_ptr(), ctypes.byref(nf)))
+    out_d, flags_d = out_d.cpu().numpy(), flags_d.cpu().numpy().astype(bool)
+    assert flags_h.sum() == nf.value >= q.shape[0] // 97
+    np.testing.assert_array_equal(flags_h, flags_d)
+    np.testing.assert_array_equal(out_h, out_d)
+    plain = m.transform(q, method="plain")
+    np.testing.assert_array_equal(out_h[flags_h], plain[flags_h])

@@ -719,7 +719,8 @@ struct TransformStages {
 // with no SGD epoch.
 void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* dist, int64_t nq,
                                int k, int64_t epoch_rows, float* out_dev,
-                               const TransformStages* stages = nullptr) {
+                               const TransformStages* stages = nullptr,
+                               const int32_t* qid = nullptr, int64_t qid_offset = 0) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int dim = static_cast<int>(p.n_components);
@@ -752,15 +753,18 @@ void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* 
     }
     transform_layout(out_dev, nq, dim, m->emb.get(), m->n_fit, g, n_epochs, m->a, m->b,
                      p.learning_rate / 4.0f, p.negative_sample_rate, p.repulsion_strength,
-                     p.random_seed ^ 0xA24BAED40B53C117ULL, s);
+                     p.random_seed ^ 0xA24BAED40B53C117ULL, s, qid, qid_offset);
 }
 
 // transform_dense (lib.rs:1593-1685) on device rows.  A model fitted on CSR
 // rows takes the dense queries' nonzeros as CSR rows
 // (exact_nearest_neighbors_dense_query, sparse.rs:753-910, gives the same
 // distances).
+// `qid`/`qid_offset` give each query's row in the whole request (the key of
+// its random stream) when Qd holds a subset of the request's rows.
 void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out_dev,
-                      int64_t epoch_rows = -1, const TransformStages* stages = nullptr) {
+                      int64_t epoch_rows = -1, const TransformStages* stages = nullptr,
+                      const int32_t* qid = nullptr, int64_t qid_offset = 0) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int k = static_cast<int>(std::min<int64_t>(p.n_neighbors, m->n_fit));
@@ -775,11 +779,13 @@ void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, fl
         knn_exact_device(Qd, nq, m->X.get(), m->n_fit, static_cast<int>(d), k, p.metric,
                          p.knn_backend, idx.get(), dist.get(), nullptr, nullptr, nullptr, s);
     }
-    transform_from_knn_device(m, idx.get(), dist.get(), nq, k, epoch_rows, out_dev, stages);
+    transform_from_knn_device(m, idx.get(), dist.get(), nq, k, epoch_rows, out_dev, stages, qid,
+                              qid_offset);
 }
 
 void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
-                        const uint8_t* flags, int64_t nf);
+                        const uint8_t* flags, int64_t nf, int64_t epoch_rows = -1,
+                        int64_t row_offset = 0);
 
 // Surrogate transform of device rows: network outputs for every row, then
 // (use_fallback) the plain transform for the rows the gate rejects.
@@ -799,16 +805,22 @@ void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int
 }
 
 // The plain transform for the `nf` rows the gate flagged, scattered into out.
+// Its epoch count follows `epoch_rows` rows (the whole request), default nq;
+// row i of Qd is row row_offset + i of the request, which keys its random
+// stream, so a gated row gets what the plain transform of the request gives.
 void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
-                        const uint8_t* flags, int64_t nf) {
+                        const uint8_t* flags, int64_t nf, int64_t epoch_rows,
+                        int64_t row_offset) {
     if (nf == 0) return;
+    if (epoch_rows < 0) epoch_rows = nq;
     cudaStream_t s = m->stream;
     const int dim = static_cast<int>(m->p.n_components);
     DevBuf<int32_t> ids(nf, s);
     select_flagged(flags, nq, ids.get(), s);
     DevBuf<float> sub(nf * d, s), sub_out(nf * dim, s);
     gather_rows(Qd, ids.get(), nf, static_cast<int>(d), sub.get(), s);
-    transform_device(m, sub.get(), nf, d, sub_out.get(), nq);
+    transform_device(m, sub.get(), nf, d, sub_out.get(), epoch_rows, nullptr, ids.get(),
+                     row_offset);
     scatter_rows(sub_out.get(), ids.get(), nf, dim, out, s);
 }
 
@@ -1694,8 +1706,26 @@ int32_t umapb_surrogate_transform(umapb_model* m, const float* query, int64_t n_
         // are read back once, before the fallback and the outputs.  (Copies
         // from pageable host memory are staged by the driver and keep the
         // host busy until they land; pinned rows let the queueing run ahead.)
+        // With the fallback on, the rows chunk c - 1 gated run their plain
+        // transform once chunk c is queued, while later chunks still upload;
+        // only the last chunk's fallback follows the upload.  Checking a chunk
+        // reads the running first-non-finite row and the chunk's gate count
+        // (one host wait per chunk on the model's stream; the copies run on).
         DevBuf<unsigned long long> bad_row(1, s);
         UMAPB_CUDA(cudaMemsetAsync(bad_row.get(), 0xFF, 8, s));
+        int64_t nf = 0;
+        auto settle = [&](int64_t c) {
+            const int64_t r0 = c * chunk, rows = std::min(chunk, n_rows - r0);
+            unsigned long long bad = 0;
+            UMAPB_CUDA(cudaMemcpyAsync(&bad, bad_row.get(), 8, cudaMemcpyDeviceToHost, s));
+            const int64_t nfc = surrogate_count_flags(fl.get() + r0, rows, s);  // synchronises s
+            if (bad != ~0ull)
+                invalid("input contains non-finite value at row " + std::to_string(bad));
+            nf += nfc;
+            if (use_fallback != 0)
+                surrogate_fallback(m, Q.get() + r0 * n_cols, rows, n_cols, outd.get() + r0 * dim,
+                                   fl.get() + r0, nfc, n_rows, r0);
+        };
         for (int64_t c = 0; c < n_chunks; ++c) {
             const int64_t r0 = c * chunk, rows = std::min(chunk, n_rows - r0);
             UMAPB_CUDA(cudaStreamWaitEvent(s, cs.done[c], 0));
@@ -1704,13 +1734,10 @@ int32_t umapb_surrogate_transform(umapb_model* m, const float* query, int64_t n_
             surrogate_infer_async(*m->surrogate, Q.get() + r0 * n_cols, rows,
                                   static_cast<int>(n_cols), outd.get() + r0 * dim, fl.get() + r0,
                                   s);
+            if (c > 0) settle(c - 1);
         }
-        unsigned long long bad = 0;
-        UMAPB_CUDA(cudaMemcpyAsync(&bad, bad_row.get(), 8, cudaMemcpyDeviceToHost, s));
-        const int64_t nf = surrogate_count_flags(fl.get(), n_rows, s);  // synchronises s
-        if (bad != ~0ull) invalid("input contains non-finite value at row " + std::to_string(bad));
+        settle(n_chunks - 1);
         if (n_fallback) *n_fallback = nf;
-        if (use_fallback != 0) surrogate_fallback(m, Q.get(), n_rows, n_cols, outd.get(), fl.get(), nf);
         UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * dim * 4, cudaMemcpyDeviceToHost, s));
         if (fallback)
             UMAPB_CUDA(cudaMemcpyAsync(fallback, fl.get(), n_rows, cudaMemcpyDeviceToHost, s));

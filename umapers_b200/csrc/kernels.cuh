@@ -247,9 +247,12 @@ int64_t density_start_epoch(int64_t n_epochs, float frac);
 
 // init_graph_transform + optimize_layout_transform
 // (rust_umap/src/lib.rs:4793-4836, 5444-5544): one thread per query.
+// Query q's random stream is keyed by (qid ? qid[q] : q) + qid_offset, its
+// row in the whole request.
 void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_t n_base,
                       const Graph& g, int64_t n_epochs, float a, float b, float lr,
-                      int64_t neg_rate, float repulsion, uint64_t seed, cudaStream_t s);
+                      int64_t neg_rate, float repulsion, uint64_t seed, cudaStream_t s,
+                      const int32_t* qid = nullptr, int64_t qid_offset = 0);
 
 // --------------------------------------------------------- surrogate.cu
 struct Surrogate;

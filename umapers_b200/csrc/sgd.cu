@@ -677,7 +677,17 @@ struct TransformArgs {
     int64_t n_epochs;
     float a, b, lr, rep, neg_rate_f;
     uint64_t seed;
+    const int32_t* qid;  // (nullable) row of each query in the whole request
+    int64_t qid_offset;  // added to qid (or to the query index)
 };
+
+// The query's row in the whole request keys its random stream, so a query
+// transformed alone, with a batch, or as a gated row of a surrogate request
+// draws the same negatives.
+__device__ __forceinline__ uint64_t query_seed(const TransformArgs& p, int64_t q) {
+    const int64_t key = (p.qid != nullptr ? static_cast<int64_t>(p.qid[q]) : q) + p.qid_offset;
+    return mix64(p.seed ^ mix64(static_cast<uint64_t>(key)));
+}
 
 __device__ inline bool row_finite(const float* v, int dim) {
     for (int c = 0; c < dim; ++c)
@@ -718,7 +728,7 @@ __device__ __forceinline__ void transform_schedule_2d(const TransformArgs& p, in
 #pragma unroll
             for (int s = 0; s < kNegPrefetch; ++s) {
                 if (static_cast<uint32_t>(s) < n_neg) {
-                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e - st),
                                                    (static_cast<uint64_t>(epoch) << 32) | s);
                     ng[s] = base[rng_below(word, p.n_base)];
                 }
@@ -745,7 +755,7 @@ __device__ __forceinline__ void transform_schedule_2d(const TransformArgs& p, in
                     for (int t = 1; t < kNegPrefetch; ++t)
                         if (s == static_cast<uint32_t>(t)) o = ng[t];
                 } else {
-                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e - st),
                                                    (static_cast<uint64_t>(epoch) << 32) | s);
                     o = base[rng_below(word, p.n_base)];
                 }
@@ -878,7 +888,7 @@ __device__ __forceinline__ void transform_schedule_2d_staged(const TransformArgs
 #pragma unroll
             for (int s = 0; s < kNegPrefetch; ++s) {
                 if (static_cast<uint32_t>(s) < n_neg) {
-                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e - st),
                                                    (static_cast<uint64_t>(epoch) << 32) | s);
                     ng[s] = base[rng_below(word, p.n_base)];
                 }
@@ -907,7 +917,7 @@ __device__ __forceinline__ void transform_schedule_2d_staged(const TransformArgs
                     for (int t = 1; t < kNegPrefetch; ++t)
                         if (s == static_cast<uint32_t>(t)) o = ng[t];
                 } else {
-                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                    const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e - st),
                                                    (static_cast<uint64_t>(epoch) << 32) | s);
                     o = base[rng_below(word, p.n_base)];
                 }
@@ -941,7 +951,7 @@ __global__ void __launch_bounds__(kTransformThreads) transform_kernel(TransformA
     if (dim == 2 && en - st <= kStageEdges) {
         float c2[2];
         stage_query_2d(p, st, en - st, sm, tid, c2);
-        const uint64_t qseed = mix64(p.seed ^ mix64(static_cast<uint64_t>(q)));
+        const uint64_t qseed = query_seed(p, q);
         transform_schedule_2d_staged(p, st, en - st, qseed, sm, tid, c2);
         p.out[q * 2] = c2[0];
         p.out[q * 2 + 1] = c2[1];
@@ -976,7 +986,7 @@ __global__ void __launch_bounds__(kTransformThreads) transform_kernel(TransformA
         }
     }
     // optimize_layout_transform (lib.rs:5444-5544)
-    const uint64_t qseed = mix64(p.seed ^ mix64(static_cast<uint64_t>(q)));
+    const uint64_t qseed = query_seed(p, q);
     if (dim == 2) {
         transform_schedule_2d(p, q, st, en, qseed, cur);
         p.out[q * 2] = cur[0];
@@ -1011,7 +1021,7 @@ __global__ void __launch_bounds__(kTransformThreads) transform_kernel(TransformA
             const float nn = p.next_neg[e];
             const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(ef, nn), eneg));
             for (uint32_t s = 0; s < n_neg; ++s) {
-                const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e),
+                const uint64_t word = rng_word(qseed, static_cast<uint64_t>(e - st),
                                                (static_cast<uint64_t>(epoch) << 32) | s);
                 const uint32_t neg = rng_below(word, p.n_base);
                 const float* o = p.base + static_cast<int64_t>(neg) * dim;
@@ -1449,7 +1459,8 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
 
 void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_t n_base,
                       const Graph& g, int64_t n_epochs, float a, float b, float lr,
-                      int64_t neg_rate, float repulsion, uint64_t seed, cudaStream_t s) {
+                      int64_t neg_rate, float repulsion, uint64_t seed, cudaStream_t s,
+                      const int32_t* qid, int64_t qid_offset) {
     if (nq == 0) return;
     if (dim > kMaxDim) invalid("n_components above 16 is not supported by the GPU layout kernel");
     const int64_t m = g.n_edges;
@@ -1482,6 +1493,8 @@ void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_
     p.rep = repulsion;
     p.neg_rate_f = nrf;
     p.seed = seed;
+    p.qid = qid;
+    p.qid_offset = qid_offset;
     transform_kernel<<<static_cast<unsigned>(ceil_div(nq, static_cast<int64_t>(kTransformThreads))),
                        kTransformThreads, 0, s>>>(p);
     UMAPB_LAUNCH_CHECK();
