@@ -117,6 +117,7 @@ def test_gate_sends_out_of_distribution_rows_to_plain(trained):
     m, fit, query, _, _ = trained
     far = query[:500] + 40.0
     out, flags = m._core.transform_surrogate(far, use_fallback=True)
+    flags = flags.astype(bool)
     assert flags.mean() > 0.99
     plain = m.transform(far)
     assert np.allclose(out[flags], plain[flags], atol=1e-4)
@@ -193,6 +194,7 @@ def test_chunked_host_transform_equals_device_path_and_plain_for_gated_rows(trai
     q = np.concatenate([query, query[:400_000] + 0.0])[:600_000].copy()
     q[::97] += 25.0  # out-of-distribution rows in every chunk: gated
     out_h, flags_h = m._core.transform_surrogate(q, use_fallback=True)
+    flags_h = flags_h.astype(bool)
     lib = _lib.load()
     qd = torch.from_numpy(q).cuda()
     out_d = torch.empty((q.shape[0], 2), dtype=torch.float32, device="cuda")
