@@ -260,7 +260,7 @@ __device__ inline void eval_any(const NdArgs& p, int64_t i, const float* qs, int
         eval_candidates_csr(p.csr, i, p.metric, reinterpret_cast<const int32_t*>(qs),
                             qs + p.csr.max_nnz, qn, keys, m);
     else
-        eval_any<SP>(p, i, qs, qn, keys, m);
+        eval_candidates(p.X, p.norms, i, p.d, p.cosine, qs, keys, m);
 }
 
 // initial lists: self + `pool` unique random rows, best k kept (lib.rs:3100-3115)
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(kWarps * 32) nd_iter_kernel(NdArgs p, uint64_t
     // evaluate every candidate
     for (int c = m + lane; c < p.cap; c += 32) keys[c] = ~0ULL;
     __syncwarp();
-    eval_candidates(p.X, p.norms, i, p.d, p.cosine, qs, keys, m);
+    eval_any<SP>(p, i, qs, qn, keys, m);
     __syncwarp();
     if (lane == 0)
         atomicAdd(p.evaluated + blockIdx.x % kEvalSlots, static_cast<unsigned long long>(m));
