@@ -234,12 +234,16 @@ def _topics(n, d, n_topics, per_row, seed):
 
 
 @pytest.mark.parametrize("metric", ["cosine", "euclidean"])
-def test_sparse_nndescent_recall_against_exact(metric):
+def test_sparse_nndescent_recall_against_exact(orc, metric):
     """NN-descent on CSR rows (the reference's candidate rule, the exact
     sparse kNN's distances): every listed distance equals the exact sparse
     distance of that pair, lists are sorted with self first, and recall@15
-    against the exact sparse kNN (itself bit-exact with the oracle) is high
-    at the reference's default 50 candidates and 14 iterations."""
+    against the exact sparse kNN (itself bit-exact with the oracle) matches
+    the recall of the oracle's NN-descent on the same rows densified, at the
+    reference's default 50 candidates and 14 iterations.  Euclidean distances
+    on these rows are hub-dominated (rows with small norms are near to
+    everyone), and the reference's algorithm itself reaches about 0.55 there;
+    cosine reaches about 0.94."""
     m = _topics(6000, 2000, 20, 20, seed=21)
     k = 15
     ai, ad, ran, ev = _gpu_nndescent_csr(m, k, metric, 50, 14)
@@ -248,8 +252,14 @@ def test_sparse_nndescent_recall_against_exact(metric):
     assert np.all(ai[:, 0] == np.arange(6000)) and np.all(ad[:, 0] == 0.0)
     assert np.all(np.diff(ad, axis=1) >= 0)
     recall = np.mean([len(set(ai[r]) & set(ei[r])) / k for r in range(6000)])
-    print(metric, "recall", recall, "iterations", ran)
-    assert recall >= 0.8
+    x = m.toarray().astype(np.float32)
+    oi = orc.nndescent(x, k, 50, 14, 99, metric=metric)[0]
+    oe = orc.exact_knn(x, k, metric=metric)[0]
+    ref = np.mean([len(set(oi[r]) & set(oe[r])) / k for r in range(6000)])
+    print(metric, "recall", recall, "oracle recall", ref, "iterations", ran)
+    assert recall >= ref - 0.02
+    if metric == "cosine":
+        assert recall >= 0.9
     # a pair listed by both has the same FP32 distance
     for r in range(0, 6000, 97):
         common = set(ai[r]) & set(ei[r])
