@@ -500,9 +500,14 @@ int32_t umapb_surrogate_fit(umapb_model* model, const umapb_surrogate_params* pa
 int32_t umapb_surrogate_ready(const umapb_model* model);
 
 /* Transform through the surrogate.  With `use_fallback` = 1, rows the gate
- * rejects are recomputed by the plain transform; with 0 every row keeps the
- * network's output.  `fallback` (may be NULL, n_rows bytes) receives 1 for
- * each gated row; `n_fallback` (may be NULL) their count.  Host buffers. */
+ * rejects are recomputed by the plain transform, each as a request of its own
+ * (its sigma floor, prune threshold and sampling periods follow its own
+ * neighbours) with the request's epoch count and the random stream of its
+ * row in the request, so a gated row's result does not depend on the other
+ * rows; with 0 every row keeps the network's output.  `fallback` (may be
+ * NULL, n_rows bytes) receives 1 for each gated row; `n_fallback` (may be
+ * NULL) their count.  Host buffers, uploaded in chunks while the gated rows
+ * of earlier chunks are recomputed. */
 int32_t umapb_surrogate_transform(umapb_model* model, const float* query, int64_t n_rows,
                                   int64_t n_cols, int32_t use_fallback, float* out,
                                   uint8_t* fallback, int64_t* n_fallback);

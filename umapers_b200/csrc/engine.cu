@@ -716,11 +716,14 @@ struct TransformStages {
 // follows the size of the whole request, `epoch_rows` (lib.rs:1650-1657).
 // With `stages`, sigma, rho and the pruned edges are copied out and out_dev
 // receives init_graph_transform's positions: the same transform kernel runs
-// with no SGD epoch.
+// with no SGD epoch.  With `row_local` every query is transformed as a
+// request of its own (its sigma floor, prune threshold and sampling periods
+// follow its own distances and weights, not the batch's).
 void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* dist, int64_t nq,
                                int k, int64_t epoch_rows, float* out_dev,
                                const TransformStages* stages = nullptr,
-                               const int32_t* qid = nullptr, int64_t qid_offset = 0) {
+                               const int32_t* qid = nullptr, int64_t qid_offset = 0,
+                               bool row_local = false) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int dim = static_cast<int>(p.n_components);
@@ -728,9 +731,10 @@ void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* 
                                              : (epoch_rows <= 10000 ? 100 : 30);
     DevBuf<float> sig(nq, s), rho(nq, s);
     const float lc = std::max(p.local_connectivity - 1.0f, 0.0f);
-    smooth_knn(dist, nq, k, static_cast<float>(k), lc, 1.0f, false, sig.get(), rho.get(), s);
+    smooth_knn(dist, nq, k, static_cast<float>(k), lc, 1.0f, false, sig.get(), rho.get(), s,
+               row_local);
     Graph g;
-    bipartite_graph(idx, dist, sig.get(), rho.get(), nq, k, n_epochs, g, s);
+    bipartite_graph(idx, dist, sig.get(), rho.get(), nq, k, n_epochs, g, s, row_local);
     if (stages) {
         if (g.n_edges > stages->capacity)
             invalid("edge capacity " + std::to_string(stages->capacity) + " below the " +
@@ -761,10 +765,12 @@ void transform_from_knn_device(umapb_model* m, const int32_t* idx, const float* 
 // (exact_nearest_neighbors_dense_query, sparse.rs:753-910, gives the same
 // distances).
 // `qid`/`qid_offset` give each query's row in the whole request (the key of
-// its random stream) when Qd holds a subset of the request's rows.
+// its random stream) when Qd holds a subset of the request's rows;
+// `row_local` transforms every row as a request of its own.
 void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out_dev,
                       int64_t epoch_rows = -1, const TransformStages* stages = nullptr,
-                      const int32_t* qid = nullptr, int64_t qid_offset = 0) {
+                      const int32_t* qid = nullptr, int64_t qid_offset = 0,
+                      bool row_local = false) {
     cudaStream_t s = m->stream;
     const umapb_params& p = m->p;
     const int k = static_cast<int>(std::min<int64_t>(p.n_neighbors, m->n_fit));
@@ -780,7 +786,7 @@ void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, fl
                          p.knn_backend, idx.get(), dist.get(), nullptr, nullptr, nullptr, s);
     }
     transform_from_knn_device(m, idx.get(), dist.get(), nq, k, epoch_rows, out_dev, stages, qid,
-                              qid_offset);
+                              qid_offset, row_local);
 }
 
 void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
@@ -805,9 +811,12 @@ void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int
 }
 
 // The plain transform for the `nf` rows the gate flagged, scattered into out.
-// Its epoch count follows `epoch_rows` rows (the whole request), default nq;
-// row i of Qd is row row_offset + i of the request, which keys its random
-// stream, so a gated row gets what the plain transform of the request gives.
+// Each gated row is transformed as a request of its own (its sigma floor,
+// prune threshold and sampling periods follow its own neighbours, not the
+// other rows'), with the epoch count of `epoch_rows` rows (the whole
+// request, default nq) and the random stream of its row in the request (row
+// i of Qd is row row_offset + i).  A gated row's result therefore does not
+// depend on which other rows were gated, nor on how the request is split.
 void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
                         const uint8_t* flags, int64_t nf, int64_t epoch_rows,
                         int64_t row_offset) {
@@ -820,7 +829,7 @@ void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, 
     DevBuf<float> sub(nf * d, s), sub_out(nf * dim, s);
     gather_rows(Qd, ids.get(), nf, static_cast<int>(d), sub.get(), s);
     transform_device(m, sub.get(), nf, d, sub_out.get(), epoch_rows, nullptr, ids.get(),
-                     row_offset);
+                     row_offset, true);
     scatter_rows(sub_out.get(), ids.get(), nf, dim, out, s);
 }
 

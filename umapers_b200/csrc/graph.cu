@@ -121,9 +121,15 @@ __global__ void smooth_knn_kernel(const float* __restrict__ dist, int64_t n, int
     float min_scale;
     if (rho > 0.0f) {
         min_scale = __fmul_rn(MIN_K_DIST_SCALE, mean_ith);
-    } else {
+    } else if (gsum != nullptr) {
         const float mean_all = gcount > 0 ? static_cast<float>(*gsum / gcount) : 0.0f;
         min_scale = __fmul_rn(MIN_K_DIST_SCALE, mean_all);
+    } else {
+        // a request of this row alone: the FP64 sum of its own distances
+        double acc = 0.0;
+        for (int c = start; c < k; ++c) acc += static_cast<double>(row[c]);
+        const float mean_row = m > 0 ? static_cast<float>(acc / static_cast<double>(m)) : 0.0f;
+        min_scale = __fmul_rn(MIN_K_DIST_SCALE, mean_row);
     }
     sigmas[i] = fmaxf(mid, min_scale);
     rhos[i] = rho;
@@ -223,6 +229,27 @@ struct KeepFlag {
     __device__ bool operator()(const int64_t& e) const { return w[e] >= thr && w[e] > 0.0f; }
 };
 
+// The same rule against each query's own threshold (row-local graphs).
+struct RowKeepFlag {
+    const float* w;
+    const float* thr;  // per query
+    int k;
+    __device__ bool operator()(const int64_t& e) const {
+        return w[e] >= thr[e / k] && w[e] > 0.0f;
+    }
+};
+
+// Each query's largest weight and its prune threshold max / denom.
+__global__ void row_max_kernel(const float* __restrict__ w, int64_t nq, int k, float denom,
+                               float* __restrict__ row_max, float* __restrict__ thr) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    float mx = -INFINITY;
+    for (int c = 0; c < k; ++c) mx = fmaxf(mx, w[i * k + c]);
+    row_max[i] = mx;
+    thr[i] = __fdiv_rn(mx, denom);
+}
+
 __global__ void bipartite_kernel(const int32_t* __restrict__ idx, const float* __restrict__ dist,
                                  const float* __restrict__ sig, const float* __restrict__ rho,
                                  int64_t nq, int k, float* __restrict__ w) {
@@ -316,11 +343,11 @@ inline unsigned grid_for(int64_t n, int threads = 256) {
 
 // Stable selection of the edges with w >= threshold && w > 0; returns the
 // indices and the count.
-int64_t select_kept(const float* w, int64_t m, float thr, DevBuf<int64_t>& sel, cudaStream_t s) {
+template <typename Flag>
+int64_t select_kept_if(int64_t m, Flag flag, DevBuf<int64_t>& sel, cudaStream_t s) {
     sel.alloc(std::max<int64_t>(m, 1), s);
     DevBuf<int64_t> nsel(1, s);
     cub::CountingInputIterator<int64_t> it(0);
-    KeepFlag flag{w, thr};
     size_t tmp_bytes = 0;
     UMAPB_CUDA(cub::DeviceSelect::If(nullptr, tmp_bytes, it, sel.get(), nsel.get(), m, flag, s));
     DevBuf<unsigned char> tmp(tmp_bytes, s);
@@ -330,6 +357,10 @@ int64_t select_kept(const float* w, int64_t m, float thr, DevBuf<int64_t>& sel, 
     UMAPB_CUDA(cudaMemcpyAsync(&h, nsel.get(), 8, cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
     return h;
+}
+
+int64_t select_kept(const float* w, int64_t m, float thr, DevBuf<int64_t>& sel, cudaStream_t s) {
+    return select_kept_if(m, KeepFlag{w, thr}, sel, s);
 }
 
 }  // namespace
@@ -349,14 +380,17 @@ bool knn_includes_self(const int32_t* idx, const float* dist, int64_t n, int k, 
 }
 
 void smooth_knn(const float* dist, int64_t n, int k, float k_f, float local_conn, float bandwidth,
-                bool include_self, float* sigmas, float* rhos, cudaStream_t s) {
+                bool include_self, float* sigmas, float* rhos, cudaStream_t s, bool row_local) {
     if (n == 0) return;
     const int start = (include_self && k > 0) ? 1 : 0;
-    DevBuf<double> gsum(1, s);
-    UMAPB_CUDA(cudaMemsetAsync(gsum.get(), 0, 8, s));
-    const unsigned mb = static_cast<unsigned>(std::min<int64_t>(ceil_div(n, 256), 148 * 8));
-    mean_dist_kernel<<<mb, 256, 0, s>>>(dist, n, k, start, gsum.get());
-    UMAPB_LAUNCH_CHECK();
+    DevBuf<double> gsum;
+    if (!row_local) {
+        gsum.alloc(1, s);
+        UMAPB_CUDA(cudaMemsetAsync(gsum.get(), 0, 8, s));
+        const unsigned mb = static_cast<unsigned>(std::min<int64_t>(ceil_div(n, 256), 148 * 8));
+        mean_dist_kernel<<<mb, 256, 0, s>>>(dist, n, k, start, gsum.get());
+        UMAPB_LAUNCH_CHECK();
+    }
     const float target = __builtin_log2f(k_f) * bandwidth;
     const double count = static_cast<double>(n) * (k - start);
     smooth_knn_kernel<<<grid_for(n, 128), 128, 0, s>>>(dist, n, k, start, target, local_conn,
@@ -525,7 +559,7 @@ void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, con
 
 void bipartite_graph(const int32_t* idx, const float* dist, const float* sigmas,
                      const float* rhos, int64_t nq, int k, int64_t n_epochs, Graph& g,
-                     cudaStream_t s) {
+                     cudaStream_t s, bool row_local) {
     const int64_t m = nq * k;
     DevBuf<float> w(std::max<int64_t>(m, 1), s);
     g.n = nq;
@@ -537,11 +571,20 @@ void bipartite_graph(const int32_t* idx, const float* dist, const float* sigmas,
     }
     bipartite_kernel<<<grid_for(m), 256, 0, s>>>(idx, dist, sigmas, rhos, nq, k, w.get());
     UMAPB_LAUNCH_CHECK();
-    const float mx = max_weight(w.get(), m, s);
     const float denom = n_epochs > 10 ? static_cast<float>(n_epochs) : 500.0f;
-    const float thr = mx / denom;
     DevBuf<int64_t> sel;
-    const int64_t kept = select_kept(w.get(), m, thr, sel, s);
+    int64_t kept = 0;
+    if (row_local) {
+        DevBuf<float> thr(nq, s);
+        g.row_max.alloc(nq, s);
+        row_max_kernel<<<grid_for(nq), 256, 0, s>>>(w.get(), nq, k, denom, g.row_max.get(),
+                                                    thr.get());
+        UMAPB_LAUNCH_CHECK();
+        kept = select_kept_if(m, RowKeepFlag{w.get(), thr.get(), k}, sel, s);
+    } else {
+        const float mx = max_weight(w.get(), m, s);
+        kept = select_kept(w.get(), m, mx / denom, sel, s);
+    }
     g.heads.alloc(std::max<int64_t>(kept, 1), s);
     g.tails.alloc(std::max<int64_t>(kept, 1), s);
     g.weights.alloc(std::max<int64_t>(kept, 1), s);

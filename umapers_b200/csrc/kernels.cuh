@@ -153,6 +153,7 @@ int64_t nndescent_csr(const CsrDevice& x, int k, int metric, int64_t candidate_p
 struct Graph {
     DevBuf<int32_t> heads, tails, row_ptr;  // row_ptr: n+1 offsets into edges
     DevBuf<float> weights;
+    DevBuf<float> row_max;  // row-local bipartite graphs: each query's largest weight
     int64_t n = 0;
     int64_t n_edges = 0;
 };
@@ -161,8 +162,11 @@ struct Graph {
 bool knn_includes_self(const int32_t* idx, const float* dist, int64_t n, int k, cudaStream_t s);
 
 // smooth_knn_dist (rust_umap/src/lib.rs:3424-3523), one thread per row.
+// `row_local`: every row as a request of its own (the floor of a row with
+// rho = 0 uses the mean of its own distances, not of all rows').
 void smooth_knn(const float* dist, int64_t n, int k, float k_f, float local_conn, float bandwidth,
-                bool include_self, float* sigmas, float* rhos, cudaStream_t s);
+                bool include_self, float* sigmas, float* rhos, cudaStream_t s,
+                bool row_local = false);
 
 // A categorical supervision target (SupervisedTarget, rust_umap/src/lib.rs:
 // 109-125) on the device: int64 labels (-1 = unlabelled), the target weight
@@ -185,10 +189,12 @@ void fuzzy_union(const int32_t* idx, const float* dist, const float* sigmas, con
                  double* phase_sec = nullptr, const CategoricalTarget* target = nullptr);
 
 // Bipartite membership + prune for transform (rust_umap/src/lib.rs:1738-1761):
-// edges grouped by query in kNN order; returns the edge count.
+// edges grouped by query in kNN order; returns the edge count.  With
+// `row_local` every query is pruned against its own largest weight (a
+// request of one row), kept in g.row_max for the sampling periods.
 void bipartite_graph(const int32_t* idx, const float* dist, const float* sigmas,
                      const float* rhos, int64_t nq, int k, int64_t n_epochs, Graph& g,
-                     cudaStream_t s);
+                     cudaStream_t s, bool row_local = false);
 
 // CSR offsets of a head-sorted edge list.
 void build_row_ptr(const int32_t* heads, int64_t n_edges, int64_t n, int32_t* row_ptr,

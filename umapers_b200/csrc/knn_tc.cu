@@ -30,8 +30,9 @@
 //    keys in a global list.  A per-list threshold skips a row's 64 columns
 //    with one vote in the common case; otherwise the row's values are
 //    transposed across the warp through a shared-memory scratch and its
-//    qualifying keys are inserted cooperatively (one list entry per lane),
-//    while the next pending row's list is already being loaded.  When the
+//    keys below the threshold are appended behind the list's sorted keys in
+//    one store.  A list is merged (bitonic, one key per lane) only when its
+//    appended keys would overflow S, which also lowers its threshold.  When the
 //    query tiles are fewer than the SMs, the candidate tiles are split too
 //    (one wave of units), with lists per split.  A self kNN over at least one
 //    wave of query groups first regroups its rows by nearest pivot ("cell
@@ -74,6 +75,7 @@ constexpr int BM = 128;     // query rows per tile (UMMA M)
 constexpr int BK = kBK;     // FP16 columns per k-block (one 128-byte swizzle row)
 constexpr int UK = kUK;     // K of one tcgen05.mma kind::f16
 constexpr int S = 32;       // shortlist length per list
+constexpr int LS = 2 * S;   // slots per list: S sorted keys, then up to S appended
 constexpr int kMaxK = 62;   // neighbours per row on the tensor path (64-entry re-rank lists)
 constexpr int kATileBytes = BM * BK * 2;  // 16 KiB: one query tile's k-block
 constexpr int kBarBytes = 256;            // mbarriers, TMEM address, abort flag
@@ -237,9 +239,38 @@ __device__ __forceinline__ T rank_of(T lo, T hi, int r) {
     return r < 32 ? a : b;
 }
 
-// A chunk with at least this many qualifying keys is merged in one bitonic
-// pass instead of key by key (about 6 sequential insertions cost as much).
+// Held keys at or above this count are merged in one bitonic pass instead of
+// key by key (about 6 sequential insertions cost as much).
 constexpr int kBulkMergeMin = 6;
+
+// A list occupies LS = 2S slots: its S smallest keys so far, sorted
+// ascending, then up to S keys appended unsorted since the last merge (every
+// one below the threshold of that merge).  Merges the `held` appended keys
+// into the sorted ones (one key per lane) and returns the new S-th smallest
+// L, or +inf while the list holds fewer than S keys.
+__device__ __forceinline__ float merge_held(uint64_t* lst, int held) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();  // the appended keys were stored by other lanes
+    uint64_t lk = lst[lane];
+    const uint64_t hk = lane < held ? lst[S + lane] : ~0ull;
+    if (held >= kBulkMergeMin) {
+        lk = warp_merge_keys(lk, hk);
+    } else {
+        for (int b = 0; b < held; ++b) {
+            const uint64_t key = __shfl_sync(0xffffffffu, hk, b);
+            const int pos = __popc(__ballot_sync(0xffffffffu, lk < key));
+            const uint64_t up = __shfl_up_sync(0xffffffffu, lk, 1);
+            if (lane > pos)
+                lk = up;
+            else if (lane == pos)
+                lk = key;
+        }
+    }
+    lst[lane] = lk;
+    __syncwarp();
+    const uint64_t last = __shfl_sync(0xffffffffu, lk, S - 1);
+    return last == ~0ull ? INFINITY : o2f(static_cast<uint32_t>(last >> 32));
+}
 
 // CTAs begin their candidate range at staggered tiles (16 groups, 2 tiles
 // apart) so they do not all request the same tile at once.  The shortlist
@@ -256,8 +287,9 @@ struct TcArgs {
     int n_split;          // candidate splits per group (1 unless query tiles are few)
     int64_t split_tiles;  // candidate tiles per split (the last split may hold fewer)
     int64_t n_ctiles;     // candidate tiles
-    uint64_t* lists;      // n_q x n_split x (BN / 64) x S keys (L order-mapped << 32 |
-                          // index), one list per (row, candidate split, 64-column group)
+    uint64_t* lists;      // n_q x n_split x (BN / 64) lists of LS slots of keys (L
+                          // order-mapped << 32 | index), one list per (row, candidate split,
+                          // 64-column group)
     const int32_t* start_tile;  // per query group, the first candidate tile to visit (rows in
                                 // cell order, one split), or null for the staggered start
     int* err;
@@ -298,8 +330,9 @@ constexpr int epi_warps() { return 4 * MT * (BN / 64); }
 template <int MT, int BN>
 constexpr int tc_threads() { return 64 + 32 * epi_warps<MT, BN>(); }
 
+// 112 registers a thread: 576 threads x 112 fit the SM's 65,536 without spills.
 template <int MT, int BN, bool SA>
-__global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
+__global__ void __maxnreg__(112)
     tc_knn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                   TcArgs p) {
     static_assert(MT * BN <= 256 && (BN == 128 || BN == 256), "at most 512 TMEM columns");
@@ -486,9 +519,10 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
             const bool row_ok = row < p.n_q;
             const int32_t list_base = w.split * GPT + cq;  // list of (row, split, group)
             auto list_of = [&](int32_t srow) {
-                return p.lists + (static_cast<int64_t>(srow) * GPT * p.n_split + list_base) * S;
+                return p.lists + (static_cast<int64_t>(srow) * GPT * p.n_split + list_base) * LS;
             };
-            float tau = INFINITY;  // this list's current S-th smallest bound
+            float tau = INFINITY;  // this row's list: its S-th smallest key at the last merge
+            int held = 0;          // keys appended behind the sorted ones since then
             for (int32_t c = 0; c < w.len; ++c, ++cg) {
                 const uint32_t buf = static_cast<uint32_t>(cg & 1);
                 if (!mbar_wait(b_tfull + 8 * buf, static_cast<uint32_t>((cg >> 1) & 1), abort_flag)) {
@@ -512,23 +546,14 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                 if (pend == 0) continue;
                 const int32_t colh = tile_at(c, w) * BN + cq * 64;
                 const int32_t valid_cols = static_cast<int32_t>(p.n_r - colh);
-                // Rows are served one at a time; the next pending row's list is
-                // loaded while the current one is merged, hiding its L2 latency.
-                int src = __ffs(pend) - 1;
-                uint64_t* lst = list_of(__shfl_sync(0xffffffffu, row, src));
-                uint64_t lk_next = lst[lane];
+                // Pending rows one at a time: the row's 64 values are
+                // transposed across the warp, and its keys below the row's
+                // threshold are appended to its list unsorted (one store).
+                // Only a list whose appended keys would overflow is merged.
                 while (pend) {
+                    const int cur = __ffs(pend) - 1;
                     pend &= pend - 1;
-                    const int cur = src;
-                    uint64_t* cur_lst = lst;
-                    uint64_t lk = lk_next;
-                    if (pend) {
-                        src = __ffs(pend) - 1;
-                        lst = list_of(__shfl_sync(0xffffffffu, row, src));
-                        lk_next = lst[lane];
-                    }
-                    // transpose through the warp's scratch: lane j takes
-                    // columns j and 32 + j of the source row
+                    // lane j takes columns j and 32 + j of the source row
                     if (lane == cur) {
 #pragma unroll
                         for (int j = 0; j < 16; ++j)
@@ -540,42 +565,40 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                     const float v0 = ld_shared_f32(scratch + 4 * lane);
                     const float v1 = ld_shared_f32(scratch + 4 * (32 + lane));
                     __syncwarp();
+                    uint64_t* lst = list_of(__shfl_sync(0xffffffffu, row, cur));
                     float stau = __shfl_sync(0xffffffffu, tau, cur);
+                    int sheld = __shfl_sync(0xffffffffu, held, cur);
 #pragma unroll
                     for (int ch = 0; ch < 2; ++ch) {
                         const float mine = ch == 0 ? v0 : v1;
-                        const bool qual = mine < stau && lane + ch * 32 < valid_cols;
-                        unsigned q = __ballot_sync(0xffffffffu, qual);
-                        if (__popc(q) >= kBulkMergeMin) {
-                            const uint64_t key =
-                                qual ? (static_cast<uint64_t>(f2o(mine)) << 32) |
-                                           static_cast<uint32_t>(colh + ch * 32 + lane)
-                                     : ~0ull;
-                            lk = warp_merge_keys(lk, key);
-                            const uint64_t last = __shfl_sync(0xffffffffu, lk, S - 1);
-                            stau = last == ~0ull ? INFINITY : o2f(static_cast<uint32_t>(last >> 32));
-                            q = 0;
+                        const bool in_range = lane + ch * 32 < valid_cols;
+                        unsigned q = __ballot_sync(0xffffffffu, in_range && mine < stau);
+                        if (q == 0) continue;
+                        if (sheld + __popc(q) > S) {
+                            stau = merge_held(lst, sheld);
+                            sheld = 0;
+                            q = __ballot_sync(0xffffffffu, in_range && mine < stau);
                         }
-                        while (q) {
-                            const int b = __ffs(q) - 1;
-                            q &= q - 1;
-                            const float val = __shfl_sync(0xffffffffu, mine, b);
-                            if (!(val < stau)) continue;
-                            const uint64_t key = (static_cast<uint64_t>(f2o(val)) << 32) |
-                                                 static_cast<uint32_t>(colh + ch * 32 + b);
-                            const int pos = __popc(__ballot_sync(0xffffffffu, lk < key));
-                            const uint64_t up = __shfl_up_sync(0xffffffffu, lk, 1);
-                            if (lane > pos)
-                                lk = up;
-                            else if (lane == pos)
-                                lk = key;
-                            const uint64_t last = __shfl_sync(0xffffffffu, lk, S - 1);
-                            stau = last == ~0ull ? INFINITY : o2f(static_cast<uint32_t>(last >> 32));
-                        }
+                        if ((q >> lane) & 1u)
+                            lst[S + sheld + __popc(q & ((1u << lane) - 1u))] =
+                                (static_cast<uint64_t>(f2o(mine)) << 32) |
+                                static_cast<uint32_t>(colh + ch * 32 + lane);
+                        sheld += __popc(q);
                     }
-                    cur_lst[lane] = lk;
-                    if (lane == cur) tau = stau;
+                    if (lane == cur) {
+                        tau = stau;
+                        held = sheld;
+                    }
                 }
+            }
+            if (!ok) break;
+            // every list of the unit ends sorted, with nothing held
+            unsigned rest = __ballot_sync(0xffffffffu, held > 0);
+            while (rest) {
+                const int cur = __ffs(rest) - 1;
+                rest &= rest - 1;
+                merge_held(list_of(__shfl_sync(0xffffffffu, row, cur)),
+                           __shfl_sync(0xffffffffu, held, cur));
             }
         }
     }
@@ -807,13 +830,13 @@ __global__ void rerank_kernel(RerankArgs a) {
     if (row >= a.n_q) return;
     const int k = a.k, d = a.d;
     const int64_t orow = a.omap != nullptr ? a.omap[row] : row;
-    const uint64_t* rl = a.lists + row * a.n_lists * S;
+    const uint64_t* rl = a.lists + row * a.n_lists * LS;
     // The smallest bound a candidate missing from every list can have: a full
     // list left out only candidates with L >= its largest entry, a list that
     // is not full kept every candidate of its range.
     double bound = INFINITY;
     for (int h = 0; h < a.n_lists; ++h) {
-        const uint64_t lk = rl[h * S + lane];
+        const uint64_t lk = rl[h * LS + lane];
         const bool valid = lk != ~0ull;
         float lmax = valid ? o2f(static_cast<uint32_t>(lk >> 32)) : -INFINITY;
 #pragma unroll
@@ -833,7 +856,7 @@ __global__ void rerank_kernel(RerankArgs a) {
     float topu = INFINITY, topu_hi = INFINITY;
     const bool wide = k > 32;
     for (int h = 0; h < a.n_lists; ++h) {
-        const uint64_t lk = rl[h * S + lane];
+        const uint64_t lk = rl[h * LS + lane];
         const float l0 = o2f(static_cast<uint32_t>(__shfl_sync(0xffffffffu, lk, 0) >> 32));
         double U = INFINITY;
         if (lk != ~0ull) {
@@ -863,7 +886,7 @@ __global__ void rerank_kernel(RerankArgs a) {
     const float qn = a.cosine ? __fsqrt_rn(a.qsq[row]) : 0.0f;
     uint64_t top = ~0ull, top_hi = ~0ull;
     for (int h = 0; h < a.n_lists; ++h) {
-        const uint64_t lk = rl[h * S + lane];
+        const uint64_t lk = rl[h * LS + lane];
         const bool take = lk != ~0ull && o2f(static_cast<uint32_t>(lk >> 32)) <= T;
         if (__ballot_sync(0xffffffffu, take) == 0) continue;
         uint64_t key = ~0ull;
@@ -1177,6 +1200,14 @@ void launch_max_sq(const float* sq, int64_t n, unsigned* out, cudaStream_t s) {
     UMAPB_LAUNCH_CHECK();
 }
 
+// Empties `count` lists: their S sorted slots become ~0 (the appended slots
+// are only read below the count a list holds).
+void clear_lists(uint64_t* lists, size_t count, cudaStream_t s) {
+    if (count == 0) return;
+    UMAPB_CUDA(cudaMemset2DAsync(lists, LS * sizeof(uint64_t), 0xFF, S * sizeof(uint64_t), count,
+                                 s));
+}
+
 void launch_rerank(const RerankArgs& ra, cudaStream_t s) {
     rerank_kernel<<<static_cast<unsigned>(ceil_div(ra.n_q * 32, 256)), 256, 0, s>>>(ra);
     UMAPB_LAUNCH_CHECK();
@@ -1260,8 +1291,8 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     launch_prep(Q, qsq.get(), n_q, d, g, sc.get(), bd, cosine, true, A.get(), s);
     launch_prep(R, rsq_p, n_r, d, g, sc.get(), bd, cosine, false, B.get(), s);
     const int n_lists = sh.lists() * a.n_split;
-    DevBuf<uint64_t> lists(static_cast<size_t>(n_q) * n_lists * S, s);
-    UMAPB_CUDA(cudaMemsetAsync(lists.get(), 0xFF, lists.bytes(), s));
+    DevBuf<uint64_t> lists(static_cast<size_t>(n_q) * n_lists * LS, s);
+    clear_lists(lists.get(), static_cast<size_t>(n_q) * n_lists, s);
     const CUtensorMap ma = make_f16_map(A.get(), n_q, g.kst, BM);
     const CUtensorMap mb = make_f16_map(B.get(), n_r, g.kst, sh.bn);
     a.lists = lists.get();
@@ -1332,8 +1363,8 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
         launch_prep(Q2.get(), q2sq.get(), fb, d, g2, sc.get(), bd2, cosine, true, A2.get(), s);
         TcArgs a2 = plan(fb, n_r, g2, sh2, true, 2);
         const int n_lists2 = sh2.lists() * a2.n_split;
-        DevBuf<uint64_t> lists2(static_cast<size_t>(fb) * n_lists2 * S, s);
-        UMAPB_CUDA(cudaMemsetAsync(lists2.get(), 0xFF, lists2.bytes(), s));
+        DevBuf<uint64_t> lists2(static_cast<size_t>(fb) * n_lists2 * LS, s);
+        clear_lists(lists2.get(), static_cast<size_t>(fb) * n_lists2, s);
         const CUtensorMap ma2 = make_f16_map(A2.get(), fb, g2.kst, BM);
         a2.lists = lists2.get();
         a2.err = flags.get() + 2;
@@ -1399,7 +1430,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
 // rows, which needs no scratch.
 namespace umapb {
 namespace {
-constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(64) << 20;
+constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(128) << 20;
 }  // namespace
 }  // namespace umapb
 
@@ -1433,7 +1464,7 @@ size_t noalloc_need(int64_t n, int d) {
     const Geom g = geom(d);
     const Shape sh = shape_for(g.kb);
     return round256(rows * 4) + 2 * round256(rows * g.kst * 2) +
-           round256(rows * sh.lists() * S * 8) + round256(8 * sizeof(int)) +
+           round256(rows * sh.lists() * LS * 8) + round256(8 * sizeof(int)) +
            round256(sizeof(ScaleInfo)) + round256(rows * 4);
 }
 
@@ -1467,7 +1498,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     __half* A = reinterpret_cast<__half*>(carve(static_cast<size_t>(n) * g.kst * 2));
     __half* B = reinterpret_cast<__half*>(carve(static_cast<size_t>(n) * g.kst * 2));
     uint64_t* lists =
-        reinterpret_cast<uint64_t*>(carve(static_cast<size_t>(n) * sh.lists() * S * 8));
+        reinterpret_cast<uint64_t*>(carve(static_cast<size_t>(n) * sh.lists() * LS * 8));
     // [0] kernel error, [1] rows to recompute, [4] largest squared norm (bits)
     int* flags = reinterpret_cast<int*>(carve(8 * sizeof(int)));
     ScaleInfo* sc = reinterpret_cast<ScaleInfo*>(carve(sizeof(ScaleInfo)));
@@ -1475,7 +1506,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
 
     // every call starts from cleared shortlists and flags (the array keeps
     // the previous call's contents)
-    UMAPB_CUDA(cudaMemsetAsync(lists, 0xFF, static_cast<size_t>(n) * sh.lists() * S * 8, s));
+    clear_lists(lists, static_cast<size_t>(n) * sh.lists(), s);
     UMAPB_CUDA(cudaMemsetAsync(flags, 0, 8 * sizeof(int), s));
     row_norms(X, n, d, nullptr, sq, s);
     unsigned* max_bits = reinterpret_cast<unsigned*>(flags + 4);

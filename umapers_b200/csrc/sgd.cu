@@ -55,13 +55,18 @@ __device__ __forceinline__ float pow_pos(float x, float y) {
     return exp2f(__fmul_rn(y, log2f(x)));
 }
 
+// `row_max`/`heads` (nullable): the largest weight of each edge's head row
+// replaces max_w (row-local transform graphs).
 __global__ void epochs_per_sample_kernel(const float* __restrict__ w, int64_t m, float max_w,
                                          float n_epochs_f, float neg_rate_f,
                                          float* __restrict__ eps, float* __restrict__ next,
-                                         float* __restrict__ next_neg) {
+                                         float* __restrict__ next_neg,
+                                         const float* __restrict__ row_max = nullptr,
+                                         const int32_t* __restrict__ heads = nullptr) {
     // make_epochs_per_sample (lib.rs:4937-4960)
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= m) return;
+    if (row_max != nullptr) max_w = fmaxf(row_max[heads[e]], 1e-12f);
     const float ns = __fmul_rn(n_epochs_f, __fdiv_rn(w[e], max_w));
     const float v = ns > 0.0f ? __fdiv_rn(n_epochs_f, ns) : INFINITY;
     eps[e] = v;
@@ -1469,9 +1474,11 @@ void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_
     const float nef = static_cast<float>(n_epochs);
     const float nrf = static_cast<float>(neg_rate);
     if (m > 0) {
-        const float mx = std::max(max_weight(g.weights.get(), m, s), 1e-12f);
+        const bool local = g.row_max.get() != nullptr;
+        const float mx = local ? 1.0f : std::max(max_weight(g.weights.get(), m, s), 1e-12f);
         epochs_per_sample_kernel<<<static_cast<unsigned>(ceil_div(m, 256)), 256, 0, s>>>(
-            g.weights.get(), m, mx, nef, nrf, eps.get(), next.get(), next_neg.get());
+            g.weights.get(), m, mx, nef, nrf, eps.get(), next.get(), next_neg.get(),
+            local ? g.row_max.get() : nullptr, local ? g.heads.get() : nullptr);
         UMAPB_LAUNCH_CHECK();
     }
     TransformArgs p{};
