@@ -159,12 +159,23 @@ __device__ __forceinline__ float min3f(float a, float b, float c) {
     return r;
 }
 
-// Minimum of 32 FP32 values held as bit patterns (16 three-input mins).
-__device__ __forceinline__ float min32(const uint32_t* r) {
-    float m = min3f(__uint_as_float(r[0]), __uint_as_float(r[1]), __uint_as_float(r[2]));
+// Minimum of the 64 FP32 values (bit patterns) of r[0] and r[1]: a tree of
+// three-input mins, five levels deep (64 -> 22 -> 8 -> 3 -> 1).
+__device__ __forceinline__ float min64(const uint32_t (&r)[2][32]) {
+    float a[22];
 #pragma unroll
-    for (int j = 3; j < 31; j += 2) m = min3f(m, __uint_as_float(r[j]), __uint_as_float(r[j + 1]));
-    return fminf(m, __uint_as_float(r[31]));
+    for (int i = 0; i < 21; ++i) {
+        const int j = 3 * i;
+        a[i] = min3f(__uint_as_float(r[j >> 5][j & 31]), __uint_as_float(r[(j + 1) >> 5][(j + 1) & 31]),
+                     __uint_as_float(r[(j + 2) >> 5][(j + 2) & 31]));
+    }
+    a[21] = __uint_as_float(r[1][31]);
+    float b[8];
+#pragma unroll
+    for (int i = 0; i < 7; ++i) b[i] = min3f(a[3 * i], a[3 * i + 1], a[3 * i + 2]);
+    b[7] = a[21];
+    const float c0 = min3f(b[0], b[1], b[2]), c1 = min3f(b[3], b[4], b[5]), c2 = fminf(b[6], b[7]);
+    return min3f(c0, c1, c2);
 }
 
 // Bitonic sort of one value per lane, ascending with the lane index.
@@ -330,9 +341,10 @@ constexpr int epi_warps() { return 4 * MT * (BN / 64); }
 template <int MT, int BN>
 constexpr int tc_threads() { return 64 + 32 * epi_warps<MT, BN>(); }
 
-// 112 registers a thread: 576 threads x 112 fit the SM's 65,536 without spills.
+// The register file is split among the SM's four schedulers: with 18 warps
+// two of them hold five warps, which caps a thread at 96 registers.
 template <int MT, int BN, bool SA>
-__global__ void __maxnreg__(112)
+__global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
     tc_knn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                   TcArgs p) {
     static_assert(MT * BN <= 256 && (BN == 128 || BN == 256), "at most 512 TMEM columns");
@@ -541,8 +553,7 @@ __global__ void __maxnreg__(112)
                 fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
-                const float m0 = min32(r[0]), m1 = min32(r[1]);
-                unsigned pend = __ballot_sync(0xffffffffu, row_ok && fminf(m0, m1) < tau);
+                unsigned pend = __ballot_sync(0xffffffffu, row_ok && min64(r) < tau);
                 if (pend == 0) continue;
                 const int32_t colh = tile_at(c, w) * BN + cq * 64;
                 const int32_t valid_cols = static_cast<int32_t>(p.n_r - colh);
