@@ -129,6 +129,7 @@ def test_gate_sends_out_of_distribution_rows_to_plain(trained):
     out_m, flags_m = m._core.transform_surrogate(mixed, use_fallback=True)
     flags_m = flags_m.astype(bool)
     both = flags & flags_m
+    both[1::2] = False  # other rows there
     assert both[0::2].mean() > 0.99
     np.testing.assert_array_equal(out_m[both], out[both])
     plain = m.transform(far)
