@@ -337,8 +337,8 @@ int32_t umapb_knn_exact(const float* data, int64_t n_rows, int64_t n_cols, int64
  * reference.  `data` (n_rows x n_cols f32), `indices` (n_rows x k int32) and
  * `dists` (n_rows x k f32) are device pointers; `stream` is a cudaStream_t
  * (NULL = legacy default stream).  Results equal umapb_knn_exact's.
- * Scratch comes from one static device array of 64 MiB that every GPU loading
- * the library holds until exit: about 49,000 rows at 64 columns; larger
+ * Scratch comes from one static device array of 160 MiB that every GPU
+ * loading the library holds until exit: about 49,000 rows at 64 columns; larger
  * inputs are rejected with UMAPB_ERR_INVALID_PARAMETER naming the limit.  No
  * cudaMalloc/cudaFree or allocating library routine is called.  The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress),

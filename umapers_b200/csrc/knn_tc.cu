@@ -23,16 +23,18 @@
 //    keeps MT query tiles of 128 rows of A resident in shared memory, streams
 //    BN-row candidate tiles of B through a TMA ring (SWIZZLE_128B, no
 //    multicast), and one thread issues 128 x BN x 16 tcgen05.mma (kind::f16,
-//    FP16 in, FP32 accumulate) into double-buffered TMEM accumulators.  One
-//    epilogue warp per (TMEM lane quarter, query tile, 64-column group) owns
-//    32 rows x 64 columns of the accumulator: it reads them with tcgen05.ld
-//    and keeps, per (row, 64-column group), the S = 32 smallest (L, index)
-//    keys in a global list.  A per-list threshold skips a row's 64 columns
-//    with one vote in the common case; otherwise the row's values are
-//    transposed across the warp through a shared-memory scratch and its
-//    keys below the threshold are appended behind the list's sorted keys in
-//    one store.  A list is merged (bitonic, one key per lane) only when its
-//    appended keys would overflow S, which also lowers its threshold.  When the
+//    FP16 in, FP32 accumulate) into double-buffered TMEM accumulators.  A
+//    last k-block of 16 or 32 columns is loaded as a narrow block (32- or
+//    64-byte rows, SWIZZLE_32B / 64B) in the same ring stage as the block
+//    before it.  One epilogue warp per (TMEM lane quarter, query tile,
+//    64-column group) owns 32 rows x 64 columns of the accumulator: it reads
+//    them with tcgen05.ld and keeps, per (row, 64-column group), the S = 32
+//    smallest (L, index) keys in a global list.  A per-list threshold skips a
+//    row's 64 columns with one vote in the common case; otherwise every
+//    pending row of the warp is served at once, one per lane: the lane
+//    appends its row's keys below the threshold behind the list's sorted
+//    keys.  A list is merged (bitonic, one key per lane) only when its
+//    appended keys would overflow, which also lowers its threshold.  When the
 //    query tiles are fewer than the SMs, the candidate tiles are split too
 //    (one wave of units), with lists per split.  A self kNN over at least one
 //    wave of query groups first regroups its rows by nearest pivot ("cell
@@ -75,11 +77,11 @@ constexpr int BM = 128;     // query rows per tile (UMMA M)
 constexpr int BK = kBK;     // FP16 columns per k-block (one 128-byte swizzle row)
 constexpr int UK = kUK;     // K of one tcgen05.mma kind::f16
 constexpr int S = 32;       // shortlist length per list
-constexpr int LS = 2 * S;   // slots per list: S sorted keys, then up to S appended
+constexpr int HC = 64;       // keys a list holds appended between merges
+constexpr int LS = S + HC;  // slots per list: S sorted keys, then up to HC appended
 constexpr int kMaxK = 62;   // neighbours per row on the tensor path (64-entry re-rank lists)
 constexpr int kATileBytes = BM * BK * 2;  // 16 KiB: one query tile's k-block
 constexpr int kBarBytes = 256;            // mbarriers, TMEM address, abort flag
-constexpr int kScratchBytes = 256;        // per epilogue warp: one row's 64 values
 constexpr int kNormCols = 6;              // 3 + 3 FP16 columns of the folded row terms
 constexpr int kMaxStages = 8;
 constexpr size_t kSmemLimit = 227 * 1024;
@@ -254,21 +256,31 @@ __device__ __forceinline__ T rank_of(T lo, T hi, int r) {
 // key by key (about 6 sequential insertions cost as much).
 constexpr int kBulkMergeMin = 6;
 
-// A list occupies LS = 2S slots: its S smallest keys so far, sorted
-// ascending, then up to S keys appended unsorted since the last merge (every
-// one below the threshold of that merge).  Merges the `held` appended keys
-// into the sorted ones (one key per lane) and returns the new S-th smallest
-// L, or +inf while the list holds fewer than S keys.
+// A list occupies LS slots: its S smallest keys so far, sorted ascending
+// (order-mapped L << 32 | index), then up to HC keys appended unsorted since
+// the last merge, each below that merge's threshold and stored with L as raw
+// FP32 bits (the epilogue appends without converting).
+__device__ __forceinline__ uint64_t held_key(uint64_t raw) {
+    return (static_cast<uint64_t>(f2o(__uint_as_float(static_cast<uint32_t>(raw >> 32)))) << 32) |
+           static_cast<uint32_t>(raw);
+}
+
+// Merges the `held` appended keys (at most HC) into the sorted ones, one key
+// per lane, and returns the new S-th smallest L, or +inf while the list holds
+// fewer than S keys.
 __device__ __forceinline__ float merge_held(uint64_t* lst, int held) {
     const int lane = threadIdx.x & 31;
     __syncwarp();  // the appended keys were stored by other lanes
     uint64_t lk = lst[lane];
-    const uint64_t hk = lane < held ? lst[S + lane] : ~0ull;
-    if (held >= kBulkMergeMin) {
-        lk = warp_merge_keys(lk, hk);
+    const uint64_t h0 = lane < held ? held_key(lst[S + lane]) : ~0ull;
+    const uint64_t h1 = lane + 32 < held ? held_key(lst[S + 32 + lane]) : ~0ull;
+    if (held > 32) lk = warp_merge_keys(lk, h1);
+    const int n0 = min(held, 32);
+    if (n0 >= kBulkMergeMin) {
+        lk = warp_merge_keys(lk, h0);
     } else {
-        for (int b = 0; b < held; ++b) {
-            const uint64_t key = __shfl_sync(0xffffffffu, hk, b);
+        for (int b = 0; b < n0; ++b) {
+            const uint64_t key = __shfl_sync(0xffffffffu, h0, b);
             const int pos = __popc(__ballot_sync(0xffffffffu, lk < key));
             const uint64_t up = __shfl_up_sync(0xffffffffu, lk, 1);
             if (lane > pos)
@@ -283,6 +295,22 @@ __device__ __forceinline__ float merge_held(uint64_t* lst, int held) {
     return last == ~0ull ? INFINITY : o2f(static_cast<uint32_t>(last >> 32));
 }
 
+// Appends, for one lane's row, its values below t (columns below lim) as
+// held keys at dst[h...]; returns the new count.
+template <bool kAll>
+__device__ __forceinline__ int append_row(const uint32_t (&r)[2][32], float t, int lim,
+                                          int32_t col0, uint64_t* dst, int h) {
+#pragma unroll
+    for (int j = 0; j < 64; ++j) {
+        if (__uint_as_float(r[j >> 5][j & 31]) < t && (kAll || j < lim)) {
+            dst[h] = (static_cast<uint64_t>(r[j >> 5][j & 31]) << 32) |
+                     static_cast<uint32_t>(col0 + j);
+            ++h;
+        }
+    }
+    return h;
+}
+
 // CTAs begin their candidate range at staggered tiles (16 groups, 2 tiles
 // apart) so they do not all request the same tile at once.  The shortlist
 // certificate does not depend on the visiting order.
@@ -293,6 +321,8 @@ struct TcArgs {
     int64_t n_r;
     int kb;               // k-blocks of 64 columns
     int tail;             // k-steps issued in the last k-block (1..4)
+    int ntail;            // 16 or 32: the last k-block is a narrow block of that many
+                          // columns, loaded with the last full one; 0: 64-column blocks only
     int st;               // stages of the candidate ring
     int64_t n_units;      // work units: (group of MT query tiles, candidate split)
     int n_split;          // candidate splits per group (1 unless query tiles are few)
@@ -343,25 +373,35 @@ constexpr int tc_threads() { return 64 + 32 * epi_warps<MT, BN>(); }
 
 // The register file is split among the SM's four schedulers: with 18 warps
 // two of them hold five warps, which caps a thread at 96 registers.
+// With a narrow last k-block (p.ntail, resident query tiles only) a tile
+// takes KB - 1 ring stages; the last holds the final 64-column block and the
+// narrow one (32- or 64-byte rows at the matching swizzle), so a 16-column
+// tail costs 8 KiB of candidate loads per 256-row tile instead of 32.
 template <int MT, int BN, bool SA>
 __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
     tc_knn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                  TcArgs p) {
+                  const __grid_constant__ CUtensorMap tmAt,
+                  const __grid_constant__ CUtensorMap tmBt, TcArgs p) {
     static_assert(MT * BN <= 256 && (BN == 128 || BN == 256), "at most 512 TMEM columns");
     constexpr int kEpiWarps = epi_warps<MT, BN>();
     constexpr int kBTileBytes = BN * BK * 2;
-    constexpr int kStageBytes = SA ? MT * kATileBytes + kBTileBytes : kBTileBytes;
     constexpr int kStageB = SA ? MT * kATileBytes : 0;  // candidate tile within a stage
     constexpr uint32_t kIdesc = idesc_f16(BM, BN);
     constexpr int GPT = BN / 64;                   // lists per candidate tile
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
-    const int KB = p.kb, TAIL = p.tail, ST = p.st;
-    const int a_bytes = SA ? 0 : MT * KB * kATileBytes;  // resident query tiles
+    const int KB = p.kb, ST = p.st;
+    const int NT = SA ? 0 : p.ntail;                  // narrow tail columns (0: none)
+    const int KBM = NT ? KB - 1 : KB;                 // 64-column k-blocks (one stage each)
+    const int TAIL = NT ? NT / UK : p.tail;           // k-steps of the last (or narrow) block
+    const int ta_bytes = BM * NT * 2, tb_bytes = BN * NT * 2;
+    const int stage_bytes = SA ? MT * kATileBytes + kBTileBytes : kBTileBytes + tb_bytes;
+    const int a_bytes = SA ? 0 : MT * (KBM * kATileBytes + ta_bytes);  // resident query tiles
     const uint32_t sA = smem_u32(smem);
+    const uint32_t sAt = sA + MT * KBM * kATileBytes;  // narrow blocks of the query tiles
     const uint32_t sB = sA + a_bytes;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + a_bytes + ST * kStageBytes);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + a_bytes + ST * stage_bytes);
     const uint32_t b_full = smem_u32(bars);
     const uint32_t b_empty = b_full + 8 * ST;
     const uint32_t b_tfull = b_empty + 8 * ST;
@@ -418,28 +458,35 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                         fail(1);
                         break;
                     }
-                    mbar_expect_tx(b_afull, MT * KB * kATileBytes);
-                    for (int mt = 0; mt < MT; ++mt)
-                        for (int kb = 0; kb < KB; ++kb)
-                            tma_load_2d(sA + (mt * KB + kb) * kATileBytes, &tmA, b_afull, kb * BK,
-                                        static_cast<int>((w.group * MT + mt) * BM));
+                    mbar_expect_tx(b_afull, a_bytes);
+                    for (int mt = 0; mt < MT; ++mt) {
+                        const int ya = static_cast<int>((w.group * MT + mt) * BM);
+                        for (int kb = 0; kb < KBM; ++kb)
+                            tma_load_2d(sA + (mt * KBM + kb) * kATileBytes, &tmA, b_afull, kb * BK,
+                                        ya);
+                        if (NT) tma_load_2d(sAt + mt * ta_bytes, &tmAt, b_afull, KBM * BK, ya);
+                    }
                 }
                 bool ok = true;
                 for (int32_t c = 0; c < w.len && ok; ++c) {
                     const int ty = static_cast<int>(tile_at(c, w) * BN);
-                    for (int kb = 0; kb < KB; ++kb) {
+                    for (int kb = 0; kb < KBM; ++kb) {
                         if (!mbar_wait(b_empty + 8 * stage, phase ^ 1, abort_flag)) {
                             fail(2);
                             ok = false;
                             break;
                         }
-                        const uint32_t sbase = sB + stage * kStageBytes;
-                        mbar_expect_tx(b_full + 8 * stage, kStageBytes);
+                        const uint32_t sbase = sB + stage * stage_bytes;
+                        const bool narrow = NT && kb + 1 == KBM;
+                        mbar_expect_tx(b_full + 8 * stage,
+                                       SA ? stage_bytes : kBTileBytes + (narrow ? tb_bytes : 0));
                         if (SA)
                             for (int mt = 0; mt < MT; ++mt)
                                 tma_load_2d(sbase + mt * kATileBytes, &tmA, b_full + 8 * stage,
                                             kb * BK, static_cast<int>((w.group * MT + mt) * BM));
                         tma_load_2d(sbase + kStageB, &tmB, b_full + 8 * stage, kb * BK, ty);
+                        if (narrow)
+                            tma_load_2d(sbase + kBTileBytes, &tmBt, b_full + 8 * stage, KBM * BK, ty);
                         if (++stage == ST) {
                             stage = 0;
                             phase ^= 1;
@@ -476,15 +523,15 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                     }
                     fence_after();
                     const uint32_t dcol = tmem_base + buf * (MT * BN);
-                    for (int kb = 0; kb < KB; ++kb) {
+                    for (int kb = 0; kb < KBM; ++kb) {
                         if (!mbar_wait(b_full + 8 * stage, phase, abort_flag)) {
                             fail(5);
                             ok = false;
                             break;
                         }
                         fence_after();
-                        const int steps = kb + 1 < KB ? BK / UK : TAIL;
-                        const uint32_t sbase = sB + stage * kStageBytes;
+                        const int steps = NT || kb + 1 < KB ? BK / UK : TAIL;
+                        const uint32_t sbase = sB + stage * stage_bytes;
                         const uint64_t db0 = desc_sw128(sbase + kStageB);
 #pragma unroll
                         for (int ks = 0; ks < BK / UK; ++ks) {
@@ -493,10 +540,24 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                                 for (int mt = 0; mt < MT; ++mt) {
                                     const uint64_t da =
                                         (SA ? desc_sw128(sbase + mt * kATileBytes)
-                                            : desc_sw128(sA + (mt * KB + kb) * kATileBytes)) +
+                                            : desc_sw128(sA + (mt * KBM + kb) * kATileBytes)) +
                                         2 * ks;
                                     umma_bf16(dcol + mt * BN, da, db0 + 2 * ks, kIdesc,
                                               (kb | ks) != 0 ? 1u : 0u);
+                                }
+                            }
+                        }
+                        if (NT && kb + 1 == KBM) {
+                            // the narrow block: rows of 2 * NT bytes, k-steps 32 bytes apart
+                            const uint64_t dbt = desc_narrow(sbase + kBTileBytes, 2 * NT);
+#pragma unroll
+                            for (int ks = 0; ks < 2; ++ks) {
+                                if (ks < TAIL) {
+#pragma unroll
+                                    for (int mt = 0; mt < MT; ++mt)
+                                        umma_bf16(dcol + mt * BN,
+                                                  desc_narrow(sAt + mt * ta_bytes, 2 * NT) + 2 * ks,
+                                                  dbt + 2 * ks, kIdesc, 1u);
                                 }
                             }
                         }
@@ -522,7 +583,6 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
         const int slot = (warp - 2) >> 2;
         const int mt = slot / GPT;
         const int cq = slot % GPT;
-        const uint32_t scratch = b_full + kBarBytes + (warp - 2) * kScratchBytes;
         uint64_t cg = 0;
         bool ok = true;
         for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x) {
@@ -557,50 +617,34 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                 if (pend == 0) continue;
                 const int32_t colh = tile_at(c, w) * BN + cq * 64;
                 const int32_t valid_cols = static_cast<int32_t>(p.n_r - colh);
-                // Pending rows one at a time: the row's 64 values are
-                // transposed across the warp, and its keys below the row's
-                // threshold are appended to its list unsorted (one store).
-                // Only a list whose appended keys would overflow is merged.
-                while (pend) {
-                    const int cur = __ffs(pend) - 1;
-                    pend &= pend - 1;
-                    // lane j takes columns j and 32 + j of the source row
-                    if (lane == cur) {
+                // Every pending row at once, one per lane: count the row's
+                // values below its threshold, merge the lists whose appended
+                // keys would overflow (one list at a time, across the warp),
+                // then append each row's keys behind its sorted ones.
+                const bool mine = (pend >> lane) & 1u;
+                const bool all = valid_cols >= 64;
+                float t = mine ? tau : -INFINITY;
+                int cnt = 0;
 #pragma unroll
-                        for (int j = 0; j < 16; ++j)
-                            st_shared_v4(scratch + 16 * j, r[j >> 3][(j & 7) * 4],
-                                         r[j >> 3][(j & 7) * 4 + 1], r[j >> 3][(j & 7) * 4 + 2],
-                                         r[j >> 3][(j & 7) * 4 + 3]);
-                    }
-                    __syncwarp();
-                    const float v0 = ld_shared_f32(scratch + 4 * lane);
-                    const float v1 = ld_shared_f32(scratch + 4 * (32 + lane));
-                    __syncwarp();
-                    uint64_t* lst = list_of(__shfl_sync(0xffffffffu, row, cur));
-                    float stau = __shfl_sync(0xffffffffu, tau, cur);
-                    int sheld = __shfl_sync(0xffffffffu, held, cur);
-#pragma unroll
-                    for (int ch = 0; ch < 2; ++ch) {
-                        const float mine = ch == 0 ? v0 : v1;
-                        const bool in_range = lane + ch * 32 < valid_cols;
-                        unsigned q = __ballot_sync(0xffffffffu, in_range && mine < stau);
-                        if (q == 0) continue;
-                        if (sheld + __popc(q) > S) {
-                            stau = merge_held(lst, sheld);
-                            sheld = 0;
-                            q = __ballot_sync(0xffffffffu, in_range && mine < stau);
-                        }
-                        if ((q >> lane) & 1u)
-                            lst[S + sheld + __popc(q & ((1u << lane) - 1u))] =
-                                (static_cast<uint64_t>(f2o(mine)) << 32) |
-                                static_cast<uint32_t>(colh + ch * 32 + lane);
-                        sheld += __popc(q);
-                    }
+                for (int j = 0; j < 64; ++j)
+                    cnt += (__uint_as_float(r[j >> 5][j & 31]) < t && (all || j < valid_cols))
+                               ? 1
+                               : 0;
+                unsigned over = __ballot_sync(0xffffffffu, held + cnt > HC);
+                while (over) {
+                    const int cur = __ffs(over) - 1;
+                    over &= over - 1;
+                    const float nt = merge_held(list_of(__shfl_sync(0xffffffffu, row, cur)),
+                                                __shfl_sync(0xffffffffu, held, cur));
                     if (lane == cur) {
-                        tau = stau;
-                        held = sheld;
+                        tau = nt;
+                        held = 0;
                     }
                 }
+                t = mine ? tau : -INFINITY;
+                uint64_t* dst = list_of(row) + S;
+                held = all ? append_row<true>(r, t, 64, colh, dst, held)
+                           : append_row<false>(r, t, valid_cols, colh, dst, held);
             }
             if (!ok) break;
             // every list of the unit ends sorted, with nothing held
@@ -941,41 +985,64 @@ __global__ void gather_rows_kernel(const float* __restrict__ X, const int32_t* _
 }
 
 // --------------------------------------------------------------- host ----
-// Kernel shape: MT query tiles x BN candidate rows, ring stages.
+// Kernel shape: MT query tiles x BN candidate rows, ring stages, and the
+// width of a narrow last k-block (0: none).
 struct Shape {
     int mt = 0, bn = 0, st = 0;
     bool stream = false;  // query tile streamed through the ring with the candidates
     size_t smem = 0;
+    int ntail = 0;
     int lists() const { return bn / 64; }  // lists per row and candidate split
 };
 
-size_t smem_bytes(int mt, int bn, int kb, int st, bool stream) {
-    // tiles + 1 KiB alignment slack + barriers/flags + epilogue scratch
-    const size_t a = stream ? 0 : static_cast<size_t>(mt) * kb * kATileBytes;
-    const size_t stage = static_cast<size_t>(bn) * BK * 2 + (stream ? mt * kATileBytes : 0);
-    return a + st * stage + 1024 + kBarBytes +
-           static_cast<size_t>(4 * mt * (bn / 64)) * kScratchBytes;
+// The last k-block is loaded narrow when the operands span at least two
+// k-blocks and it issues one or two k-steps (16 or 32 columns).
+int narrow_cols(const Geom& g) { return g.kb >= 2 && g.tail <= 2 ? g.tail * UK : 0; }
+
+size_t smem_bytes(int mt, int bn, int kb, int st, bool stream, int ntail) {
+    // tiles + 1 KiB alignment slack + barriers/flags
+    const int kbm = ntail ? kb - 1 : kb;
+    const size_t a = stream ? 0
+                            : static_cast<size_t>(mt) *
+                                  (static_cast<size_t>(kbm) * kATileBytes + BM * ntail * 2);
+    const size_t stage = static_cast<size_t>(bn) * BK * 2 + static_cast<size_t>(bn) * ntail * 2 +
+                         (stream ? mt * kATileBytes : 0);
+    return a + st * stage + 1024 + kBarBytes;
 }
 
 // One resident query tile against 256-candidate tiles (four lists per row)
 // while the operands fit with at least three ring stages, else against
 // 128-candidate tiles (two lists per row, eight epilogue warps); rows too
-// wide for a resident tile stream it with 256-candidate tiles.
-Shape shape_for(int kb) {
+// wide for a resident tile stream it with 256-candidate tiles (64-column
+// blocks only).
+Shape shape_for(const Geom& g) {
+    const int kb = g.kb, nt = narrow_cols(g);
     const int cand[2][2] = {{1, 256}, {1, 128}};
     for (const auto& c : cand) {
         int st = kMaxStages;
-        while (st >= 2 && smem_bytes(c[0], c[1], kb, st, false) > kSmemLimit) --st;
+        while (st >= 2 && smem_bytes(c[0], c[1], kb, st, false, nt) > kSmemLimit) --st;
         if (st >= (c[1] == 256 ? 3 : 2))
-            return Shape{c[0], c[1], st, false, smem_bytes(c[0], c[1], kb, st, false)};
+            return Shape{c[0], c[1], st, false, smem_bytes(c[0], c[1], kb, st, false, nt), nt};
     }
     int st = kMaxStages;
-    while (st >= 3 && smem_bytes(1, 256, kb, st, true) > kSmemLimit) --st;
-    return Shape{1, 256, st, true, smem_bytes(1, 256, kb, st, true)};
+    while (st >= 3 && smem_bytes(1, 256, kb, st, true, 0) > kSmemLimit) --st;
+    return Shape{1, 256, st, true, smem_bytes(1, 256, kb, st, true, 0), 0};
+}
+
+// The operand maps of one side: 64-column blocks of `rows_box` rows, and the
+// narrow last block when the shape uses one (else a copy of the first).
+struct SideMaps {
+    CUtensorMap full, tail;
+};
+SideMaps side_maps(const __half* X, int64_t n, const Geom& g, const Shape& sh, int rows_box) {
+    SideMaps m;
+    m.full = make_f16_map(X, n, g.kst, rows_box);
+    m.tail = sh.ntail ? make_f16_tail_map(X, n, g.kst, sh.ntail, rows_box) : m.full;
+    return m;
 }
 
 template <int MT, int BN, bool SA>
-void launch_tc_t(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, size_t smem,
+void launch_tc_t(const SideMaps& ma, const SideMaps& mb, const TcArgs& a, size_t smem,
                  cudaStream_t s) {
     auto kern = tc_knn_kernel<MT, BN, SA>;
     UMAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -984,11 +1051,12 @@ void launch_tc_t(const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a, 
     UMAPB_CUDA(cudaGetDevice(&dev));
     UMAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int64_t grid = std::min<int64_t>(a.n_units, sms);
-    kern<<<static_cast<unsigned>(grid), tc_threads<MT, BN>(), smem, s>>>(ma, mb, a);
+    kern<<<static_cast<unsigned>(grid), tc_threads<MT, BN>(), smem, s>>>(ma.full, mb.full,
+                                                                          ma.tail, mb.tail, a);
     UMAPB_LAUNCH_CHECK();
 }
 
-void launch_tc(const Shape& sh, const CUtensorMap& ma, const CUtensorMap& mb, const TcArgs& a,
+void launch_tc(const Shape& sh, const SideMaps& ma, const SideMaps& mb, const TcArgs& a,
                cudaStream_t s) {
     if (sh.stream && sh.mt == 1 && sh.bn == 256)
         launch_tc_t<1, 256, true>(ma, mb, a, sh.smem, s);
@@ -1012,6 +1080,7 @@ TcArgs plan(int64_t n_q, int64_t n_r, const Geom& g, const Shape& sh, bool allow
     a.n_r = n_r;
     a.kb = g.kb;
     a.tail = g.tail;
+    a.ntail = sh.ntail;
     a.st = sh.st;
     a.n_ctiles = ceil_div(n_r, sh.bn);
     const int64_t groups = ceil_div(n_q, static_cast<int64_t>(BM) * sh.mt);
@@ -1249,7 +1318,7 @@ struct EventPair {
 bool knn_tc_supported(int d, int k, int metric) {
     if (metric != UMAPB_METRIC_EUCLIDEAN && metric != UMAPB_METRIC_COSINE) return false;
     if (k < 1 || k > kMaxK || d < 1) return false;
-    if (shape_for(geom(d).kb).st == 0) return false;
+    if (shape_for(geom(d)).st == 0) return false;
     // rows the certificate cannot settle go to the plain kernel, whose tiles
     // bound the width
     if (!knn_plain_supported(d, k)) return false;
@@ -1267,7 +1336,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     const float* const Q0 = Q;  // original rows: later passes read rows of these
     const float* const R0 = R;
     const Geom g = geom(d);
-    const Shape sh = shape_for(g.kb);
+    const Shape sh = shape_for(g);
     const Bound bd = bound_for(d, g, cosine);
     TcArgs a = plan(n_q, n_r, g, sh, true, 1);
     CellOrder co;
@@ -1304,8 +1373,8 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
     const int n_lists = sh.lists() * a.n_split;
     DevBuf<uint64_t> lists(static_cast<size_t>(n_q) * n_lists * LS, s);
     clear_lists(lists.get(), static_cast<size_t>(n_q) * n_lists, s);
-    const CUtensorMap ma = make_f16_map(A.get(), n_q, g.kst, BM);
-    const CUtensorMap mb = make_f16_map(B.get(), n_r, g.kst, sh.bn);
+    const SideMaps ma = side_maps(A.get(), n_q, g, sh, BM);
+    const SideMaps mb = side_maps(B.get(), n_r, g, sh, sh.bn);
     a.lists = lists.get();
     a.err = flags.get();
     EventPair ev;
@@ -1351,19 +1420,19 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
         lists.release();
         A.release();
         Geom g2 = geom(d, 3);
-        Shape sh2 = shape_for(g2.kb);
+        Shape sh2 = shape_for(g2);
         if (sh2.st == 0 || sh2.stream) {
             g2 = g;
             sh2 = sh;
         }
         const Bound bd2 = bound_for(d, g2, cosine);
         DevBuf<__half> B2;
-        CUtensorMap mb2 = mb;
+        SideMaps mb2 = mb;
         if (g2.terms != g.terms) {
             B.release();
             B2.alloc(static_cast<size_t>(n_r) * g2.kst, s);
             launch_prep(R, rsq_p, n_r, d, g2, sc.get(), bd2, cosine, false, B2.get(), s);
-            mb2 = make_f16_map(B2.get(), n_r, g2.kst, sh2.bn);
+            mb2 = side_maps(B2.get(), n_r, g2, sh2, sh2.bn);
         }
         DevBuf<float> Q2(static_cast<size_t>(fb) * d, s), q2sq(fb, s);
         gather_rows_kernel<<<static_cast<unsigned>(ceil_div(fb * 32, 256)), 256, 0, s>>>(
@@ -1376,7 +1445,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
         const int n_lists2 = sh2.lists() * a2.n_split;
         DevBuf<uint64_t> lists2(static_cast<size_t>(fb) * n_lists2 * LS, s);
         clear_lists(lists2.get(), static_cast<size_t>(fb) * n_lists2, s);
-        const CUtensorMap ma2 = make_f16_map(A2.get(), fb, g2.kst, BM);
+        const SideMaps ma2 = side_maps(A2.get(), fb, g2, sh2, BM);
         a2.lists = lists2.get();
         a2.err = flags.get() + 2;
         EventPair ev2;
@@ -1441,7 +1510,7 @@ void knn_tc(const float* Q, int64_t n_q, const float* R, int64_t n_r, int d, int
 // rows, which needs no scratch.
 namespace umapb {
 namespace {
-constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(128) << 20;
+constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(160) << 20;
 }  // namespace
 }  // namespace umapb
 
@@ -1473,7 +1542,7 @@ inline size_t round256(size_t b) { return (b + 255) & ~static_cast<size_t>(255);
 size_t noalloc_need(int64_t n, int d) {
     const size_t rows = static_cast<size_t>(n);
     const Geom g = geom(d);
-    const Shape sh = shape_for(g.kb);
+    const Shape sh = shape_for(g);
     return round256(rows * 4) + 2 * round256(rows * g.kst * 2) +
            round256(rows * sh.lists() * LS * 8) + round256(8 * sizeof(int)) +
            round256(sizeof(ScaleInfo)) + round256(rows * 4);
@@ -1496,7 +1565,7 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
                 std::to_string(max_rows) + " rows at " + std::to_string(d) + " columns)");
     }
     const Geom g = geom(d);
-    const Shape sh = shape_for(g.kb);
+    const Shape sh = shape_for(g);
     const Bound bd = bound_for(d, g, false);
     unsigned char* base = noalloc_scratch();
     size_t off = 0;
@@ -1526,8 +1595,8 @@ void knn_noalloc(const float* X, int64_t n, int d, int k, int32_t* out_idx, floa
     UMAPB_LAUNCH_CHECK();
     launch_prep(X, sq, n, d, g, sc, bd, false, true, A, s);
     launch_prep(X, sq, n, d, g, sc, bd, false, false, B, s);
-    const CUtensorMap ma = make_f16_map(A, n, g.kst, BM);
-    const CUtensorMap mb = make_f16_map(B, n, g.kst, sh.bn);
+    const SideMaps ma = side_maps(A, n, g, sh, BM);
+    const SideMaps mb = side_maps(B, n, g, sh, sh.bn);
     TcArgs a = plan(n, n, g, sh, false, 1);  // one split: the scratch holds one set of lists
     a.lists = lists;
     a.err = flags;

@@ -114,6 +114,19 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
     return d;
 }
 
+// K-major operand descriptor of a narrow k-block whose rows are `row_bytes`
+// = 32 or 64 bytes (16 or 32 FP16 columns) with the matching TMA swizzle:
+// SBO = 8 rows, layout type 6 (SWIZZLE_32B) or 4 (SWIZZLE_64B).  The tile's
+// base must be aligned to the swizzle's 256- or 512-byte period.
+__device__ __forceinline__ uint64_t desc_narrow(uint32_t saddr, int row_bytes) {
+    uint64_t d = static_cast<uint64_t>((saddr & 0x3FFFF) >> 4);
+    d |= static_cast<uint64_t>(1) << 16;
+    d |= static_cast<uint64_t>((8 * row_bytes) >> 4) << 32;
+    d |= static_cast<uint64_t>(1) << 46;
+    d |= static_cast<uint64_t>(row_bytes == 32 ? 6 : 4) << 61;
+    return d;
+}
+
 // kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both
 // K-major, shape M x N.
 constexpr uint32_t idesc_bf16(int m, int n) {
@@ -241,6 +254,31 @@ inline CUtensorMap make_f16_map(const void* base, int64_t rows, int64_t cols, in
                                  dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(UMAPB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+// Tensor map over the same FP16 matrix for its last, narrow k-block: box
+// {tail_cols, box_rows} at the matching swizzle (16 columns = 32 bytes:
+// SWIZZLE_32B; 32 columns: SWIZZLE_64B), rows past the end read as zero.
+// The box starts at column cols - tail_cols, which the caller keeps a
+// multiple of 64.
+inline CUtensorMap make_f16_tail_map(const void* base, int64_t rows, int64_t cols, int tail_cols,
+                                     int box_rows) {
+    if ((tail_cols != 16 && tail_cols != 32) || cols % 16 != 0 || cols < tail_cols ||
+        (reinterpret_cast<uintptr_t>(base) & 15) != 0 || box_rows < 1 || box_rows > 256)
+        throw Error(UMAPB_ERR_CUDA, "narrow tensor map: unsupported tail width or alignment");
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols) * 2};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(tail_cols),
+                               static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encoder()(
+        &m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+        CU_TENSOR_MAP_INTERLEAVE_NONE,
+        tail_cols == 16 ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B,
+        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw Error(UMAPB_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     return m;
 }
