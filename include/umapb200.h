@@ -506,8 +506,9 @@ int32_t umapb_surrogate_ready(const umapb_model* model);
  * row in the request, so a gated row's result does not depend on the other
  * rows; with 0 every row keeps the network's output.  `fallback` (may be
  * NULL, n_rows bytes) receives 1 for each gated row; `n_fallback` (may be
- * NULL) their count.  Host buffers, uploaded in chunks while the gated rows
- * of earlier chunks are recomputed. */
+ * NULL) their count.  Host buffers: the rows go up in chunks and the network
+ * runs on each chunk as it lands; the gated rows are recomputed once, after
+ * the last chunk. */
 int32_t umapb_surrogate_transform(umapb_model* model, const float* query, int64_t n_rows,
                                   int64_t n_cols, int32_t use_fallback, float* out,
                                   uint8_t* fallback, int64_t* n_fallback);

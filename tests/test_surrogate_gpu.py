@@ -197,14 +197,14 @@ def test_umap_transform_mode_surrogate_trains_on_fit():
 
 
 def test_chunked_host_transform_equals_device_path_and_gated_rows_are_row_local(trained):
-    """The host surrogate transform uploads 131,072-row chunks and recomputes
-    each chunk's gated rows while later chunks still upload.  A gated row is
-    transformed as a request of its own (its sigma floor, prune threshold and
-    sampling periods from its own neighbours) with the random stream of its
-    row in the request, so the host path equals the device-resident path bit
-    for bit, and a gated row's result does not change when the request holds
-    other rows: the first chunk sent alone gives its gated rows the same
-    positions (both requests exceed 10,000 rows, so both run 30 epochs)."""
+    """The host surrogate transform uploads 131,072-row chunks and runs the
+    network on each as it lands.  A gated row is transformed as a request of
+    its own (its sigma floor, prune threshold and sampling periods from its
+    own neighbours) with the random stream of its row in the request, so the
+    host path equals the device-resident path bit for bit, and a gated row's
+    result does not change when the request holds other rows: the first chunk
+    sent alone gives its gated rows the same positions (both requests exceed
+    10,000 rows, so both run 30 epochs)."""
     import torch
 
     m, fit, query, _, _ = trained

@@ -700,6 +700,28 @@ void trim_precomputed(const int64_t* idx, const float* dist, int64_t n, int64_t 
     }
 }
 
+// A copy stream with one completion event per chunk.  Its destructor waits
+// for every copy issued on it, so buffers it writes outlive its work.
+struct CopyStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ready = nullptr;
+    std::vector<cudaEvent_t> done;
+    explicit CopyStream(int64_t n) : done(static_cast<size_t>(n), nullptr) {
+        UMAPB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        UMAPB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        for (auto& e : done) UMAPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    CopyStream(const CopyStream&) = delete;
+    CopyStream& operator=(const CopyStream&) = delete;
+    ~CopyStream() {
+        if (s) cudaStreamSynchronize(s);
+        for (auto e : done)
+            if (e) cudaEventDestroy(e);
+        if (ready) cudaEventDestroy(ready);
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
 // Host buffers for the deterministic transform stages (umapb_transform_graph).
 struct TransformStages {
     float* sigmas = nullptr;
@@ -791,10 +813,14 @@ void transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d, fl
 
 void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
                         const uint8_t* flags, int64_t nf, int64_t epoch_rows = -1,
-                        int64_t row_offset = 0);
+                        int64_t row_offset = 0, cudaEvent_t before_scatter = nullptr);
 
 // Surrogate transform of device rows: network outputs for every row, then
-// (use_fallback) the plain transform for the rows the gate rejects.
+// (use_fallback) the plain transform for the rows the gate rejects.  The gate
+// needs only the input rows, so it runs first; with gated rows, the network
+// then runs on a second stream while the plain transform of the gated rows
+// runs on the model's stream, and its results are scattered over the
+// network's once both are done.
 void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int64_t d,
                                 bool use_fallback, float* out, uint8_t* flags_out,
                                 int64_t* n_fallback) {
@@ -805,9 +831,22 @@ void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int
         own.alloc(nq, s);
         flags = own.get();
     }
-    const int64_t nf = surrogate_infer(*m->surrogate, Qd, nq, static_cast<int>(d), out, flags, s);
+    const Surrogate& sg = *m->surrogate;
+    surrogate_gate_async(sg, Qd, nq, static_cast<int>(d), flags, s);
+    const int64_t nf = surrogate_count_flags(flags, nq, s);  // synchronises s
     if (n_fallback) *n_fallback = nf;
-    if (use_fallback) surrogate_fallback(m, Qd, nq, d, out, flags, nf);
+    if (!use_fallback || nf == 0) {
+        surrogate_forward_async(sg, Qd, nq, static_cast<int>(d), out, s);
+        surrogate_check(s);
+        return;
+    }
+    CopyStream net(1);
+    UMAPB_CUDA(cudaEventRecord(net.ready, s));
+    UMAPB_CUDA(cudaStreamWaitEvent(net.s, net.ready, 0));
+    surrogate_forward_async(sg, Qd, nq, static_cast<int>(d), out, net.s);
+    UMAPB_CUDA(cudaEventRecord(net.done[0], net.s));
+    surrogate_fallback(m, Qd, nq, d, out, flags, nf, -1, 0, net.done[0]);
+    surrogate_check(net.s);
 }
 
 // The plain transform for the `nf` rows the gate flagged, scattered into out.
@@ -819,7 +858,7 @@ void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int
 // depend on which other rows were gated, nor on how the request is split.
 void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, float* out,
                         const uint8_t* flags, int64_t nf, int64_t epoch_rows,
-                        int64_t row_offset) {
+                        int64_t row_offset, cudaEvent_t before_scatter) {
     if (nf == 0) return;
     if (epoch_rows < 0) epoch_rows = nq;
     cudaStream_t s = m->stream;
@@ -830,6 +869,8 @@ void surrogate_fallback(umapb_model* m, const float* Qd, int64_t nq, int64_t d, 
     gather_rows(Qd, ids.get(), nf, static_cast<int>(d), sub.get(), s);
     transform_device(m, sub.get(), nf, d, sub_out.get(), epoch_rows, nullptr, ids.get(),
                      row_offset, true);
+    // the network's outputs for these rows (another stream) land first
+    if (before_scatter) UMAPB_CUDA(cudaStreamWaitEvent(s, before_scatter, 0));
     scatter_rows(sub_out.get(), ids.get(), nf, dim, out, s);
 }
 
@@ -851,27 +892,6 @@ void check_transform(umapb_model* m, int64_t n_cols) {
 // Rows per upload chunk of a host surrogate transform (64 MB at 128 features).
 constexpr int64_t kUploadChunkRows = 131072;
 
-// A copy stream with one completion event per chunk.  Its destructor waits
-// for every copy issued on it, so buffers it writes outlive its work.
-struct CopyStream {
-    cudaStream_t s = nullptr;
-    cudaEvent_t ready = nullptr;
-    std::vector<cudaEvent_t> done;
-    explicit CopyStream(int64_t n) : done(static_cast<size_t>(n), nullptr) {
-        UMAPB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-        UMAPB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-        for (auto& e : done) UMAPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    }
-    CopyStream(const CopyStream&) = delete;
-    CopyStream& operator=(const CopyStream&) = delete;
-    ~CopyStream() {
-        if (s) cudaStreamSynchronize(s);
-        for (auto e : done)
-            if (e) cudaEventDestroy(e);
-        if (ready) cudaEventDestroy(ready);
-        if (s) cudaStreamDestroy(s);
-    }
-};
 
 }  // namespace
 
@@ -1711,30 +1731,15 @@ int32_t umapb_surrogate_transform(umapb_model* m, const float* query, int64_t n_
             UMAPB_CUDA(cudaEventRecord(cs.done[c], cs.s));
         }
         // The checks and the network are queued chunk by chunk with no host
-        // wait; the first non-finite row, the GEMM status and the gate count
-        // are read back once, before the fallback and the outputs.  (Copies
-        // from pageable host memory are staged by the driver and keep the
-        // host busy until they land; pinned rows let the queueing run ahead.)
-        // With the fallback on, the rows chunk c - 1 gated run their plain
-        // transform once chunk c is queued, while later chunks still upload;
-        // only the last chunk's fallback follows the upload.  Checking a chunk
-        // reads the running first-non-finite row and the chunk's gate count
-        // (one host wait per chunk on the model's stream; the copies run on).
+        // wait; the first non-finite row and the gate count are read back
+        // once, after the last chunk.  (Copies from pageable host memory are
+        // staged by the driver and keep the host busy until they land; pinned
+        // rows let the queueing run ahead.)  Every gated row is transformed
+        // as a request of its own, so one fallback over the gated rows of
+        // all chunks gives each the result a per-chunk fallback would, and
+        // pays the fallback's fixed latency once.
         DevBuf<unsigned long long> bad_row(1, s);
         UMAPB_CUDA(cudaMemsetAsync(bad_row.get(), 0xFF, 8, s));
-        int64_t nf = 0;
-        auto settle = [&](int64_t c) {
-            const int64_t r0 = c * chunk, rows = std::min(chunk, n_rows - r0);
-            unsigned long long bad = 0;
-            UMAPB_CUDA(cudaMemcpyAsync(&bad, bad_row.get(), 8, cudaMemcpyDeviceToHost, s));
-            const int64_t nfc = surrogate_count_flags(fl.get() + r0, rows, s);  // synchronises s
-            if (bad != ~0ull)
-                invalid("input contains non-finite value at row " + std::to_string(bad));
-            nf += nfc;
-            if (use_fallback != 0)
-                surrogate_fallback(m, Q.get() + r0 * n_cols, rows, n_cols, outd.get() + r0 * dim,
-                                   fl.get() + r0, nfc, n_rows, r0);
-        };
         for (int64_t c = 0; c < n_chunks; ++c) {
             const int64_t r0 = c * chunk, rows = std::min(chunk, n_rows - r0);
             UMAPB_CUDA(cudaStreamWaitEvent(s, cs.done[c], 0));
@@ -1743,9 +1748,13 @@ int32_t umapb_surrogate_transform(umapb_model* m, const float* query, int64_t n_
             surrogate_infer_async(*m->surrogate, Q.get() + r0 * n_cols, rows,
                                   static_cast<int>(n_cols), outd.get() + r0 * dim, fl.get() + r0,
                                   s);
-            if (c > 0) settle(c - 1);
         }
-        settle(n_chunks - 1);
+        unsigned long long bad = 0;
+        UMAPB_CUDA(cudaMemcpyAsync(&bad, bad_row.get(), 8, cudaMemcpyDeviceToHost, s));
+        const int64_t nf = surrogate_count_flags(fl.get(), n_rows, s);  // synchronises s
+        if (bad != ~0ull) invalid("input contains non-finite value at row " + std::to_string(bad));
+        if (use_fallback != 0)
+            surrogate_fallback(m, Q.get(), n_rows, n_cols, outd.get(), fl.get(), nf);
         if (n_fallback) *n_fallback = nf;
         UMAPB_CUDA(cudaMemcpyAsync(out, outd.get(), n_rows * dim * 4, cudaMemcpyDeviceToHost, s));
         if (fallback)

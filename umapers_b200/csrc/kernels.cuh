@@ -276,16 +276,21 @@ SurrogatePtr surrogate_train(const float* X, int64_t n, int d, const float* emb,
                              umapb_surrogate_info* info, std::vector<double>* history,
                              cudaStream_t s);
 
-// Network outputs of nq query rows (device) into out (nq x dim); `flags`
-// (nullable) receives 1 for each row the gate rejects.  Returns the number of
-// rejected rows (0 when flags is null).
-int64_t surrogate_infer(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
-                        uint8_t* flags, cudaStream_t s);
-// The same inference with no host synchronisation (no gate count, no GEMM
-// status read); surrogate_count_flags then reads the GEMM status and counts
-// the gated rows of a whole request once.
+// Network outputs of nq query rows (device) into out (nq x dim) and, in
+// `flags` (nullable), 1 for each row the gate rejects, with no host
+// synchronisation (no gate count, no GEMM status read);
+// surrogate_count_flags then reads the GEMM status and counts the gated rows
+// of a whole request once.
 void surrogate_infer_async(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
                            uint8_t* flags, cudaStream_t s);
+// The gate alone (flags, no network outputs) and the network alone (outputs,
+// no gate), queued on `s` with no host wait; surrogate_check then waits for
+// `s` and reports a GEMM wait timeout.
+void surrogate_gate_async(const Surrogate& sg, const float* Q, int64_t nq, int d, uint8_t* flags,
+                          cudaStream_t s);
+void surrogate_forward_async(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
+                             cudaStream_t s);
+void surrogate_check(cudaStream_t s);
 int64_t surrogate_count_flags(const uint8_t* flags, int64_t nq, cudaStream_t s);
 
 // dst[r] = src[ids[r]] and dst[ids[r]] = src[r] for rows of d floats.

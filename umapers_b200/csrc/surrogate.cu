@@ -676,7 +676,8 @@ void infer_rows(const Surrogate& sg, const float* Q, const int32_t* ids, int64_t
     const int64_t chunk = std::min<int64_t>(rows, kInferChunk);
     Pass P;
     P.alloc(L, chunk, false, s);
-    const bool gate = sg.n_anchors > 0;
+    // the gate runs only when its flags or nearest anchors are asked for
+    const bool gate = sg.n_anchors > 0 && (flags || anchor_of || anchor_d2);
     const int a_tiles = gate ? static_cast<int>(ceil_div(sg.n_anchors, 128)) : 0;
     DevBuf<float> row_sq, amin;
     DevBuf<int32_t> amin_idx;
@@ -1019,26 +1020,25 @@ void surrogate_infer_async(const Surrogate& sg, const float* Q, int64_t nq, int 
     infer_rows(sg, Q, nullptr, nq, out, flags, nullptr, nullptr, s);
 }
 
+void surrogate_gate_async(const Surrogate& sg, const float* Q, int64_t nq, int d, uint8_t* flags,
+                          cudaStream_t s) {
+    if (d != sg.L.din) invalid("surrogate input width differs from the fitted rows");
+    if (nq == 0) return;
+    infer_rows(sg, Q, nullptr, nq, nullptr, flags, nullptr, nullptr, s);
+}
+
+void surrogate_forward_async(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
+                             cudaStream_t s) {
+    if (d != sg.L.din) invalid("surrogate input width differs from the fitted rows");
+    if (nq == 0) return;
+    infer_rows(sg, Q, nullptr, nq, out, nullptr, nullptr, nullptr, s);
+}
+
+void surrogate_check(cudaStream_t s) { check_gemm(s); }
+
 int64_t surrogate_count_flags(const uint8_t* flags, int64_t nq, cudaStream_t s) {
     check_gemm(s);
     if (!flags || nq == 0) return 0;
-    DevBuf<unsigned long long> cnt(1, s);
-    UMAPB_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, s));
-    count_flags_kernel<<<std::min<int64_t>(grid_for(nq), 4096), 256, 0, s>>>(flags, nq, cnt.get());
-    UMAPB_LAUNCH_CHECK();
-    unsigned long long h = 0;
-    UMAPB_CUDA(cudaMemcpyAsync(&h, cnt.get(), 8, cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
-    return static_cast<int64_t>(h);
-}
-
-int64_t surrogate_infer(const Surrogate& sg, const float* Q, int64_t nq, int d, float* out,
-                        uint8_t* flags, cudaStream_t s) {
-    if (d != sg.L.din) invalid("surrogate input width differs from the fitted rows");
-    if (nq == 0) return 0;
-    infer_rows(sg, Q, nullptr, nq, out, flags, nullptr, nullptr, s);
-    check_gemm(s);
-    if (!flags) return 0;
     DevBuf<unsigned long long> cnt(1, s);
     UMAPB_CUDA(cudaMemsetAsync(cnt.get(), 0, 8, s));
     count_flags_kernel<<<std::min<int64_t>(grid_for(nq), 4096), 256, 0, s>>>(flags, nq, cnt.get());
