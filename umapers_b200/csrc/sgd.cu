@@ -155,6 +155,9 @@ __device__ __forceinline__ void count_block_samples(uint32_t* slots, bool sample
     if (threadIdx.x == 0) slots[blockIdx.x] += cnt;
 }
 
+// Negative samples drawn and loaded together in the 2-D epoch.
+constexpr int kNegBatch = 4;
+
 // One epoch for dim == 2 (the reference's flat fast path, lib.rs:5172-5244).
 __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -190,22 +193,36 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
             if (isfinite(en) && en > 0.0f) {
                 const float nn = p.next_neg[e];
                 const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(p.epoch_f, nn), en));
-                for (uint32_t s = 0; s < n_neg; ++s) {
-                    const uint64_t word = rng_word(p.seed, static_cast<uint64_t>(e),
-                                                   (p.epoch << 32) | s);
-                    const uint32_t neg = rng_below(word, p.n_vertices);
-                    if (neg == static_cast<uint32_t>(head)) continue;
-                    const float2 o = emb[neg];
-                    const float dx = __fsub_rn(hx, o.x), dy = __fsub_rn(hy, o.y);
-                    const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-                    if (d2 > 0.0f) {
-                        const float pb = pow_pos(d2, p.b);
-                        const float gc =
-                            __fdiv_rn(p.rep_factor, __fmul_rn(__fadd_rn(0.001f, d2),
-                                                              __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
-                        if (gc > 0.0f) {
-                            hx = __fadd_rn(hx, __fmul_rn(clip4(__fmul_rn(gc, dx)), p.alpha));
-                            hy = __fadd_rn(hy, __fmul_rn(clip4(__fmul_rn(gc, dy)), p.alpha));
+                // The negatives' positions do not depend on the head's moves:
+                // kNegBatch are drawn and loaded at once, then applied in order.
+                for (uint32_t s0 = 0; s0 < n_neg; s0 += kNegBatch) {
+                    float2 o[kNegBatch];
+                    bool use[kNegBatch];
+#pragma unroll
+                    for (int j = 0; j < kNegBatch; ++j) {
+                        const uint32_t s = s0 + j;
+                        uint32_t neg = static_cast<uint32_t>(head);
+                        if (s < n_neg)
+                            neg = rng_below(rng_word(p.seed, static_cast<uint64_t>(e),
+                                                     (p.epoch << 32) | s),
+                                            p.n_vertices);
+                        use[j] = neg != static_cast<uint32_t>(head);
+                        o[j] = use[j] ? emb[neg] : make_float2(0.0f, 0.0f);
+                    }
+#pragma unroll
+                    for (int j = 0; j < kNegBatch; ++j) {
+                        if (!use[j]) continue;
+                        const float dx = __fsub_rn(hx, o[j].x), dy = __fsub_rn(hy, o[j].y);
+                        const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+                        if (d2 > 0.0f) {
+                            const float pb = pow_pos(d2, p.b);
+                            const float gc = __fdiv_rn(
+                                p.rep_factor,
+                                __fmul_rn(__fadd_rn(0.001f, d2), __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
+                            if (gc > 0.0f) {
+                                hx = __fadd_rn(hx, __fmul_rn(clip4(__fmul_rn(gc, dx)), p.alpha));
+                                hy = __fadd_rn(hy, __fmul_rn(clip4(__fmul_rn(gc, dy)), p.alpha));
+                            }
                         }
                     }
                 }
