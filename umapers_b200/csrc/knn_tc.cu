@@ -197,6 +197,24 @@ __device__ __forceinline__ T warp_sort_asc(T v) {
     return v;
 }
 
+// Two independent bitonic sorts (one value per lane each) stage by stage, so
+// their shuffles overlap.
+template <typename T>
+__device__ __forceinline__ void warp_sort_asc2(T& a, T& b) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const T oa = __shfl_xor_sync(0xffffffffu, a, stride);
+            const T ob = __shfl_xor_sync(0xffffffffu, b, stride);
+            const bool keep_min = ((lane & size) == 0) == ((lane & stride) == 0);
+            a = keep_min ? (a < oa ? a : oa) : (a < oa ? oa : a);
+            b = keep_min ? (b < ob ? b : ob) : (b < ob ? ob : b);
+        }
+    }
+}
+
 // Merges 32 keys (one per lane, any order) into a list sorted ascending
 // across the lanes and keeps the 32 smallest: sort the keys, reverse them,
 // take the lane-wise minimum (a bitonic sequence holding the 32 smallest of
@@ -272,14 +290,21 @@ __device__ __forceinline__ float merge_held(uint64_t* lst, int held) {
     const int lane = threadIdx.x & 31;
     __syncwarp();  // the appended keys were stored by other lanes
     uint64_t lk = lst[lane];
-    const uint64_t h0 = lane < held ? held_key(lst[S + lane]) : ~0ull;
-    const uint64_t h1 = lane + 32 < held ? held_key(lst[S + 32 + lane]) : ~0ull;
-    if (held > 32) lk = warp_merge_keys(lk, h1);
-    const int n0 = min(held, 32);
-    if (n0 >= kBulkMergeMin) {
+    uint64_t h0 = lane < held ? held_key(lst[S + lane]) : ~0ull;
+    uint64_t h1 = lane + 32 < held ? held_key(lst[S + 32 + lane]) : ~0ull;
+    if (held > 32) {
+        // both halves sorted at once; the 32 smallest of them (lane-wise min
+        // of one and the other reversed, a bitonic sequence), sorted, then
+        // merged with the list the same way
+        warp_sort_asc2<uint64_t>(h0, h1);
+        const uint64_t r1 = __shfl_sync(0xffffffffu, h1, 31 - lane);
+        const uint64_t m = warp_bitonic_sort<uint64_t>(h0 < r1 ? h0 : r1);
+        const uint64_t rm = __shfl_sync(0xffffffffu, m, 31 - lane);
+        lk = warp_bitonic_sort<uint64_t>(lk < rm ? lk : rm);
+    } else if (held >= kBulkMergeMin) {
         lk = warp_merge_keys(lk, h0);
     } else {
-        for (int b = 0; b < n0; ++b) {
+        for (int b = 0; b < held; ++b) {
             const uint64_t key = __shfl_sync(0xffffffffu, h0, b);
             const int pos = __popc(__ballot_sync(0xffffffffu, lk < key));
             const uint64_t up = __shfl_up_sync(0xffffffffu, lk, 1);
