@@ -7,8 +7,12 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
+#include <vector>
 
 #include "../../include/umapb200.h"
 
@@ -52,20 +56,95 @@ struct Error : public std::runtime_error {
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-// Stream-ordered device buffer.  Memory comes from the device's default
-// memory pool (cudaMallocAsync), which keeps freed blocks cached so repeated
-// fits of the same size do not go back to the driver.
+// Blocks released by DevBuf are kept per (device, stream, exact size) and
+// handed to the next request of that size on that stream, in stream order.
+// A fit asks for the same sizes in the same order every time, so repeated
+// fits of one size make no allocator call: a pool allocation, even one served
+// from memory the pool already holds, occasionally took most of a second on
+// a shared machine.  At most kBlockCacheBytes are kept; a block that would go
+// beyond returns to the device's stream-ordered pool (cudaFreeAsync on its
+// own stream).  Blocks of a stream that is gone stay until the process ends,
+// within the same limit.
+constexpr size_t kBlockCacheBytes = static_cast<size_t>(12) << 30;
+
+struct BlockCache {
+    std::mutex mu;
+    std::map<std::tuple<int, cudaStream_t, size_t>, std::vector<void*>> free_blocks;
+    size_t held = 0;
+    static BlockCache& get() {
+        static BlockCache c;
+        return c;
+    }
+};
+
+inline void* dev_alloc(size_t bytes, cudaStream_t s, int* dev_out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    *dev_out = dev;
+    BlockCache& c = BlockCache::get();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = c.free_blocks.find(std::make_tuple(dev, s, bytes));
+        if (it != c.free_blocks.end() && !it->second.empty()) {
+            void* p = it->second.back();
+            it->second.pop_back();
+            c.held -= bytes;
+            return p;
+        }
+    }
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    if (e != cudaSuccess) throw_cuda(e, "cudaMallocAsync", __FILE__, __LINE__);
+    return p;
+}
+
+inline void dev_free(void* p, size_t bytes, cudaStream_t s, int dev) {
+    BlockCache& c = BlockCache::get();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.held + bytes <= kBlockCacheBytes) {
+            c.free_blocks[std::make_tuple(dev, s, bytes)].push_back(p);
+            c.held += bytes;
+            return;
+        }
+    }
+    cudaFreeAsync(p, s);
+}
+
+// Returns the blocks kept for stream `s` to the pool; called before the
+// stream is destroyed (its work has finished).
+inline void dev_release_stream(cudaStream_t s) {
+    std::vector<void*> blocks;
+    BlockCache& c = BlockCache::get();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        for (auto it = c.free_blocks.begin(); it != c.free_blocks.end();) {
+            if (std::get<1>(it->first) == s) {
+                c.held -= std::get<2>(it->first) * it->second.size();
+                blocks.insert(blocks.end(), it->second.begin(), it->second.end());
+                it = c.free_blocks.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+    for (void* p : blocks) cudaFreeAsync(p, s);
+}
+
+// Stream-ordered device buffer on the block cache above (backed by the
+// device's default memory pool, cudaMallocAsync).
 template <typename T>
 struct DevBuf {
     T* ptr = nullptr;
     size_t count = 0;
     cudaStream_t stream = nullptr;
+    int device = 0;
 
     DevBuf() = default;
     DevBuf(size_t n, cudaStream_t s) { alloc(n, s); }
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream) {
+    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream), device(o.device) {
         o.ptr = nullptr;
         o.count = 0;
     }
@@ -75,6 +154,7 @@ struct DevBuf {
             ptr = o.ptr;
             count = o.count;
             stream = o.stream;
+            device = o.device;
             o.ptr = nullptr;
             o.count = 0;
         }
@@ -86,10 +166,10 @@ struct DevBuf {
         release();
         stream = s;
         count = n;
-        if (n > 0) UMAPB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), s));
+        if (n > 0) ptr = static_cast<T*>(dev_alloc(n * sizeof(T), s, &device));
     }
     void release() {
-        if (ptr) cudaFreeAsync(ptr, stream);
+        if (ptr) dev_free(ptr, count * sizeof(T), stream, device);
         ptr = nullptr;
         count = 0;
     }

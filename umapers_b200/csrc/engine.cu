@@ -718,7 +718,10 @@ struct CopyStream {
         for (auto e : done)
             if (e) cudaEventDestroy(e);
         if (ready) cudaEventDestroy(ready);
-        if (s) cudaStreamDestroy(s);
+        if (s) {
+            dev_release_stream(s);
+            cudaStreamDestroy(s);
+        }
     }
 };
 
@@ -975,6 +978,7 @@ void umapb_destroy(umapb_model* m) {
             // every device array is freed on the model's stream, before it goes
             m->begin_fit();
             cudaStreamSynchronize(m->stream);
+            dev_release_stream(m->stream);
             cudaStreamDestroy(m->stream);
             m->stream = nullptr;
         }
@@ -1333,6 +1337,7 @@ struct ScopedStream {
     ~ScopedStream() {
         if (s) {
             cudaStreamSynchronize(s);
+            dev_release_stream(s);
             cudaStreamDestroy(s);
         }
     }
