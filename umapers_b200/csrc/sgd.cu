@@ -183,8 +183,8 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
                     const float mx = __fmul_rn(gx, p.alpha), my = __fmul_rn(gy, p.alpha);
                     hx = __fadd_rn(hx, mx);
                     hy = __fadd_rn(hy, my);
-                    atomicAdd(&p.emb[2 * tail], -mx);
-                    atomicAdd(&p.emb[2 * tail + 1], -my);
+                    // one vector atomic moves both coordinates (each added atomically)
+                    atomicAdd(reinterpret_cast<float2*>(p.emb) + tail, make_float2(-mx, -my));
                 }
             }
             const float eps = p.eps[e];
@@ -228,8 +228,9 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
                 }
                 p.next_neg[e] = __fadd_rn(nn, __fmul_rn(static_cast<float>(n_neg), en));
             }
-            if (hx != h0.x) atomicAdd(&p.emb[2 * head], __fsub_rn(hx, h0.x));
-            if (hy != h0.y) atomicAdd(&p.emb[2 * head + 1], __fsub_rn(hy, h0.y));
+            if (hx != h0.x || hy != h0.y)
+                atomicAdd(reinterpret_cast<float2*>(p.emb) + head,
+                          make_float2(__fsub_rn(hx, h0.x), __fsub_rn(hy, h0.y)));
         }
     }
     if (p.block_samples) count_block_samples(p.block_samples, sampled);
