@@ -50,6 +50,9 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "fit s @1M×64 TC vs FP32 kNN; transform rows/s MLP vs plain at equal trust@15"
 N_ROWS, N_DIM, K, EPOCHS = 1_000_000, 64, 15, 200
+# DRAM bytes of one first-pass tc_knn_kernel launch on the headline fit (ncu, 1M x 64):
+# 166.41 GB read + 13.57 GB written in 194.9 ms.
+KNN_DRAM_BYTES_1M = 179_980_000_000
 KNN_BLOCK = 2_000               # query rows of the CPU kNN block (against all N_ROWS)
 CAL_SIZES = (25_000, 50_000)   # rows of the two CPU fits that time the other stages
 T_FIT, T_QUERY, T_DIM = 200_000, 1_000_000, 128
@@ -356,9 +359,13 @@ def run_gpu(args) -> None:
             "peak": pk["bf16_tflops_sustained"],
             "unit": "TFLOP/s",
             "frac": round(flops / knn_t / 1e12 / pk["bf16_tflops_sustained"], 4),
-            "traffic": None,
+            # DRAM bytes read + written by the first-pass launch at this size, from one ncu
+            # capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass, -c 1)
+            "traffic": KNN_DRAM_BYTES_1M,
             "note": "algorithmic 2*N*N*D flop per fit; peak = sustained bf16 ("
-                    + pk["source"] + ")",
+                    + pk["source"] + "); traffic = DRAM bytes of the first-pass launch (ncu): "
+                    "the 160 MB candidate operand streamed past L2 by each wave of query groups, "
+                    "and the lists",
         }
         roof_sgd = {
             "kernel": "sgd_epoch_2d (200 launches)",
@@ -722,6 +729,15 @@ def transform_leg(args, lib, device: int) -> dict:
             "bound": "tensor", "achieved": round(achieved, 2), "peak": pk["bf16_tflops"],
             "unit": "TFLOP/s", "frac": round(achieved / pk["bf16_tflops"], 4), "traffic": None,
             "note": f"{flop_row:.0f} flop per row; peak = burst bf16 ({pk['source']})"},
+        # the same call against HBM: per query the FP32 row read (T_DIM x 4 B), the 2-D output
+        # written (8 B) and its gate flag (1 B), over the device-resident call's time
+        "roofline_hbm": {
+            "kernel": "surrogate transform (whole device-resident call)", "bound": "hbm",
+            "achieved": round(T_QUERY * (T_DIM * 4 + 8 + 1) / ts / 1e9, 1),
+            "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": round(T_QUERY * (T_DIM * 4 + 8 + 1) / ts / 1e9 / pk["hbm_gbs"], 4),
+            "traffic": None,
+            "note": f"{T_DIM * 4 + 9} B per query; peak = measured HBM copy ({pk['source']})"},
         "config": {"workload": f"fit {T_FIT} x {T_DIM} (20-component mixture, seed 5), "
                                f"{T_QUERY} queries (seed 6), k={K}, 2-D",
                    "surrogate": "MLP 128-512-512-2 GELU, BF16 GEMMs / FP32 master, Adam 1e-3, "

@@ -289,7 +289,13 @@ struct umapb_model {
             return;
         }
         UMAPB_CUDA(cudaGetDevice(&device));
-        UMAPB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        // The model's stream has the device's highest priority: where a call
+        // runs work beside it on another stream (the surrogate's network
+        // beside the gated rows' plain transform), the latency-bound chain on
+        // this stream gets freed SMs first.
+        int least = 0, greatest = 0;
+        UMAPB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        UMAPB_CUDA(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, greatest));
         // keep freed pool memory cached across fits
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {

@@ -1,7 +1,7 @@
 """Small, self-contained GPU cases for profiling one kernel family at a time.
 
     python -m umapers_b200.profiling knn_tc [--rows 262144] [--dim 64]
-    python -m umapers_b200.profiling surrogate [--rows 262144]
+    python -m umapers_b200.profiling surrogate [--rows 262144] [--fit-rows 50000]
     python -m umapers_b200.profiling fit [--rows 262144] [--dim 64]
     python -m umapers_b200.profiling sparse [--rows 200000] [--dim 2000]
 
@@ -67,15 +67,15 @@ def case_knn_tc(rows: int, dim: int) -> None:
     print(f"knn_tc rows={rows} dim={dim}: {r.dt:.4f} s, fallback rows {fb.value}")
 
 
-def case_surrogate(rows: int) -> None:
+def case_surrogate(rows: int, fit_rows: int = 50_000) -> None:
     """Surrogate transform of `rows` queries (128 features), gated rows
-    recomputed by the plain transform, after training on a 50,000-row fit of
-    the same mixture."""
+    recomputed by the plain transform, after training on a `fit_rows`-row fit
+    of the same mixture."""
     import torch
 
     from umapers import Umap
 
-    fit, query = workloads.transform_mixture(n_fit=50_000, n_query=rows, d=128)
+    fit, query = workloads.transform_mixture(n_fit=fit_rows, n_query=rows, d=128)
     m = Umap(n_neighbors=15, random_seed=5, ann_mode="exact")
     m.fit(fit)
     m.fit_surrogate(batch_size=1024)
@@ -133,13 +133,14 @@ def main() -> None:
     ap.add_argument("case", choices=["knn_tc", "surrogate", "fit", "sparse"])
     ap.add_argument("--rows", type=int, default=262_144)
     ap.add_argument("--dim", type=int, default=None)
+    ap.add_argument("--fit-rows", type=int, default=50_000, help="surrogate case: fitted rows")
     a = ap.parse_args()
     if a.dim is None:
         a.dim = 2000 if a.case == "sparse" else 64
     if a.case == "knn_tc":
         case_knn_tc(a.rows, a.dim)
     elif a.case == "surrogate":
-        case_surrogate(a.rows)
+        case_surrogate(a.rows, a.fit_rows)
     elif a.case == "sparse":
         case_sparse(a.rows, a.dim)
     else:
