@@ -367,14 +367,14 @@ struct TcArgs {
 struct Unit {
     int32_t group, split, begin, len, rot;  // tile counts stay far below 2^31
 };
-__device__ __forceinline__ Unit unit_of(const TcArgs& p, int64_t u) {
+__device__ __forceinline__ Unit unit_of(const TcArgs& p, int64_t u, int64_t stagger) {
     Unit r;
     r.group = static_cast<int32_t>(u / p.n_split);
     r.split = static_cast<int32_t>(u - static_cast<int64_t>(r.group) * p.n_split);
     r.begin = r.split * static_cast<int32_t>(p.split_tiles);
     r.len = static_cast<int32_t>(min(p.split_tiles, p.n_ctiles - r.begin));
     r.rot = p.start_tile != nullptr ? p.start_tile[r.group]
-                                    : static_cast<int32_t>(blockIdx.x % kStaggerGroups) * kStaggerStep;
+                                    : static_cast<int32_t>(stagger % kStaggerGroups) * kStaggerStep;
     if (r.rot >= r.len || r.rot < 0) r.rot = 0;
     return r;
 }
@@ -398,6 +398,110 @@ constexpr int tc_threads() { return 64 + 32 * epi_warps<MT, BN>(); }
 
 // The register file is split among the SM's four schedulers: with 18 warps
 // two of them hold five warps, which caps a thread at 96 registers.
+// The epilogue role of one warp, for both kernel forms.  Warp w reads TMEM
+// lanes 32 * (w % 4) (hardware rule); the warps of each quarter split (query
+// tile, 64-column group).  Units are first_unit, first_unit + unit_step, ...
+// With PAIR the TMEM tiles come from a CTA pair: this CTA's query tile of a
+// unit is 2 * group + rank, waits acquire at cluster scope, and releasing a
+// TMEM buffer arrives on the leader CTA's barrier.  False after a wait ran
+// out.
+template <int MT, int BN, bool PAIR>
+__device__ __forceinline__ bool tc_epilogue(const TcArgs& p, int warp, int lane,
+                                            uint32_t tmem_base, uint32_t b_tfull,
+                                            uint32_t b_tempty, int64_t first_unit,
+                                            int64_t unit_step, int64_t stagger, uint32_t rank,
+                                            volatile int* abort_flag) {
+    constexpr int GPT = BN / 64;  // lists per candidate tile
+    // Warp w reads TMEM lanes 32 * (w % 4) (hardware rule); the warps of
+    // each quarter split (query tile, 64-column group).
+    const int quarter = warp & 3;
+    const int slot = (warp - 2) >> 2;
+    const int mt = slot / GPT;
+    const int cq = slot % GPT;
+    uint64_t cg = 0;
+    bool ok = true;
+    for (int64_t unit = first_unit; unit < p.n_units && ok; unit += unit_step) {
+        const Unit w = unit_of(p, unit, stagger);
+        const int32_t row =
+            (PAIR ? w.group * 2 + static_cast<int32_t>(rank) : w.group * MT + mt) * BM +
+            quarter * 32 + lane;
+        const bool row_ok = row < p.n_q;
+        const int32_t list_base = w.split * GPT + cq;  // list of (row, split, group)
+        auto list_of = [&](int32_t srow) {
+            return p.lists + (static_cast<int64_t>(srow) * GPT * p.n_split + list_base) * LS;
+        };
+        float tau = INFINITY;  // this row's list: its S-th smallest key at the last merge
+        int held = 0;          // keys appended behind the sorted ones since then
+        for (int32_t c = 0; c < w.len; ++c, ++cg) {
+            const uint32_t buf = static_cast<uint32_t>(cg & 1);
+            const uint32_t par = static_cast<uint32_t>((cg >> 1) & 1);
+            if (!(PAIR ? mbar_wait_cluster(b_tfull + 8 * buf, par, abort_flag)
+                       : mbar_wait(b_tfull + 8 * buf, par, abort_flag))) {
+                ok = false;
+                break;
+            }
+            fence_after();
+            const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
+                                   buf * (MT * BN) + mt * BN + cq * 64;
+            uint32_t r[2][32];
+            tmem_ld32(taddr, r[0]);
+            tmem_ld32(taddr + 32, r[1]);
+            tmem_wait_ld();
+            // the accumulator buffer can be overwritten as soon as it is in registers
+            fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                if (PAIR)
+                    mbar_arrive_cluster(mapa(b_tempty + 8 * buf, 0));  // the leader's barrier
+                else
+                    mbar_arrive(b_tempty + 8 * buf);
+            }
+            unsigned pend = __ballot_sync(0xffffffffu, row_ok && min64(r) < tau);
+            if (pend == 0) continue;
+            const int32_t colh = tile_at(c, w) * BN + cq * 64;
+            const int32_t valid_cols = static_cast<int32_t>(p.n_r - colh);
+            // Every pending row at once, one per lane: count the row's
+            // values below its threshold, merge the lists whose appended
+            // keys would overflow (one list at a time, across the warp),
+            // then append each row's keys behind its sorted ones.
+            const bool mine = (pend >> lane) & 1u;
+            const bool all = valid_cols >= 64;
+            float t = mine ? tau : -INFINITY;
+            int cnt = 0;
+#pragma unroll
+            for (int j = 0; j < 64; ++j)
+                cnt += (__uint_as_float(r[j >> 5][j & 31]) < t && (all || j < valid_cols))
+                           ? 1
+                           : 0;
+            unsigned over = __ballot_sync(0xffffffffu, held + cnt > HC);
+            while (over) {
+                const int cur = __ffs(over) - 1;
+                over &= over - 1;
+                const float nt = merge_held(list_of(__shfl_sync(0xffffffffu, row, cur)),
+                                            __shfl_sync(0xffffffffu, held, cur));
+                if (lane == cur) {
+                    tau = nt;
+                    held = 0;
+                }
+            }
+            t = mine ? tau : -INFINITY;
+            uint64_t* dst = list_of(row) + S;
+            held = all ? append_row<true>(r, t, 64, colh, dst, held)
+                       : append_row<false>(r, t, valid_cols, colh, dst, held);
+        }
+        if (!ok) break;
+        // every list of the unit ends sorted, with nothing held
+        unsigned rest = __ballot_sync(0xffffffffu, held > 0);
+        while (rest) {
+            const int cur = __ffs(rest) - 1;
+            rest &= rest - 1;
+            merge_held(list_of(__shfl_sync(0xffffffffu, row, cur)),
+                       __shfl_sync(0xffffffffu, held, cur));
+        }
+    }
+    return ok;
+}
+
 // With a narrow last k-block (p.ntail, resident query tiles only) a tile
 // takes KB - 1 ring stages; the last holds the final 64-column block and the
 // narrow one (32- or 64-byte rows at the matching swizzle), so a 16-column
@@ -412,7 +516,6 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
     constexpr int kBTileBytes = BN * BK * 2;
     constexpr int kStageB = SA ? MT * kATileBytes : 0;  // candidate tile within a stage
     constexpr uint32_t kIdesc = idesc_f16(BM, BN);
-    constexpr int GPT = BN / 64;                   // lists per candidate tile
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -476,7 +579,7 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
             int64_t u_iter = 0;
             for (int64_t unit = blockIdx.x; unit < p.n_units && !*abort_flag;
                  unit += gridDim.x, ++u_iter) {
-                const Unit w = unit_of(p, unit);
+                const Unit w = unit_of(p, unit, blockIdx.x);
                 if (!SA) {
                     if (u_iter > 0 &&
                         !mbar_wait(b_aempty, static_cast<uint32_t>((u_iter - 1) & 1), abort_flag)) {
@@ -537,7 +640,7 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
                     }
                     fence_after();
                 }
-                const int32_t len = unit_of(p, unit).len;
+                const int32_t len = unit_of(p, unit, blockIdx.x).len;
                 for (int32_t c = 0; c < len && ok; ++c, ++cg) {
                     const uint32_t buf = static_cast<uint32_t>(cg & 1);
                     if (!mbar_wait(b_tempty + 8 * buf, static_cast<uint32_t>(((cg >> 1) & 1) ^ 1),
@@ -602,85 +705,9 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
         }
     } else {
         // --------------------------------------------------- epilogue
-        // Warp w reads TMEM lanes 32 * (w % 4) (hardware rule); the warps of
-        // each quarter split (query tile, 64-column group).
-        const int quarter = warp & 3;
-        const int slot = (warp - 2) >> 2;
-        const int mt = slot / GPT;
-        const int cq = slot % GPT;
-        uint64_t cg = 0;
-        bool ok = true;
-        for (int64_t unit = blockIdx.x; unit < p.n_units && ok; unit += gridDim.x) {
-            const Unit w = unit_of(p, unit);
-            const int32_t row = (w.group * MT + mt) * BM + quarter * 32 + lane;
-            const bool row_ok = row < p.n_q;
-            const int32_t list_base = w.split * GPT + cq;  // list of (row, split, group)
-            auto list_of = [&](int32_t srow) {
-                return p.lists + (static_cast<int64_t>(srow) * GPT * p.n_split + list_base) * LS;
-            };
-            float tau = INFINITY;  // this row's list: its S-th smallest key at the last merge
-            int held = 0;          // keys appended behind the sorted ones since then
-            for (int32_t c = 0; c < w.len; ++c, ++cg) {
-                const uint32_t buf = static_cast<uint32_t>(cg & 1);
-                if (!mbar_wait(b_tfull + 8 * buf, static_cast<uint32_t>((cg >> 1) & 1), abort_flag)) {
-                    fail(6);
-                    ok = false;
-                    break;
-                }
-                fence_after();
-                const uint32_t taddr = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) +
-                                       buf * (MT * BN) + mt * BN + cq * 64;
-                uint32_t r[2][32];
-                tmem_ld32(taddr, r[0]);
-                tmem_ld32(taddr + 32, r[1]);
-                tmem_wait_ld();
-                // the accumulator buffer can be overwritten as soon as it is in registers
-                fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
-                unsigned pend = __ballot_sync(0xffffffffu, row_ok && min64(r) < tau);
-                if (pend == 0) continue;
-                const int32_t colh = tile_at(c, w) * BN + cq * 64;
-                const int32_t valid_cols = static_cast<int32_t>(p.n_r - colh);
-                // Every pending row at once, one per lane: count the row's
-                // values below its threshold, merge the lists whose appended
-                // keys would overflow (one list at a time, across the warp),
-                // then append each row's keys behind its sorted ones.
-                const bool mine = (pend >> lane) & 1u;
-                const bool all = valid_cols >= 64;
-                float t = mine ? tau : -INFINITY;
-                int cnt = 0;
-#pragma unroll
-                for (int j = 0; j < 64; ++j)
-                    cnt += (__uint_as_float(r[j >> 5][j & 31]) < t && (all || j < valid_cols))
-                               ? 1
-                               : 0;
-                unsigned over = __ballot_sync(0xffffffffu, held + cnt > HC);
-                while (over) {
-                    const int cur = __ffs(over) - 1;
-                    over &= over - 1;
-                    const float nt = merge_held(list_of(__shfl_sync(0xffffffffu, row, cur)),
-                                                __shfl_sync(0xffffffffu, held, cur));
-                    if (lane == cur) {
-                        tau = nt;
-                        held = 0;
-                    }
-                }
-                t = mine ? tau : -INFINITY;
-                uint64_t* dst = list_of(row) + S;
-                held = all ? append_row<true>(r, t, 64, colh, dst, held)
-                           : append_row<false>(r, t, valid_cols, colh, dst, held);
-            }
-            if (!ok) break;
-            // every list of the unit ends sorted, with nothing held
-            unsigned rest = __ballot_sync(0xffffffffu, held > 0);
-            while (rest) {
-                const int cur = __ffs(rest) - 1;
-                rest &= rest - 1;
-                merge_held(list_of(__shfl_sync(0xffffffffu, row, cur)),
-                           __shfl_sync(0xffffffffu, held, cur));
-            }
-        }
+        if (!tc_epilogue<MT, BN, false>(p, warp, lane, tmem_base, b_tfull, b_tempty, blockIdx.x,
+                                        gridDim.x, blockIdx.x, 0, abort_flag))
+            fail(6);
     }
 
     __syncthreads();
