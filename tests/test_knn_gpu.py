@@ -123,6 +123,18 @@ def test_tensor_knn_in_cell_order_matches_plain():
     assert fb <= 600
 
 
+def test_tensor_knn_large_query_set_matches_plain():
+    # a query set of more query tiles than SMs (no candidate splits) runs
+    # without the cell order, its candidate walks staggered by unit; 19,000
+    # rows leave the last query tile partial
+    x = workloads.anisotropic_mixture(30_000, 64, 20, seed=4)
+    q = workloads.anisotropic_mixture(19_000, 64, 20, seed=5)
+    ti, td = gu.knn_query(q, x, 15, backend="tensor")
+    pi, pd = gu.knn_query(q, x, 15, backend="plain")
+    np.testing.assert_array_equal(ti, pi)
+    np.testing.assert_array_equal(td, pd)
+
+
 def test_tensor_knn_1m_x_64_sampled_rows(orc):
     x = workloads.anisotropic_mixture(1_000_000, 64, 50, seed=11)
     ti, td, fb = gu.knn_exact(x, 15, backend="tensor")

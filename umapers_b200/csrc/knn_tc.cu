@@ -398,18 +398,15 @@ constexpr int tc_threads() { return 64 + 32 * epi_warps<MT, BN>(); }
 
 // The register file is split among the SM's four schedulers: with 18 warps
 // two of them hold five warps, which caps a thread at 96 registers.
-// The epilogue role of one warp, for both kernel forms.  Warp w reads TMEM
-// lanes 32 * (w % 4) (hardware rule); the warps of each quarter split (query
-// tile, 64-column group).  Units are first_unit, first_unit + unit_step, ...
-// With PAIR the TMEM tiles come from a CTA pair: this CTA's query tile of a
-// unit is 2 * group + rank, waits acquire at cluster scope, and releasing a
-// TMEM buffer arrives on the leader CTA's barrier.  False after a wait ran
-// out.
-template <int MT, int BN, bool PAIR>
+// The epilogue role of one warp.  Warp w reads TMEM lanes 32 * (w % 4)
+// (hardware rule); the warps of each quarter split (query tile, 64-column
+// group).  Units are first_unit, first_unit + unit_step, ...  False after a
+// wait ran out.
+template <int MT, int BN>
 __device__ __forceinline__ bool tc_epilogue(const TcArgs& p, int warp, int lane,
                                             uint32_t tmem_base, uint32_t b_tfull,
                                             uint32_t b_tempty, int64_t first_unit,
-                                            int64_t unit_step, int64_t stagger, uint32_t rank,
+                                            int64_t unit_step, int64_t stagger,
                                             volatile int* abort_flag) {
     constexpr int GPT = BN / 64;  // lists per candidate tile
     // Warp w reads TMEM lanes 32 * (w % 4) (hardware rule); the warps of
@@ -422,9 +419,7 @@ __device__ __forceinline__ bool tc_epilogue(const TcArgs& p, int warp, int lane,
     bool ok = true;
     for (int64_t unit = first_unit; unit < p.n_units && ok; unit += unit_step) {
         const Unit w = unit_of(p, unit, stagger);
-        const int32_t row =
-            (PAIR ? w.group * 2 + static_cast<int32_t>(rank) : w.group * MT + mt) * BM +
-            quarter * 32 + lane;
+        const int32_t row = (w.group * MT + mt) * BM + quarter * 32 + lane;
         const bool row_ok = row < p.n_q;
         const int32_t list_base = w.split * GPT + cq;  // list of (row, split, group)
         auto list_of = [&](int32_t srow) {
@@ -435,8 +430,7 @@ __device__ __forceinline__ bool tc_epilogue(const TcArgs& p, int warp, int lane,
         for (int32_t c = 0; c < w.len; ++c, ++cg) {
             const uint32_t buf = static_cast<uint32_t>(cg & 1);
             const uint32_t par = static_cast<uint32_t>((cg >> 1) & 1);
-            if (!(PAIR ? mbar_wait_cluster(b_tfull + 8 * buf, par, abort_flag)
-                       : mbar_wait(b_tfull + 8 * buf, par, abort_flag))) {
+            if (!mbar_wait(b_tfull + 8 * buf, par, abort_flag)) {
                 ok = false;
                 break;
             }
@@ -450,12 +444,7 @@ __device__ __forceinline__ bool tc_epilogue(const TcArgs& p, int warp, int lane,
             // the accumulator buffer can be overwritten as soon as it is in registers
             fence_before();
             __syncwarp();
-            if (lane == 0) {
-                if (PAIR)
-                    mbar_arrive_cluster(mapa(b_tempty + 8 * buf, 0));  // the leader's barrier
-                else
-                    mbar_arrive(b_tempty + 8 * buf);
-            }
+            if (lane == 0) mbar_arrive(b_tempty + 8 * buf);
             unsigned pend = __ballot_sync(0xffffffffu, row_ok && min64(r) < tau);
             if (pend == 0) continue;
             const int32_t colh = tile_at(c, w) * BN + cq * 64;
@@ -705,8 +694,8 @@ __global__ void __launch_bounds__(tc_threads<MT, BN>(), 1)
         }
     } else {
         // --------------------------------------------------- epilogue
-        if (!tc_epilogue<MT, BN, false>(p, warp, lane, tmem_base, b_tfull, b_tempty, blockIdx.x,
-                                        gridDim.x, blockIdx.x, 0, abort_flag))
+        if (!tc_epilogue<MT, BN>(p, warp, lane, tmem_base, b_tfull, b_tempty, blockIdx.x,
+                                 gridDim.x, blockIdx.x, abort_flag))
             fail(6);
     }
 

@@ -197,112 +197,6 @@ __device__ __forceinline__ void tmem_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// ------------------------------------------------------- CTA pairs ------
-// A cluster of two CTAs issuing tcgen05 work as one pair (cta_group::2): the
-// leader (rank 0) issues 256-row MMAs whose A and B halves sit in the two
-// CTAs' shared memory at the same offsets, and each CTA's TMEM holds its own
-// 128 rows of the accumulator.  No load here uses .multicast::cluster; only
-// MMA commits signal both CTAs' barriers.
-
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-
-// All threads of both CTAs: release this CTA's prior writes, acquire the
-// peer's.
-__device__ __forceinline__ void cluster_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;"
-                 ::: "memory");
-}
-
-// The shared::cluster address of the variable at shared::cta address `addr`
-// in the CTA of cluster rank `rank`.
-__device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
-    return r;
-}
-
-// Arrive on an mbarrier of either CTA (shared::cluster address), releasing
-// this thread's prior work at cluster scope.
-__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cbar) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cbar)
-                 : "memory");
-}
-
-__device__ __forceinline__ void st_cluster_u32(uint32_t caddr, uint32_t v) {
-    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(caddr), "r"(v) : "memory");
-}
-
-// Bounded wait (as mbar_wait) with acquire at cluster scope: for phases that
-// the peer CTA or the pair's MMAs complete.
-__device__ __forceinline__ bool mbar_wait_cluster(uint32_t bar, uint32_t parity,
-                                                  volatile int* abort_flag) {
-    auto attempt = [&](uint32_t hint) {
-        uint32_t ok;
-        asm volatile(
-            "{\n .reg .pred P1;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 P1, "
-            "[%1], %2, %3;\n selp.b32 %0, 1, 0, P1;\n}\n"
-            : "=r"(ok)
-            : "r"(bar), "r"(parity), "r"(hint)
-            : "memory");
-        return ok != 0;
-    };
-    if (attempt(0u)) return true;
-    const uint64_t t0 = global_ns();
-    while (true) {
-        if (attempt(1000000u)) return true;
-        if (*abort_flag) return false;
-        if (global_ns() - t0 > kWaitNs) return false;
-    }
-}
-
-// 2-D tile load into this CTA's shared memory whose completed bytes count on
-// the leader CTA's mbarrier: `lbar` is the shared::cluster address of that
-// barrier (mapa of its offset to rank 0).  No multicast.
-__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map,
-                                                 uint32_t lbar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(lbar)
-        : "memory");
-}
-
-__device__ __forceinline__ void umma_f16_pair(uint32_t tmem_d, uint64_t da, uint64_t db,
-                                              uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(idesc), "r"(acc)
-        : "memory");
-}
-
-// Arrives on the mbarrier at offset `bar` of every CTA in `mask` once every
-// pair MMA this thread issued before has completed.
-__device__ __forceinline__ void umma_commit_pair(uint32_t bar, uint16_t mask) {
-    asm volatile(
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
-        " [%0], %1;" ::"r"(bar), "h"(mask)
-        : "memory");
-}
-
-// Pair TMEM allocation: one warp of each CTA (the same warp index) with the
-// same holder offset; both receive the same base address.
-__device__ __forceinline__ void tmem_alloc_pair(uint32_t holder, uint32_t cols) {
-    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(holder),
-                 "r"(cols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_dealloc_pair(uint32_t base, uint32_t cols) {
-    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(cols)
-                 : "memory");
-}
-
 // ----------------------------------------------------------------- host --
 using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                               const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
