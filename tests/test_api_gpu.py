@@ -142,3 +142,30 @@ def test_device_rows_are_validated_before_the_fit():
         fit_device(flat.data_ptr() + 4)
     fit_device(torch.from_numpy(x).cuda().data_ptr())  # finite rows fit
     assert torch.isfinite(out).all()
+
+
+def test_repeated_fits_reuse_their_device_buffers():
+    """A model's second and later fits of the same rows make no new device
+    allocation: released buffers are kept per stream and exact size and
+    handed back, so the memory pool's mapped and handed-out bytes stay as the
+    second fit left them."""
+    import ctypes
+
+    from umapers_b200 import _lib
+
+    lib = _lib.load()
+    x = workloads.anisotropic_mixture(60_000, 32, 20, seed=9)
+    m = Umap(n_neighbors=15, n_epochs=50, ann_mode="exact")
+
+    def pool():
+        reserved, used = ctypes.c_int64(0), ctypes.c_int64(0)
+        _lib.check(lib.umapb_pool_bytes(ctypes.byref(reserved), ctypes.byref(used)))
+        return reserved.value, used.value
+
+    m.fit(x)
+    m.fit(x)
+    after_second = pool()
+    for _ in range(3):
+        m.fit(x)
+        assert pool() == after_second
+    assert np.all(np.isfinite(m.embedding_))
