@@ -651,7 +651,8 @@ def transform_leg(args, lib, device: int) -> dict:
     q_dev = torch.from_numpy(query).cuda()
     out_sur = torch.empty((T_QUERY, 2), dtype=torch.float32, device="cuda")
     out_plain = torch.empty_like(out_sur)
-    q_pinned = torch.from_numpy(query).pin_memory().numpy()
+    q_pin_t = torch.from_numpy(query).pin_memory()
+    q_pinned = q_pin_t.numpy()
     h_out = torch.empty((T_QUERY, 2), dtype=torch.float32).pin_memory().numpy()
     n_fb = ctypes.c_int64(0)
 
@@ -694,6 +695,17 @@ def transform_leg(args, lib, device: int) -> dict:
         t_plain = [dev(False) for _ in range(args.steps)]
         e_sur = [e2e(True) for _ in range(args.steps)]
         e_plain = [e2e(False) for _ in range(args.steps)]
+    # the upload alone: the pinned query block copied to the device (bounds e2e)
+    h2d = []
+    for _ in range(3):
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        q_dev.copy_(q_pin_t, non_blocking=True)
+        stop.record()
+        torch.cuda.synchronize()
+        h2d.append(start.elapsed_time(stop) / 1000.0)
     ts, tp = float(np.mean(t_sur)), float(np.mean(t_plain))
     es, ep = float(np.mean(e_sur)), float(np.mean(e_plain))
     sur, plain = out_sur.cpu().numpy(), out_plain.cpu().numpy()
@@ -717,6 +729,12 @@ def transform_leg(args, lib, device: int) -> dict:
         "speedup_device": round(tp / ts, 2),
         "speedup_e2e": round(ep / es, 2),
         "fallback_rows": int(n_fb.value),
+        "step_sec": {"surrogate": [round(v, 5) for v in t_sur],
+                     "plain": [round(v, 5) for v in t_plain],
+                     "surrogate_e2e": [round(v, 5) for v in e_sur],
+                     "plain_e2e": [round(v, 5) for v in e_plain]},
+        "h2d_upload": {"bytes": int(q_pin_t.numel() * 4), "sec": [round(v, 5) for v in h2d],
+                       "gbs": round(q_pin_t.numel() * 4 / float(np.median(h2d)) / 1e9, 1)},
         "quality": {"surrogate_trust15": round(q_s["trustworthiness"], 4),
                     "plain_trust15": round(q_p["trustworthiness"], 4),
                     "surrogate_knn_pres": round(q_s["knn_preservation"], 4),

@@ -228,6 +228,11 @@ __host__ __device__ inline uint32_t rng_below(uint64_t word, uint32_t n) {
     return static_cast<uint32_t>(((word >> 32) * static_cast<uint64_t>(n)) >> 32);
 }
 
+// Uniform integer in [0, n) from 32 random bits (multiply-high reduction).
+__host__ __device__ inline uint32_t rng_below32(uint32_t word, uint32_t n) {
+    return static_cast<uint32_t>((static_cast<uint64_t>(word) * n) >> 32);
+}
+
 // Uniform float in [0, 1) from 24 random bits.
 __host__ __device__ inline float rng_unit_f32(uint64_t word) {
     return static_cast<float>(word >> 40) * (1.0f / 16777216.0f);

@@ -268,6 +268,12 @@ struct umapb_model {
     umapb_params p{};
     int device = -1;
     cudaStream_t stream = nullptr;
+    // A second stream at the device's lowest priority, for work beside the
+    // model's stream: the chunked uploads of a host surrogate transform and
+    // the surrogate's network beside the gated rows' plain transform.  It
+    // lives as long as the model, so the device blocks freed on it stay
+    // cached for the next call.
+    cudaStream_t side = nullptr;
     std::mutex mu;
     float a = 0.0f, b = 0.0f;
     bool fitted = false;
@@ -296,6 +302,7 @@ struct umapb_model {
         int least = 0, greatest = 0;
         UMAPB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         UMAPB_CUDA(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, greatest));
+        UMAPB_CUDA(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, least));
         // keep freed pool memory cached across fits
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -706,28 +713,24 @@ void trim_precomputed(const int64_t* idx, const float* dist, int64_t n, int64_t 
     }
 }
 
-// A copy stream with one completion event per chunk.  Its destructor waits
-// for every copy issued on it, so buffers it writes outlive its work.
-struct CopyStream {
+// Work on the model's side stream with one completion event per chunk.  Its
+// destructor waits for everything queued on the stream, so buffers that work
+// reads or writes outlive it, on error paths too.
+struct SideWork {
     cudaStream_t s = nullptr;
     cudaEvent_t ready = nullptr;
     std::vector<cudaEvent_t> done;
-    explicit CopyStream(int64_t n) : done(static_cast<size_t>(n), nullptr) {
-        UMAPB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    SideWork(cudaStream_t side, int64_t n) : s(side), done(static_cast<size_t>(n), nullptr) {
         UMAPB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
         for (auto& e : done) UMAPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    CopyStream(const CopyStream&) = delete;
-    CopyStream& operator=(const CopyStream&) = delete;
-    ~CopyStream() {
+    SideWork(const SideWork&) = delete;
+    SideWork& operator=(const SideWork&) = delete;
+    ~SideWork() {
         if (s) cudaStreamSynchronize(s);
         for (auto e : done)
             if (e) cudaEventDestroy(e);
         if (ready) cudaEventDestroy(ready);
-        if (s) {
-            dev_release_stream(s);
-            cudaStreamDestroy(s);
-        }
     }
 };
 
@@ -849,7 +852,7 @@ void surrogate_transform_device(umapb_model* m, const float* Qd, int64_t nq, int
         surrogate_check(s);
         return;
     }
-    CopyStream net(1);
+    SideWork net(m->side, 1);
     UMAPB_CUDA(cudaEventRecord(net.ready, s));
     UMAPB_CUDA(cudaStreamWaitEvent(net.s, net.ready, 0));
     surrogate_forward_async(sg, Qd, nq, static_cast<int>(d), out, net.s);
@@ -987,6 +990,12 @@ void umapb_destroy(umapb_model* m) {
             dev_release_stream(m->stream);
             cudaStreamDestroy(m->stream);
             m->stream = nullptr;
+            if (m->side) {
+                cudaStreamSynchronize(m->side);
+                dev_release_stream(m->side);
+                cudaStreamDestroy(m->side);
+                m->side = nullptr;
+            }
         }
     }
     delete m;
@@ -1732,7 +1741,7 @@ int32_t umapb_surrogate_transform(umapb_model* m, const float* query, int64_t n_
         // waits for every copy before Q can be freed, errors included.
         const int64_t chunk = n_rows >= 4 * kUploadChunkRows ? kUploadChunkRows : n_rows;
         const int64_t n_chunks = ceil_div(n_rows, chunk);
-        CopyStream cs(n_chunks);
+        SideWork cs(m->side, n_chunks);
         UMAPB_CUDA(cudaEventRecord(cs.ready, s));  // Q is allocated on s
         UMAPB_CUDA(cudaStreamWaitEvent(cs.s, cs.ready, 0));
         for (int64_t c = 0; c < n_chunks; ++c) {

@@ -55,6 +55,14 @@ __device__ __forceinline__ float pow_pos(float x, float y) {
     return exp2f(__fmul_rn(y, log2f(x)));
 }
 
+// x^y for finite x > 0 and y = b > 0 with CUDA's fast __powf intrinsic (the
+// hardware base-2 logarithm and exponential), for the Hogwild epochs of large
+// graphs, whose update order is not reproducible anyway.  Its relative error
+// is about 2^-22 plus |y log2 x| * 2^-24: under 2e-6 at squared distances in
+// [1e-6, 1e6].  Subnormal x gives 0 (x^b is then below 1e-28 for the b of
+// any min_dist / spread in use).
+__device__ __forceinline__ float pow_fast(float x, float y) { return __powf(x, y); }
+
 // `row_max`/`heads` (nullable): the largest weight of each edge's head row
 // replaces max_w (row-local transform graphs).
 __global__ void epochs_per_sample_kernel(const float* __restrict__ w, int64_t m, float max_w,
@@ -155,8 +163,10 @@ __device__ __forceinline__ void count_block_samples(uint32_t* slots, bool sample
     if (threadIdx.x == 0) slots[blockIdx.x] += cnt;
 }
 
-// Negative samples drawn and loaded together in the 2-D epoch.
+// Negative samples drawn and loaded together in the 2-D epoch (even: two
+// samples share one random word).
 constexpr int kNegBatch = 4;
+static_assert(kNegBatch % 2 == 0, "samples are drawn in pairs");
 
 // One epoch for dim == 2 (the reference's flat fast path, lib.rs:5172-5244).
 __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
@@ -176,7 +186,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
                 const float dx = __fsub_rn(hx, t.x), dy = __fsub_rn(hy, t.y);
                 const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
                 if (d2 > 0.0f) {
-                    const float pb = pow_pos(d2, p.b);
+                    const float pb = pow_fast(d2, p.b);
                     const float gc = __fdiv_rn(__fmul_rn(p.att_factor, __fdiv_rn(pb, d2)),
                                                __fadd_rn(__fmul_rn(p.a, pb), 1.0f));
                     const float gx = clip4(__fmul_rn(gc, dx)), gy = clip4(__fmul_rn(gc, dy));
@@ -195,17 +205,27 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
                 const uint32_t n_neg = floor_count(__fdiv_rn(__fsub_rn(p.epoch_f, nn), en));
                 // The negatives' positions do not depend on the head's moves:
                 // kNegBatch are drawn and loaded at once, then applied in order.
+                // Sample s takes the high (even s) or low (odd s) 32 bits of
+                // the word keyed by (edge, epoch, s / 2).
+                const uint64_t stream = mix64(p.seed ^ mix64(static_cast<uint64_t>(e)));
                 for (uint32_t s0 = 0; s0 < n_neg; s0 += kNegBatch) {
                     float2 o[kNegBatch];
                     bool use[kNegBatch];
+                    uint64_t wd[kNegBatch / 2];
+#pragma unroll
+                    for (int j = 0; j < kNegBatch / 2; ++j)
+                        wd[j] = s0 + 2 * j < n_neg
+                                    ? mix64(stream ^ ((p.epoch << 32) | ((s0 >> 1) + j)))
+                                    : 0;
 #pragma unroll
                     for (int j = 0; j < kNegBatch; ++j) {
                         const uint32_t s = s0 + j;
                         uint32_t neg = static_cast<uint32_t>(head);
-                        if (s < n_neg)
-                            neg = rng_below(rng_word(p.seed, static_cast<uint64_t>(e),
-                                                     (p.epoch << 32) | s),
-                                            p.n_vertices);
+                        if (s < n_neg) {
+                            const uint64_t w = wd[j >> 1];
+                            neg = rng_below32(static_cast<uint32_t>(j & 1 ? w : w >> 32),
+                                              p.n_vertices);
+                        }
                         use[j] = neg != static_cast<uint32_t>(head);
                         o[j] = use[j] ? emb[neg] : make_float2(0.0f, 0.0f);
                     }
@@ -215,7 +235,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
                         const float dx = __fsub_rn(hx, o[j].x), dy = __fsub_rn(hy, o[j].y);
                         const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
                         if (d2 > 0.0f) {
-                            const float pb = pow_pos(d2, p.b);
+                            const float pb = pow_fast(d2, p.b);
                             const float gc = __fdiv_rn(
                                 p.rep_factor,
                                 __fmul_rn(__fadd_rn(0.001f, d2), __fadd_rn(__fmul_rn(p.a, pb), 1.0f)));
