@@ -217,52 +217,130 @@ struct Chunk {
 };
 
 // Upper triangle of A^T B per slot over contiguous position ranges, FP64.
-constexpr int kGramRows = 64;
+// S is a multiple of 3 ((dim + 1) * 6), so the upper triangle is covered by
+// NT = T (T + 1) / 2 tiles of 3 x 3 entries (T = S / 3); thread t owns tile
+// t % NT for the rows t / NT, t / NT + G, ... of each staged slab (G row
+// groups).  Slabs of R rows are staged in shared memory as FP64, the next
+// slab's FP32 rows wait in registers meanwhile; at the end the G partial
+// tiles are summed in shared memory and added to G atomically.
+template <int S, int SP>
+struct GramShape {
+    static_assert(S % 3 == 0, "the block width is a multiple of 3");
+    static constexpr int T = S / 3;
+    static constexpr int NT = T * (T + 1) / 2;
+    static constexpr int G = 256 / NT;
+    static constexpr int R = SP <= 20 ? 128 : 64;  // rows per slab
+    static constexpr int V4 = R * SP / 4;          // float4 per slab and operand
+    static constexpr int PF = (V4 + 255) / 256;    // float4 per thread and operand
+    static constexpr int kStage = 2 * R * SP;      // doubles
+    static constexpr int kReduce = G * NT * 9;     // doubles
+    static constexpr int kSmem = kStage > kReduce ? kStage : kReduce;
+    static_assert(kSmem * 8 <= 48 * 1024, "static shared memory");
+};
+
 template <int S, int SP>
 __global__ void __launch_bounds__(256)
     gram_kernel(const Chunk* __restrict__ chunks, const float* __restrict__ A,
                 const float* __restrict__ B, double* __restrict__ G) {
+    using Sh = GramShape<S, SP>;
+    __shared__ double sm[Sh::kSmem];
+    // A^T A (every orthonormalisation) stages one operand; A^T B (the Ritz
+    // step) two
+    const bool same = A == B;
+    double* As = sm;
+    double* Bs = same ? sm : sm + Sh::R * SP;
     const Chunk ch = chunks[blockIdx.x];
-    __shared__ __align__(16) float As[kGramRows * SP];
-    __shared__ __align__(16) float Bs[kGramRows * SP];
     const int tid = threadIdx.x;
-    constexpr int NE = S * (S + 1) / 2;  // <= 465 for S <= 30: at most 2 entries per thread
-    int ea[2], eb[2];
-    double acc[2] = {0.0, 0.0};
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        int t = tid + q * 256, a = 0;
-        ea[q] = eb[q] = -1;
-        if (t >= NE) continue;
-        while (t >= S - a) {
-            t -= S - a;
-            ++a;
-        }
-        ea[q] = a;
-        eb[q] = a + t;
+    const bool worker = tid < Sh::G * Sh::NT;
+    const int tile = tid % Sh::NT, grp = tid / Sh::NT;
+    int tp = 0, tq = tile;  // tile (tp, tq), tp <= tq
+    while (tq >= Sh::T - tp) {
+        tq -= Sh::T - tp;
+        ++tp;
     }
-    for (int r0 = ch.start; r0 < ch.end; r0 += kGramRows) {
-        const int rows = min(kGramRows, ch.end - r0);
-        __syncthreads();
+    tq += tp;
+    double acc[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) acc[i][j] = 0.0;
+
+    float4 pa[Sh::PF], pb[Sh::PF];
+    auto prefetch = [&](int r0) {
+        const int rows = min(Sh::R, ch.end - r0);
         const float4* a4 = reinterpret_cast<const float4*>(A + static_cast<int64_t>(r0) * SP);
         const float4* b4 = reinterpret_cast<const float4*>(B + static_cast<int64_t>(r0) * SP);
-        for (int e = tid; e < rows * SP / 4; e += 256) {
-            reinterpret_cast<float4*>(As)[e] = a4[e];
-            reinterpret_cast<float4*>(Bs)[e] = b4[e];
+#pragma unroll
+        for (int k = 0; k < Sh::PF; ++k) {
+            const int e = tid + k * 256;
+            if (e < rows * SP / 4) {
+                pa[k] = a4[e];
+                if (!same) pb[k] = b4[e];
+            }
+        }
+    };
+    if (ch.start < ch.end) prefetch(ch.start);
+    for (int r0 = ch.start; r0 < ch.end; r0 += Sh::R) {
+        const int rows = min(Sh::R, ch.end - r0);
+        __syncthreads();  // the previous slab's products are done
+#pragma unroll
+        for (int k = 0; k < Sh::PF; ++k) {
+            const int e = tid + k * 256;
+            if (e < rows * SP / 4) {
+                As[4 * e] = pa[k].x;
+                As[4 * e + 1] = pa[k].y;
+                As[4 * e + 2] = pa[k].z;
+                As[4 * e + 3] = pa[k].w;
+                if (!same) {
+                    Bs[4 * e] = pb[k].x;
+                    Bs[4 * e + 1] = pb[k].y;
+                    Bs[4 * e + 2] = pb[k].z;
+                    Bs[4 * e + 3] = pb[k].w;
+                }
+            }
         }
         __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            if (ea[q] < 0) continue;
-            double v = 0.0;
-            for (int r = 0; r < rows; ++r)
-                v += static_cast<double>(As[r * SP + ea[q]]) * static_cast<double>(Bs[r * SP + eb[q]]);
-            acc[q] += v;
+        if (r0 + Sh::R < ch.end) prefetch(r0 + Sh::R);
+        if (worker) {
+            for (int r = grp; r < rows; r += Sh::G) {
+                const double* ar = As + r * SP + 3 * tp;
+                const double* br = Bs + r * SP + 3 * tq;
+                const double a0 = ar[0], a1 = ar[1], a2 = ar[2];
+                const double b0 = br[0], b1 = br[1], b2 = br[2];
+                acc[0][0] = fma(a0, b0, acc[0][0]);
+                acc[0][1] = fma(a0, b1, acc[0][1]);
+                acc[0][2] = fma(a0, b2, acc[0][2]);
+                acc[1][0] = fma(a1, b0, acc[1][0]);
+                acc[1][1] = fma(a1, b1, acc[1][1]);
+                acc[1][2] = fma(a1, b2, acc[1][2]);
+                acc[2][0] = fma(a2, b0, acc[2][0]);
+                acc[2][1] = fma(a2, b1, acc[2][1]);
+                acc[2][2] = fma(a2, b2, acc[2][2]);
+            }
         }
     }
+    __syncthreads();  // the staging buffer becomes the reduction buffer
+    if (worker) {
 #pragma unroll
-    for (int q = 0; q < 2; ++q)
-        if (ea[q] >= 0) atomicAdd(&G[static_cast<int64_t>(ch.slot) * S * S + ea[q] * S + eb[q]], acc[q]);
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) sm[(grp * Sh::NT + tile) * 9 + i * 3 + j] = acc[i][j];
+    }
+    __syncthreads();
+    for (int o = tid; o < Sh::NT * 9; o += 256) {
+        const int t = o / 9, ij = o - t * 9, i = ij / 3, j = ij - i * 3;
+        int p = 0, q = t;
+        while (q >= Sh::T - p) {
+            q -= Sh::T - p;
+            ++p;
+        }
+        q += p;
+        const int ea = 3 * p + i, eb = 3 * q + j;
+        if (ea > eb) continue;  // lower part of a diagonal tile
+        double v = 0.0;
+        for (int g = 0; g < Sh::G; ++g) v += sm[(g * Sh::NT + t) * 9 + ij];
+        atomicAdd(&G[static_cast<int64_t>(ch.slot) * S * S + ea * S + eb], v);
+    }
 }
 
 // G = L L^T per slot, one warp: lane i keeps row i; right-looking updates
