@@ -393,41 +393,81 @@ __global__ void chol_kernel(const double* __restrict__ G, double* __restrict__ L
     }
 }
 
-// X = Y L^-T by forward substitution per row, FP64.
+// X = Y L^-T by forward substitution per row, FP64.  A block takes 256
+// consecutive rows: they are staged in shared memory with coalesced loads,
+// solved in place, and written back with coalesced stores (a row stride of
+// SP floats, a multiple of 4, keeps the 16-byte shared accesses of a
+// quarter-warp on distinct banks).  Each thread solves rows t and t + 128;
+// when both lie in the same slot (the common case: slots are contiguous
+// position ranges of at least 128 rows) every load of L serves both rows.
+constexpr int kApplyRows = 256;
+constexpr int kApplyThreads = 128;
+
+template <int S, int SP, int NR>
+__device__ __forceinline__ void solve_rows(float* const (&row)[NR], const double* __restrict__ Ls,
+                                           const double* __restrict__ di) {
+    double x[NR][S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+        double v[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) v[q] = static_cast<double>(row[q][c]);
+#pragma unroll
+        for (int a = 0; a < c; ++a) {
+            const double l = __ldg(Ls + c * S + a);
+#pragma unroll
+            for (int q = 0; q < NR; ++q) v[q] -= x[q][a] * l;
+        }
+        const double d = __ldg(di + c);
+#pragma unroll
+        for (int q = 0; q < NR; ++q) x[q][c] = v[q] * d;
+    }
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+        float4* r4 = reinterpret_cast<float4*>(row[q]);
+#pragma unroll
+        for (int v = 0; v < SP / 4; ++v) {
+            float o[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                o[k] = 4 * v + k < S ? static_cast<float>(x[q][4 * v + k]) : 0.0f;
+            r4[v] = make_float4(o[0], o[1], o[2], o[3]);
+        }
+    }
+}
+
 template <int S, int SP>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kApplyThreads)
     apply_kernel(int64_t cnt, const int32_t* __restrict__ slot_of_pos,
                  const double* __restrict__ L, const double* __restrict__ dinv,
                  const float* __restrict__ Y, float* __restrict__ X) {
-    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= cnt) return;
-    const int slot = slot_of_pos[t];
-    const double* Ls = L + static_cast<int64_t>(slot) * S * S;
-    const double* di = dinv + slot * S;
-    float y[SP];
-    const float4* y4 = reinterpret_cast<const float4*>(Y + t * SP);
-#pragma unroll
-    for (int v = 0; v < SP / 4; ++v) {
-        const float4 q = y4[v];
-        y[4 * v] = q.x;
-        y[4 * v + 1] = q.y;
-        y[4 * v + 2] = q.z;
-        y[4 * v + 3] = q.w;
+    __shared__ __align__(16) float rows[kApplyRows * SP];
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kApplyRows;
+    const int nrows = static_cast<int>(min(static_cast<int64_t>(kApplyRows), cnt - r0));
+    const float4* y4 = reinterpret_cast<const float4*>(Y + r0 * SP);
+    float4* s4 = reinterpret_cast<float4*>(rows);
+    for (int e = threadIdx.x; e < nrows * SP / 4; e += kApplyThreads) s4[e] = y4[e];
+    __syncthreads();
+    const int ta = threadIdx.x, tb = threadIdx.x + kApplyThreads;
+    const int sa = ta < nrows ? slot_of_pos[r0 + ta] : -1;
+    const int sb = tb < nrows ? slot_of_pos[r0 + tb] : -1;
+    auto Lof = [&](int slot) { return L + static_cast<int64_t>(slot) * S * S; };
+    if (sa >= 0 && sa == sb) {
+        float* const both[2] = {rows + ta * SP, rows + tb * SP};
+        solve_rows<S, SP, 2>(both, Lof(sa), dinv + sa * S);
+    } else {
+        if (sa >= 0) {
+            float* const one[1] = {rows + ta * SP};
+            solve_rows<S, SP, 1>(one, Lof(sa), dinv + sa * S);
+        }
+        if (sb >= 0) {
+            float* const one[1] = {rows + tb * SP};
+            solve_rows<S, SP, 1>(one, Lof(sb), dinv + sb * S);
+        }
     }
-    double x[S];
-#pragma unroll
-    for (int c = 0; c < S; ++c) {
-        double v = static_cast<double>(y[c]);
-#pragma unroll
-        for (int a = 0; a < c; ++a) v -= x[a] * __ldg(Ls + c * S + a);
-        x[c] = v * __ldg(di + c);
-    }
-    float o[SP];
-#pragma unroll
-    for (int c = 0; c < SP; ++c) o[c] = c < S ? static_cast<float>(x[c]) : 0.0f;
-    float4* x4 = reinterpret_cast<float4*>(X + t * SP);
-#pragma unroll
-    for (int v = 0; v < SP / 4; ++v) x4[v] = make_float4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+    __syncthreads();
+    float4* x4 = reinterpret_cast<float4*>(X + r0 * SP);
+    for (int e = threadIdx.x; e < nrows * SP / 4; e += kApplyThreads) x4[e] = s4[e];
 }
 
 // coords = X V (V: s x dim per slot), FP64; and per-slot max |coord|.
@@ -725,6 +765,7 @@ bool run_iterative(const std::vector<int64_t>& it_comps, const std::vector<int64
     UMAPB_LAUNCH_CHECK();
     const unsigned nch = static_cast<unsigned>(chunks.size());
     const unsigned gr = grid_for(cnt);
+    const unsigned ga = grid_for(cnt, kApplyRows);
     // CholQR2: src -> dst -> src; the orthonormal block ends in src
     auto cholqr = [&](float* src, float* dst) {
         for (int pass = 0; pass < 2; ++pass) {
@@ -736,7 +777,7 @@ bool run_iterative(const std::vector<int64_t>& it_comps, const std::vector<int64
             chol_kernel<S><<<static_cast<unsigned>(n_slots), 32, 0, s>>>(G.get(), L.get(), dg.get(),
                                                                         fail.get());
             UMAPB_LAUNCH_CHECK();
-            apply_kernel<S, SP><<<gr, 256, 0, s>>>(cnt, slots.get(), L.get(), dg.get(), a, b);
+            apply_kernel<S, SP><<<ga, kApplyThreads, 0, s>>>(cnt, slots.get(), L.get(), dg.get(), a, b);
             UMAPB_LAUNCH_CHECK();
         }
     };
