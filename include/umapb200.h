@@ -139,6 +139,7 @@ typedef struct umapb_fit_info {
                                      at the stage boundaries (device still busy) */
     double stage_host_sec;        /* with timings: the rest of the staged time (host work,
                                      launch overhead) */
+    double sgd_kernel_sec;        /* with timings: the layout epochs alone, CUDA events */
 } umapb_fit_info;
 
 typedef struct umapb_model umapb_model;

@@ -169,3 +169,30 @@ def test_repeated_fits_reuse_their_device_buffers():
         m.fit(x)
         assert pool() == after_second
     assert np.all(np.isfinite(m.embedding_))
+
+
+def test_device_fit_profile_outputs_do_not_change_the_fit():
+    """umapb_fit_transform_device with and without timings / info: the same
+    embedding (1,000 rows run the deterministic one-CTA layout), and the
+    profile fields are filled only when asked for."""
+    import ctypes
+
+    import torch
+
+    from umapers_b200 import _lib
+
+    lib = _lib.load()
+    n, d = 1000, 16
+    x = np.random.default_rng(3).normal(size=(n, d)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    m = Umap(n_neighbors=15, n_epochs=50, ann_mode="exact", random_seed=9)
+    plain = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    prof = torch.empty_like(plain)
+    _lib.check(lib.umapb_fit_transform_device(m._core._handle, xd.data_ptr(), n, d,
+                                              plain.data_ptr(), None, None))
+    t, info = _lib.Timings(), _lib.FitInfo()
+    _lib.check(lib.umapb_fit_transform_device(m._core._handle, xd.data_ptr(), n, d,
+                                              prof.data_ptr(), ctypes.byref(t), ctypes.byref(info)))
+    assert torch.equal(plain, prof)
+    assert info.n_samples == n and info.n_edges > 0 and info.sgd_edge_samples > 0
+    assert t.total_sec > 0.0 and t.knn_sec > 0.0

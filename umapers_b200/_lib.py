@@ -112,6 +112,7 @@ class FitInfo(ctypes.Structure):
         ("knn_second_pass_rows", ctypes.c_int64),
         ("stage_wait_sec", ctypes.c_double),
         ("stage_host_sec", ctypes.c_double),
+        ("sgd_kernel_sec", ctypes.c_double),
     ]
 
 

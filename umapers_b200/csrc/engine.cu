@@ -451,6 +451,7 @@ void fit_from_knn(umapb_model* m, const float* Xd, int64_t n, int64_t d, const i
     if (out) {
         out->t.optimize_sec = clk.lap();
         out->info.sgd_edge_samples = samples;
+        out->info.sgd_kernel_sec = sgd_ms * 1e-3;
         out->info.n_epochs = n_epochs;
     }
     m->emb = std::move(emb);
@@ -1142,7 +1143,8 @@ int32_t umapb_fit_transform_device(umapb_model* m, const float* data, int64_t n_
         check_engine_support(m->p);
         fo.t.validation_sec = clk.lap();
         m->begin_fit();
-        fit_device(m, data, n_rows, n_cols, true, &fo, clk);
+        // profile outputs (stage laps, sampled-edge counts) only when asked for
+        fit_device(m, data, n_rows, n_cols, true, timings || info ? &fo : nullptr, clk);
         if (out)
             UMAPB_CUDA(cudaMemcpyAsync(out, m->emb.get(), n_rows * m->p.n_components * 4,
                                        cudaMemcpyDeviceToDevice, m->stream));
