@@ -46,3 +46,28 @@ def test_layout_three_dimensions(orc, problem):
     g = gu.optimize_layout(init, h, t, w, 100, a, b, seed=3)
     assert g.shape == (x.shape[0], 3) and np.all(np.isfinite(g))
     assert diagnostics.quality(x, g)["trustworthiness"] > 0.85
+
+
+def test_sampled_edge_count_is_the_schedules_replay():
+    """The profile's attractive-sample count, replayed on the device from each
+    edge's schedule, equals a NumPy FP32 replay of make_epochs_per_sample and
+    the epoch rule (lib.rs:4937-4960, 5172-5178) on the same graph (20,000
+    rows: the Hogwild epoch kernels, not the one-CTA layout)."""
+    from umapers import Umap
+    from umapers_b200 import workloads
+
+    x = workloads.anisotropic_mixture(20_000, 16, 10, seed=4)
+    prof = Umap(n_neighbors=15, n_epochs=200, ann_mode="exact").profile_fit_transform(x)
+    idx, dist, _ = gu.knn_exact(x, 15, backend="plain")  # the tensor path's, bit for bit
+    _, _, w, _, _ = gu.fuzzy_graph(idx, dist, n_epochs=200)
+    ne = np.float32(200)
+    mx = np.float32(max(float(w.max()), 1e-12))
+    ns = (ne * (w / mx)).astype(np.float32)
+    with np.errstate(divide="ignore"):
+        eps = np.where(ns > 0, ne / ns, np.float32(np.inf)).astype(np.float32)
+    nxt, count = eps.copy(), 0
+    for ep in range(200):
+        fire = ~(nxt > np.float32(ep))
+        count += int(fire.sum())
+        nxt = np.where(fire, nxt + eps, nxt).astype(np.float32)
+    assert prof["sgd_edge_samples"] == count

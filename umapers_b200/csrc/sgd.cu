@@ -144,23 +144,34 @@ struct SgdArgs {
     float neg_rate_f;
     uint64_t seed;
     uint64_t epoch;
-    uint32_t* block_samples;  // (nullable) per-block count of attractive samples, all epochs
     // densMAP (sgd_epoch_dens only)
     const float* radii;       // local_radii_from_knn of the input rows
     float dens_lambda, dens_var_shift;
     int dens_on;              // epoch >= density_start_epoch
 };
 
-// Adds this block's sampled-edge count to its own slot: shared-memory
-// atomics inside the block, one plain store per block, no global atomics.
-__device__ __forceinline__ void count_block_samples(uint32_t* slots, bool sampled) {
-    __shared__ uint32_t cnt;
-    if (threadIdx.x == 0) cnt = 0;
-    __syncthreads();
-    const unsigned ballot = __ballot_sync(0xffffffffu, sampled);
-    if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(&cnt, static_cast<uint32_t>(__popc(ballot)));
-    __syncthreads();
-    if (threadIdx.x == 0) slots[blockIdx.x] += cnt;
+// The attractive samples of all epochs, replayed from each edge's schedule:
+// an edge fires in an epoch when its next-sample epoch is not above it, and
+// its next-sample epoch then advances by its period, in the same FP32
+// arithmetic as the epoch kernels.  The schedule does not depend on the
+// layout, so the count is exact, and the epochs themselves count nothing.
+__global__ void count_samples_kernel(const float* __restrict__ eps, int64_t m, int64_t n_epochs,
+                                     unsigned long long* __restrict__ total) {
+    unsigned long long c = 0;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < m;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float v = eps[e];
+        float nxt = v;
+        for (int64_t ep = 0; ep < n_epochs; ++ep) {
+            if (!(nxt > static_cast<float>(ep))) {
+                ++c;
+                nxt = __fadd_rn(nxt, v);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(total, c);
 }
 
 // Negative samples drawn and loaded together in the 2-D epoch (even: two
@@ -171,11 +182,9 @@ static_assert(kNegBatch % 2 == 0, "samples are drawn in pairs");
 // One epoch for dim == 2 (the reference's flat fast path, lib.rs:5172-5244).
 __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    bool sampled = false;
     if (e < p.n_edges) {
         const float nxt = p.next[e];
         if (!(nxt > p.epoch_f)) {
-            sampled = true;
             const int32_t head = p.heads[e];
             const int32_t tail = p.tails[e];
             float2* emb = reinterpret_cast<float2*>(p.emb);
@@ -253,7 +262,6 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d(SgdArgs p) {
                           make_float2(__fsub_rn(hx, h0.x), __fsub_rn(hy, h0.y)));
         }
     }
-    if (p.block_samples) count_block_samples(p.block_samples, sampled);
 }
 
 // One epoch for any dim (lib.rs:5248-5318).  The head moves in a per-thread
@@ -267,11 +275,9 @@ constexpr int kMaxDim = 16;
 // negative samples.  Head in registers, tail moves published with atomics.
 __global__ void __launch_bounds__(256) sgd_epoch_dens(SgdArgs p) {
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    bool sampled = false;
     if (e < p.n_edges) {
         const float nxt = p.next[e];
         if (!(nxt > p.epoch_f)) {
-            sampled = true;
             const int dim = p.dim;
             const int32_t head = p.heads[e];
             const int32_t tail = p.tails[e];
@@ -353,7 +359,6 @@ __global__ void __launch_bounds__(256) sgd_epoch_dens(SgdArgs p) {
                     atomicAdd(&p.emb[static_cast<int64_t>(head) * dim + c], __fsub_rn(h[c], h0[c]));
         }
     }
-    if (p.block_samples) count_block_samples(p.block_samples, sampled);
 }
 
 // local_radii_from_knn (lib.rs:5057-5082): one thread per row, FP32
@@ -397,11 +402,9 @@ __global__ void embedding_radii_kernel(const float* __restrict__ emb, int dim,
 
 __global__ void __launch_bounds__(256) sgd_epoch_nd(SgdArgs p) {
     const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    bool sampled = false;
     if (e < p.n_edges) {
         const float nxt = p.next[e];
         if (!(nxt > p.epoch_f)) {
-            sampled = true;
             const int dim = p.dim;
             const int32_t head = p.heads[e];
             const int32_t tail = p.tails[e];
@@ -463,7 +466,6 @@ __global__ void __launch_bounds__(256) sgd_epoch_nd(SgdArgs p) {
                     atomicAdd(&p.emb[static_cast<int64_t>(head) * dim + c], __fsub_rn(h[c], h0[c]));
         }
     }
-    if (p.block_samples) count_block_samples(p.block_samples, sampled);
 }
 
 // ------------------------------------------------------ small graphs ----
@@ -1436,11 +1438,6 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
                                                  next_neg.get());
         UMAPB_LAUNCH_CHECK();
     }
-    DevBuf<uint32_t> samples;
-    if (count_samples) {
-        samples.alloc(grid, s);
-        UMAPB_CUDA(cudaMemsetAsync(samples.get(), 0, grid * 4, s));
-    }
     SgdArgs p{};
     p.emb = emb;
     p.heads = sorted_heads.get();
@@ -1457,7 +1454,6 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
     p.rep_factor = 2.0f * repulsion * b;
     p.neg_rate_f = nrf;
     p.seed = seed;
-    p.block_samples = samples.get();
     if (dens) {
         p.radii = dens->radii;
         p.dens_lambda = dens->lambda;
@@ -1492,12 +1488,15 @@ double optimize_layout(float* emb, int64_t n_vertices, int dim, const Graph& g, 
         cudaEventDestroy(e1);
     }
     if (!count_samples) return 0.0;
-    std::vector<uint32_t> h(grid);
-    UMAPB_CUDA(cudaMemcpyAsync(h.data(), samples.get(), grid * 4, cudaMemcpyDeviceToHost, s));
+    DevBuf<unsigned long long> total(1, s);
+    UMAPB_CUDA(cudaMemsetAsync(total.get(), 0, 8, s));
+    count_samples_kernel<<<std::min<unsigned>(grid, 148u * 8u), 256, 0, s>>>(eps.get(), m, n_epochs,
+                                                                         total.get());
+    UMAPB_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&h, total.get(), 8, cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
-    double total = 0.0;
-    for (uint32_t v : h) total += v;
-    return total;
+    return static_cast<double>(h);
 }
 
 void transform_layout(float* out, int64_t nq, int dim, const float* base, int64_t n_base,
