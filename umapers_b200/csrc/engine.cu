@@ -522,14 +522,32 @@ void fit_host(umapb_model* m, const float* data, int64_t n, int64_t d, FitOutput
               float* emb_out) {
     StageClock clk(nullptr, out != nullptr);
     const double t_start = now_sec();
-    validate_data_host(data, n, d);
-    validate_params(m->p, n);
-    check_engine_support(m->p);
-    m->ensure_device();
+    // validate_data, validate_params and the engine's own limits, in that
+    // order; the fitted state is replaced only once all of them pass
+    auto checks = [&] {
+        validate_data_host(data, n, d);
+        validate_params(m->p, n);
+        check_engine_support(m->p);
+    };
+    if (n == 0 || d == 0) checks();  // nothing to upload
+    try {
+        m->ensure_device();
+    } catch (...) {
+        checks();  // without a usable device the input's own errors come first
+        throw;
+    }
     clk.s = m->stream;
-    m->begin_fit();
     DevBuf<float> X;
+    // the copy of pinned rows runs while the host scans them; a rejected
+    // input waits for its copy, so the caller's rows are not read afterwards
     upload(X, data, n * d, m->stream);
+    try {
+        checks();
+    } catch (...) {
+        cudaStreamSynchronize(m->stream);
+        throw;
+    }
+    m->begin_fit();
     if (out) out->t.validation_sec = clk.lap();
     fit_device(m, X.get(), n, d, false, out, clk);
     m->X = std::move(X);
