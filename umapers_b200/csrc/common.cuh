@@ -61,11 +61,13 @@ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 // A fit asks for the same sizes in the same order every time, so repeated
 // fits of one size make no allocator call: a pool allocation, even one served
 // from memory the pool already holds, occasionally took most of a second on
-// a shared machine.  At most kBlockCacheBytes are kept; a block that would go
-// beyond returns to the device's stream-ordered pool (cudaFreeAsync on its
-// own stream).  Blocks of a stream that is gone stay until the process ends,
-// within the same limit.
-constexpr size_t kBlockCacheBytes = static_cast<size_t>(12) << 30;
+// a shared machine.  At most kBlockCacheBytes are kept (a 1M-query transform
+// beside a 1M-row fit cycles several GB); a block that would go beyond
+// returns to the device's stream-ordered pool (cudaFreeAsync on its own
+// stream).  Blocks of a stream that is gone stay until the process ends,
+// within the same limit.  An allocation the pool cannot serve returns every
+// block kept for the device and is tried once more.
+constexpr size_t kBlockCacheBytes = static_cast<size_t>(32) << 30;
 
 struct BlockCache {
     std::mutex mu;
@@ -93,7 +95,29 @@ inline void* dev_alloc(size_t bytes, cudaStream_t s, int* dev_out) {
         }
     }
     void* p = nullptr;
-    const cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();  // clear the failed request's error
+        std::vector<void*> blocks;
+        {
+            std::lock_guard<std::mutex> lk(c.mu);
+            for (auto it = c.free_blocks.begin(); it != c.free_blocks.end();) {
+                if (std::get<0>(it->first) == dev) {
+                    c.held -= std::get<2>(it->first) * it->second.size();
+                    blocks.insert(blocks.end(), it->second.begin(), it->second.end());
+                    it = c.free_blocks.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+        }
+        if (!blocks.empty()) {
+            // their streams may be gone: wait for the device, then free directly
+            cudaDeviceSynchronize();
+            for (void* b : blocks) cudaFree(b);
+            e = cudaMallocAsync(&p, bytes, s);
+        }
+    }
     if (e != cudaSuccess) throw_cuda(e, "cudaMallocAsync", __FILE__, __LINE__);
     return p;
 }
