@@ -345,7 +345,8 @@ int32_t umapb_knn_exact(const float* data, int64_t n_rows, int64_t n_cols, int64
  * call on a device looks up the array's device address (cudaGetSymbolAddress),
  * so make that first call before any stream capture.  The call reads the
  * kernel's status and the count of rows it recomputes on the plain path back
- * to the host, so it waits for `stream` before it returns.  Every call reuses
+ * to the host, so it waits for `stream` before it returns: no call may be made
+ * while `stream` is being captured into a graph.  Every call reuses
  * the same array: calls that overlap on the GPU (other streams, other
  * threads) race and must be serialised by the caller. */
 int32_t umapb_knn_exact_noalloc(const float* data, int64_t n_rows, int64_t n_cols, int64_t k,
