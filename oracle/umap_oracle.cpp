@@ -18,7 +18,7 @@
 // by SplitMix64; UniformInt/UniformFloat single-sample rules), except the
 // Normal noise of rand_distr 0.4.3 (ziggurat), which is replaced by
 // Box-Muller.  No reference test fixes those streams against vectors, so
-// RNG-consuming stages are parity-unpinned at the bit level and are judged
+// RNG-consuming stages are parity-unpinned at the bit level and are compared
 // statistically.  SymmetricEigen (nalgebra 0.33.3) is replaced by a
 // Householder tridiagonalisation + implicit QL solver; eigenvector signs may
 // differ, which the spectral tests of the reference do not constrain.

@@ -4,7 +4,7 @@ density state, rust_umap/src/lib.rs:5045-5134, 5355-5440; radii outputs
 
 The input radii depend only on the kNN table, which is bit-exact, so they
 match the oracle to FP32 log rounding.  The layout races Hogwild-style, so it
-is judged statistically: trustworthiness@15 within 0.01 of the oracle's
+is compared statistically: trustworthiness@15 within 0.01 of the oracle's
 densMAP layout, 15-NN preservation and the correlation between input and
 embedding radii (what densMAP exists to raise) no lower than the oracle's by
 more than 0.01 / 0.1, and that correlation above plain UMAP's.

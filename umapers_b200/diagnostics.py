@@ -1,4 +1,4 @@
-"""Quality metrics used to judge embeddings.
+"""Quality metrics used to assess embeddings.
 
 ``trustworthiness_report`` mirrors umap_rs/python/umapers/diagnostics.py:1-53
 (sklearn's trustworthiness).  ``knn_preservation`` is the kNN-recall measure of
